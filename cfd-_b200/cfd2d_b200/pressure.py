@@ -1,0 +1,214 @@
+"""Pressure Poisson solver (drop-in for cfd2d/pressure.py).
+
+The host assembles the operator data once, in the reference's accumulation order
+(cfd2d/pressure.py:43-131): the diagonal of A = -Lap over the fluid cells
+(neighbour couplings, +2/h^2 on outflow Dirichlet faces, +1/dx^2 on the first cell
+of every component without a Dirichlet face), the coupling bits of every cell and
+the Neumann-component labels. The solve itself is the on-chip Jacobi-PCG of
+``cfd2d_pressure_solve`` (scipy's CG iteration form, warm-started from the
+previous solution).
+
+Methods: ``"cg"`` runs to the relative residual ``tol`` (reference default 1e-10).
+``"direct"`` (alias ``"lu"``) has no GPU LU; it runs the same CG to a relative
+residual of 1e-13, which agrees with a sparse LU solve to about 1e-15.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import warnings
+
+import numpy as np
+import scipy.sparse as sp
+from scipy.sparse.csgraph import connected_components
+
+from . import _lib
+from .boundary import DomainBoundary
+from .grid import Grid
+
+DIRECT_RTOL = 1e-13
+DIRECT_MAXITER = 50000
+
+
+class PressureSolver:
+    METHODS = ("direct", "cg", "lu")
+
+    def __init__(self, grid: Grid, boundary: DomainBoundary, method: str = "direct",
+                 tol: float = 1e-10):
+        if method not in self.METHODS:
+            raise ValueError(f"Unbekannter Drucklöser {method!r}, erlaubt: {self.METHODS}")
+        self.grid = grid
+        self.method = "direct" if method == "lu" else method
+        self._tol = float(tol)
+        self.on_change = None
+        nx, ny = grid.nx, grid.ny
+        self.dx2 = dx2 = 1.0 / grid.dx ** 2
+        self.dy2 = dy2 = 1.0 / grid.dy ** 2
+        fluid = grid.fluid_interior.copy()
+        self.fluid = fluid
+        n = int(fluid.sum())
+        if n == 0:
+            raise ValueError("Das Gebiet enthält keine Fluidzellen.")
+        idx = -np.ones((nx, ny), dtype=np.int64)
+        idx[fluid] = np.arange(n)
+        self.idx, self.n = idx, n
+        bx = fluid[:-1, :] & fluid[1:, :]
+        by = fluid[:, :-1] & fluid[:, 1:]
+        self.periodic = boundary.periodic
+        bp = (fluid[-1, :] & fluid[0, :]) if self.periodic else np.zeros(ny, dtype=bool)
+        self._both = (bx, by, bp)
+        diag = np.zeros((nx, ny))
+        diag[:-1, :][bx] += dx2
+        diag[1:, :][bx] += dx2
+        diag[:, :-1][by] += dy2
+        diag[:, 1:][by] += dy2
+        if self.periodic:
+            diag[-1, :][bp] += dx2
+            diag[0, :][bp] += dx2
+        self.dirichlet = {s: boundary.outflow_mask(s) for s in ("left", "right", "bottom", "top")}
+        diag[0, :][self.dirichlet["left"]] += 2 * dx2
+        diag[-1, :][self.dirichlet["right"]] += 2 * dx2
+        diag[:, 0][self.dirichlet["bottom"]] += 2 * dy2
+        diag[:, -1][self.dirichlet["top"]] += 2 * dy2
+        has_dir = np.zeros((nx, ny), dtype=bool)
+        has_dir[0, :] |= self.dirichlet["left"]
+        has_dir[-1, :] |= self.dirichlet["right"]
+        has_dir[:, 0] |= self.dirichlet["bottom"]
+        has_dir[:, -1] |= self.dirichlet["top"]
+        a = np.concatenate([idx[:-1, :][bx], idx[:, :-1][by], idx[-1, :][bp]])
+        b = np.concatenate([idx[1:, :][bx], idx[:, 1:][by], idx[0, :][bp]])
+        adj = sp.csr_matrix((np.ones(a.size), (a, b)), shape=(n, n))
+        ncomp, comp_of = connected_components(adj, directed=False)
+        labels = np.zeros((nx, ny), dtype=np.int64)
+        labels[fluid] = comp_of + 1
+        self.labels = labels
+        dir_comps = set(np.unique(labels[has_dir & fluid]).tolist())
+        self.neumann_components, self._pinned = [], []
+        for c in range(1, ncomp + 1):
+            if c not in dir_comps:
+                first = int(np.argmax(comp_of == c - 1))
+                fi, fj = np.argwhere(idx == first)[0]
+                diag[fi, fj] += dx2
+                self.neumann_components.append(c)
+                self._pinned.append((int(fi), int(fj)))
+        if len(self.neumann_components) > _lib.MAX_COMPONENTS:
+            raise ValueError(f"{len(self.neumann_components)} Neumann-Komponenten; der GPU-Löser "
+                             f"verfolgt höchstens {_lib.MAX_COMPONENTS}")
+        self.diag = diag
+        self.last_iterations = 0
+        self._A = None
+        self._upload()
+
+    # ------------------------------------------------------------------ device
+    def _upload(self):
+        t = _lib.torch()
+        g = self.grid
+        nx, ny = g.nx, g.ny
+        f = self.fluid
+        bx, by, bp = self._both
+        nbr = np.zeros((nx, ny), dtype=np.uint8)
+        nbr[1:, :][bx] |= 1       # west neighbour coupled
+        nbr[:, 1:][by] |= 2       # south
+        nbr[:, :-1][by] |= 4      # north
+        nbr[:-1, :][bx] |= 8      # east
+        if self.periodic:
+            nbr[0, :][bp] |= 1
+            nbr[-1, :][bp] |= 8
+        nbr[f] |= 0x80
+        dinv = np.zeros((nx, ny))
+        dinv[f] = 1.0 / self.diag[f]
+        lab = -np.ones((nx, ny), dtype=np.int16)
+        counts = []
+        for k, c in enumerate(self.neumann_components):
+            m = self.labels == c
+            lab[m] = k
+            counts.append(float(m.sum()))
+        self._d_diag = _lib.to_dev(self.diag)
+        self._d_dinv = _lib.to_dev(dinv)
+        self._d_nbr = _lib.to_dev(nbr)
+        self._d_lab = _lib.to_dev(lab)
+        self._d_cnt = _lib.to_dev(np.array(counts + [1.0], dtype=np.float64))
+        self._d_x0 = t.zeros((nx, ny), dtype=t.float64, device=_lib.device())
+        cl = C.c_int(0)
+        rc = _lib.lib().cfd2d_pcg_plan(nx, ny, C.byref(cl))
+        if rc != _lib.OK:
+            raise ValueError(f"Gitter {nx}x{ny} ist zu groß für den On-Chip-CG-Löser "
+                             f"(Cluster aus höchstens 16 CTAs)")
+        self.cluster = cl.value
+        self._d_iters = t.zeros(2, dtype=t.int32, device=_lib.device())
+        P = _lib.Poisson()
+        P.nx, P.ny, P.periodic = nx, ny, int(self.periodic)
+        P.dx2, P.dy2 = self.dx2, self.dy2
+        P.diag, P.dinv = self._d_diag.data_ptr(), self._d_dinv.data_ptr()
+        P.nbr, P.label = self._d_nbr.data_ptr(), self._d_lab.data_ptr()
+        P.ncomp = len(self.neumann_components)
+        P.comp_count = self._d_cnt.data_ptr()
+        P.x0 = self._d_x0.data_ptr()
+        P.work, P.work_bytes = 0, 0
+        P.cluster = self.cluster
+        self.op = P
+
+    @property
+    def tol(self) -> float:
+        return self._tol
+
+    @tol.setter
+    def tol(self, value: float) -> None:
+        self._tol = float(value)
+        if self.on_change is not None:
+            self.on_change()
+
+    @property
+    def rtol(self) -> float:
+        """Relative residual the CG runs to (``tol``, or 1e-13 for 'direct')."""
+        return DIRECT_RTOL if self.method == "direct" else self._tol
+
+    @property
+    def maxiter(self) -> int:
+        return DIRECT_MAXITER if self.method == "direct" else 5000
+
+    @property
+    def _x0(self) -> np.ndarray:
+        return self._d_x0.cpu().numpy()[self.fluid]
+
+    @_x0.setter
+    def _x0(self, x) -> None:
+        full = np.zeros(self.fluid.shape)
+        full[self.fluid] = np.asarray(x, dtype=float)
+        self._d_x0.copy_(_lib.to_dev(full))
+
+    @property
+    def A(self):
+        """The assembled sparse operator (built on demand, for inspection)."""
+        if self._A is None:
+            bx, by, bp = self._both
+            idx = self.idx
+            rows = [idx[:-1, :][bx], idx[1:, :][bx], idx[:, :-1][by], idx[:, 1:][by],
+                    idx[-1, :][bp], idx[0, :][bp], np.arange(self.n)]
+            cols = [idx[1:, :][bx], idx[:-1, :][bx], idx[:, 1:][by], idx[:, :-1][by],
+                    idx[0, :][bp], idx[-1, :][bp], np.arange(self.n)]
+            vals = [np.full(bx.sum(), -self.dx2)] * 2 + [np.full(by.sum(), -self.dy2)] * 2 + \
+                   [np.full(bp.sum(), -self.dx2)] * 2 + [self.diag[self.fluid]]
+            self._A = sp.csc_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                                    shape=(self.n, self.n))
+        return self._A
+
+    def solve(self, rhs):
+        """Solve Lap(p) = rhs (cfd2d/pressure.py:143-185); returns p (nx, ny), 0 in solids.
+
+        rhs may be a host array (the result is a host array) or a CUDA tensor.
+        """
+        t = _lib.torch()
+        host = not isinstance(rhs, t.Tensor)
+        r = _lib.to_dev(rhs, t.float64)
+        p = t.empty_like(r)
+        st = t.zeros(1, dtype=t.int32, device=_lib.device())
+        rc = _lib.lib().cfd2d_pressure_solve(C.byref(self.op), _lib.ptr(r), _lib.ptr(p), self.rtol,
+                                             self.maxiter, _lib.ptr(self._d_iters), _lib.ptr(st),
+                                             _lib.stream_ptr())
+        _lib.check(rc, "cfd2d_pressure_solve")
+        info = st.cpu().numpy()
+        self.last_iterations = int(self._d_iters[0].item())
+        if info[0] & _lib.S_CG_MAXITER:
+            warnings.warn(f"CG-Drucklöser nicht konvergiert ({self.maxiter} Iterationen)")
+        return p.cpu().numpy() if host else p

@@ -1,0 +1,244 @@
+// capi.cu - the extern "C" entry points declared in include/cfd2d_b200.h.
+//
+// Thin wrappers: argument checks, launch configuration, and the sequence of
+// stage kernels that makes up one projection step (cfd2d/solver.py:326-403).
+#include <cuda_runtime.h>
+
+#include "../../include/cfd2d_b200.h"
+#include "kernels.cuh"
+#include "pcg.cuh"
+
+using namespace cfd;
+
+namespace {
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+inline int status_of(cudaError_t e) { return e == cudaSuccess ? CFD2D_OK : CFD2D_E_CUDA; }
+#define CFD_TRY(x)                                   \
+    do {                                             \
+        cudaError_t e_ = (x);                        \
+        if (e_ != cudaSuccess) return CFD2D_E_CUDA;  \
+    } while (0)
+
+bool grid_ok(int nx, int ny) { return nx >= 4 && ny >= 4 && (long long)(nx + 2) * (ny + 2) < (1LL << 31); }
+
+// Main or auxiliary pressure projection inside a step: rhs = div(F, G)/dt.
+int project(const cfd2d_sim* sim, double* p_out, bool unit_dt, bool main_solve, cudaStream_t s) {
+    PcgLaunch L = {};
+    L.op = sim->pcg;
+    L.rhs_mode = 1;
+    L.F = sim->F;
+    L.G = sim->G;
+    L.dx = sim->dx;
+    L.dy = sim->dy;
+    L.dt_ptr = unit_dt ? nullptr : &sim->state->dt;
+    L.dt_const = 1.0;
+    L.rtol = sim->cg_rtol;
+    L.maxiter = sim->cg_maxiter;
+    L.p_out = p_out;
+    L.p_padded = 1;
+    L.iters_out = &sim->state->cg_iters;
+    L.iters_out2 = main_solve ? &sim->state->cg_iters_step : nullptr;
+    L.status_out = &sim->state->status;
+    L.active = &sim->state->active;
+    return status_of(pcg_launch(L, s));
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* cfd2d_version(void) { return "cfd2d_b200 0.1 (sm_100a)"; }
+
+int cfd2d_momentum_tendencies(const double* u, const double* v, const uint8_t* fluid, int nx,
+                              int ny, double dx, double dy, const double* nu, int variable,
+                              double gamma, int periodic, double* hu, double* hv,
+                              const double* rho, int var_density, void* stream) {
+    if (!u || !v || !fluid || !nu || !hu || !hv || !grid_ok(nx, ny)) return CFD2D_E_ARG;
+    if (var_density && !rho) return CFD2D_E_ARG;
+    return status_of(launch_momentum(u, v, fluid, nx, ny, dx, dy, nu, variable, gamma, periodic, hu, hv,
+                                     rho, var_density, as_stream(stream)));
+}
+
+int cfd2d_obstacle_bc(double* u, double* v, const uint8_t* fluid, int nx, int ny, int periodic,
+                      void* stream) {
+    if (!u || !v || !fluid || !grid_ok(nx, ny)) return CFD2D_E_ARG;
+    return status_of(launch_obstacle_bc(u, v, fluid, nx, ny, periodic, nullptr, as_stream(stream)));
+}
+
+int cfd2d_scalar_transport(const double* phi, const double* u, const double* v,
+                           const uint8_t* fluid, int nx, int ny, double dx, double dy,
+                           const double* diff, int limiter, int periodic, const int64_t* bt_l,
+                           const double* bv_l, const int64_t* bt_r, const double* bv_r,
+                           const int64_t* bt_b, const double* bv_b, const int64_t* bt_t,
+                           const double* bv_t, int obs_t, double obs_v, double* out,
+                           void* stream) {
+    if (!phi || !u || !v || !fluid || !diff || !out || !grid_ok(nx, ny)) return CFD2D_E_ARG;
+    if (!bt_l || !bv_l || !bt_r || !bv_r || !bt_b || !bv_b || !bt_t || !bv_t) return CFD2D_E_ARG;
+    ScalarBCView bc;
+    bc.bt[0] = bt_l; bc.bv[0] = bv_l;
+    bc.bt[1] = bt_r; bc.bv[1] = bv_r;
+    bc.bt[2] = bt_b; bc.bv[2] = bv_b;
+    bc.bt[3] = bt_t; bc.bv[3] = bv_t;
+    return status_of(launch_scalar_transport(phi, u, v, fluid, nx, ny, dx, dy, diff, limiter, periodic, bc,
+                                             obs_t, obs_v, out, as_stream(stream)));
+}
+
+int cfd2d_domain_bc(const cfd2d_sim* sim, double* u, double* v, void* stream) {
+    if (!sim || !u || !v) return CFD2D_E_ARG;
+    cfd2d_sim S = *sim;
+    S.state = nullptr;
+    return status_of(stage_domain_bc(S, u, v, 0, as_stream(stream)));
+}
+
+int cfd2d_mask_circle(int nx, int ny, double dx, double dy, double xc, double yc, double r,
+                      uint8_t* mask, void* stream) {
+    if (!mask || nx < 1 || ny < 1) return CFD2D_E_ARG;
+    const double q[3] = {xc, yc, r};
+    return status_of(launch_mask(0, nx, ny, dx, dy, q, mask, as_stream(stream)));
+}
+
+int cfd2d_mask_ellipse(int nx, int ny, double dx, double dy, double xc, double yc, double a,
+                       double b, double cos_phi, double sin_phi, uint8_t* mask, void* stream) {
+    if (!mask || nx < 1 || ny < 1) return CFD2D_E_ARG;
+    const double q[6] = {xc, yc, a, b, cos_phi, sin_phi};
+    return status_of(launch_mask(1, nx, ny, dx, dy, q, mask, as_stream(stream)));
+}
+
+int cfd2d_mask_rectangle(int nx, int ny, double dx, double dy, double xa, double ya, double xb,
+                         double yb, uint8_t* mask, void* stream) {
+    if (!mask || nx < 1 || ny < 1) return CFD2D_E_ARG;
+    const double q[4] = {xa, ya, xb, yb};
+    return status_of(launch_mask(2, nx, ny, dx, dy, q, mask, as_stream(stream)));
+}
+
+size_t cfd2d_pcg_workspace_bytes(int nx, int ny) {
+    return ((size_t)4 * nx * ny + 4096) * sizeof(double);
+}
+
+int cfd2d_pcg_plan(int nx, int ny, int* cluster) {
+    if (!cluster || !grid_ok(nx, ny)) return CFD2D_E_ARG;
+    *cluster = pcg_cluster_plan(nx, ny);
+    return *cluster > 0 ? CFD2D_OK : CFD2D_E_CAPACITY;
+}
+
+int cfd2d_pressure_solve(const cfd2d_poisson* op, const double* rhs, double* p, double rtol,
+                         int maxiter, int32_t* iters_out, int32_t* status_out, void* stream) {
+    if (!op || !rhs || !p || maxiter < 0 || !grid_ok(op->nx, op->ny)) return CFD2D_E_ARG;
+    if (op->cluster < 1) return CFD2D_E_CAPACITY;
+    if (op->ncomp > CFD2D_MAX_COMPONENTS) return CFD2D_E_CAPACITY;
+    PcgLaunch L = {};
+    L.op = *op;
+    L.rhs_mode = 0;
+    L.rhs = rhs;
+    L.rtol = rtol;
+    L.maxiter = maxiter;
+    L.p_out = p;
+    L.p_padded = 0;
+    L.iters_out = iters_out;
+    L.status_out = status_out;
+    return status_of(pcg_launch(L, as_stream(stream)));
+}
+
+size_t cfd2d_sim_scratch_doubles(int nx, int ny) {
+    return (size_t)16 * reduction_blocks((nx + 2) * (ny + 2)) + 64;
+}
+
+int cfd2d_sim_apply_bc(const cfd2d_sim* sim, void* stream) {
+    if (!sim || !sim->state) return CFD2D_E_ARG;
+    return status_of(stage_apply_bc(*sim, 0, as_stream(stream)));
+}
+
+int cfd2d_sim_project_initial(const cfd2d_sim* sim, void* stream) {
+    if (!sim || !sim->state) return CFD2D_E_ARG;
+    if (sim->pcg.cluster < 1) return CFD2D_E_CAPACITY;
+    const cudaStream_t s = as_stream(stream);
+    // F = u, G = v, outflow extrapolation; solve with dt = 1; correct; p = 0; BCs
+    // (cfd2d/solver.py:195-204)
+    CFD_TRY(stage_predictor(*sim, 1, s));
+    int rc = project(sim, sim->p, true, false, s);
+    if (rc) return rc;
+    CFD_TRY(stage_correct(*sim, sim->p, 1, s));
+    CFD_TRY(stage_fill(*sim, sim->p, (sim->nx + 2) * (sim->ny + 2), 0.0, s));
+    return status_of(stage_apply_bc(*sim, 0, s));
+}
+
+int cfd2d_sim_step(const cfd2d_sim* sim, void* stream) {
+    if (!sim || !sim->state || !grid_ok(sim->nx, sim->ny)) return CFD2D_E_ARG;
+    if (sim->pcg.cluster < 1) return CFD2D_E_CAPACITY;
+    const cfd2d_sim& S = *sim;
+    const cudaStream_t s = as_stream(stream);
+    // 1. boundary conditions (and the run() stop decision for this step)
+    CFD_TRY(stage_apply_bc(S, 1, s));
+    // 2. model pre-momentum hooks: k-omega SST blending, nu_t, nu_eff
+    if (S.sst_on) CFD_TRY(stage_sst_pre(S, s));
+    // 3. time step and upwind fraction
+    CFD_TRY(stage_dt(S, s));
+    // 4. tendencies, AB2, predictor, outflow extrapolation
+    CFD_TRY(stage_predictor(S, 0, s));
+    // 5. pressure Poisson (divergence fused into the solver prologue) and correction
+    int rc = project(sim, S.p, false, true, s);
+    if (rc) return rc;
+    CFD_TRY(stage_correct(S, S.p, 0, s));
+    CFD_TRY(stage_apply_bc(S, 0, s));
+    // 6. volume-flow forcing (cfd2d/solver.py:410-425)
+    if (S.has_flow_rate) {
+        CFD_TRY(stage_flow_shift(S, s));
+        if (S.has_solid) {
+            CFD_TRY(stage_predictor(S, 1, s));
+            rc = project(sim, S.p_tmp, true, false, s);
+            if (rc) return rc;
+            CFD_TRY(stage_correct(S, S.p_tmp, 1, s));
+        }
+        CFD_TRY(stage_apply_bc(S, 0, s));
+    }
+    // 7. model post-step hooks: scalar transport (k then omega for SST)
+    for (int k = 0; k < S.nscalars; ++k) CFD_TRY(stage_scalar(S, k, s));
+    // 8. residual, counters, history record
+    CFD_TRY(stage_end(S, s));
+    return CFD2D_OK;
+}
+
+int cfd2d_sim_scalar_fill_ghosts(const cfd2d_sim* sim, int slot, void* stream) {
+    if (!sim || slot < 0 || slot >= sim->nscalars) return CFD2D_E_ARG;
+    return status_of(stage_scalar_ghosts(*sim, slot, as_stream(stream)));
+}
+
+int cfd2d_sim_sst_pre_momentum(const cfd2d_sim* sim, void* stream) {
+    if (!sim || !sim->sst_on) return CFD2D_E_ARG;
+    return status_of(stage_sst_pre(*sim, as_stream(stream)));
+}
+
+int cfd2d_graph_capture_steps(const cfd2d_sim* sim, int nsteps, void* stream, void** graph_out) {
+    if (!sim || nsteps < 1 || !graph_out) return CFD2D_E_ARG;
+    const cudaStream_t s = as_stream(stream);
+    if (s == nullptr) return CFD2D_E_ARG;  // the legacy default stream cannot be captured
+    CFD_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+    int rc = CFD2D_OK;
+    for (int k = 0; k < nsteps && rc == CFD2D_OK; ++k) rc = cfd2d_sim_step(sim, stream);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s, &g);
+    if (rc != CFD2D_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) return CFD2D_E_CUDA;
+    cudaGraphExec_t exec = nullptr;
+    e = cudaGraphInstantiate(&exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return CFD2D_E_CUDA;
+    *graph_out = (void*)exec;
+    return CFD2D_OK;
+}
+
+int cfd2d_graph_launch(void* graph, void* stream) {
+    if (!graph) return CFD2D_E_ARG;
+    return status_of(cudaGraphLaunch((cudaGraphExec_t)graph, as_stream(stream)));
+}
+
+int cfd2d_graph_destroy(void* graph) {
+    if (!graph) return CFD2D_OK;
+    return status_of(cudaGraphExecDestroy((cudaGraphExec_t)graph));
+}
+
+}  // extern "C"

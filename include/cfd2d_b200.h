@@ -1,0 +1,279 @@
+/*
+ * cfd2d_b200.h - C ABI of the B200 (sm_100a) projection-step library.
+ *
+ * Every entry point takes plain pointers, sizes and a CUDA stream (as void*),
+ * launches asynchronously on that stream and returns an int status
+ * (CFD2D_OK or a negative CFD2D_E* code). Array pointers are DEVICE pointers
+ * unless a comment says otherwise. Arrays use the reference's layout: cell
+ * (i, j) with one ghost layer, row-major with j contiguous; p-like fields are
+ * (nx+2) x (ny+2), u is (nx+1) x (ny+2), v is (nx+2) x (ny+1), float64;
+ * fluid flags are one byte per cell (nonzero = fluid).
+ *
+ * The reference is the Python package cfd2d (kaeptnzursee1910/CFD-); each
+ * declaration names the reference interface it replaces as file:line.
+ */
+#ifndef CFD2D_B200_H
+#define CFD2D_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define CFD2D_OK 0
+#define CFD2D_E_ARG (-1)        /* invalid argument (sizes, null pointers) */
+#define CFD2D_E_CUDA (-2)       /* a CUDA runtime call failed */
+#define CFD2D_E_CAPACITY (-3)   /* problem larger than a fixed-capacity path supports */
+#define CFD2D_E_UNSUPPORTED (-4)
+
+/* device-side status bits, written into cfd2d_state.status by the kernels */
+#define CFD2D_S_NONFINITE 1     /* residual not finite or > 1e8 (FloatingPointError) */
+#define CFD2D_S_CG_MAXITER 2    /* CG stopped at maxiter (reference: warnings.warn) */
+#define CFD2D_S_BARRIER_TIMEOUT 4 /* a bounded inter-block wait gave up */
+#define CFD2D_S_COMPONENTS 8    /* more Neumann components than the solver tracks */
+
+/* side order used by every per-side array: left, right, bottom, top */
+#define CFD2D_LEFT 0
+#define CFD2D_RIGHT 1
+#define CFD2D_BOTTOM 2
+#define CFD2D_TOP 3
+
+/* boundary kinds, cfd2d/boundary.py:31 */
+#define CFD2D_BC_NOSLIP 0
+#define CFD2D_BC_SLIP 1
+#define CFD2D_BC_INFLOW 2
+#define CFD2D_BC_OUTFLOW 3
+#define CFD2D_BC_PERIODIC 4
+
+#define CFD2D_MAX_COMPONENTS 16
+#define CFD2D_MAX_SCALARS 4
+#define CFD2D_HIST_FIELDS 10
+
+/* Device-resident per-simulation state: everything that changes from step to
+ * step lives here so that a captured CUDA graph of one step can be replayed. */
+typedef struct cfd2d_state {
+    double t, dt, dt_old, gamma;
+    double ab_a, ab_b;        /* AB2 weights of this step */
+    double flow_force;        /* cfd2d/solver.py:152 */
+    double residual;          /* max|du|/dt, cfd2d/solver.py:390-392 */
+    double dt_fixed;          /* > 0: fixed step (cfd2d/solver.py:210-211) */
+    double t_end;             /* run(): clamp the last step to land on t_end */
+    double steady_tol;        /* run(): stop when residual < steady_tol after 10 steps */
+    double bulk_du;           /* flow-rate correction of this step */
+    int64_t n;                /* steps taken */
+    int64_t max_steps;        /* run(): stop after this many steps (<0: none) */
+    int32_t have_old;         /* hu_old valid (AB2 after the first step) */
+    int32_t status;           /* CFD2D_S_* bits (sticky) */
+    int32_t active;           /* this step runs (0 after a stop condition) */
+    int32_t cg_iters;         /* iterations of the last pressure solve */
+    int32_t cg_iters_step;    /* iterations of this step's main solve */
+    int32_t error_step;       /* step number at which status first became nonzero */
+    int32_t stop_reason;      /* 0 none, 1 t_end, 2 max_steps, 3 steady */
+    int32_t pad0;
+    /* reduction slots (bit patterns of non-negative doubles, max via atomicMax) */
+    unsigned long long umax_bits, vmax_bits, numax_bits, numin_bits;
+    unsigned long long dmax_bits[CFD2D_MAX_SCALARS];
+    unsigned long long du_bits, dv_bits, div_bits;
+    unsigned int ticket[8];   /* last-block-done counters */
+} cfd2d_state;
+
+/* Pressure operator on the interior cells (cfd2d/pressure.py:32-140), built by
+ * the host in the reference's accumulation order. */
+typedef struct cfd2d_poisson {
+    int nx, ny, periodic;
+    double dx2, dy2;          /* 1/dx^2, 1/dy^2 */
+    const double* diag;       /* nx*ny, 0 in solid cells */
+    const double* dinv;       /* nx*ny, 1/diag in fluid cells, 0 in solids */
+    const uint8_t* nbr;       /* nx*ny: bit0 W, bit1 S, bit2 N, bit3 E coupled, bit7 fluid */
+    const int16_t* label;     /* nx*ny: Neumann-component index (0..ncomp-1) or -1 */
+    int ncomp;                /* Neumann-only components (mean removed before/after) */
+    const double* comp_count; /* ncomp cell counts (as double) */
+    double* x0;               /* nx*ny warm start, updated by every solve */
+    double* work;             /* scratch, cfd2d_pcg_workspace_bytes() */
+    size_t work_bytes;
+    int cluster;              /* CTAs of the on-chip solver (0 = grid-persistent solver) */
+} cfd2d_poisson;
+
+/* One scalar transport equation (cfd2d/models.py:73-250). */
+typedef struct cfd2d_scalar {
+    double* phi;              /* (nx+2)(ny+2) */
+    double* diff;             /* (nx+2)(ny+2) */
+    double* rhs;              /* (nx+2)(ny+2) transport output */
+    const int64_t* bt[4];     /* per-side BC codes: 0 zero-gradient, 1 fixed, 2 flux */
+    const double* bv[4];      /* per-side BC values */
+    int limiter;              /* cfd2d/kernels.py:33 */
+    int obs_t;                /* 1: obstacle fixed value obs_v in the transport */
+    double obs_v;
+    double D0;                /* molecular diffusivity */
+    double turb_div;          /* > 0: diff = D0 + nu_t / turb_div each step */
+    int has_lower, has_upper;
+    double lower, upper;
+    int source;               /* 0 none, 1 SST k, 2 SST omega */
+    int pad;
+} cfd2d_scalar;
+
+/* k-omega SST model data (cfd2d/turbulence.py:166-325). */
+typedef struct cfd2d_sst {
+    double* S2;               /* nx*ny strain rate squared */
+    double* F1;               /* nx*ny */
+    double* cross;            /* nx*ny */
+    double* Pk;               /* nx*ny production (k source) */
+    const double* d;          /* nx*ny wall distance (>= 1e-12) */
+    const uint8_t* wall_adj;  /* nx*ny */
+    const double* w_wall;     /* nx*ny */
+    int k_index, w_index;     /* scalar slots of k and omega */
+} cfd2d_sst;
+
+/* A whole simulation: geometry, boundary data, device fields and parameters.
+ * Filled by the host once; every pointer is a device pointer. */
+typedef struct cfd2d_sim {
+    int nx, ny;
+    double dx, dy;
+    int periodic;
+    int scheme_ab2;           /* 1 AB2, 0 explicit Euler */
+    int gamma_auto;
+    double gamma_fixed;
+    double tau;
+    double nu;
+    double body_fx, body_fy;
+    int has_flow_rate;
+    double flow_rate;
+    double flow_count;        /* number of fluid u faces in columns 1..nx (bulk mean) */
+    int variable_viscosity;
+    int compute_forces;
+    int has_solid;            /* interior solids exist (flow-rate re-projection) */
+    int bc_kind[4];
+    double bc_vel[4];
+    const double* inflow[4];  /* inflow values per side (NULL if not inflow) */
+    const uint8_t* open[4];   /* open masks: left/right length ny, bottom/top length nx */
+    const uint8_t* fluid;     /* (nx+2)(ny+2) */
+    double *u, *v, *p, *F, *G, *hu, *hv, *u_prev, *v_prev, *nu_eff, *nu_t;
+    cfd2d_poisson pcg;
+    double cg_rtol;
+    int cg_maxiter;
+    int nscalars;
+    cfd2d_scalar scalars[CFD2D_MAX_SCALARS];
+    double scalar_dtlim_const[CFD2D_MAX_SCALARS]; /* > 0: constant diffusion dt limit */
+    int thermal_index;        /* scalar slot of the Boussinesq temperature, -1 none */
+    double gx, gy, T_ref;     /* buoyancy beta*g and reference temperature */
+    int sst_on;
+    cfd2d_sst sst;
+    cfd2d_state* state;
+    double* red;              /* reduction scratch, cfd2d_sim_scratch_doubles() */
+    double* hist;             /* history ring: hist_cap records of CFD2D_HIST_FIELDS doubles:
+                                 t, dt, residual, max|div u|, kinetic energy, fx, fy,
+                                 flow_force, CG iterations, gamma */
+    int hist_cap;
+    double* p_tmp;            /* (nx+2)(ny+2) scratch: pressure of the flow-rate re-projection */
+} cfd2d_sim;
+
+/* ---- kernel-level entry points (drop-in for cfd2d/kernels.py) ------------ */
+
+/* hu, hv = diffusion - convection on fluid faces; zero elsewhere.
+ * Replaces cfd2d/kernels.py:44-46 momentum_tendencies(u, v, fluid, nx, ny, dx,
+ * dy, nu, variable, gamma, periodic, hu, hv, rho, var_density). */
+int cfd2d_momentum_tendencies(const double* u, const double* v, const uint8_t* fluid, int nx,
+                              int ny, double dx, double dy, const double* nu, int variable,
+                              double gamma, int periodic, double* hu, double* hv,
+                              const double* rho, int var_density, void* stream);
+
+/* Velocities on faces touching solid cells, in place.
+ * Replaces cfd2d/kernels.py:158-159 obstacle_bc(u, v, fluid, nx, ny, periodic). */
+int cfd2d_obstacle_bc(double* u, double* v, const uint8_t* fluid, int nx, int ny, int periodic,
+                      void* stream);
+
+/* out = -div(u phi) + div(D grad phi) on fluid cells (TVD faces).
+ * Replaces cfd2d/kernels.py:254-256 scalar_transport(phi, u, v, fluid, nx, ny,
+ * dx, dy, diff, limiter, periodic, bt_l, bv_l, bt_r, bv_r, bt_b, bv_b, bt_t,
+ * bv_t, obs_t, obs_v, out). bt_* are int64 arrays, bv_* float64 arrays of
+ * length ny (left/right) or nx (bottom/top). */
+int cfd2d_scalar_transport(const double* phi, const double* u, const double* v,
+                           const uint8_t* fluid, int nx, int ny, double dx, double dy,
+                           const double* diff, int limiter, int periodic, const int64_t* bt_l,
+                           const double* bv_l, const int64_t* bt_r, const double* bv_r,
+                           const int64_t* bt_b, const double* bv_b, const int64_t* bt_t,
+                           const double* bv_t, int obs_t, double obs_v, double* out,
+                           void* stream);
+
+/* Domain boundary values on u and v (ghost cells and boundary faces).
+ * Replaces cfd2d/boundary.py:143 DomainBoundary.apply(u, v). */
+int cfd2d_domain_bc(const cfd2d_sim* sim, double* u, double* v, void* stream);
+
+/* Cell-centre obstacle masks (nx, ny), one byte per cell, bit-exact with the
+ * reference's float64 expressions. Replace cfd2d/geometry.py:17 circle,
+ * :25 ellipse (cos/sin of the angle are passed in, computed by numpy as in the
+ * reference) and :35 rectangle (corners already sorted). */
+int cfd2d_mask_circle(int nx, int ny, double dx, double dy, double xc, double yc, double r,
+                      uint8_t* mask, void* stream);
+int cfd2d_mask_ellipse(int nx, int ny, double dx, double dy, double xc, double yc, double a,
+                       double b, double cos_phi, double sin_phi, uint8_t* mask, void* stream);
+int cfd2d_mask_rectangle(int nx, int ny, double dx, double dy, double xa, double ya, double xb,
+                         double yb, uint8_t* mask, void* stream);
+
+/* ---- pressure Poisson (drop-in for cfd2d/pressure.py) -------------------- */
+
+/* Bytes of scratch the solver needs for an nx x ny grid (cfd2d_poisson.work). */
+size_t cfd2d_pcg_workspace_bytes(int nx, int ny);
+
+/* Choose the solver variant for this grid on the current device: the number of
+ * CTAs of the on-chip (cluster) solver, or 0 for the grid-persistent solver. */
+int cfd2d_pcg_plan(int nx, int ny, int* cluster);
+
+/* Solve Lap(p) = rhs on the fluid cells: Neumann-component mean removal, sign
+ * flip, Jacobi-preconditioned CG in scipy's iteration form from the warm start
+ * op->x0 (updated), then per-component mean removal of p. rhs and p are nx*ny
+ * arrays (p is 0 in solid cells). iters_out (device int32, may be NULL) gets
+ * the iteration count, status_out (device int32, may be NULL) gets
+ * CFD2D_S_CG_MAXITER / CFD2D_S_BARRIER_TIMEOUT bits.
+ * Replaces cfd2d/pressure.py:143 PressureSolver.solve(rhs) with
+ * method="cg" (scipy.sparse.linalg.cg at cfd2d/pressure.py:171). */
+int cfd2d_pressure_solve(const cfd2d_poisson* op, const double* rhs, double* p, double rtol,
+                         int maxiter, int32_t* iters_out, int32_t* status_out, void* stream);
+
+/* ---- whole projection step (drop-in for cfd2d/solver.py) ----------------- */
+
+/* Doubles of reduction scratch a simulation needs (cfd2d_sim.red). */
+size_t cfd2d_sim_scratch_doubles(int nx, int ny);
+
+/* Boundary conditions on u, v: domain sides then obstacle faces.
+ * Replaces cfd2d/solver.py:189 Simulation._apply_bc(). */
+int cfd2d_sim_apply_bc(const cfd2d_sim* sim, void* stream);
+
+/* Projection of the initial field with dt = 1, p reset to 0 afterwards.
+ * Replaces cfd2d/solver.py:195 Simulation._project_initial() (the caller skips
+ * it when u and v are zero, as the reference does). */
+int cfd2d_sim_project_initial(const cfd2d_sim* sim, void* stream);
+
+/* One projection time step, all on the device; skipped entirely when
+ * state->active is 0 at its start (run() stop conditions).
+ * Replaces cfd2d/solver.py:326 Simulation.step(). */
+int cfd2d_sim_step(const cfd2d_sim* sim, void* stream);
+
+/* Fill the ghost and solid cells of scalar slot `slot` from its interior values.
+ * Replaces cfd2d/models.py:139 ScalarField.fill_ghosts(). */
+int cfd2d_sim_scalar_fill_ghosts(const cfd2d_sim* sim, int slot, void* stream);
+
+/* k-omega SST blending functions, nu_t, blended diffusivities and nu_eff.
+ * Replaces cfd2d/turbulence.py:262 KOmegaSST.pre_momentum(sim). */
+int cfd2d_sim_sst_pre_momentum(const cfd2d_sim* sim, void* stream);
+
+/* Capture nsteps consecutive calls of cfd2d_sim_step on `stream` (a created,
+ * non-default stream) into an instantiated CUDA graph returned as an opaque
+ * handle; cfd2d_graph_launch replays it, cfd2d_graph_destroy frees it. The
+ * graph reads every step-varying scalar from sim->state, so it may be replayed
+ * any number of times while the device buffers named in *sim stay valid. */
+int cfd2d_graph_capture_steps(const cfd2d_sim* sim, int nsteps, void* stream, void** graph_out);
+int cfd2d_graph_launch(void* graph, void* stream);
+int cfd2d_graph_destroy(void* graph);
+
+/* Library version string (host memory, static). */
+const char* cfd2d_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CFD2D_B200_H */

@@ -1,0 +1,294 @@
+"""Generate the golden fixtures in this folder by running the reference solver.
+
+Run in a container that holds the reference checkout (default
+``/root/reference``; override with ``CFD2D_REFERENCE``)::
+
+    python tests/golden/make_golden.py [group ...]
+
+Groups: kernels geometry pressure cavity cylinder sst misc (default: all).
+The reference imports matplotlib at module load; ``mplstub/`` stands in for it
+(no fixture case needs plotting or polygon masks). Every pressure solve uses the
+reference's own ``PressureSolver`` (scipy CG or SuperLU) with
+``sim.pressure.tol`` set after construction, exactly as a user of the reference
+would. Nothing at test time imports this script or the reference.
+"""
+
+from __future__ import annotations
+
+import os
+import sys
+import time
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+REF = os.environ.get("CFD2D_REFERENCE", "/root/reference")
+sys.path.insert(0, str(HERE / "mplstub"))
+sys.path.insert(0, REF)
+sys.path.insert(0, str(HERE))
+
+import numpy as np  # noqa: E402
+
+from cfd2d import cases, geometry, kernels  # noqa: E402
+from cfd2d.boundary import BoundaryCondition as BC  # noqa: E402
+from cfd2d.grid import Grid  # noqa: E402
+from cfd2d.models import PassiveScalar  # noqa: E402
+from cfd2d.solver import Simulation  # noqa: E402
+from cfd2d.turbulence import KOmegaSST  # noqa: E402
+
+TOL = 1e-8
+
+
+def _save(name, d):
+    path = HERE / f"{name}.npz"
+    np.savez_compressed(path, **d)
+    print(f"wrote {path.name}: {path.stat().st_size / 1024:.0f} KiB", flush=True)
+
+
+def gen_kernels():
+    from inputs import momentum_cases, scalar_cases
+
+    out = {}
+    k = 0
+    for c in momentum_cases():
+        u, v = c["u"], c["v"]
+        hu = np.full_like(u, 7.0)
+        hv = np.full_like(v, 7.0)
+        kernels.momentum_tendencies(u, v, c["fluid"], c["nx"], c["ny"], c["dx"], c["dy"], c["nu"],
+                                    c["variable"], c["gamma"], c["periodic"], hu, hv, c["rho"],
+                                    c["var_density"])
+        uo, vo = u.copy(), v.copy()
+        kernels.obstacle_bc(uo, vo, c["fluid"], c["nx"], c["ny"], c["periodic"])
+        out.update({f"m{k}_hu": hu, f"m{k}_hv": hv, f"m{k}_u_obc": uo, f"m{k}_v_obc": vo})
+        k += 1
+    out["n_momentum"] = np.array(k)
+    k = 0
+    for c in scalar_cases():
+        o = np.full_like(c["phi"], 3.0)
+        bt, bv = c["bt"], c["bv"]
+        kernels.scalar_transport(c["phi"], c["u"], c["v"], c["fluid"], c["nx"], c["ny"], c["dx"],
+                                 c["dy"], c["diff"], c["limiter"], c["periodic"], bt["l"], bv["l"],
+                                 bt["r"], bv["r"], bt["b"], bv["b"], bt["t"], bv["t"], c["obs_t"],
+                                 c["obs_v"], o)
+        out[f"s{k}_out"] = o
+        k += 1
+    out["n_scalar"] = np.array(k)
+    _save("golden_kernels", out)
+
+
+# --------------------------------------------------------------------------- #
+def gen_geometry():
+    rng = np.random.default_rng(77)
+    out = {}
+    k = 0
+    for nx, ny, lx, ly in ((440, 82, 2.2, 0.41), (97, 61, 1.0, 0.7), (256, 128, 2.0, 1.0),
+                           (1024, 512, 2.0, 1.0)):
+        g = Grid(nx, ny, lx, ly)
+        for _ in range(4):
+            xc = float(rng.uniform(0.1, 0.9) * lx)
+            yc = float(rng.uniform(0.1, 0.9) * ly)
+            r = float(rng.uniform(0.02, 0.2) * ly)
+            a = float(rng.uniform(0.02, 0.2) * ly)
+            b = float(rng.uniform(0.02, 0.2) * ly)
+            ang = float(rng.uniform(0, 180))
+            out[f"g{k}_grid"] = np.array([nx, ny, lx, ly])
+            out[f"g{k}_circle"] = np.array([xc, yc, r])
+            out[f"g{k}_circle_mask"] = geometry.circle(g, xc, yc, r)
+            out[f"g{k}_ellipse"] = np.array([xc, yc, a, b, ang])
+            out[f"g{k}_ellipse_mask"] = geometry.ellipse(g, xc, yc, a, b, ang)
+            rect = (xc - a, yc - b, xc + a, yc + b)
+            out[f"g{k}_rect"] = np.array(rect)
+            out[f"g{k}_rect_mask"] = geometry.rectangle(g, *rect)
+            k += 1
+    # the cylinder of the cylinder case exactly (cases.py:92-94)
+    g = Grid(440, 82, 2.2, 0.41)
+    out["cyl_mask"] = geometry.circle(g, 0.2, 0.2, 0.1 / 2)
+    out["n_shapes"] = np.array(k)
+    # finalize: a ring encloses fluid, and a second case with a single region
+    g = Grid(60, 40, 1.5, 1.0)
+    X, Y = g.cell_centers()
+    ring = ((X - 0.7) ** 2 + (Y - 0.5) ** 2 <= 0.3 ** 2) & ((X - 0.7) ** 2 + (Y - 0.5) ** 2 > 0.2 ** 2)
+    g.add_obstacle(ring)
+    out["fin_before"] = g.fluid.copy()
+    out["fin_removed"] = np.array(g.finalize())
+    out["fin_after"] = g.fluid.copy()
+    _save("golden_geometry", out)
+
+
+# --------------------------------------------------------------------------- #
+def _pressure_case(name, sim, rng, out):
+    ps = sim.pressure
+    nx, ny = sim.grid.nx, sim.grid.ny
+    diag = np.zeros((nx, ny))
+    diag[ps.fluid] = ps.A.diagonal()
+    out[name + "_fluid"] = sim.grid.fluid.copy()
+    out[name + "_diag"] = diag
+    out[name + "_labels"] = ps.labels
+    out[name + "_pinned"] = np.array(ps._pinned, dtype=np.int64).reshape(-1, 2)
+    out[name + "_neumann"] = np.array(ps.neumann_components, dtype=np.int64)
+    for s in ("left", "right", "bottom", "top"):
+        out[name + "_dir_" + s] = np.asarray(ps.dirichlet[s])
+    rhs = rng.standard_normal((nx, ny))
+    rhs[~ps.fluid] = 0.0
+    ps.tol = 1e-10
+    p = ps.solve(rhs)
+    out[name + "_rhs"] = rhs
+    out[name + "_p"] = p
+    out[name + "_its"] = np.array(ps.last_iterations)
+    # second solve warm-started from the first (the CG keeps x0 between solves)
+    rhs2 = rhs + 0.1 * rng.standard_normal((nx, ny))
+    rhs2[~ps.fluid] = 0.0
+    p2 = ps.solve(rhs2)
+    out[name + "_rhs2"] = rhs2
+    out[name + "_p2"] = p2
+    out[name + "_its2"] = np.array(ps.last_iterations)
+
+
+def gen_pressure():
+    rng = np.random.default_rng(99)
+    out = {}
+    _pressure_case("cav", cases.lid_driven_cavity(re=100, n=24, pressure_solver="cg").sim, rng, out)
+    _pressure_case("cyl", cases.cylinder_flow(re=20, nx=110, ny=21, pressure_solver="cg").sim, rng, out)
+    g = Grid(32, 32, 1.0, 1.0)
+    g.add_obstacle(geometry.circle(g, 0.5, 0.5, 0.15))
+    bcs = dict(left=BC("periodic"), right=BC("periodic"), bottom=BC("slip"), top=BC("slip"))
+    _pressure_case("per", Simulation(g, bcs, nu=0.02, pressure_solver="cg"), rng, out)
+    # a wall across a closed box gives two Neumann components
+    g = Grid(30, 20, 1.5, 1.0)
+    g.add_obstacle(geometry.rectangle(g, 0.7, -1.0, 0.8, 2.0))
+    bcs = {s: BC("noslip") for s in ("left", "right", "bottom", "top")}
+    _pressure_case("two", Simulation(g, bcs, nu=0.02, pressure_solver="cg"), rng, out)
+    _save("golden_pressure", out)
+
+
+# --------------------------------------------------------------------------- #
+def _run(sim, nsteps, keep_at, fields, out, prefix):
+    its, dts = [], []
+    hist_keys = ("divergence", "kinetic_energy", "fx", "fy")
+    t0 = time.time()
+    for n in range(1, nsteps + 1):
+        sim.step()
+        its.append(sim.pressure.last_iterations)
+        dts.append(sim.dt)
+        if n in keep_at:
+            for name, getter in fields.items():
+                out[f"{prefix}_{name}_{n}"] = np.array(getter(sim), copy=True)
+    out[prefix + "_its"] = np.array(its)
+    out[prefix + "_dt"] = np.array(dts)
+    out[prefix + "_residual_last"] = np.array(sim.residual)
+    out[prefix + "_t"] = np.array(sim.t)
+    for k in hist_keys:
+        val = getattr(sim.history, k)
+        if val:
+            out[prefix + "_hist_" + k] = np.array(val)
+    if sim.flow_rate is not None:
+        out[prefix + "_hist_flow_force"] = np.array(sim.history.extra["antriebskraft"])
+    print(f"{prefix}: {nsteps} steps in {time.time() - t0:.1f}s, mean CG it {np.mean(its):.1f}",
+          flush=True)
+
+
+UVP = {"u": lambda s: s.u, "v": lambda s: s.v, "p": lambda s: s.p}
+
+
+def gen_cavity():
+    out = {}
+    case = cases.lid_driven_cavity(re=100, n=64, scheme="ab2", gamma=0.1, tau=0.5,
+                                   pressure_solver="cg")
+    case.sim.pressure.tol = TOL
+    _run(case.sim, 2000, {1, 10, 200, 2000}, UVP, out, "cav")
+    _save("golden_cavity64", out)
+
+
+def gen_cylinder():
+    out = {}
+    case = cases.build_case({"fall": "cylinder", "parameter": {"re": 100, "nx": 440, "ny": 82},
+                             "numerik": {"pressure_solver": "cg"},
+                             "skalar": {"name": "c", "diffusivity": 1e-3, "inflow_band": [0.15, 0.25],
+                                        "limiter": "vanleer"}})
+    case.sim.pressure.tol = TOL
+    f = dict(UVP)
+    f["c"] = lambda s: s.scalars["c"].phi
+    _run(case.sim, 10, {1, 10}, f, out, "cyl")
+    _save("golden_cylinder440", out)
+
+
+def _sst_channel(nx, ny, seed):
+    g = Grid(nx, ny, 2 * np.pi, 2.0)
+    bcs = dict(left=BC("periodic"), right=BC("periodic"), bottom=BC("noslip"), top=BC("noslip"))
+    nu = 2.0 / 1e4
+    k0, w0 = 1e-3, 10.0
+    sst = KOmegaSST(intensity=np.sqrt(k0 / 1.5), viscosity_ratio=k0 / (nu * w0), U_ref=1.0)
+    sim = Simulation(g, bcs, nu=nu, flow_rate=1.0, models=[sst], pressure_solver="cg")
+    sim.pressure.tol = TOL
+    rng = np.random.default_rng(seed)
+    y = (np.arange(ny) + 0.5) * g.dy
+    prof = 1.5 * y * (2.0 - y)
+    sim.u[1:nx + 1, 1:ny + 1] = prof[None, :] * (1.0 + 0.05 * rng.uniform(-1.0, 1.0, (nx, ny)))
+    sim.v[1:nx + 1, 1:ny] = 0.05 * rng.uniform(-1.0, 1.0, (nx, ny - 1))
+    sim.u[~sim.u_fluid] = 0.0
+    sim.v[~sim.v_fluid] = 0.0
+    sim._apply_bc()
+    sim._project_initial()
+    return sim
+
+
+def gen_sst():
+    out = {}
+    sim = _sst_channel(128, 192, 0)
+    f = dict(UVP)
+    f["k"] = lambda s: s.scalars["k"].phi
+    f["w"] = lambda s: s.scalars["omega"].phi
+    f["nut"] = lambda s: s.nu_t
+    _run(sim, 20, {1, 20}, f, out, "sst")
+    out["sst_flow_force"] = np.array(sim.flow_force)
+    _save("golden_sst128x192", out)
+
+
+def gen_misc():
+    out = {}
+    # heated cavity (Boussinesq) 32x32
+    case = cases.heated_cavity(ra=1e5, n=32, pressure_solver="cg")
+    case.sim.pressure.tol = TOL
+    f = dict(UVP)
+    f["T"] = lambda s: s.scalars["T"].phi
+    _run(case.sim, 100, {100}, f, out, "hot")
+    # periodic channel with an obstacle, flow-rate control with re-projection
+    g = Grid(32, 32, 1.0, 1.0)
+    g.add_obstacle(geometry.circle(g, 0.5, 0.5, 0.15))
+    bcs = dict(left=BC("periodic"), right=BC("periodic"), bottom=BC("slip"), top=BC("slip"))
+    sim = Simulation(g, bcs, nu=0.02, flow_rate=1.0, pressure_solver="cg")
+    sim.pressure.tol = TOL
+    _run(sim, 50, {50}, UVP, out, "pob")
+    out["pob_flow_force"] = np.array(sim.flow_force)
+    # explicit Euler, fixed gamma (tests/test_cfd2d.py:97-102 setting)
+    case = cases.lid_driven_cavity(re=100, n=16, scheme="euler", pressure_solver="cg", gamma=0.5)
+    case.sim.pressure.tol = TOL
+    _run(case.sim, 30, {30}, UVP, out, "eul")
+    # obstacle flow of the learned-preconditioner family at reduced size
+    obst = [{"typ": "kreis", "x": 0.5, "y": 0.45, "r": 0.06},
+            {"typ": "ellipse", "x": 1.0, "y": 0.6, "a": 0.07, "b": 0.03, "winkel": 30.0},
+            {"typ": "rechteck", "x0": 1.4, "y0": 0.2, "x1": 1.48, "y1": 0.3}]
+    case = cases.custom_obstacles(obst, lx=2.0, ly=1.0, nx=256, ny=128, re=500.0,
+                                  inflow_profile="uniform", walls="slip", pressure_solver="cg")
+    case.sim.pressure.tol = TOL
+    _run(case.sim, 5, {5}, UVP, out, "obs")
+    # run() with the last step shortened to land on t_end (cfd2d/solver.py:466-480)
+    case = cases.cylinder_flow(re=20, nx=110, ny=21, t_end=0.1, pressure_solver="cg")
+    case.sim.pressure.tol = TOL
+    reason = case.sim.run(0.1, verbose=False)
+    out["run_u"] = case.sim.u.copy()
+    out["run_n"] = np.array(case.sim.n)
+    out["run_t"] = np.array(case.sim.t)
+    out["run_dt_last"] = np.array(case.sim.dt)
+    out["run_reason"] = np.array(reason)
+    _save("golden_misc", out)
+
+
+GROUPS = {"kernels": gen_kernels, "geometry": gen_geometry, "pressure": gen_pressure,
+          "cavity": gen_cavity, "cylinder": gen_cylinder, "sst": gen_sst, "misc": gen_misc}
+
+if __name__ == "__main__":
+    import warnings
+
+    warnings.simplefilter("ignore")
+    for name in (sys.argv[1:] or list(GROUPS)):
+        GROUPS[name]()

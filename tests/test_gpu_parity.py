@@ -1,0 +1,247 @@
+"""Parity of the CUDA path against the reference's own outputs and the oracle (GPU).
+
+Kernel-level: bit-for-bit equality with the reference's Numba kernels on the
+seeded fixture inputs. Step-level: u, v, p and scalars within 1e-10 relative
+(max-norm of the difference / max-norm of the reference) after the stated step
+counts; the GPU CG follows scipy's iteration form but adds its dot products in a
+different order, which moves the fields by ~1e-11 over 2000 steps.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import golden
+from inputs import momentum_cases, scalar_cases
+
+pytestmark = [pytest.mark.gpu, pytest.mark.filterwarnings("ignore::RuntimeWarning")]
+
+TOL = 1e-10
+
+
+def rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    s = np.abs(b).max()
+    return np.abs(a - b).max() / s if s > 0 else np.abs(a - b).max()
+
+
+@pytest.fixture(scope="module")
+def pkg(cuda_lib):
+    import cfd2d_b200
+    from cfd2d_b200 import cases, geometry, kernels
+
+    return cfd2d_b200, cases, geometry, kernels
+
+
+# ---------------------------------------------------------------- kernels, bitwise
+def test_momentum_and_obstacle_bc_bitwise(pkg):
+    _, _, _, K = pkg
+    g = golden("golden_kernels")
+    for k, c in enumerate(momentum_cases()):
+        hu = np.full_like(c["u"], 7.0)
+        hv = np.full_like(c["v"], 7.0)
+        K.momentum_tendencies(c["u"], c["v"], c["fluid"], c["nx"], c["ny"], c["dx"], c["dy"], c["nu"],
+                              c["variable"], c["gamma"], c["periodic"], hu, hv, c["rho"], c["var_density"])
+        assert np.array_equal(hu, g[f"m{k}_hu"]), k
+        assert np.array_equal(hv, g[f"m{k}_hv"]), k
+        uo, vo = c["u"].copy(), c["v"].copy()
+        K.obstacle_bc(uo, vo, c["fluid"], c["nx"], c["ny"], c["periodic"])
+        assert np.array_equal(uo, g[f"m{k}_u_obc"]), k
+        assert np.array_equal(vo, g[f"m{k}_v_obc"]), k
+
+
+def test_scalar_transport_bitwise(pkg):
+    _, _, _, K = pkg
+    g = golden("golden_kernels")
+    for k, c in enumerate(scalar_cases()):
+        o = np.full_like(c["phi"], 3.0)
+        bt, bv = c["bt"], c["bv"]
+        K.scalar_transport(c["phi"], c["u"], c["v"], c["fluid"], c["nx"], c["ny"], c["dx"], c["dy"],
+                           c["diff"], c["limiter"], c["periodic"], bt["l"], bv["l"], bt["r"], bv["r"],
+                           bt["b"], bv["b"], bt["t"], bv["t"], c["obs_t"], c["obs_v"], o)
+        assert np.array_equal(o, g[f"s{k}_out"]), (k, c["limiter"], c["periodic"], c["obs_t"])
+
+
+def test_masks_bitwise(pkg):
+    _, _, G, _ = pkg
+    from cfd2d_b200.grid import Grid
+
+    g = golden("golden_geometry")
+    for k in range(int(g["n_shapes"])):
+        nx, ny, lx, ly = g[f"g{k}_grid"]
+        grid = Grid(int(nx), int(ny), lx, ly)
+        assert np.array_equal(G.circle(grid, *g[f"g{k}_circle"]), g[f"g{k}_circle_mask"])
+        assert np.array_equal(G.ellipse(grid, *g[f"g{k}_ellipse"]), g[f"g{k}_ellipse_mask"])
+        assert np.array_equal(G.rectangle(grid, *g[f"g{k}_rect"]), g[f"g{k}_rect_mask"])
+    grid = Grid(440, 82, 2.2, 0.41)
+    assert np.array_equal(G.circle(grid, 0.2, 0.2, 0.05), g["cyl_mask"])
+    grid = Grid(60, 40, 1.5, 1.0)
+    grid.fluid[:] = g["fin_before"]
+    assert grid.finalize() == int(g["fin_removed"])
+    assert np.array_equal(grid.fluid, g["fin_after"])
+
+
+# ---------------------------------------------------------------- pressure
+def _pressure_sim(pkg, name):
+    _, cases, G, _ = pkg
+    from cfd2d_b200.boundary import BoundaryCondition as BC
+    from cfd2d_b200.grid import Grid
+    from cfd2d_b200.solver import Simulation
+
+    if name == "cav":
+        return cases.lid_driven_cavity(re=100, n=24, pressure_solver="cg").sim
+    if name == "cyl":
+        return cases.cylinder_flow(re=20, nx=110, ny=21, pressure_solver="cg").sim
+    if name == "per":
+        g = Grid(32, 32, 1.0, 1.0)
+        g.add_obstacle(G.circle(g, 0.5, 0.5, 0.15))
+        bcs = dict(left=BC("periodic"), right=BC("periodic"), bottom=BC("slip"), top=BC("slip"))
+        return Simulation(g, bcs, nu=0.02, pressure_solver="cg")
+    g = Grid(30, 20, 1.5, 1.0)
+    g.add_obstacle(G.rectangle(g, 0.7, -1.0, 0.8, 2.0))
+    return Simulation(g, {s: BC("noslip") for s in ("left", "right", "bottom", "top")}, nu=0.02,
+                      pressure_solver="cg")
+
+
+@pytest.mark.parametrize("name", ["cav", "cyl", "per", "two"])
+def test_pressure_solve(pkg, name):
+    g = golden("golden_pressure")
+    sim = _pressure_sim(pkg, name)
+    ps = sim.pressure
+    assert np.array_equal(sim.grid.fluid, g[name + "_fluid"])
+    assert np.array_equal(ps.diag[ps.fluid], g[name + "_diag"][ps.fluid])
+    assert list(ps.neumann_components) == list(g[name + "_neumann"])
+    ps.tol = 1e-10
+    p = ps.solve(g[name + "_rhs"])
+    assert abs(ps.last_iterations - int(g[name + "_its"])) <= 1
+    assert rel(p, g[name + "_p"]) < 1e-8
+    p2 = ps.solve(g[name + "_rhs2"])
+    assert abs(ps.last_iterations - int(g[name + "_its2"])) <= 1
+    assert rel(p2, g[name + "_p2"]) < 1e-8
+
+
+# ---------------------------------------------------------------- full steps
+def test_cavity_2000_steps(pkg):
+    _, cases, _, _ = pkg
+    g = golden("golden_cavity64")
+    case = cases.lid_driven_cavity(re=100, n=64, scheme="ab2", gamma=0.1, tau=0.5, pressure_solver="cg")
+    sim = case.sim
+    sim.pressure.tol = 1e-8
+    done = 0
+    for n in (1, 10, 200, 2000):
+        sim.advance(n - done)
+        done = n
+        for f in "uvp":
+            r = rel(getattr(sim, f), g[f"cav_{f}_{n}"])
+            assert r < TOL, (f, n, r)
+    its = np.array(sim.history.extra["cg_iterationen"])
+    assert np.abs(its - g["cav_its"]).max() <= 1
+    assert np.array_equal(np.array(sim.history.dt), g["cav_dt"])
+
+
+def test_cylinder_with_scalar_10_steps(pkg):
+    _, cases, _, _ = pkg
+    g = golden("golden_cylinder440")
+    case = cases.build_case({"fall": "cylinder", "parameter": {"re": 100, "nx": 440, "ny": 82},
+                             "numerik": {"pressure_solver": "cg"},
+                             "skalar": {"name": "c", "diffusivity": 1e-3, "inflow_band": [0.15, 0.25],
+                                        "limiter": "vanleer"}})
+    sim = case.sim
+    sim.pressure.tol = 1e-8
+    sim.step()
+    for f in "uvp":
+        assert rel(getattr(sim, f), g[f"cyl_{f}_1"]) < TOL, f
+    assert rel(sim.scalars["c"].phi, g["cyl_c_1"]) < TOL
+    sim.advance(9)
+    for f in "uvp":
+        assert rel(getattr(sim, f), g[f"cyl_{f}_10"]) < TOL, f
+    assert rel(sim.scalars["c"].phi, g["cyl_c_10"]) < TOL
+    assert rel(sim.history.fx, g["cyl_hist_fx"]) < 1e-9
+    assert rel(sim.history.fy, g["cyl_hist_fy"]) < 1e-8
+
+
+def test_sst_channel_20_steps(pkg):
+    _, _, _, _ = pkg
+    from cfd2d_b200.boundary import BoundaryCondition as BC
+    from cfd2d_b200.grid import Grid
+    from cfd2d_b200.solver import Simulation
+    from cfd2d_b200.turbulence import KOmegaSST
+
+    g = golden("golden_sst128x192")
+    nx, ny = 128, 192
+    grid = Grid(nx, ny, 2 * np.pi, 2.0)
+    bcs = dict(left=BC("periodic"), right=BC("periodic"), bottom=BC("noslip"), top=BC("noslip"))
+    nu = 2.0 / 1e4
+    sst = KOmegaSST(intensity=np.sqrt(1e-3 / 1.5), viscosity_ratio=1e-3 / (nu * 10.0), U_ref=1.0)
+    sim = Simulation(grid, bcs, nu=nu, flow_rate=1.0, models=[sst], pressure_solver="cg")
+    sim.pressure.tol = 1e-8
+    rng = np.random.default_rng(0)
+    y = (np.arange(ny) + 0.5) * grid.dy
+    prof = 1.5 * y * (2.0 - y)
+    u, v = sim.u, sim.v
+    u[1:nx + 1, 1:ny + 1] = prof[None, :] * (1.0 + 0.05 * rng.uniform(-1.0, 1.0, (nx, ny)))
+    v[1:nx + 1, 1:ny] = 0.05 * rng.uniform(-1.0, 1.0, (nx, ny - 1))
+    u[~sim.u_fluid] = 0.0
+    v[~sim.v_fluid] = 0.0
+    sim._apply_bc()
+    sim._project_initial()
+    sim.step()
+    for f in "uvp":
+        assert rel(getattr(sim, f), g[f"sst_{f}_1"]) < 1e-9, f
+    sim.advance(19)
+    for f in "uvp":
+        assert rel(getattr(sim, f), g[f"sst_{f}_20"]) < 1e-9, f
+    assert rel(sim.scalars["k"].phi, g["sst_k_20"]) < 1e-9
+    assert rel(sim.scalars["omega"].phi, g["sst_w_20"]) < 1e-9
+    assert rel(sim.nu_t, g["sst_nut_20"]) < 1e-9
+    assert sim.flow_force == pytest.approx(float(g["sst_flow_force"]), rel=1e-9)
+
+
+def test_misc_runs(pkg):
+    _, cases, G, _ = pkg
+    from cfd2d_b200.boundary import BoundaryCondition as BC
+    from cfd2d_b200.grid import Grid
+    from cfd2d_b200.solver import Simulation
+
+    g = golden("golden_misc")
+    case = cases.heated_cavity(ra=1e5, n=32, pressure_solver="cg")
+    case.sim.pressure.tol = 1e-8
+    case.sim.advance(100)
+    for f in "uvp":
+        assert rel(getattr(case.sim, f), g[f"hot_{f}_100"]) < TOL, f
+    assert rel(case.sim.scalars["T"].phi, g["hot_T_100"]) < TOL
+
+    grid = Grid(32, 32, 1.0, 1.0)
+    grid.add_obstacle(G.circle(grid, 0.5, 0.5, 0.15))
+    bcs = dict(left=BC("periodic"), right=BC("periodic"), bottom=BC("slip"), top=BC("slip"))
+    sim = Simulation(grid, bcs, nu=0.02, flow_rate=1.0, pressure_solver="cg")
+    sim.pressure.tol = 1e-8
+    sim.advance(50)
+    for f in "uvp":
+        assert rel(getattr(sim, f), g[f"pob_{f}_50"]) < TOL, f
+    assert sim.flow_force == pytest.approx(float(g["pob_flow_force"]), rel=1e-9)
+
+    case = cases.lid_driven_cavity(re=100, n=16, scheme="euler", pressure_solver="cg", gamma=0.5)
+    case.sim.pressure.tol = 1e-8
+    case.sim.advance(30)
+    for f in "uvp":
+        assert rel(getattr(case.sim, f), g[f"eul_{f}_30"]) < TOL, f
+
+    obst = [{"typ": "kreis", "x": 0.5, "y": 0.45, "r": 0.06},
+            {"typ": "ellipse", "x": 1.0, "y": 0.6, "a": 0.07, "b": 0.03, "winkel": 30.0},
+            {"typ": "rechteck", "x0": 1.4, "y0": 0.2, "x1": 1.48, "y1": 0.3}]
+    case = cases.custom_obstacles(obst, lx=2.0, ly=1.0, nx=256, ny=128, re=500.0,
+                                  inflow_profile="uniform", walls="slip", pressure_solver="cg")
+    case.sim.pressure.tol = 1e-8
+    case.sim.advance(5)
+    for f in "uvp":
+        assert rel(getattr(case.sim, f), g[f"obs_{f}_5"]) < TOL, f
+
+    case = cases.cylinder_flow(re=20, nx=110, ny=21, t_end=0.1, pressure_solver="cg")
+    case.sim.pressure.tol = 1e-8
+    reason = case.sim.run(0.1, verbose=False)
+    assert reason == str(g["run_reason"])
+    assert case.sim.n == int(g["run_n"])
+    assert case.sim.t == pytest.approx(float(g["run_t"]), rel=1e-14)
+    assert rel(case.sim.u, g["run_u"]) < TOL

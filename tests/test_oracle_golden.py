@@ -1,0 +1,194 @@
+"""Pin the CPU oracle against outputs of the reference itself (CPU only).
+
+The fixtures were produced by ``tests/golden/make_golden.py`` running the reference
+(Numba kernels, scipy CG / SuperLU). Stencils and masks must agree bit for bit;
+the time-stepping runs must agree to 1e-12 relative (bitwise on the machine that
+made the fixtures, where the oracle calls the same BLAS dot as scipy's CG).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import golden
+from inputs import momentum_cases, scalar_cases
+
+pytestmark = pytest.mark.filterwarnings("ignore::RuntimeWarning")
+
+
+def rel(a, b):
+    d = np.abs(np.asarray(a) - np.asarray(b)).max()
+    s = np.abs(np.asarray(b)).max()
+    return d / s if s > 0 else d
+
+
+# ---------------------------------------------------------------- stencils
+def test_momentum_and_obstacle_bc_bitwise():
+    g = golden("golden_kernels")
+    n = 0
+    for k, c in enumerate(momentum_cases()):
+        u, v = c["u"], c["v"]
+        hu = np.full_like(u, 7.0)
+        hv = np.full_like(v, 7.0)
+        O.momentum_tendencies(u, v, c["fluid"], c["nx"], c["ny"], c["dx"], c["dy"], c["nu"],
+                              c["variable"], c["gamma"], c["periodic"], hu, hv, c["rho"],
+                              c["var_density"])
+        assert np.array_equal(hu, g[f"m{k}_hu"]), k
+        assert np.array_equal(hv, g[f"m{k}_hv"]), k
+        uo, vo = u.copy(), v.copy()
+        O.obstacle_bc(uo, vo, c["fluid"], c["nx"], c["ny"], c["periodic"])
+        assert np.array_equal(uo, g[f"m{k}_u_obc"]), k
+        assert np.array_equal(vo, g[f"m{k}_v_obc"]), k
+        n += 1
+    assert n == int(g["n_momentum"])
+
+
+def test_scalar_transport_bitwise_all_limiters():
+    g = golden("golden_kernels")
+    n = 0
+    for k, c in enumerate(scalar_cases()):
+        o = np.full_like(c["phi"], 3.0)
+        bt, bv = c["bt"], c["bv"]
+        O.scalar_transport(c["phi"], c["u"], c["v"], c["fluid"], c["nx"], c["ny"], c["dx"], c["dy"],
+                           c["diff"], c["limiter"], c["periodic"], bt["l"], bv["l"], bt["r"],
+                           bv["r"], bt["b"], bv["b"], bt["t"], bv["t"], c["obs_t"], c["obs_v"], o)
+        assert np.array_equal(o, g[f"s{k}_out"]), (k, c["limiter"], c["periodic"], c["obs_t"])
+        n += 1
+    assert n == int(g["n_scalar"])
+
+
+# ---------------------------------------------------------------- geometry
+def test_masks_and_finalize_bitwise():
+    g = golden("golden_geometry")
+    for k in range(int(g["n_shapes"])):
+        nx, ny, lx, ly = g[f"g{k}_grid"]
+        grid = O.OGrid(int(nx), int(ny), lx, ly)
+        assert np.array_equal(O.circle_mask(grid, *g[f"g{k}_circle"]), g[f"g{k}_circle_mask"])
+        assert np.array_equal(O.ellipse_mask(grid, *g[f"g{k}_ellipse"]), g[f"g{k}_ellipse_mask"])
+        assert np.array_equal(O.rectangle_mask(grid, *g[f"g{k}_rect"]), g[f"g{k}_rect_mask"])
+    grid = O.OGrid(440, 82, 2.2, 0.41)
+    assert np.array_equal(O.circle_mask(grid, 0.2, 0.2, 0.1 / 2), g["cyl_mask"])
+    grid = O.OGrid(60, 40, 1.5, 1.0)
+    grid.fluid[:] = g["fin_before"]
+    assert grid.finalize() == int(g["fin_removed"])
+    assert np.array_equal(grid.fluid, g["fin_after"])
+
+
+# ---------------------------------------------------------------- pressure
+def _pressure_oracle(name, g):
+    """Build the same simulation as the fixture generator and return its solver.
+
+    Constructing the simulation matters: its initial projection (cfd2d/solver.py:195-204)
+    runs whenever a boundary value makes u nonzero, and leaves the CG warm start x0 set.
+    """
+    if name == "cav":
+        sim = O.cavity(re=100, n=24, pressure_solver="cg", tol=None)
+    elif name == "cyl":
+        sim = O.cylinder(re=20, nx=110, ny=21, pressure_solver="cg", tol=None)
+    elif name == "per":
+        grid = O.OGrid(32, 32, 1.0, 1.0)
+        grid.add_obstacle(O.circle_mask(grid, 0.5, 0.5, 0.15))
+        bcs = {"left": O.OBC("periodic"), "right": O.OBC("periodic"), "bottom": O.OBC("slip"),
+               "top": O.OBC("slip")}
+        sim = O.OSimulation(grid, bcs, nu=0.02, pressure_solver="cg")
+    else:
+        grid = O.OGrid(30, 20, 1.5, 1.0)
+        grid.add_obstacle(O.rectangle_mask(grid, 0.7, -1.0, 0.8, 2.0))
+        sim = O.OSimulation(grid, {s: O.OBC("noslip") for s in O.SIDES}, nu=0.02,
+                            pressure_solver="cg")
+    assert np.array_equal(sim.grid.fluid, g[name + "_fluid"])
+    sim.pressure.tol = 1e-10
+    return sim.pressure
+
+
+@pytest.mark.parametrize("name", ["cav", "cyl", "per", "two"])
+def test_pressure_operator_and_cg(name):
+    g = golden("golden_pressure")
+    ps = _pressure_oracle(name, g)
+    assert np.array_equal(ps.diag[ps.fluid], g[name + "_diag"][ps.fluid])
+    assert np.array_equal(ps.labels, g[name + "_labels"])
+    assert np.array_equal(np.array(ps.pinned, dtype=np.int64).reshape(-1, 2), g[name + "_pinned"])
+    assert list(ps.neumann_components) == list(g[name + "_neumann"])
+    for s in O.SIDES:
+        assert np.array_equal(ps.dirichlet[s], g[name + "_dir_" + s])
+    # the stencil matvec equals the assembled CSR product bit for bit
+    rng = np.random.default_rng(5)
+    x = rng.standard_normal(ps.n)
+    assert np.array_equal(ps.matvec(x), ps._assemble() @ x)
+    p = ps.solve(g[name + "_rhs"])
+    assert ps.last_iterations == int(g[name + "_its"])
+    assert rel(p, g[name + "_p"]) < 1e-12
+    p2 = ps.solve(g[name + "_rhs2"])
+    assert ps.last_iterations == int(g[name + "_its2"])
+    assert rel(p2, g[name + "_p2"]) < 1e-12
+
+
+# ---------------------------------------------------------------- time stepping
+def test_cavity_200_steps():
+    g = golden("golden_cavity64")
+    sim = O.cavity(re=100, n=64, gamma=0.1, tau=0.5, tol=1e-8)
+    for n in range(1, 201):
+        sim.step()
+        if n in (1, 10, 200):
+            for f in "uvp":
+                assert rel(getattr(sim, f), g[f"cav_{f}_{n}"]) < 1e-12, (f, n)
+    assert np.array_equal(np.array(sim.iterations), g["cav_its"][:200])
+    assert np.array_equal(np.array(sim.hist["dt"]), g["cav_dt"][:200])
+
+
+def test_cylinder_with_scalar_10_steps():
+    g = golden("golden_cylinder440")
+    sim = O.cylinder(re=100, nx=440, ny=82, tol=1e-8)
+    O.add_scalar(sim, "c", 1e-3, inflow_band=(0.15, 0.25), limiter="vanleer")
+    for n in range(1, 11):
+        sim.step()
+        if n in (1, 10):
+            for f in "uvp":
+                assert rel(getattr(sim, f), g[f"cyl_{f}_{n}"]) < 1e-12, (f, n)
+            assert rel(sim.scalars["c"].phi, g[f"cyl_c_{n}"]) < 1e-12
+    assert np.array_equal(np.array(sim.iterations), g["cyl_its"])
+    assert rel(sim.hist["fx"], g["cyl_hist_fx"]) < 1e-12
+    assert rel(sim.hist["fy"], g["cyl_hist_fy"]) < 1e-10
+
+
+def test_sst_channel_20_steps():
+    g = golden("golden_sst128x192")
+    sim = O.sst_channel(128, 192, seed=0, tol=1e-8)
+    for n in range(1, 21):
+        sim.step()
+        if n in (1, 20):
+            for f in "uvp":
+                assert rel(getattr(sim, f), g[f"sst_{f}_{n}"]) < 1e-12, (f, n)
+            assert rel(sim.scalars["k"].phi, g[f"sst_k_{n}"]) < 1e-12
+            assert rel(sim.scalars["omega"].phi, g[f"sst_w_{n}"]) < 1e-12
+            assert rel(sim.nu_t, g[f"sst_nut_{n}"]) < 1e-12
+    assert sim.flow_force == pytest.approx(float(g["sst_flow_force"]), rel=1e-12)
+
+
+def test_misc_runs():
+    g = golden("golden_misc")
+    sim = O.heated_cavity(ra=1e5, n=32, tol=1e-8)
+    for _ in range(100):
+        sim.step()
+    for f in "uvp":
+        assert rel(getattr(sim, f), g[f"hot_{f}_100"]) < 1e-12
+    assert rel(sim.scalars["T"].phi, g["hot_T_100"]) < 1e-12
+
+    grid = O.OGrid(32, 32, 1.0, 1.0)
+    grid.add_obstacle(O.circle_mask(grid, 0.5, 0.5, 0.15))
+    bcs = {"left": O.OBC("periodic"), "right": O.OBC("periodic"), "bottom": O.OBC("slip"),
+           "top": O.OBC("slip")}
+    sim = O.OSimulation(grid, bcs, nu=0.02, flow_rate=1.0, pressure_solver="cg", tol=1e-8)
+    for _ in range(50):
+        sim.step()
+    for f in "uvp":
+        assert rel(getattr(sim, f), g[f"pob_{f}_50"]) < 1e-12
+    assert sim.flow_force == pytest.approx(float(g["pob_flow_force"]), rel=1e-12)
+
+    sim = O.cavity(re=100, n=16, scheme="euler", gamma=0.5, tol=1e-8)
+    for _ in range(30):
+        sim.step()
+    for f in "uvp":
+        assert rel(getattr(sim, f), g[f"eul_{f}_30"]) < 1e-12
