@@ -1,0 +1,361 @@
+"""Benchmark of the projection step on B200 (one JSON line on rank 0).
+
+Workload: the cylinder channel with a passive scalar -- 440 x 82 MAC grid, domain
+2.2 x 0.41, circle D = 0.1 at (0.2, 0.2), parabolic inflow U = 1, Re = 100,
+van Leer scalar entering on 0.15 < y < 0.25 (D = 1e-3), AB2 with automatic upwind
+fraction, tau 0.5, pressure by Jacobi-PCG to a relative residual of 1e-8 in FP64.
+Synthetic: the flow starts from rest, as the reference case does.
+
+A step is one full projection step (all stages, one captured CUDA graph).
+value     = cell-updates/s (nx*ny cells per step, summed over ranks) from CUDA
+            events around every timed step on the solver's stream; L2 is flushed
+            (256 MiB write) between timed steps.
+e2e       = the same metric through the public API (``sim.step()``) with the state
+            copied in from pinned host memory and u, v, p, c copied back out every step.
+roofline  = the pressure solver kernel: algorithmic bytes 88 B per cell per CG
+            iteration (FP64 x, r, p, q, z traffic of a streaming implementation)
+            over its event-timed duration.
+--impl reference times the CPU restatement of the reference (the oracle: NumPy
+stencils and scipy's CG iteration) on the same workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+for p in (str(ROOT / "cfd-_b200"), str(ROOT)):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+METRIC = "cell-updates/s and Poisson ms at 1e-8 residual: learned-PC vs plain CG on B200"
+NX, NY = 440, 82
+CG_RTOL = 1e-8
+BYTES_PER_CELL_ITER = 88.0
+BYTES_PER_CELL_SOLVE = 32.0
+SPEC = {"fall": "cylinder", "parameter": {"re": 100, "nx": NX, "ny": NY},
+        "numerik": {"pressure_solver": "cg"},
+        "skalar": {"name": "c", "diffusivity": 1e-3, "inflow_band": [0.15, 0.25], "limiter": "vanleer"}}
+WORKLOAD = "cylinder 440x82 Re100 + van Leer scalar, FP64 Jacobi-PCG rtol 1e-8"
+
+
+def _peaks():
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        d = json.loads(f.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws <= 1:
+        return None, 0, 1
+    import torch
+    import torch.distributed as dist
+
+    backend = "nccl" if torch.cuda.is_available() else "gloo"
+    from datetime import timedelta
+
+    dist.init_process_group(backend=backend, timeout=timedelta(seconds=120))
+    return dist, dist.get_rank(), dist.get_world_size()
+
+
+def _max_over_ranks(dist, x: float) -> float:
+    if dist is None:
+        return x
+    import torch
+
+    dev = torch.device("cuda", torch.cuda.current_device()) if torch.cuda.is_available() else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+class _Clocks:
+    """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
+
+    def __init__(self, path):
+        self.path = path
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            self.proc.wait(timeout=5)
+            self.f.close()
+
+    def summary(self, dev_index: int):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in Path(self.path).read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9 or parts[0] != str(dev_index):
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": smax, "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def _ncu_traffic():
+    """DRAM bytes per launch of the solver kernel from the committed ncu summary, if any."""
+    f = ROOT / "profiles" / "pcg_cluster_cylinder440x82.txt"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        if line.startswith("dram_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+# ------------------------------------------------------------------ CPU timings
+def cpu_oracle_rate(steps: int, warmup: int, threads: int | None) -> dict:
+    """Time the oracle (CPU restatement) on the bench workload in a child process."""
+    env = dict(os.environ)
+    if threads is not None:
+        for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+            env[k] = str(threads)
+    code = f"""
+import sys, time, json, warnings
+sys.path.insert(0, {str(ROOT)!r})
+warnings.simplefilter("ignore")
+import oracle as O
+sim = O.cylinder(re=100, nx={NX}, ny={NY}, tol={CG_RTOL})
+O.add_scalar(sim, "c", 1e-3, inflow_band=(0.15, 0.25), limiter="vanleer")
+for _ in range({warmup}):
+    sim.step()
+t0 = time.perf_counter()
+for _ in range({steps}):
+    sim.step()
+el = time.perf_counter() - t0
+print(json.dumps({{"seconds": el, "steps": {steps}, "its": sim.iterations[-{steps}:]}}))
+"""
+    out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, check=True)
+    d = json.loads(out.stdout.strip().splitlines()[-1])
+    d["rate"] = NX * NY * d["steps"] / d["seconds"]
+    return d
+
+
+def run_reference(args, dist, rank, world):
+    # the reference arm runs on rank 0 only; the other ranks exit without work
+    if rank != 0:
+        return
+    steps = max(1, min(args.steps, 8))
+    warm = max(0, min(args.warmup, 2))
+    d = cpu_oracle_rate(steps, warm, None)
+    value = d["rate"]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "cell-updates/s",
+        "n_gpus": world, "steps": steps, "warmup": warm, "ms_per_step": 1e3 * d["seconds"] / steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (flow from rest, as the reference case)",
+        "config": {"workload": WORKLOAD, "grid": [NX, NY], "cells": NX * NY, "parallelism": "replicas"},
+        "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": os.cpu_count(),
+                         "kind": "port",
+                         "sample": f"{steps} steps after {warm} warm-up steps of the oracle "
+                                   f"(NumPy + scipy-form CG) on the same workload"},
+        "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "poisson_iters_per_step": float(sum(d["its"]) / len(d["its"])),
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ GPU arm
+def run_b200(args, dist, rank, world):
+    import numpy as np
+    import torch
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    from cfd2d_b200 import _lib, cases
+
+    L = _lib.lib()
+    case = cases.build_case(SPEC)
+    sim = case.sim
+    sim.pressure.tol = CG_RTOL
+    stream = sim._stream
+    sptr = _lib.stream_ptr(stream)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    ev = (C.c_void_p * 4)()
+    _lib.check(L.cfd2d_events_create(4, ev), "events")
+    graph = C.c_void_p(0)
+    knodes = C.c_int(0)
+    with torch.cuda.stream(stream):
+        sim._flush_mirrors()
+        sim._set_run_limits()
+        _lib.check(L.cfd2d_graph_capture_steps_ex(C.byref(sim._S), 1, sptr, ev, C.byref(graph),
+                                                  C.byref(knodes)), "capture")
+
+        def one_step():
+            flush.fill_(1.0)  # L2 flush (256 MiB write) outside the timed events
+            _lib.check(L.cfd2d_graph_launch(graph, sptr), "launch")
+            ms_step, ms_solve = C.c_float(), C.c_float()
+            _lib.check(L.cfd2d_event_elapsed_ms(ev[0], ev[3], C.byref(ms_step)), "elapsed")
+            _lib.check(L.cfd2d_event_elapsed_ms(ev[1], ev[2], C.byref(ms_solve)), "elapsed")
+            return ms_step.value, ms_solve.value
+
+        for _ in range(args.warmup):
+            one_step()
+        n0 = sim._pull().n
+        _barrier(dist)
+        torch.cuda.synchronize()
+        step_ms, solve_ms = [], []
+        with _Clocks(str(ROOT / "gpurun_out" / f"clocks_rank{rank}.csv")
+                     if (ROOT / "gpurun_out").exists() else "/tmp/cfd2d_clocks.csv") as clk:
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                a, b = one_step()
+                step_ms.append(a)
+                solve_ms.append(b)
+            torch.cuda.synchronize()
+            wall = time.perf_counter() - t0
+        _barrier(dist)
+        st = sim._pull()
+        if st.status & (_lib.S_NONFINITE | _lib.S_BARRIER_TIMEOUT):
+            raise RuntimeError(f"device status {st.status} during the bench")
+        sim._pull_history()
+        its = np.array(sim.history.extra["cg_iterationen"][-args.steps:], dtype=float)
+    assert st.n - n0 == args.steps
+    dev_s = sum(step_ms) / 1e3
+    dev_s_max = _max_over_ranks(dist, dev_s)
+    cells = NX * NY
+    value = world * cells * args.steps / dev_s_max
+    solve_s = sum(solve_ms) / 1e3
+    iters = float(its.mean())
+    achieved = (BYTES_PER_CELL_ITER * cells * its.sum() + BYTES_PER_CELL_SOLVE * cells * len(its)) / solve_s / 1e9
+    peak, peak_kind = _peaks()
+
+    # ---- end to end through the public API with host buffers
+    e2e_steps = max(1, min(args.steps, 100))
+    host = {}
+    names = ("u", "v")
+    phi_dev = sim.scalars["c"].phi_gpu
+    with torch.cuda.stream(stream):
+        for nm in names:
+            host[nm] = torch.empty(getattr(sim, "_" + nm).shape, dtype=torch.float64).pin_memory()
+            host[nm].copy_(getattr(sim, "_" + nm))
+        host["c"] = torch.empty(phi_dev.shape, dtype=torch.float64).pin_memory()
+        host["c"].copy_(phi_dev)
+        out = {nm: torch.empty(t.shape, dtype=torch.float64).pin_memory()
+               for nm, t in (("u", sim._u), ("v", sim._v), ("p", sim._p), ("c", phi_dev))}
+        h2d = sum(t.numel() * 8 for t in host.values())
+        d2h = sum(t.numel() * 8 for t in out.values())
+        _barrier(dist)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            sim._u.copy_(host["u"], non_blocking=True)
+            sim._v.copy_(host["v"], non_blocking=True)
+            phi_dev.copy_(host["c"], non_blocking=True)
+            sim.step()
+            out["u"].copy_(sim._u, non_blocking=True)
+            out["v"].copy_(sim._v, non_blocking=True)
+            out["p"].copy_(sim._p, non_blocking=True)
+            out["c"].copy_(phi_dev, non_blocking=True)
+            stream.synchronize()
+            host["u"].copy_(out["u"])
+            host["v"].copy_(out["v"])
+            host["c"].copy_(out["c"])
+        e2e_s = time.perf_counter() - t0
+    e2e_s = _max_over_ranks(dist, e2e_s)
+    e2e = world * cells * e2e_steps / e2e_s
+    L.cfd2d_graph_destroy(graph)
+    L.cfd2d_events_destroy(4, ev)
+    clocks = clk.summary(local)
+
+    if rank != 0:
+        return
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        d = cpu_oracle_rate(3, 1, 1)
+        cpu = {"value": d["rate"], "unit": "cell-updates/s", "cores": 1, "kind": "port",
+               "sample": "3 steps after 1 warm-up step of the oracle (NumPy + scipy-form CG, "
+                         "1 thread) on the same workload from rest"}
+    line = {
+        "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dev_s_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (flow from rest, as the reference case)",
+        "config": {"workload": WORKLOAD, "grid": [NX, NY], "cells": cells, "fluid_cells": int(sim.pressure.n),
+                   "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"replicas x{world}",
+                   "pcg_cluster_ctas": int(sim.pressure.cluster)},
+        "poisson_ms": 1e3 * solve_s / args.steps,
+        "poisson_iters_per_step": iters,
+        "wall_ms_per_step": 1e3 * wall / args.steps,
+        "e2e": {"value": e2e, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "steps": e2e_steps},
+        "gpu_launches": int(knodes.value) * args.steps,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": _ncu_traffic(),
+                     "kernel": "k_pcg_cluster (on-chip FP64 Jacobi-PCG)", "peak_kind": peak_kind},
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference" and int(os.environ.get("RANK", "0")) != 0:
+        return  # the CPU reference arm runs on rank 0 alone; other ranks exit without work
+    if args.impl == "reference":
+        run_reference(args, None, 0, int(os.environ.get("WORLD_SIZE", "1")))
+        return
+    dist, rank, world = _dist()
+    try:
+        run_b200(args, dist, rank, world)
+    finally:
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -132,6 +132,10 @@ def lib():
         "cfd2d_graph_capture_steps": ([vp, i, vp, C.POINTER(C.c_void_p)], i),
         "cfd2d_graph_launch": ([vp, vp], i),
         "cfd2d_graph_destroy": ([vp], i),
+        "cfd2d_graph_capture_steps_ex": ([vp, i, vp, vp, C.POINTER(C.c_void_p), C.POINTER(C.c_int)], i),
+        "cfd2d_events_create": ([i, vp], i),
+        "cfd2d_events_destroy": ([i, vp], i),
+        "cfd2d_event_elapsed_ms": ([vp, vp, C.POINTER(C.c_float)], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -150,6 +154,8 @@ def exported_symbols():
         "cfd2d_sim_scratch_doubles", "cfd2d_sim_apply_bc", "cfd2d_sim_project_initial",
         "cfd2d_sim_step", "cfd2d_sim_scalar_fill_ghosts", "cfd2d_sim_sst_pre_momentum",
         "cfd2d_graph_capture_steps", "cfd2d_graph_launch", "cfd2d_graph_destroy",
+        "cfd2d_graph_capture_steps_ex", "cfd2d_events_create", "cfd2d_events_destroy",
+        "cfd2d_event_elapsed_ms",
     ]
 
 

@@ -163,11 +163,27 @@ int cfd2d_sim_project_initial(const cfd2d_sim* sim, void* stream) {
     return status_of(stage_apply_bc(*sim, 0, s));
 }
 
-int cfd2d_sim_step(const cfd2d_sim* sim, void* stream) {
+}  // extern "C"
+
+namespace {
+
+// Event record that becomes an externally visible event node when the stream is
+// being captured into a graph (plain record otherwise).
+cudaError_t record(cudaEvent_t e, cudaStream_t s) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaError_t err = cudaStreamIsCapturing(s, &cs);
+    if (err != cudaSuccess) return err;
+    if (cs == cudaStreamCaptureStatusActive) return cudaEventRecordWithFlags(e, s, cudaEventRecordExternal);
+    return cudaEventRecord(e, s);
+}
+
+// One projection step; ev (may be null) gets four events recorded: step start,
+// before and after the main pressure solve, step end.
+int sim_step_impl(const cfd2d_sim* sim, cudaStream_t s, cudaEvent_t* ev) {
     if (!sim || !sim->state || !grid_ok(sim->nx, sim->ny)) return CFD2D_E_ARG;
     if (sim->pcg.cluster < 1) return CFD2D_E_CAPACITY;
     const cfd2d_sim& S = *sim;
-    const cudaStream_t s = as_stream(stream);
+    if (ev) CFD_TRY(record(ev[0], s));
     // 1. boundary conditions (and the run() stop decision for this step)
     CFD_TRY(stage_apply_bc(S, 1, s));
     // 2. model pre-momentum hooks: k-omega SST blending, nu_t, nu_eff
@@ -177,8 +193,10 @@ int cfd2d_sim_step(const cfd2d_sim* sim, void* stream) {
     // 4. tendencies, AB2, predictor, outflow extrapolation
     CFD_TRY(stage_predictor(S, 0, s));
     // 5. pressure Poisson (divergence fused into the solver prologue) and correction
+    if (ev) CFD_TRY(record(ev[1], s));
     int rc = project(sim, S.p, false, true, s);
     if (rc) return rc;
+    if (ev) CFD_TRY(record(ev[2], s));
     CFD_TRY(stage_correct(S, S.p, 0, s));
     CFD_TRY(stage_apply_bc(S, 0, s));
     // 6. volume-flow forcing (cfd2d/solver.py:410-425)
@@ -196,7 +214,16 @@ int cfd2d_sim_step(const cfd2d_sim* sim, void* stream) {
     for (int k = 0; k < S.nscalars; ++k) CFD_TRY(stage_scalar(S, k, s));
     // 8. residual, counters, history record
     CFD_TRY(stage_end(S, s));
+    if (ev) CFD_TRY(record(ev[3], s));
     return CFD2D_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cfd2d_sim_step(const cfd2d_sim* sim, void* stream) {
+    return sim_step_impl(sim, as_stream(stream), nullptr);
 }
 
 int cfd2d_sim_scalar_fill_ghosts(const cfd2d_sim* sim, int slot, void* stream) {
@@ -209,13 +236,18 @@ int cfd2d_sim_sst_pre_momentum(const cfd2d_sim* sim, void* stream) {
     return status_of(stage_sst_pre(*sim, as_stream(stream)));
 }
 
-int cfd2d_graph_capture_steps(const cfd2d_sim* sim, int nsteps, void* stream, void** graph_out) {
+int cfd2d_graph_capture_steps_ex(const cfd2d_sim* sim, int nsteps, void* stream, void* const* events,
+                                 void** graph_out, int* kernel_nodes) {
     if (!sim || nsteps < 1 || !graph_out) return CFD2D_E_ARG;
+    if (events && nsteps != 1) return CFD2D_E_ARG;
     const cudaStream_t s = as_stream(stream);
     if (s == nullptr) return CFD2D_E_ARG;  // the legacy default stream cannot be captured
+    cudaEvent_t ev[4];
+    if (events)
+        for (int k = 0; k < 4; ++k) ev[k] = (cudaEvent_t)events[k];
     CFD_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
     int rc = CFD2D_OK;
-    for (int k = 0; k < nsteps && rc == CFD2D_OK; ++k) rc = cfd2d_sim_step(sim, stream);
+    for (int k = 0; k < nsteps && rc == CFD2D_OK; ++k) rc = sim_step_impl(sim, s, events ? ev : nullptr);
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(s, &g);
     if (rc != CFD2D_OK) {
@@ -223,12 +255,53 @@ int cfd2d_graph_capture_steps(const cfd2d_sim* sim, int nsteps, void* stream, vo
         return rc;
     }
     if (e != cudaSuccess) return CFD2D_E_CUDA;
+    if (kernel_nodes) {
+        size_t n = 0;
+        if (cudaGraphGetNodes(g, nullptr, &n) != cudaSuccess) { cudaGraphDestroy(g); return CFD2D_E_CUDA; }
+        cudaGraphNode_t* nodes = new cudaGraphNode_t[n > 0 ? n : 1];
+        size_t m = n;
+        int kn = 0;
+        if (cudaGraphGetNodes(g, nodes, &m) == cudaSuccess) {
+            for (size_t k = 0; k < m; ++k) {
+                cudaGraphNodeType t;
+                if (cudaGraphNodeGetType(nodes[k], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++kn;
+            }
+        }
+        delete[] nodes;
+        *kernel_nodes = kn;
+    }
     cudaGraphExec_t exec = nullptr;
     e = cudaGraphInstantiate(&exec, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return CFD2D_E_CUDA;
     *graph_out = (void*)exec;
     return CFD2D_OK;
+}
+
+int cfd2d_graph_capture_steps(const cfd2d_sim* sim, int nsteps, void* stream, void** graph_out) {
+    return cfd2d_graph_capture_steps_ex(sim, nsteps, stream, nullptr, graph_out, nullptr);
+}
+
+int cfd2d_events_create(int n, void** events) {
+    if (n < 0 || (n > 0 && !events)) return CFD2D_E_ARG;
+    for (int k = 0; k < n; ++k) {
+        cudaEvent_t e;
+        CFD_TRY(cudaEventCreate(&e));
+        events[k] = (void*)e;
+    }
+    return CFD2D_OK;
+}
+
+int cfd2d_events_destroy(int n, void** events) {
+    for (int k = 0; k < n; ++k)
+        if (events[k]) cudaEventDestroy((cudaEvent_t)events[k]);
+    return CFD2D_OK;
+}
+
+int cfd2d_event_elapsed_ms(void* start, void* end, float* ms) {
+    if (!start || !end || !ms) return CFD2D_E_ARG;
+    CFD_TRY(cudaEventSynchronize((cudaEvent_t)end));
+    return status_of(cudaEventElapsedTime(ms, (cudaEvent_t)start, (cudaEvent_t)end));
 }
 
 int cfd2d_graph_launch(void* graph, void* stream) {

@@ -666,9 +666,21 @@ __global__ void k_scalar_update(cfd2d_sim S, int s) {
     }
     if (sc.has_lower) nw = npmax(nw, sc.lower);
     if (sc.has_upper) nw = npmin(nw, sc.upper);
-    double out = S.fluid[c] ? nw : phi_i;
-    if (sc.source == 2 && S.sst.wall_adj[ci]) out = S.sst.w_wall[ci];
-    sc.phi[c] = out;
+    sc.phi[c] = S.fluid[c] ? nw : phi_i;
+}
+
+// viscous omega in the wall-adjacent cells after the omega update
+// (cfd2d/turbulence.py:239-242); the ghosts are filled before and after, as the
+// reference does (a periodic corner keeps the value of the first fill)
+__global__ void k_sst_wall_omega(cfd2d_sim S) {
+    if (!is_active(S.state)) return;
+    const int nx = S.nx, ny = S.ny;
+    const Grid2 g{nx, ny};
+    const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int i = blockIdx.y + 1;
+    if (j > ny) return;
+    const int ci = (i - 1) * ny + (j - 1);
+    if (S.sst.wall_adj[ci]) S.scalars[S.sst.w_index].phi[g.c(i, j)] = S.sst.w_wall[ci];
 }
 
 // Domain ghost cells of a scalar (cfd2d/models.py:157-166). With periodic x the
@@ -947,6 +959,9 @@ cudaError_t stage_scalar(const cfd2d_sim& S, int slot, cudaStream_t s) {
         k_scalar_turb_diff<<<reduction_blocks((S.nx + 2) * (S.ny + 2)), kBlock, 0, s>>>(S, slot);
     k_scalar_rhs<<<grid_rows(S.ny + 2, S.nx + 2), kBlock, 0, s>>>(S, slot);
     k_scalar_update<<<grid_rows(S.ny, S.nx), kBlock, 0, s>>>(S, slot);
+    cudaError_t e = stage_scalar_ghosts(S, slot, s);
+    if (e != cudaSuccess || sc.source != 2) return e;
+    k_sst_wall_omega<<<grid_rows(S.ny, S.nx), kBlock, 0, s>>>(S);
     return stage_scalar_ghosts(S, slot, s);
 }
 

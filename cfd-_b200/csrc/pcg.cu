@@ -446,8 +446,6 @@ int pcg_cluster_plan(int nx, int ny) {
         const long long lim = pass == 0 ? 4LL * kPcgThreads : 8LL * kPcgThreads;
         if (cells > capmax || cells > lim) continue;
         // co-scheduling check
-        PcgLaunch dummy = {};
-        dummy.cap_cells = (int)cells;
         const int cpt = cpt_for((int)cells);
         if (!cpt) continue;
         cudaLaunchConfig_t cfg = {};

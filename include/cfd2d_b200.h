@@ -269,6 +269,18 @@ int cfd2d_graph_capture_steps(const cfd2d_sim* sim, int nsteps, void* stream, vo
 int cfd2d_graph_launch(void* graph, void* stream);
 int cfd2d_graph_destroy(void* graph);
 
+/* As cfd2d_graph_capture_steps; with events != NULL (four cudaEvent_t, only for
+ * nsteps == 1) the graph records them at step start, before and after the main
+ * pressure solve, and at step end. kernel_nodes (may be NULL) receives the number
+ * of kernel launches in the graph. */
+int cfd2d_graph_capture_steps_ex(const cfd2d_sim* sim, int nsteps, void* stream, void* const* events,
+                                 void** graph_out, int* kernel_nodes);
+
+/* Timing events for the measurement harness (cudaEvent_t as void*). */
+int cfd2d_events_create(int n, void** events);
+int cfd2d_events_destroy(int n, void** events);
+int cfd2d_event_elapsed_ms(void* start, void* end, float* ms);
+
 /* Library version string (host memory, static). */
 const char* cfd2d_version(void);
 
