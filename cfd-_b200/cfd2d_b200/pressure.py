@@ -16,6 +16,7 @@ residual of 1e-13, which agrees with a sparse LU solve to about 1e-15.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import warnings
 
 import numpy as np
@@ -130,11 +131,14 @@ class PressureSolver:
         self._d_cnt = _lib.to_dev(np.array(counts + [1.0], dtype=np.float64))
         self._d_x0 = t.zeros((nx, ny), dtype=t.float64, device=_lib.device())
         cl = C.c_int(0)
-        rc = _lib.lib().cfd2d_pcg_plan(nx, ny, C.byref(cl))
-        if rc != _lib.OK:
-            raise ValueError(f"Gitter {nx}x{ny} ist zu groß für den On-Chip-CG-Löser "
-                             f"(Cluster aus höchstens 16 CTAs)")
-        self.cluster = cl.value
+        _lib.check(_lib.lib().cfd2d_pcg_plan(nx, ny, C.byref(cl)), "cfd2d_pcg_plan")
+        # > 0: CTAs of the on-chip cluster solver; 0: grid-persistent solver with a workspace.
+        # CFD2D_PCG_VARIANT=grid selects the grid-persistent solver for any size.
+        self.cluster = 0 if os.environ.get("CFD2D_PCG_VARIANT") == "grid" else cl.value
+        self._work = None
+        if self.cluster == 0:
+            nbytes = int(_lib.lib().cfd2d_pcg_workspace_bytes(nx, ny))
+            self._work = t.zeros(nbytes // 8, dtype=t.float64, device=_lib.device())
         self._d_iters = t.zeros(2, dtype=t.int32, device=_lib.device())
         P = _lib.Poisson()
         P.nx, P.ny, P.periodic = nx, ny, int(self.periodic)
@@ -144,7 +148,10 @@ class PressureSolver:
         P.ncomp = len(self.neumann_components)
         P.comp_count = self._d_cnt.data_ptr()
         P.x0 = self._d_x0.data_ptr()
-        P.work, P.work_bytes = 0, 0
+        if self._work is not None:
+            P.work, P.work_bytes = self._work.data_ptr(), self._work.numel() * 8
+        else:
+            P.work, P.work_bytes = 0, 0
         P.cluster = self.cluster
         self.op = P
 
@@ -209,6 +216,8 @@ class PressureSolver:
         _lib.check(rc, "cfd2d_pressure_solve")
         info = st.cpu().numpy()
         self.last_iterations = int(self._d_iters[0].item())
+        if info[0] & _lib.S_BARRIER_TIMEOUT:
+            raise RuntimeError("pressure solve abandoned: a bounded inter-block wait timed out")
         if info[0] & _lib.S_CG_MAXITER:
             warnings.warn(f"CG-Drucklöser nicht konvergiert ({self.maxiter} Iterationen)")
         return p.cpu().numpy() if host else p

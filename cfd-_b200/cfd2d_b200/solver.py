@@ -420,6 +420,9 @@ class Simulation:
             if not (bool((self._u != 0).any()) or bool((self._v != 0).any())):
                 return
             self._call("cfd2d_sim_project_initial")
+            self._sync()
+            if self._pull().status & _lib.S_BARRIER_TIMEOUT:
+                raise RuntimeError("initial projection abandoned: a bounded inter-block wait timed out")
             self._device_changed()
 
     def _graph(self, nsteps: int):

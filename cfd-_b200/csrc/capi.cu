@@ -113,19 +113,20 @@ int cfd2d_mask_rectangle(int nx, int ny, double dx, double dy, double xa, double
 }
 
 size_t cfd2d_pcg_workspace_bytes(int nx, int ny) {
-    return ((size_t)4 * nx * ny + 4096) * sizeof(double);
+    return pcg_grid_workspace_doubles(nx, ny) * sizeof(double);
 }
 
 int cfd2d_pcg_plan(int nx, int ny, int* cluster) {
     if (!cluster || !grid_ok(nx, ny)) return CFD2D_E_ARG;
     *cluster = pcg_cluster_plan(nx, ny);
-    return *cluster > 0 ? CFD2D_OK : CFD2D_E_CAPACITY;
+    return CFD2D_OK;
 }
 
 int cfd2d_pressure_solve(const cfd2d_poisson* op, const double* rhs, double* p, double rtol,
                          int maxiter, int32_t* iters_out, int32_t* status_out, void* stream) {
     if (!op || !rhs || !p || maxiter < 0 || !grid_ok(op->nx, op->ny)) return CFD2D_E_ARG;
-    if (op->cluster < 1) return CFD2D_E_CAPACITY;
+    if (op->cluster < 0) return CFD2D_E_ARG;
+    if (op->cluster == 0 && !op->work) return CFD2D_E_ARG;
     if (op->ncomp > CFD2D_MAX_COMPONENTS) return CFD2D_E_CAPACITY;
     PcgLaunch L = {};
     L.op = *op;
@@ -151,7 +152,7 @@ int cfd2d_sim_apply_bc(const cfd2d_sim* sim, void* stream) {
 
 int cfd2d_sim_project_initial(const cfd2d_sim* sim, void* stream) {
     if (!sim || !sim->state) return CFD2D_E_ARG;
-    if (sim->pcg.cluster < 1) return CFD2D_E_CAPACITY;
+    if (sim->pcg.cluster == 0 && !sim->pcg.work) return CFD2D_E_ARG;
     const cudaStream_t s = as_stream(stream);
     // F = u, G = v, outflow extrapolation; solve with dt = 1; correct; p = 0; BCs
     // (cfd2d/solver.py:195-204)
@@ -181,7 +182,7 @@ cudaError_t record(cudaEvent_t e, cudaStream_t s) {
 // before and after the main pressure solve, step end.
 int sim_step_impl(const cfd2d_sim* sim, cudaStream_t s, cudaEvent_t* ev) {
     if (!sim || !sim->state || !grid_ok(sim->nx, sim->ny)) return CFD2D_E_ARG;
-    if (sim->pcg.cluster < 1) return CFD2D_E_CAPACITY;
+    if (sim->pcg.cluster == 0 && !sim->pcg.work) return CFD2D_E_ARG;
     const cfd2d_sim& S = *sim;
     if (ev) CFD_TRY(record(ev[0], s));
     // 1. boundary conditions (and the run() stop decision for this step)

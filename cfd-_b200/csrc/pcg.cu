@@ -29,8 +29,10 @@ namespace cfd {
 
 namespace {
 
-constexpr int kPcgThreads = 1024;
-constexpr int kSlot = 4 + CFD2D_MAX_COMPONENTS;  // doubles per reduction slot
+constexpr int kPcgThreads = 512;
+constexpr int kSlot = 4 + CFD2D_MAX_COMPONENTS;  // doubles per CTA partial (grid kernel)
+constexpr int kArrays = 7;                       // X, R, P0, P1, DI, DG, Z per cell
+constexpr int kMaxK = 4;                         // values per cluster reduction
 
 __device__ __forceinline__ int owner_of(int i, int nx, int C) {
     return (int)(((long long)(i + 1) * C - 1) / nx);
@@ -47,26 +49,40 @@ __device__ __forceinline__ double row_sum(bool periodic, int i, int nx, double t
     return (((tW + tS) + tC) + tN) + tE;
 }
 
-// cluster-wide sum of K per-thread values: block tree, then the C CTA partials
-// added in rank order by every CTA. Returns the same value in every thread.
+// Cluster-wide sum of K per-thread values. Block tree first; then lane r of warp 0
+// pushes this CTA's K partials into slot[me*K + k] of CTA r, so that after the
+// cluster barrier every CTA holds all C partials in its own shared memory and each
+// thread adds them in rank order: all threads of all CTAs get the same value.
 template <int K>
 __device__ __forceinline__ void cluster_sum(cg::cluster_group& cluster, double (&v)[K],
-                                            double* red_smem, double* slot, int C) {
-    block_sum<K>(v, red_smem);
-    if (threadIdx.x == 0) {
+                                            double* red_smem, double* slots, int C, int me) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
-        for (int k = 0; k < K; ++k) slot[k] = v[k];
+    for (int k = 0; k < K; ++k) v[k] = warp_sum(v[k]);
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) red_smem[k * 32 + w] = v[k];
+    }
+    __syncthreads();
+    if (w == 0) {
+        double x[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            x[k] = warp_sum((lane < nw) ? red_smem[k * 32 + lane] : 0.0);
+            x[k] = __shfl_sync(0xffffffffu, x[k], 0);
+        }
+        if (lane < C) {
+            double* dst = cluster.map_shared_rank(slots, lane);
+#pragma unroll
+            for (int k = 0; k < K; ++k) dst[me * K + k] = x[k];
+        }
     }
     cluster.sync();
-    const int lane = threadIdx.x & 31;
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-        double x = 0.0;
-        if (lane < C) x = cluster.map_shared_rank(slot, lane)[k];
-        // fixed-shape tree over the (at most 16) partials
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-        v[k] = x;
+        double s = slots[k];
+        for (int r = 1; r < C; ++r) s = s + slots[r * K + k];
+        v[k] = s;
     }
 }
 
@@ -83,10 +99,12 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cluster(PcgLaunch L) {
     const int nx = op.nx, ny = op.ny;
     const bool periodic = op.periodic != 0;
     const int r0 = row0_of(me, nx, C), r1 = row0_of(me + 1, nx, C);
-    const int nloc = (r1 - r0) * ny;
+    const int rows = r1 - r0;
+    const int nloc = rows * ny;
     const int cap = L.cap_cells;
     const int tid = threadIdx.x;
     const double mdx2 = -op.dx2, mdy2 = -op.dy2;
+    const int goff = r0 * ny;  // global index of local cell 0
 
     extern __shared__ __align__(16) double sm[];
     double* X = sm;
@@ -95,24 +113,48 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cluster(PcgLaunch L) {
     double* P1 = P0 + cap;
     double* DI = P1 + cap;
     double* DG = DI + cap;
-    uint8_t* NB = reinterpret_cast<uint8_t*>(DG + cap);
-    __shared__ double red_smem[32 * kSlot];
-    __shared__ double slotA[kSlot];
-    __shared__ double slotB[kSlot];
+    double* Z = DG + cap;
+    uint8_t* NB = reinterpret_cast<uint8_t*>(Z + cap);
+    __shared__ double red_smem[32 * kMaxK];
+    __shared__ double slotsA[16 * kMaxK];
+    __shared__ double slotsB[16 * kMaxK];
+    __shared__ double cmean[CFD2D_MAX_COMPONENTS];
+    // consecutive reductions alternate between the two slot buffers, so a buffer is
+    // rewritten only after the barrier of the reduction in between, which every CTA
+    // reaches after reading it
+    int nred = 0;
+#define SLOTS() ((nred++ & 1) ? slotsB : slotsA)
 
-    // ------------------------------------------------------------ prologue: load
-    const int ncomp = op.ncomp;
+    // c / ny by multiply-high: exact for c * ny < 2^32
+    const unsigned magic = (unsigned)(((1ull << 32) + (unsigned)ny - 1) / (unsigned)ny);
+    // halo rows owned by other CTAs (or by this one when periodic wraps onto itself):
+    // generic pointers to their X entries at j = 0; the other arrays follow at
+    // multiples of cap, identically in every CTA
+    const double* baseW = nullptr;
+    const double* baseE = nullptr;
+    {
+        const int iw = (r0 == 0) ? (periodic ? nx - 1 : -1) : r0 - 1;
+        const int ie = (r1 == nx) ? (periodic ? 0 : -1) : r1;
+        if (iw >= 0) {
+            const int o = owner_of(iw, nx, C);
+            baseW = cluster.map_shared_rank(X, o) + (iw - row0_of(o, nx, C)) * ny;
+        }
+        if (ie >= 0) {
+            const int o = owner_of(ie, nx, C);
+            baseE = cluster.map_shared_rank(X, o) + (ie - row0_of(o, nx, C)) * ny;
+        }
+    }
+
+    // ------------------------------------------------------------ prologue
     double dt = 1.0;
     if (L.rhs_mode == 1) dt = L.dt_ptr ? *L.dt_ptr : L.dt_const;
-    double csum[CFD2D_MAX_COMPONENTS + 1];
-#pragma unroll
-    for (int k = 0; k <= CFD2D_MAX_COMPONENTS; ++k) csum[k] = 0.0;
+    double nzx = 0.0;
     for (int c = tid; c < nloc; c += kPcgThreads) {
-        const int i = r0 + c / ny, j = c % ny;
-        const int gidx = i * ny + j;
+        const int gidx = goff + c;
         const uint8_t nb = op.nbr[gidx];
         NB[c] = nb;
-        X[c] = op.x0[gidx];
+        const double x0 = op.x0[gidx];
+        X[c] = x0;
         DI[c] = op.dinv[gidx];
         DG[c] = op.diag[gidx];
         double braw = 0.0;
@@ -121,87 +163,73 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cluster(PcgLaunch L) {
                 braw = L.rhs[gidx];
             } else {
                 // div(F, G) / dt at interior cell (i+1, j+1) (cfd2d/solver.py:264-266)
+                const int li = (int)__umulhi((unsigned)c, magic);
+                const int j = c - li * ny;
                 const int pu = ny + 2, pv = ny + 1;
-                const int ig = i + 1, jg = j + 1;
+                const int ig = r0 + li + 1, jg = j + 1;
                 const double div = (L.F[ig * pu + jg] - L.F[(ig - 1) * pu + jg]) / L.dx +
                                    (L.G[ig * pv + jg] - L.G[ig * pv + jg - 1]) / L.dy;
                 braw = div / dt;
             }
-            const int lab = op.label[gidx];
-            if (lab >= 0 && lab < CFD2D_MAX_COMPONENTS) {
-#pragma unroll
-                for (int k = 0; k < CFD2D_MAX_COMPONENTS; ++k)
-                    if (k == lab) csum[k] += braw;
-            }
-            if (X[c] != 0.0) csum[CFD2D_MAX_COMPONENTS] += 1.0;
+            if (x0 != 0.0) nzx += 1.0;
         }
         R[c] = braw;
     }
-    // component sums of b (mean removal, cfd2d/pressure.py:155-160) and "x0.any()"
+    // scipy computes A x0 only if x0 has a nonzero (iterative.py: "if x.any()")
     {
-        double v[CFD2D_MAX_COMPONENTS + 1];
-#pragma unroll
-        for (int k = 0; k <= CFD2D_MAX_COMPONENTS; ++k) v[k] = csum[k];
-        cluster_sum<CFD2D_MAX_COMPONENTS + 1>(cluster, v, red_smem, slotA, C);
-#pragma unroll
-        for (int k = 0; k <= CFD2D_MAX_COMPONENTS; ++k) csum[k] = v[k];
+        double v[1] = {nzx};
+        cluster_sum<1>(cluster, v, red_smem, SLOTS(), C, me);
+        nzx = v[0];
     }
-    const bool x_any = csum[CFD2D_MAX_COMPONENTS] > 0.0;
+    const bool x_any = nzx > 0.0;
+    // Neumann-component means of b (cfd2d/pressure.py:155-160), one reduction each
+    const int ncomp = op.ncomp;
+    for (int k = 0; k < ncomp; ++k) {
+        double v[1] = {0.0};
+        for (int c = tid; c < nloc; c += kPcgThreads)
+            if ((NB[c] & 0x80) && op.label[goff + c] == k) v[0] += R[c];
+        cluster_sum<1>(cluster, v, red_smem, SLOTS(), C, me);
+        if (tid == 0) cmean[k] = v[0] / op.comp_count[k];
+    }
+    __syncthreads();
 
-    // b = -(b_raw - mean), r = b - A x0 (only if x0 has a nonzero), norms
+    // b = -(b_raw - mean), r = b - A x0, z = M^-1 r, norms
     double part[3] = {0.0, 0.0, 0.0};
     for (int c = tid; c < nloc; c += kPcgThreads) {
         const uint8_t nb = NB[c];
-        if (!(nb & 0x80)) { P1[c] = 0.0; P0[c] = 0.0; R[c] = 0.0; continue; }
-        const int i = r0 + c / ny, j = c % ny;
-        const int gidx = i * ny + j;
+        if (!(nb & 0x80)) { P1[c] = 0.0; P0[c] = 0.0; R[c] = 0.0; Z[c] = 0.0; continue; }
         double b = R[c];
-        const int lab = op.label[gidx];
-        if (lab >= 0) {
-            double mean = 0.0;
-#pragma unroll
-            for (int k = 0; k < CFD2D_MAX_COMPONENTS; ++k)
-                if (k == lab) mean = csum[k] / op.comp_count[k];
-            b = b - mean;
+        if (ncomp > 0) {
+            const int lab = op.label[goff + c];
+            if (lab >= 0) b = b - cmean[lab];
         }
         b = -b;
         P1[c] = b;  // kept for the ||b|| == 0 return
         double r = b;
         if (x_any) {
+            const int li = (int)__umulhi((unsigned)c, magic);
+            const int j = c - li * ny;
             double tW = 0.0, tS = 0.0, tN = 0.0, tE = 0.0;
             if (nb & 2) tS = mdy2 * X[c - 1];
             if (nb & 4) tN = mdy2 * X[c + 1];
-            if (nb & 1) {
-                const int iw = (i == 0) ? nx - 1 : i - 1;
-                const double* row = (iw >= r0 && iw < r1)
-                                        ? X + (iw - r0) * ny
-                                        : cluster.map_shared_rank(X, owner_of(iw, nx, C)) +
-                                              (iw - row0_of(owner_of(iw, nx, C), nx, C)) * ny;
-                tW = mdx2 * row[j];
-            }
-            if (nb & 8) {
-                const int ie = (i == nx - 1) ? 0 : i + 1;
-                const double* row = (ie >= r0 && ie < r1)
-                                        ? X + (ie - r0) * ny
-                                        : cluster.map_shared_rank(X, owner_of(ie, nx, C)) +
-                                              (ie - row0_of(owner_of(ie, nx, C), nx, C)) * ny;
-                tE = mdx2 * row[j];
-            }
-            const double ax = row_sum(periodic, i, nx, tW, tS, DG[c] * X[c], tN, tE);
-            r = b - ax;
+            if (nb & 1) tW = mdx2 * ((li > 0) ? X[c - ny] : baseW[j]);
+            if (nb & 8) tE = mdx2 * ((li < rows - 1) ? X[c + ny] : baseE[j]);
+            r = b - row_sum(periodic, r0 + li, nx, tW, tS, DG[c] * X[c], tN, tE);
         }
-        // R is only read by other CTAs inside the iteration loop, after the
-        // barrier of the reduction below; X (read here across CTAs) is unchanged
+        // R and Z are read by other CTAs only inside the loop, after the barrier of
+        // the reduction below; X (read here across CTAs) is unchanged until then
         R[c] = r;
         P0[c] = 0.0;
+        const double z = DI[c] * r;
+        Z[c] = z;
         part[0] += b * b;
         part[1] += r * r;
-        part[2] += r * (DI[c] * r);
+        part[2] += r * z;
     }
-    cluster_sum<3>(cluster, part, red_smem, slotB, C);
+    cluster_sum<3>(cluster, part, red_smem, SLOTS(), C, me);
     const double bnrm2 = sqrt(part[0]);
     double rr = part[1];
-    double rho = part[2];  // r . (M r) for the first iteration
+    double rho = part[2];  // r . z for the first iteration
     const double atol = L.rtol * bnrm2;
     int it = 0;
     bool converged = false;
@@ -211,12 +239,13 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cluster(PcgLaunch L) {
         converged = true;
     } else {
         double beta = 0.0;
-        int cur = 0;  // p of this iteration goes to buffer cur
+        int cur = 0;  // p of this iteration goes to buffer cur (P0 or P1)
         double q[CPT];
         for (it = 0; it < L.maxiter; ++it) {
             if (sqrt(rr) < atol) { converged = true; break; }
-            double* Pn = cur ? P1 : P0;  // new p
-            const double* Po = cur ? P0 : P1;  // previous p
+            double* Pn = cur ? P1 : P0;
+            const double* Po = cur ? P0 : P1;
+            const int po = cur ? 2 * cap : 3 * cap;  // offset of the previous p from X
             const bool first = (it == 0);
             double pq = 0.0;
 #pragma unroll
@@ -226,50 +255,30 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cluster(PcgLaunch L) {
                 if (c >= nloc) continue;
                 const uint8_t nb = NB[c];
                 if (!(nb & 0x80)) continue;
-                const int i = r0 + c / ny, j = c % ny;
-                // p_new = beta * p_old + dinv * r at a cell with local arrays po/rr_/di
-#define PNEW(po, r_, di, idx) (first ? ((di)[idx] * (r_)[idx]) : ((po)[idx] * beta + (di)[idx] * (r_)[idx]))
-                const double pC = PNEW(Po, R, DI, c);
+                const int li = (int)__umulhi((unsigned)c, magic);
+                const int j = c - li * ny;
+                // p_new = beta * p_old + z, recomputed for the neighbours from their
+                // previous p and z instead of waiting for their owners
+                const double pC = first ? Z[c] : Po[c] * beta + Z[c];
                 double tW = 0.0, tS = 0.0, tN = 0.0, tE = 0.0;
-                if (nb & 2) tS = mdy2 * PNEW(Po, R, DI, c - 1);
-                if (nb & 4) tN = mdy2 * PNEW(Po, R, DI, c + 1);
+                if (nb & 2) tS = mdy2 * (first ? Z[c - 1] : Po[c - 1] * beta + Z[c - 1]);
+                if (nb & 4) tN = mdy2 * (first ? Z[c + 1] : Po[c + 1] * beta + Z[c + 1]);
                 if (nb & 1) {
-                    const int iw = (i == 0) ? nx - 1 : i - 1;
-                    if (iw >= r0 && iw < r1) {
-                        const int o = (iw - r0) * ny + j;
-                        tW = mdx2 * PNEW(Po, R, DI, o);
-                    } else {
-                        const int ow = owner_of(iw, nx, C);
-                        const int o = (iw - row0_of(ow, nx, C)) * ny + j;
-                        const double* po = cluster.map_shared_rank(Po, ow);
-                        const double* rr_ = cluster.map_shared_rank(R, ow);
-                        const double* di = cluster.map_shared_rank(DI, ow);
-                        tW = mdx2 * PNEW(po, rr_, di, o);
-                    }
+                    const double* g = (li > 0) ? (X + c - ny) : (baseW + j);
+                    tW = mdx2 * (first ? g[6 * cap] : g[po] * beta + g[6 * cap]);
                 }
                 if (nb & 8) {
-                    const int ie = (i == nx - 1) ? 0 : i + 1;
-                    if (ie >= r0 && ie < r1) {
-                        const int o = (ie - r0) * ny + j;
-                        tE = mdx2 * PNEW(Po, R, DI, o);
-                    } else {
-                        const int oe = owner_of(ie, nx, C);
-                        const int o = (ie - row0_of(oe, nx, C)) * ny + j;
-                        const double* po = cluster.map_shared_rank(Po, oe);
-                        const double* rr_ = cluster.map_shared_rank(R, oe);
-                        const double* di = cluster.map_shared_rank(DI, oe);
-                        tE = mdx2 * PNEW(po, rr_, di, o);
-                    }
+                    const double* g = (li < rows - 1) ? (X + c + ny) : (baseE + j);
+                    tE = mdx2 * (first ? g[6 * cap] : g[po] * beta + g[6 * cap]);
                 }
-#undef PNEW
-                const double qq = row_sum(periodic, i, nx, tW, tS, DG[c] * pC, tN, tE);
+                const double qq = row_sum(periodic, r0 + li, nx, tW, tS, DG[c] * pC, tN, tE);
                 Pn[c] = pC;
                 q[k] = qq;
                 pq += pC * qq;
             }
             {
                 double v[1] = {pq};
-                cluster_sum<1>(cluster, v, red_smem, slotA, C);
+                cluster_sum<1>(cluster, v, red_smem, SLOTS(), C, me);
                 pq = v[0];
             }
             const double alpha = rho / pq;
@@ -282,10 +291,12 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cluster(PcgLaunch L) {
                 X[c] = X[c] + alpha * Pn[c];
                 const double r = R[c] - alpha * q[k];
                 R[c] = r;
+                const double z = DI[c] * r;
+                Z[c] = z;
                 v2[0] += r * r;
-                v2[1] += r * (DI[c] * r);
+                v2[1] += r * z;
             }
-            cluster_sum<2>(cluster, v2, red_smem, slotB, C);
+            cluster_sum<2>(cluster, v2, red_smem, SLOTS(), C, me);
             rr = v2[0];
             beta = v2[1] / rho;
             rho = v2[1];
@@ -294,44 +305,34 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cluster(PcgLaunch L) {
     }
     // ------------------------------------------------------------ epilogue
     __syncthreads();
-    double xs[CFD2D_MAX_COMPONENTS];
-#pragma unroll
-    for (int k = 0; k < CFD2D_MAX_COMPONENTS; ++k) xs[k] = 0.0;
-    for (int c = tid; c < nloc; c += kPcgThreads) {
-        const int i = r0 + c / ny, j = c % ny;
-        const int gidx = i * ny + j;
-        const double x = X[c];
-        op.x0[gidx] = x;
-        if (ncomp > 0 && (NB[c] & 0x80)) {
-            const int lab = op.label[gidx];
-#pragma unroll
-            for (int k = 0; k < CFD2D_MAX_COMPONENTS; ++k)
-                if (k == lab) xs[k] += x;
-        }
+    for (int c = tid; c < nloc; c += kPcgThreads) op.x0[goff + c] = X[c];
+    for (int k = 0; k < ncomp; ++k) {
+        double v[1] = {0.0};
+        for (int c = tid; c < nloc; c += kPcgThreads)
+            if ((NB[c] & 0x80) && op.label[goff + c] == k) v[0] += X[c];
+        cluster_sum<1>(cluster, v, red_smem, SLOTS(), C, me);
+        if (tid == 0) cmean[k] = v[0] / op.comp_count[k];
     }
-    if (ncomp > 0) cluster_sum<CFD2D_MAX_COMPONENTS>(cluster, xs, red_smem, slotA, C);
+    __syncthreads();
     const int pp = ny + 2;
     for (int c = tid; c < nloc; c += kPcgThreads) {
-        const int i = r0 + c / ny, j = c % ny;
-        const int gidx = i * ny + j;
+        const int li = (int)__umulhi((unsigned)c, magic);
+        const int j = c - li * ny;
+        const int i = r0 + li;
         double pv = 0.0;
         if (NB[c] & 0x80) {
             pv = X[c];
-            const int lab = op.label[gidx];
-            if (lab >= 0) {
-                double mean = 0.0;
-#pragma unroll
-                for (int k = 0; k < CFD2D_MAX_COMPONENTS; ++k)
-                    if (k == lab) mean = xs[k] / op.comp_count[k];
-                pv = pv - mean;
+            if (ncomp > 0) {
+                const int lab = op.label[goff + c];
+                if (lab >= 0) pv = pv - cmean[lab];
             }
         }
         if (!L.p_padded) {
-            L.p_out[gidx] = pv;
+            L.p_out[goff + c] = pv;
         } else {
             L.p_out[(i + 1) * pp + j + 1] = pv;
             // periodic ghost rows: p[0,:] = p[nx,:], p[nx+1,:] = p[1,:]
-            if (periodic && i == nx - 1) L.p_out[0 * pp + j + 1] = pv;
+            if (periodic && i == nx - 1) L.p_out[j + 1] = pv;
             if (periodic && i == 0) L.p_out[(nx + 1) * pp + j + 1] = pv;
         }
     }
@@ -342,14 +343,12 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cluster(PcgLaunch L) {
             L.p_out[(i + 1) * pp + ny + 1] = 0.0;
         }
         if (me == 0) {
-            for (int j = tid; j < pp; j += kPcgThreads) {
+            for (int j = tid; j < pp; j += kPcgThreads)
                 if (!periodic || j == 0 || j == ny + 1) L.p_out[j] = 0.0;
-            }
         }
         if (me == C - 1) {
-            for (int j = tid; j < pp; j += kPcgThreads) {
+            for (int j = tid; j < pp; j += kPcgThreads)
                 if (!periodic || j == 0 || j == ny + 1) L.p_out[(nx + 1) * pp + j] = 0.0;
-            }
         }
     }
     if (me == 0 && tid == 0) {
@@ -359,12 +358,348 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cluster(PcgLaunch L) {
     }
     // keep every CTA's shared memory alive until all remote readers are done
     cluster.sync();
+#undef SLOTS
+}
+
+// ---------------------------------------------------------------- grid-persistent variant
+// For grids beyond the on-chip capacity of one cluster: a cooperative launch of
+// G co-resident CTAs over all SMs, vectors in global memory (the workspace),
+// the same iteration form and operation order. CTA b owns a contiguous range of
+// cells. p_new of a cell's neighbours is recomputed from r, p_old and 1/diag
+// (as in the cluster kernel), and q = A p_new is recomputed in the update phase
+// from the stored p_new instead of being kept, so the kernel holds no per-cell
+// registers and runs at any size. Inter-CTA ordering uses a sense-counting grid
+// barrier whose waits are bounded: a wait that gives up sets
+// CFD2D_S_BARRIER_TIMEOUT and the kernel returns without further barriers.
+namespace {
+
+constexpr int kGridThreads = 256;
+
+struct GridWork {
+    double* R;
+    double* P0;
+    double* P1;
+    double* partA;
+    double* partB;
+    double* partC;
+    unsigned int* bar;  // [0] arrival count, [1] generation
+};
+
+__device__ __forceinline__ GridWork grid_work(double* w, int n, int G) {
+    GridWork W;
+    W.R = w;
+    W.P0 = w + n;
+    W.P1 = w + 2 * (size_t)n;
+    W.partA = w + 3 * (size_t)n;
+    W.partB = W.partA + (size_t)G * kSlot;
+    W.partC = W.partB + (size_t)G * kSlot;
+    W.bar = reinterpret_cast<unsigned int*>(W.partC + (size_t)G * kSlot);
+    return W;
+}
+
+__device__ __forceinline__ unsigned int ld_acquire_gpu(const unsigned int* p) {
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ bool grid_barrier(unsigned int* bar, int* status) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ok = 1;
+        unsigned int* gen = bar + 1;
+        const unsigned int g0 = ld_acquire_gpu(gen);
+        __threadfence();
+        const unsigned int arrived = atomicAdd(bar, 1u) + 1u;
+        if (arrived == gridDim.x) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(gen, 1u);
+        } else {
+            long long spins = 0;
+            while (ld_acquire_gpu(gen) == g0) {
+                if (++spins > (1LL << 25)) {
+                    if (status) atomicOr(status, CFD2D_S_BARRIER_TIMEOUT);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+// grid-wide sum of K values: block tree, partials to part[b*kSlot + k], barrier,
+// then every warp adds the G partials in the same fixed order.
+template <int K>
+__device__ __forceinline__ bool grid_sum(double (&v)[K], double* red_smem, double* part,
+                                         unsigned int* bar, int* status) {
+    block_sum<K>(v, red_smem);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) part[(size_t)blockIdx.x * kSlot + k] = v[k];
+    }
+    if (!grid_barrier(bar, status)) return false;
+    const int lane = threadIdx.x & 31;
+    const int G = gridDim.x;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        double x = 0.0;
+        for (int b = lane; b < G; b += 32) x += __ldcg(&part[(size_t)b * kSlot + k]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        v[k] = x;
+    }
+    return true;
+}
+
+// A x at cell (i, j) from a global vector (csc_matvec order)
+__device__ __forceinline__ double apply_A(const cfd2d_poisson& op, const double* X, int i, int j,
+                                          uint8_t nb, double dg) {
+    const int nx = op.nx, ny = op.ny;
+    const int c = i * ny + j;
+    double tW = 0.0, tS = 0.0, tN = 0.0, tE = 0.0;
+    if (nb & 2) tS = -op.dy2 * X[c - 1];
+    if (nb & 4) tN = -op.dy2 * X[c + 1];
+    if (nb & 1) tW = -op.dx2 * X[((i == 0) ? nx - 1 : i - 1) * ny + j];
+    if (nb & 8) tE = -op.dx2 * X[((i == nx - 1) ? 0 : i + 1) * ny + j];
+    return row_sum(op.periodic != 0, i, nx, tW, tS, dg * X[c], tN, tE);
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kGridThreads) k_pcg_grid(PcgLaunch L) {
+    if (L.active && *L.active == 0) return;
+    const cfd2d_poisson& op = L.op;
+    const int nx = op.nx, ny = op.ny;
+    const int n = nx * ny;
+    const int G = gridDim.x;
+    const int chunk = (n + G - 1) / G;
+    const int c0 = blockIdx.x * chunk;
+    const int c1 = min(n, c0 + chunk);
+    GridWork W = grid_work(op.work, n, G);
+    double* X = op.x0;
+    double* R = W.R;
+    const int tid = threadIdx.x;
+    const double mdx2 = -op.dx2, mdy2 = -op.dy2;
+    __shared__ double red_smem[32 * kSlot];
+    int* status = L.status_out;
+
+    double dt = 1.0;
+    if (L.rhs_mode == 1) dt = L.dt_ptr ? *L.dt_ptr : L.dt_const;
+    double csum[CFD2D_MAX_COMPONENTS + 1];
+#pragma unroll
+    for (int k = 0; k <= CFD2D_MAX_COMPONENTS; ++k) csum[k] = 0.0;
+    for (int c = c0 + tid; c < c1; c += kGridThreads) {
+        const uint8_t nb = op.nbr[c];
+        double braw = 0.0;
+        if (nb & 0x80) {
+            const int i = c / ny, j = c % ny;
+            if (L.rhs_mode == 0) {
+                braw = L.rhs[c];
+            } else {
+                const int pu = ny + 2, pv = ny + 1;
+                const int ig = i + 1, jg = j + 1;
+                const double div = (L.F[ig * pu + jg] - L.F[(ig - 1) * pu + jg]) / L.dx +
+                                   (L.G[ig * pv + jg] - L.G[ig * pv + jg - 1]) / L.dy;
+                braw = div / dt;
+            }
+            const int lab = op.label[c];
+#pragma unroll
+            for (int k = 0; k < CFD2D_MAX_COMPONENTS; ++k)
+                if (k == lab) csum[k] += braw;
+            if (X[c] != 0.0) csum[CFD2D_MAX_COMPONENTS] += 1.0;
+        }
+        R[c] = braw;
+    }
+    if (!grid_sum<CFD2D_MAX_COMPONENTS + 1>(csum, red_smem, W.partA, W.bar, status)) return;
+    const bool x_any = csum[CFD2D_MAX_COMPONENTS] > 0.0;
+    double part[3] = {0.0, 0.0, 0.0};
+    for (int c = c0 + tid; c < c1; c += kGridThreads) {
+        const uint8_t nb = op.nbr[c];
+        if (!(nb & 0x80)) { W.P1[c] = 0.0; W.P0[c] = 0.0; R[c] = 0.0; continue; }
+        const int i = c / ny, j = c % ny;
+        double b = R[c];
+        const int lab = op.label[c];
+        if (lab >= 0) {
+            double mean = 0.0;
+#pragma unroll
+            for (int k = 0; k < CFD2D_MAX_COMPONENTS; ++k)
+                if (k == lab) mean = csum[k] / op.comp_count[k];
+            b = b - mean;
+        }
+        b = -b;
+        W.P1[c] = b;
+        double r = b;
+        if (x_any) r = b - apply_A(op, X, i, j, nb, op.diag[c]);
+        R[c] = r;
+        W.P0[c] = 0.0;
+        part[0] += b * b;
+        part[1] += r * r;
+        part[2] += r * (op.dinv[c] * r);
+    }
+    if (!grid_sum<3>(part, red_smem, W.partB, W.bar, status)) return;
+    const double bnrm2 = sqrt(part[0]);
+    double rr = part[1];
+    double rho = part[2];
+    const double atol = L.rtol * bnrm2;
+    int it = 0;
+    bool converged = false;
+    if (bnrm2 == 0.0) {
+        for (int c = c0 + tid; c < c1; c += kGridThreads) X[c] = W.P1[c];
+        converged = true;
+    } else {
+        double beta = 0.0;
+        int cur = 0;
+        for (it = 0; it < L.maxiter; ++it) {
+            if (sqrt(rr) < atol) { converged = true; break; }
+            double* Pn = cur ? W.P1 : W.P0;
+            const double* Po = cur ? W.P0 : W.P1;
+            const bool first = (it == 0);
+            double pq = 0.0;
+            for (int c = c0 + tid; c < c1; c += kGridThreads) {
+                const uint8_t nb = op.nbr[c];
+                if (!(nb & 0x80)) continue;
+                const int i = c / ny, j = c % ny;
+#define PNEWG(idx) (first ? (op.dinv[idx] * R[idx]) : (Po[idx] * beta + op.dinv[idx] * R[idx]))
+                const double pC = PNEWG(c);
+                double tW = 0.0, tS = 0.0, tN = 0.0, tE = 0.0;
+                if (nb & 2) tS = mdy2 * PNEWG(c - 1);
+                if (nb & 4) tN = mdy2 * PNEWG(c + 1);
+                if (nb & 1) { const int o = ((i == 0) ? nx - 1 : i - 1) * ny + j; tW = mdx2 * PNEWG(o); }
+                if (nb & 8) { const int o = ((i == nx - 1) ? 0 : i + 1) * ny + j; tE = mdx2 * PNEWG(o); }
+#undef PNEWG
+                const double qq = row_sum(op.periodic != 0, i, nx, tW, tS, op.diag[c] * pC, tN, tE);
+                Pn[c] = pC;
+                pq += pC * qq;
+            }
+            {
+                double v[1] = {pq};
+                if (!grid_sum<1>(v, red_smem, W.partA, W.bar, status)) return;
+                pq = v[0];
+            }
+            const double alpha = rho / pq;
+            double v2[2] = {0.0, 0.0};
+            for (int c = c0 + tid; c < c1; c += kGridThreads) {
+                const uint8_t nb = op.nbr[c];
+                if (!(nb & 0x80)) continue;
+                const int i = c / ny, j = c % ny;
+                const double qq = apply_A(op, Pn, i, j, nb, op.diag[c]);
+                X[c] = X[c] + alpha * Pn[c];
+                const double r = R[c] - alpha * qq;
+                R[c] = r;
+                v2[0] += r * r;
+                v2[1] += r * (op.dinv[c] * r);
+            }
+            if (!grid_sum<2>(v2, red_smem, W.partB, W.bar, status)) return;
+            rr = v2[0];
+            beta = v2[1] / rho;
+            rho = v2[1];
+            cur ^= 1;
+        }
+    }
+    double xs[CFD2D_MAX_COMPONENTS];
+#pragma unroll
+    for (int k = 0; k < CFD2D_MAX_COMPONENTS; ++k) xs[k] = 0.0;
+    if (op.ncomp > 0) {
+        for (int c = c0 + tid; c < c1; c += kGridThreads) {
+            if (!(op.nbr[c] & 0x80)) continue;
+            const int lab = op.label[c];
+#pragma unroll
+            for (int k = 0; k < CFD2D_MAX_COMPONENTS; ++k)
+                if (k == lab) xs[k] += X[c];
+        }
+        if (!grid_sum<CFD2D_MAX_COMPONENTS>(xs, red_smem, W.partC, W.bar, status)) return;
+    }
+    const int pp = ny + 2;
+    for (int c = c0 + tid; c < c1; c += kGridThreads) {
+        const int i = c / ny, j = c % ny;
+        double pv = 0.0;
+        if (op.nbr[c] & 0x80) {
+            pv = X[c];
+            const int lab = op.label[c];
+            if (lab >= 0) {
+                double mean = 0.0;
+#pragma unroll
+                for (int k = 0; k < CFD2D_MAX_COMPONENTS; ++k)
+                    if (k == lab) mean = xs[k] / op.comp_count[k];
+                pv = pv - mean;
+            }
+        }
+        if (!L.p_padded) {
+            L.p_out[c] = pv;
+        } else {
+            L.p_out[(i + 1) * pp + j + 1] = pv;
+            if (op.periodic && i == nx - 1) L.p_out[j + 1] = pv;
+            if (op.periodic && i == 0) L.p_out[(nx + 1) * pp + j + 1] = pv;
+            if (j == 0) L.p_out[(i + 1) * pp] = 0.0;
+            if (j == ny - 1) L.p_out[(i + 1) * pp + ny + 1] = 0.0;
+        }
+    }
+    if (L.p_padded && blockIdx.x == 0) {
+        for (int j = tid; j < pp; j += kGridThreads) {
+            if (!op.periodic || j == 0 || j == ny + 1) {
+                L.p_out[j] = 0.0;
+                L.p_out[(nx + 1) * pp + j] = 0.0;
+            }
+        }
+    }
+    if (blockIdx.x == 0 && tid == 0) {
+        if (L.iters_out) *L.iters_out = it;
+        if (L.iters_out2) *L.iters_out2 = it;
+        if (L.status_out && !converged) atomicOr(L.status_out, CFD2D_S_CG_MAXITER);
+    }
+}
+
+namespace {
+
+int grid_blocks_for(int n) {
+    static int per_sm = -1, sms = 0;
+    if (per_sm < 0) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_grid, kGridThreads, 0) != cudaSuccess)
+            return 0;
+    }
+    long long g = (long long)per_sm * sms;
+    const long long need = (n + kGridThreads - 1) / kGridThreads;
+    if (g > need) g = need;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
+}  // namespace
+
+size_t pcg_grid_workspace_doubles(int nx, int ny) {
+    // R, P0, P1 + three partial arrays for up to 148 * 32 CTAs + barrier words
+    return (size_t)3 * nx * ny + (size_t)3 * 148 * 32 * kSlot + 8;
+}
+
+cudaError_t pcg_grid_launch(const PcgLaunch& L, cudaStream_t s) {
+    const int n = L.op.nx * L.op.ny;
+    const int G = grid_blocks_for(n);
+    if (G < 1 || G > 148 * 32) return cudaErrorInvalidConfiguration;
+    if (L.op.work == nullptr || L.op.work_bytes < pcg_grid_workspace_doubles(L.op.nx, L.op.ny) * sizeof(double))
+        return cudaErrorInvalidValue;
+    PcgLaunch Lc = L;
+    // the barrier words start from zero on every launch, whatever an earlier
+    // launch that gave up on a wait left behind
+    const size_t n3 = (size_t)3 * n + (size_t)3 * G * kSlot;
+    cudaError_t e = cudaMemsetAsync(L.op.work + n3, 0, 2 * sizeof(unsigned int), s);
+    if (e != cudaSuccess) return e;
+    void* args[] = {&Lc};
+    return cudaLaunchCooperativeKernel((const void*)k_pcg_grid, dim3(G), dim3(kGridThreads), args, 0, s);
 }
 
 // ---------------------------------------------------------------- launch
 namespace {
 
-size_t smem_bytes(int cap) { return (size_t)cap * (6 * sizeof(double) + 1) + 16; }
+size_t smem_bytes(int cap) { return (size_t)cap * (kArrays * sizeof(double) + 1) + 16; }
 
 // Kernel attributes are set once per instantiation, outside any stream capture
 // (cfd2d_pcg_plan runs before the first launch): the maximum dynamic shared
@@ -378,7 +713,7 @@ cudaError_t configure_cpt() {
     if (e != cudaSuccess) return e;
     e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     if (e != cudaSuccess) return e;
-    const int dyn = optin - (int)((32 * kSlot + 2 * kSlot) * sizeof(double)) - 1024;
+    const int dyn = optin - (int)((32 * kMaxK + 2 * 16 * kMaxK + CFD2D_MAX_COMPONENTS) * sizeof(double)) - 1024;
     e = cudaFuncSetAttribute(k_pcg_cluster<CPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_pcg_cluster<CPT>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
@@ -421,7 +756,7 @@ int cpt_for(int cap) {
 
 // Max cells one CTA can hold for a given dynamic shared-memory budget.
 int pcg_cluster_capacity(size_t smem_limit) {
-    return (int)((smem_limit - 16) / (6 * sizeof(double) + 1));
+    return (int)((smem_limit - 16) / (kArrays * sizeof(double) + 1));
 }
 
 // Pick the cluster size for an nx x ny grid: smallest C (power of two, <= 16)
@@ -433,7 +768,7 @@ int pcg_cluster_plan(int nx, int ny) {
     if (cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
         return 0;
     // leave room for the static shared arrays of the kernel
-    const size_t budget = (size_t)smem_optin - (32 * kSlot + 2 * kSlot) * sizeof(double) - 1024;
+    const size_t budget = (size_t)smem_optin - (32 * kMaxK + 2 * 16 * kMaxK + CFD2D_MAX_COMPONENTS) * sizeof(double) - 1024;
     const int capmax = pcg_cluster_capacity(budget);
     // target ~ 2-4 cells per thread before growing the cluster: fewer CTAs mean
     // cheaper barriers, and on-chip state is the point
@@ -480,6 +815,7 @@ int pcg_cluster_plan(int nx, int ny) {
 cudaError_t pcg_launch(const PcgLaunch& L0, cudaStream_t s) {
     PcgLaunch L = L0;
     const int C = L.op.cluster;
+    if (C == 0) return pcg_grid_launch(L, s);
     if (C < 1 || C > 16) return cudaErrorInvalidValue;
     const int rows = (L.op.nx + C - 1) / C;
     L.cap_cells = rows * L.op.ny;

@@ -29,6 +29,7 @@ struct PcgLaunch {
 };
 
 int pcg_cluster_plan(int nx, int ny);
+size_t pcg_grid_workspace_doubles(int nx, int ny);
 cudaError_t pcg_launch(const PcgLaunch& L, cudaStream_t s);
 
 }  // namespace cfd

@@ -251,3 +251,55 @@ def test_misc_runs(pkg):
     assert case.sim.n == int(g["run_n"])
     assert case.sim.t == pytest.approx(float(g["run_t"]), rel=1e-14)
     assert rel(case.sim.u, g["run_u"]) < TOL
+
+
+# ---------------------------------------------------------------- grid-persistent solver
+@pytest.mark.parametrize("name", ["cav", "cyl", "per", "two"])
+def test_pressure_solve_grid_variant(pkg, name, monkeypatch):
+    """The grid-persistent CG (used beyond on-chip capacity) on the same fixtures."""
+    monkeypatch.setenv("CFD2D_PCG_VARIANT", "grid")
+    g = golden("golden_pressure")
+    sim = _pressure_sim(pkg, name)
+    ps = sim.pressure
+    assert ps.cluster == 0
+    ps.tol = 1e-10
+    for key in ("", "2"):
+        p = ps.solve(g[name + "_rhs" + key])
+        its = int(g[name + "_its" + key])
+        assert abs(ps.last_iterations - its) <= max(2, its // 20), (ps.last_iterations, its)
+        assert rel(p, g[name + "_p" + key]) < 1e-7
+
+
+def test_large_grid_uses_grid_variant_and_matches_oracle(pkg):
+    """A grid beyond one cluster's shared memory: solve against the oracle's CG."""
+    import oracle as O
+
+    _, cases, _, _ = pkg
+    obst = [{"typ": "kreis", "x": 0.5, "y": 0.5, "r": 0.1}]
+    case = cases.custom_obstacles(obst, lx=2.0, ly=1.0, nx=512, ny=256, re=200.0, pressure_solver="cg")
+    ps = case.sim.pressure
+    assert ps.cluster == 0
+    ref = O.custom_obstacles(obst, lx=2.0, ly=1.0, nx=512, ny=256, re=200.0, tol=None)
+    rng = np.random.default_rng(3)
+    rhs = rng.standard_normal((512, 256))
+    ps.tol = 1e-9
+    ref.pressure.tol = 1e-9
+    ps._x0 = ref.pressure.x0
+    p = ps.solve(rhs)
+    pr = ref.pressure.solve(rhs)
+    assert rel(p, pr) < 1e-7
+    assert abs(ps.last_iterations - ref.pressure.last_iterations) <= max(3, ref.pressure.last_iterations // 20)
+
+
+def test_cavity_step_with_grid_variant(pkg, monkeypatch):
+    """Whole steps with the grid-persistent solver agree with the golden run."""
+    monkeypatch.setenv("CFD2D_PCG_VARIANT", "grid")
+    _, cases, _, _ = pkg
+    g = golden("golden_cavity64")
+    case = cases.lid_driven_cavity(re=100, n=64, scheme="ab2", gamma=0.1, tau=0.5, pressure_solver="cg")
+    sim = case.sim
+    assert sim.pressure.cluster == 0
+    sim.pressure.tol = 1e-8
+    sim.advance(200)
+    for f in "uvp":
+        assert rel(getattr(sim, f), g[f"cav_{f}_200"]) < TOL, f
