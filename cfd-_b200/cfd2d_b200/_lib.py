@@ -93,6 +93,11 @@ class Sim(C.Structure):
     ]
 
 
+class FcgScalars(C.Structure):
+    _fields_ = [("alpha", C.c_double), ("beta", C.c_double), ("rz", C.c_double), ("pq", C.c_double),
+                ("rr", C.c_double), ("bb", C.c_double), ("iters", C.c_int32), ("ticket", C.c_uint32)]
+
+
 _LIB = None
 
 
@@ -136,6 +141,31 @@ def lib():
         "cfd2d_events_create": ([i, vp], i),
         "cfd2d_events_destroy": ([i, vp], i),
         "cfd2d_event_elapsed_ms": ([vp, vp, C.POINTER(C.c_float)], i),
+        "cfd2d_sim_step_begin": ([vp, vp], i),
+        "cfd2d_sim_step_finish": ([vp, vp], i),
+        "cfd2d_poisson_matvec": ([vp, vp, vp, vp], i),
+        "cfd2d_pressure_solve_snapshots": ([vp, vp, vp, d, i, vp, i, i, vp, vp, vp], i),
+        "cfd2d_lpc_w32_bytes": ([], sz),
+        "cfd2d_lpc_pack_w32": ([vp, vp, vp], i),
+        "cfd2d_lpc_conv32": ([vp, vp, vp, vp, vp, vp, i, i, i, vp, vp], i),
+        "cfd2d_lpc_conv": ([i, i, vp, i, vp, vp, vp, vp, i, i, i, i, i, vp], i),
+        "cfd2d_lpc_pool2": ([vp, vp, i, i, vp], i),
+        "cfd2d_lpc_pool_mask": ([vp, vp, i, i, vp], i),
+        "cfd2d_lpc_upadd": ([vp, vp, vp, i, i, vp], i),
+        "cfd2d_lpc_relu_bwd": ([vp, vp, vp, vp, i, i, i, vp], i),
+        "cfd2d_lpc_upadd_bwd": ([vp, vp, i, i, vp], i),
+        "cfd2d_lpc_pool_bwd": ([vp, vp, i, i, vp], i),
+        "cfd2d_lpc_conv_dw_partial_floats": ([i, i, i, i, i], sz),
+        "cfd2d_lpc_conv_dw": ([i, i, vp, i, vp, i, i, i, vp, vp, vp], i),
+        "cfd2d_fcg_partial_doubles": ([i], sz),
+        "cfd2d_fcg_init": ([vp, vp, vp, vp, d, d, vp, vp, vp, vp, vp, vp, vp], i),
+        "cfd2d_fcg_pq": ([vp, vp, vp, vp, vp, vp], i),
+        "cfd2d_fcg_update": ([i, vp, vp, vp, vp, vp, vp, vp, vp], i),
+        "cfd2d_fcg_zr": ([i, vp, vp, vp, i, vp, vp, vp], i),
+        "cfd2d_fcg_dir": ([i, vp, vp, vp, vp], i),
+        "cfd2d_fcg_net_in": ([i, vp, vp, vp, vp, vp], i),
+        "cfd2d_fcg_net_out": ([i, vp, vp, vp, vp, vp, d, vp, vp], i),
+        "cfd2d_fcg_scatter_p": ([vp, vp, vp, vp], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -155,7 +185,12 @@ def exported_symbols():
         "cfd2d_sim_step", "cfd2d_sim_scalar_fill_ghosts", "cfd2d_sim_sst_pre_momentum",
         "cfd2d_graph_capture_steps", "cfd2d_graph_launch", "cfd2d_graph_destroy",
         "cfd2d_graph_capture_steps_ex", "cfd2d_events_create", "cfd2d_events_destroy",
-        "cfd2d_event_elapsed_ms",
+        "cfd2d_event_elapsed_ms", "cfd2d_sim_step_begin", "cfd2d_sim_step_finish", "cfd2d_poisson_matvec",
+        "cfd2d_pressure_solve_snapshots", "cfd2d_lpc_w32_bytes", "cfd2d_lpc_pack_w32", "cfd2d_lpc_conv32",
+        "cfd2d_lpc_conv", "cfd2d_lpc_pool2", "cfd2d_lpc_pool_mask", "cfd2d_lpc_upadd", "cfd2d_lpc_relu_bwd",
+        "cfd2d_lpc_upadd_bwd", "cfd2d_lpc_pool_bwd", "cfd2d_lpc_conv_dw_partial_floats", "cfd2d_lpc_conv_dw",
+        "cfd2d_fcg_partial_doubles", "cfd2d_fcg_init", "cfd2d_fcg_pq", "cfd2d_fcg_update", "cfd2d_fcg_zr",
+        "cfd2d_fcg_dir", "cfd2d_fcg_net_in", "cfd2d_fcg_net_out", "cfd2d_fcg_scatter_p",
     ]
 
 

@@ -1,0 +1,531 @@
+"""Learned Poisson preconditioner inside flexible CG (no counterpart in the reference).
+
+Network (4 levels, 32 channels, 3x3 convolutions, BF16 weights and activations,
+FP32 accumulation, 65,025 parameters):
+
+    a0  = relu(conv 1->32 (r / ||r||))                      level 0 (CUDA cores)
+    a0b = relu(conv 32->32 (a0))                            level 0 (tensor cores)
+    a1  = relu(conv 32->32 (pool a0b))                      level 1
+    a2  = relu(conv 32->32 (pool a1))                       level 2
+    a3  = relu(conv 32->32 (pool a2))                       level 3
+    d2  = relu(conv 32->32 (up a3 + a2))                    level 2
+    d1  = relu(conv 32->32 (up d2 + a1))                    level 1
+    d0  = relu(conv 32->32 (up d1 + a0b))                   level 0
+    out = conv 32->1 (d0)                                   level 0 (CUDA cores)
+
+Every layer output is multiplied by the fluid mask of its level. The 32->32
+layers run on tcgen05 (``cfd2d_lpc_conv32``); the 1-channel layers, pooling,
+upsampling and the whole backward pass are hand-written CUDA-core kernels of the
+same library. Training uses these kernels through ``torch.autograd.Function``; the
+optimiser (Adam) is PyTorch's. The preconditioner applied inside flexible CG is
+M(r) = ||r|| * net(r / ||r||) + omega * D^-1 r; flexible CG (Polak-Ribiere) falls
+back to the plain Jacobi-PCG when it stalls.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import math
+import time
+
+import numpy as np
+
+from . import _lib
+
+CH = 32
+LAYERS = [  # name, cin, cout, level, relu
+    ("a0", 1, CH, 0, True), ("a0b", CH, CH, 0, True), ("a1", CH, CH, 1, True), ("a2", CH, CH, 2, True),
+    ("a3", CH, CH, 3, True), ("d2", CH, CH, 2, True), ("d1", CH, CH, 1, True), ("d0", CH, CH, 0, True),
+    ("out", CH, 1, 0, False),
+]
+NLEVELS = 4
+
+
+def _t():
+    return _lib.torch()
+
+
+def level_shapes(H, W):
+    shapes = [(H, W)]
+    for _ in range(NLEVELS - 1):
+        h, w = shapes[-1]
+        shapes.append(((h + 1) // 2, (w + 1) // 2))
+    return shapes
+
+
+class LPCNet:
+    """Weights (FP32 masters) and the packed BF16 tensor-core images of the 32->32 layers."""
+
+    def __init__(self, seed: int = 0):
+        t = _t()
+        g = t.Generator().manual_seed(seed)
+        self.w, self.b = {}, {}
+        for name, cin, cout, _lvl, relu in LAYERS:
+            fan_in = cin * 9
+            std = math.sqrt(2.0 / fan_in) if relu else math.sqrt(1.0 / fan_in) * 0.1
+            self.w[name] = (t.randn((cout, cin, 3, 3), generator=g) * std).to(_lib.device())
+            self.b[name] = t.zeros(cout, device=_lib.device())
+        self._images = {}
+        self.repack()
+
+    @property
+    def n_params(self) -> int:
+        return sum(v.numel() for v in self.w.values()) + sum(v.numel() for v in self.b.values())
+
+    def parameters(self):
+        out = []
+        for name, *_ in LAYERS:
+            out += [self.w[name], self.b[name]]
+        return out
+
+    def repack(self):
+        """BF16 weights: round the masters and pack the tensor-core images."""
+        t = _t()
+        L = _lib.lib()
+        nbytes = int(L.cfd2d_lpc_w32_bytes())
+        for name, cin, cout, _lvl, _relu in LAYERS:
+            if cin == CH and cout == CH:
+                img = self._images.get(name)
+                if img is None:
+                    img = t.zeros(nbytes // 2, dtype=t.bfloat16, device=_lib.device())
+                    self._images[name] = img
+                w = self.w[name].detach().float().contiguous()
+                _lib.check(L.cfd2d_lpc_pack_w32(_lib.ptr(w), _lib.ptr(img), _lib.stream_ptr()), "pack_w32")
+
+    def wq(self, name):
+        """The BF16-rounded weights the kernels use, as FP32 (for the CUDA-core layers)."""
+        return self.w[name].detach().to(_t().bfloat16).float().contiguous()
+
+    def state_dict(self):
+        return {f"{k}.w": v.detach().cpu() for k, v in self.w.items()} | \
+               {f"{k}.b": v.detach().cpu() for k, v in self.b.items()}
+
+    def load_state_dict(self, d):
+        for name, *_ in LAYERS:
+            self.w[name].copy_(d[f"{name}.w"].to(self.w[name].device))
+            self.b[name].copy_(d[f"{name}.b"].to(self.b[name].device))
+        self.repack()
+
+
+class Workspace:
+    """Activation buffers of one grid size (reused across applications)."""
+
+    def __init__(self, H: int, W: int, mask):
+        t = _t()
+        dev = _lib.device()
+        L = _lib.lib()
+        self.H, self.W = H, W
+        self.shapes = level_shapes(H, W)
+        self.masks = [t.zeros(s, dtype=t.uint8, device=dev) for s in self.shapes]
+        self.mask_src = None
+        self.set_mask(mask)
+        act = lambda lvl: t.zeros(self.shapes[lvl] + (CH,), dtype=t.bfloat16, device=dev)  # noqa: E731
+        self.a = {name: act(lvl) for name, cin, cout, lvl, _ in LAYERS if cout == CH}
+        self.pool = {lvl: act(lvl) for lvl in (1, 2, 3)}
+        self.up = {lvl: act(lvl) for lvl in (0, 1, 2)}
+        self.out = t.zeros((H, W), dtype=t.float32, device=dev)
+        self.err = t.zeros(1, dtype=t.int32, device=dev)
+
+
+def _ws_set_mask(self, mask):
+    """Fluid mask of level 0 (H, W) and its pooled masks (any child fluid)."""
+    t = _t()
+    L = _lib.lib()
+    m0 = mask if isinstance(mask, t.Tensor) else _lib.to_dev(np.asarray(mask, dtype=np.uint8))
+    self.masks[0].copy_(m0.reshape(self.H, self.W).to(t.uint8))
+    for lvl in range(1, NLEVELS):
+        h, w = self.shapes[lvl - 1]
+        _lib.check(L.cfd2d_lpc_pool_mask(_lib.ptr(self.masks[lvl - 1]), _lib.ptr(self.masks[lvl]), h, w,
+                                         _lib.stream_ptr()), "pool_mask")
+    self.mask_src = mask
+
+
+Workspace.set_mask = _ws_set_mask
+
+
+def net_forward(net: LPCNet, ws: Workspace, x_in):
+    """out = net(x_in) on the device (x_in: FP32 (H, W)); activations stay in ``ws``."""
+    L = _lib.lib()
+    s = _lib.stream_ptr()
+    P = _lib.ptr
+    sh = ws.shapes
+
+    def conv32(name, src, lvl, skip=None):
+        h, w = sh[lvl]
+        rc = L.cfd2d_lpc_conv32(P(src), P(net._images[name]), P(net.b[name]), P(skip), P(ws.masks[lvl]),
+                                P(ws.a[name]), h, w, 1, P(ws.err), s)
+        _lib.check(rc, "lpc_conv32")
+
+    H, W = sh[0]
+    _lib.check(L.cfd2d_lpc_conv(1, CH, P(x_in), 0, P(net.wq("a0")), P(net.b["a0"]), P(ws.masks[0]), P(ws.a["a0"]),
+                                1, H, W, 1, 0, s), "lpc_conv a0")
+    conv32("a0b", ws.a["a0"], 0)
+    prev = ws.a["a0b"]
+    for lvl, name in ((1, "a1"), (2, "a2"), (3, "a3")):
+        h, w = sh[lvl - 1]
+        _lib.check(L.cfd2d_lpc_pool2(P(prev), P(ws.pool[lvl]), h, w, s), "pool2")
+        conv32(name, ws.pool[lvl], lvl)
+        prev = ws.a[name]
+    for lvl, name, skip in ((2, "d2", "a2"), (1, "d1", "a1"), (0, "d0", "a0b")):
+        h, w = sh[lvl]
+        _lib.check(L.cfd2d_lpc_upadd(P(prev), P(ws.a[skip]), P(ws.up[lvl]), h, w, s), "upadd")
+        conv32(name, ws.up[lvl], lvl)
+        prev = ws.a[name]
+    _lib.check(L.cfd2d_lpc_conv(CH, 1, P(prev), 1, P(net.wq("out")), P(net.b["out"]), P(ws.masks[0]), P(ws.out),
+                                0, H, W, 0, 0, s), "lpc_conv out")
+    return ws.out
+
+
+def net_backward(net: LPCNet, ws: Workspace, x_in, dout):
+    """Gradients of sum(out * dout) w.r.t. every weight and bias (FP32), from the
+    activations left in ``ws`` by net_forward(x_in)."""
+    t = _t()
+    L = _lib.lib()
+    s = _lib.stream_ptr()
+    P = _lib.ptr
+    sh = ws.shapes
+    dev = _lib.device()
+    grads = {}
+
+    def zeros(lvl, ch=CH):
+        return t.zeros(sh[lvl] + (ch,), dtype=t.float32, device=dev)
+
+    def dw(name, cin, cout, x, xbf, g, lvl):
+        h, w = sh[lvl]
+        ppb = 256
+        part = t.empty(int(L.cfd2d_lpc_conv_dw_partial_floats(cin, cout, h, w, ppb)), dtype=t.float32, device=dev)
+        out = t.empty(cout * cin * 9 + cout, dtype=t.float32, device=dev)
+        _lib.check(L.cfd2d_lpc_conv_dw(cin, cout, P(x), xbf, P(g), h, w, ppb, P(part), P(out), s), "conv_dw")
+        grads[name] = (out[:cout * cin * 9].view(cout, cin, 3, 3), out[cout * cin * 9:])
+
+    def relu_g(dy, y, lvl, relu=True, ch=CH):
+        h, w = sh[lvl]
+        g = t.empty_like(dy)
+        _lib.check(L.cfd2d_lpc_relu_bwd(P(dy), P(y), P(ws.masks[lvl]), P(g), h * w, ch, int(relu), s), "relu_bwd")
+        return g
+
+    def conv_t(name, cin_f, cout_f, g, lvl):
+        # data gradient of a forward layer (cin_f -> cout_f): adjoint conv of g (cout_f channels)
+        h, w = sh[lvl]
+        dx = zeros(lvl, cin_f)
+        _lib.check(L.cfd2d_lpc_conv(cout_f, cin_f, P(g), 0, P(net.wq(name)), None, None, P(dx), 0, h, w, 0, 1, s),
+                   "conv transposed")
+        return dx
+
+    H, W = sh[0]
+    g = relu_g(dout.contiguous(), None, 0, relu=False, ch=1)
+    dw("out", CH, 1, ws.a["d0"], 1, g, 0)
+    dd = conv_t("out", CH, 1, g, 0)
+    skip_grad = {}
+    for lvl, name, skip, inp in ((0, "d0", "a0b", ws.up[0]), (1, "d1", "a1", ws.up[1]), (2, "d2", "a2", ws.up[2])):
+        g = relu_g(dd, ws.a[name], lvl)
+        dw(name, CH, CH, inp, 1, g, lvl)
+        du = conv_t(name, CH, CH, g, lvl)
+        skip_grad[skip] = du
+        h, w = sh[lvl]
+        dc = zeros(lvl + 1)
+        _lib.check(L.cfd2d_lpc_upadd_bwd(P(du), P(dc), h, w, s), "upadd_bwd")
+        dd = dc
+    # encoder, deepest first: da3 = dd
+    da = dd
+    for lvl, name in ((3, "a3"), (2, "a2"), (1, "a1")):
+        g = relu_g(da, ws.a[name], lvl)
+        dw(name, CH, CH, ws.pool[lvl], 1, g, lvl)
+        dp = conv_t(name, CH, CH, g, lvl)
+        below = {3: "a2", 2: "a1", 1: "a0b"}[lvl]
+        nxt = skip_grad[below].clone()
+        h, w = sh[lvl - 1]
+        _lib.check(L.cfd2d_lpc_pool_bwd(P(dp), P(nxt), h, w, s), "pool_bwd")
+        da = nxt
+    g = relu_g(da, ws.a["a0b"], 0)
+    dw("a0b", CH, CH, ws.a["a0"], 1, g, 0)
+    da0 = conv_t("a0b", CH, CH, g, 0)
+    g = relu_g(da0, ws.a["a0"], 0)
+    dw("a0", 1, CH, x_in.contiguous(), 0, g, 0)
+    return grads
+
+
+def torch_reference_forward(net: LPCNet, x_in, masks):
+    """The same network in PyTorch (CPU, FP32 on BF16-rounded weights and activations):
+    the checker of the CUDA kernels and their gradients."""
+    t = _t()
+    F = t.nn.functional
+
+    def bf(a):
+        return a.to(t.bfloat16).float()
+
+    def conv(name, a, relu, lvl, round_out=True):
+        y = F.conv2d(a, net.wq(name).cpu(), net.b[name].detach().cpu(), padding=1)
+        if relu:
+            y = t.relu(y)
+        y = y * masks[lvl]
+        return bf(y) if round_out else y
+
+    def pool(a):
+        # mean over the in-range children of each coarse cell
+        h, w = a.shape[-2:]
+        ap = F.pad(a, (0, w % 2, 0, h % 2))
+        cnt = F.avg_pool2d(F.pad(t.ones((1, 1, h, w)), (0, w % 2, 0, h % 2)), 2) * 4
+        return bf(F.avg_pool2d(ap, 2) * 4 / cnt)
+
+    def up(a, skip):
+        h, w = skip.shape[-2:]
+        u = a.repeat_interleave(2, -2).repeat_interleave(2, -1)[..., :h, :w]
+        return bf(u + skip)
+
+    x = x_in.cpu().float()[None, None]
+    a0 = conv("a0", x, True, 0)
+    a0b = conv("a0b", a0, True, 0)
+    a1 = conv("a1", pool(a0b), True, 1)
+    a2 = conv("a2", pool(a1), True, 2)
+    a3 = conv("a3", pool(a2), True, 3)
+    d2 = conv("d2", up(a3, a2), True, 2)
+    d1 = conv("d1", up(d2, a1), True, 1)
+    d0 = conv("d0", up(d1, a0b), True, 0)
+    return conv("out", d0, False, 0, round_out=False)[0, 0]
+
+
+# ------------------------------------------------------------------ flexible CG
+class LearnedPCG:
+    """Flexible CG with the learned preconditioner for one PressureSolver's operator.
+
+    solve(rhs) mirrors PressureSolver.solve on domains with an outflow (Dirichlet)
+    boundary: same operator, warm start, stop test ||r|| < tol ||b||. If the
+    residual fails to fall by ``stall_factor`` over ``stall_window`` iterations,
+    the solve continues with the plain Jacobi-PCG from the current iterate.
+    """
+
+    def __init__(self, pressure, net: LPCNet, omega: float = 0.6, stall_window: int = 20,
+                 stall_factor: float = 0.5, maxiter: int = 2000):
+        t = _t()
+        if pressure.neumann_components:
+            raise ValueError("the learned preconditioner path needs an outflow (Dirichlet) boundary")
+        self.ps, self.net = pressure, net
+        self.omega, self.stall_window, self.stall_factor = omega, stall_window, stall_factor
+        self.maxiter = maxiter
+        g = pressure.grid
+        self.nx, self.ny = g.nx, g.ny
+        n = self.nx * self.ny
+        dev = _lib.device()
+        z = lambda: t.zeros(n, dtype=t.float64, device=dev)  # noqa: E731
+        self.b, self.r, self.r_old, self.p, self.q, self.z = z(), z(), z(), z(), z(), z()
+        self.net_in = t.zeros((self.nx, self.ny), dtype=t.float32, device=dev)
+        self.partial = t.zeros(int(_lib.lib().cfd2d_fcg_partial_doubles(n)), dtype=t.float64, device=dev)
+        self.scal = t.zeros(C.sizeof(_lib.FcgScalars) // 8, dtype=t.float64, device=dev)
+        self.mask = pressure._d_nbr.view(self.nx, self.ny) >= 0x80
+        self.mask_u8 = self.mask.to(t.uint8).contiguous()
+        self.ws = Workspace(self.nx, self.ny, self.mask_u8)
+        self.last_iterations = 0
+        self.last_fallback = False
+        self.history = []
+
+    def _scalars(self):
+        raw = self.scal.cpu().numpy().tobytes()
+        return _lib.FcgScalars.from_buffer_copy(raw)
+
+    def precondition(self):
+        L = _lib.lib()
+        s = _lib.stream_ptr()
+        P = _lib.ptr
+        n = self.nx * self.ny
+        _lib.check(L.cfd2d_fcg_net_in(n, P(self.r), P(self.scal), P(self.mask_u8), P(self.net_in), s), "net_in")
+        out = net_forward(self.net, self.ws, self.net_in)
+        _lib.check(L.cfd2d_fcg_net_out(n, P(out), P(self.r), P(self.ps._d_dinv), P(self.mask_u8), P(self.scal),
+                                       self.omega, P(self.z), s), "net_out")
+
+    def solve_into_x(self, rhs=None, F=None, G=None, dx=1.0, dy=1.0, dt_ptr=None, tol=None):
+        """Run FCG on x = pressure x0 (in place). Returns the iteration count."""
+        L = _lib.lib()
+        s = _lib.stream_ptr()
+        P = _lib.ptr
+        n = self.nx * self.ny
+        op = C.byref(self.ps.op)
+        x = self.ps._d_x0.view(-1)
+        tol = self.ps.rtol if tol is None else tol
+        _lib.check(L.cfd2d_fcg_init(op, P(F), P(G), P(rhs), dx, dy, dt_ptr, P(self.b), P(x), P(self.r),
+                                    P(self.scal), P(self.partial), s), "fcg_init")
+        st = self._scalars()
+        atol = tol * math.sqrt(st.bb)
+        self.history = [math.sqrt(st.rr)]
+        self.last_fallback = False
+        if st.bb == 0.0:
+            x.copy_(self.b)
+            self.last_iterations = 0
+            return 0
+        it = 0
+        self.precondition()
+        _lib.check(L.cfd2d_fcg_zr(n, P(self.z), P(self.r), P(self.r_old), 1, P(self.scal), P(self.partial), s), "zr")
+        self.p.copy_(self.z)
+        while math.sqrt(st.rr) >= atol and it < self.maxiter:
+            _lib.check(L.cfd2d_fcg_pq(op, P(self.p), P(self.q), P(self.scal), P(self.partial), s), "pq")
+            _lib.check(L.cfd2d_fcg_update(n, P(x), P(self.r), P(self.r_old), P(self.p), P(self.q), P(self.scal),
+                                          P(self.partial), s), "update")
+            it += 1
+            st = self._scalars()
+            res = math.sqrt(st.rr)
+            self.history.append(res)
+            if not math.isfinite(res):
+                raise FloatingPointError("flexible CG produced a non-finite residual")
+            if res < atol:
+                break
+            k = len(self.history) - 1
+            if k >= self.stall_window and res > self.stall_factor * self.history[k - self.stall_window]:
+                self.last_fallback = True
+                break
+            self.precondition()
+            _lib.check(L.cfd2d_fcg_zr(n, P(self.z), P(self.r), P(self.r_old), 0, P(self.scal), P(self.partial), s),
+                       "zr")
+            _lib.check(L.cfd2d_fcg_dir(n, P(self.z), P(self.p), P(self.scal), s), "dir")
+        self.last_iterations = it
+        return it
+
+    def solve(self, rhs):
+        """Lap(p) = rhs (same conventions as PressureSolver.solve); host or device rhs."""
+        t = _t()
+        host = not isinstance(rhs, t.Tensor)
+        r = _lib.to_dev(rhs, t.float64).reshape(-1)
+        self.solve_into_x(rhs=r)
+        extra = 0
+        if self.last_fallback:
+            # continue with the plain Jacobi-PCG from the current iterate
+            self.ps.solve(rhs)
+            extra = self.ps.last_iterations
+        out = self.ps._d_x0.clone()
+        out[~self.mask] = 0.0
+        self.last_total_iterations = self.last_iterations + extra
+        return out.cpu().numpy() if host else out
+
+
+# ------------------------------------------------------------------ data and training
+def random_obstacles(rng, lx: float = 2.0, ly: float = 1.0, nmin: int = 2, nmax: int = 12):
+    """2-12 circles, ellipses or rectangles with centres uniform in the interior and
+    sizes 0.02-0.08 of the domain height (the obstacle-flow generator)."""
+    specs = []
+    for _ in range(int(rng.integers(nmin, nmax + 1))):
+        kind = rng.integers(0, 3)
+        x = float(rng.uniform(0.15 * lx, 0.85 * lx))
+        y = float(rng.uniform(0.15 * ly, 0.85 * ly))
+        size = float(rng.uniform(0.02, 0.08) * ly)
+        if kind == 0:
+            specs.append({"typ": "kreis", "x": x, "y": y, "r": size})
+        elif kind == 1:
+            specs.append({"typ": "ellipse", "x": x, "y": y, "a": size, "b": size * float(rng.uniform(0.4, 1.0)),
+                          "winkel": float(rng.uniform(0, 180))})
+        else:
+            specs.append({"typ": "rechteck", "x0": x - size, "y0": y - 0.6 * size, "x1": x + size,
+                          "y1": y + 0.6 * size})
+    return specs
+
+
+def obstacle_case(rng, nx: int, ny: int, pressure_solver: str = "cg"):
+    from . import cases
+
+    re = float(np.exp(rng.uniform(np.log(200.0), np.log(2000.0))))
+    return cases.custom_obstacles(random_obstacles(rng), lx=2.0, ly=1.0, nx=nx, ny=ny, re=re,
+                                  inflow_profile="uniform", walls="slip", pressure_solver=pressure_solver)
+
+
+def harvest_pairs(n_cases: int = 100, nx: int = 256, ny: int = 128, seed: int = 0, steps: int = 3,
+                  every: int = 8, max_snaps: int = 100, rtol: float = 1e-11):
+    """Residual -> error pairs from the solver's own runs.
+
+    For each seeded obstacle case: a few projection steps, then the pressure system
+    of the next predictor solved from zero by the plain Jacobi-PCG with iterate
+    snapshots; each snapshot x_k gives e_k = x* - x_k and r_k = A e_k. Returns FP32
+    tensors R, E (normalised by ||r_k||) and the fluid masks, on the device.
+    """
+    import os
+
+    from .pressure import PressureSolver
+
+    t = _t()
+    L = _lib.lib()
+    rng = np.random.default_rng(seed)
+    Rs, Es, Ms = [], [], []
+    for _ in range(n_cases):
+        case = obstacle_case(rng, nx, ny)
+        sim = case.sim
+        sim.pressure.tol = 1e-8
+        sim.advance(steps)
+        F, G, dt = sim.F, sim.G, sim.dt
+        g = sim.grid
+        rhs = ((F[1:, 1:-1] - F[:-1, 1:-1]) / g.dx + (G[1:-1, 1:] - G[1:-1, :-1]) / g.dy) / dt
+        old = os.environ.get("CFD2D_PCG_VARIANT")
+        os.environ["CFD2D_PCG_VARIANT"] = "grid"
+        try:
+            ps = PressureSolver(g, sim.boundary, method="cg", tol=rtol)
+        finally:
+            if old is None:
+                os.environ.pop("CFD2D_PCG_VARIANT")
+            else:
+                os.environ["CFD2D_PCG_VARIANT"] = old
+        n = nx * ny
+        snap = t.zeros((max_snaps, n), dtype=t.float64, device=_lib.device())
+        rd = _lib.to_dev(rhs)
+        p = t.empty_like(rd)
+        st = t.zeros(1, dtype=t.int32, device=_lib.device())
+        _lib.check(L.cfd2d_pressure_solve_snapshots(C.byref(ps.op), _lib.ptr(rd), _lib.ptr(p), rtol, 20000,
+                                                    _lib.ptr(snap), every, max_snaps, _lib.ptr(ps._d_iters),
+                                                    _lib.ptr(st), _lib.stream_ptr()), "snapshots")
+        its = int(ps._d_iters[0].item())
+        xstar = ps._d_x0.view(-1)
+        mask = (ps._d_nbr >= 0x80).to(t.uint8).contiguous()
+        k = min(max_snaps, its // every)
+        for s_ in range(k):
+            e = xstar - snap[s_]
+            r = t.empty_like(e)
+            _lib.check(L.cfd2d_poisson_matvec(C.byref(ps.op), _lib.ptr(e), _lib.ptr(r), _lib.stream_ptr()),
+                       "matvec")
+            rn = float(t.linalg.vector_norm(r))
+            if rn == 0.0 or not math.isfinite(rn):
+                continue
+            Rs.append((r / rn).float().view(nx, ny))
+            Es.append((e / rn).float().view(nx, ny))
+            Ms.append(mask)
+    return t.stack(Rs), t.stack(Es), Ms
+
+
+def train(net: LPCNet, R, E, masks, steps: int = 1000, batch: int = 4, lr: float = 1e-3, seed: int = 0,
+          log_every: int = 100, time_budget_s: float | None = None):
+    """Fit net(r) ~ e (relative L2 over the fluid cells) with the project's forward and
+    backward kernels; Adam on FP32 master weights, BF16 copies repacked every step."""
+    t = _t()
+    params = net.parameters()
+    for p_ in params:
+        p_.requires_grad_(False)
+    opt = t.optim.Adam(params, lr=lr)
+    H, W = R.shape[1:]
+    ws = Workspace(H, W, masks[0])
+    gen = np.random.default_rng(seed)
+    log = []
+    t0 = time.time()
+    for step in range(steps):
+        idx = gen.integers(0, R.shape[0], batch)
+        acc = {name: (t.zeros_like(net.w[name]), t.zeros_like(net.b[name])) for name, *_ in LAYERS}
+        loss = 0.0
+        for k in idx:
+            if ws.mask_src is not masks[k]:
+                ws.set_mask(masks[k])
+            x = R[k].contiguous()
+            out = net_forward(net, ws, x)
+            e = E[k]
+            den = float((e * e).sum()) + 1e-30
+            diff = out - e
+            loss += float((diff * diff).sum()) / den / batch
+            dout = (2.0 / den / batch) * diff
+            grads = net_backward(net, ws, x, dout)
+            for name in grads:
+                acc[name][0].add_(grads[name][0])
+                acc[name][1].add_(grads[name][1])
+        opt.zero_grad(set_to_none=False)
+        for name, *_ in LAYERS:
+            net.w[name].grad = acc[name][0]
+            net.b[name].grad = acc[name][1]
+        opt.step()
+        net.repack()
+        log.append(loss)
+        if log_every and step % log_every == 0:
+            print(f"train step {step}: loss {np.mean(log[-log_every:]):.4f}", flush=True)
+        if time_budget_s is not None and time.time() - t0 > time_budget_s:
+            break
+    return log

@@ -178,6 +178,9 @@ cudaError_t record(cudaEvent_t e, cudaStream_t s) {
     return cudaEventRecord(e, s);
 }
 
+int step_begin(const cfd2d_sim& S, cudaStream_t s);
+int step_finish(const cfd2d_sim* sim, cudaStream_t s);
+
 // One projection step; ev (may be null) gets four events recorded: step start,
 // before and after the main pressure solve, step end.
 int sim_step_impl(const cfd2d_sim* sim, cudaStream_t s, cudaEvent_t* ev) {
@@ -185,6 +188,20 @@ int sim_step_impl(const cfd2d_sim* sim, cudaStream_t s, cudaEvent_t* ev) {
     if (sim->pcg.cluster == 0 && !sim->pcg.work) return CFD2D_E_ARG;
     const cfd2d_sim& S = *sim;
     if (ev) CFD_TRY(record(ev[0], s));
+    int rc = step_begin(S, s);
+    if (rc) return rc;
+    // 5. pressure Poisson (divergence fused into the solver prologue) and correction
+    if (ev) CFD_TRY(record(ev[1], s));
+    rc = project(sim, S.p, false, true, s);
+    if (rc) return rc;
+    if (ev) CFD_TRY(record(ev[2], s));
+    rc = step_finish(sim, s);
+    if (rc) return rc;
+    if (ev) CFD_TRY(record(ev[3], s));
+    return CFD2D_OK;
+}
+
+int step_begin(const cfd2d_sim& S, cudaStream_t s) {
     // 1. boundary conditions (and the run() stop decision for this step)
     CFD_TRY(stage_apply_bc(S, 1, s));
     // 2. model pre-momentum hooks: k-omega SST blending, nu_t, nu_eff
@@ -193,11 +210,12 @@ int sim_step_impl(const cfd2d_sim* sim, cudaStream_t s, cudaEvent_t* ev) {
     CFD_TRY(stage_dt(S, s));
     // 4. tendencies, AB2, predictor, outflow extrapolation
     CFD_TRY(stage_predictor(S, 0, s));
-    // 5. pressure Poisson (divergence fused into the solver prologue) and correction
-    if (ev) CFD_TRY(record(ev[1], s));
-    int rc = project(sim, S.p, false, true, s);
-    if (rc) return rc;
-    if (ev) CFD_TRY(record(ev[2], s));
+    return CFD2D_OK;
+}
+
+int step_finish(const cfd2d_sim* sim, cudaStream_t s) {
+    const cfd2d_sim& S = *sim;
+    int rc = CFD2D_OK;
     CFD_TRY(stage_correct(S, S.p, 0, s));
     CFD_TRY(stage_apply_bc(S, 0, s));
     // 6. volume-flow forcing (cfd2d/solver.py:410-425)
@@ -215,7 +233,6 @@ int sim_step_impl(const cfd2d_sim* sim, cudaStream_t s, cudaEvent_t* ev) {
     for (int k = 0; k < S.nscalars; ++k) CFD_TRY(stage_scalar(S, k, s));
     // 8. residual, counters, history record
     CFD_TRY(stage_end(S, s));
-    if (ev) CFD_TRY(record(ev[3], s));
     return CFD2D_OK;
 }
 
@@ -225,6 +242,42 @@ extern "C" {
 
 int cfd2d_sim_step(const cfd2d_sim* sim, void* stream) {
     return sim_step_impl(sim, as_stream(stream), nullptr);
+}
+
+int cfd2d_sim_step_begin(const cfd2d_sim* sim, void* stream) {
+    if (!sim || !sim->state || !grid_ok(sim->nx, sim->ny)) return CFD2D_E_ARG;
+    return step_begin(*sim, as_stream(stream));
+}
+
+int cfd2d_sim_step_finish(const cfd2d_sim* sim, void* stream) {
+    if (!sim || !sim->state || !grid_ok(sim->nx, sim->ny)) return CFD2D_E_ARG;
+    if (sim->pcg.cluster == 0 && !sim->pcg.work) return CFD2D_E_ARG;
+    return step_finish(sim, as_stream(stream));
+}
+
+int cfd2d_poisson_matvec(const cfd2d_poisson* op, const double* x, double* y, void* stream) {
+    if (!op || !x || !y || !grid_ok(op->nx, op->ny)) return CFD2D_E_ARG;
+    return status_of(pcg_matvec(*op, x, y, as_stream(stream)));
+}
+
+int cfd2d_pressure_solve_snapshots(const cfd2d_poisson* op, const double* rhs, double* p, double rtol,
+                                   int maxiter, double* snap, int every, int max_snaps, int32_t* iters_out,
+                                   int32_t* status_out, void* stream) {
+    if (!op || !rhs || !p || !snap || every < 1 || max_snaps < 1 || maxiter < 0) return CFD2D_E_ARG;
+    if (op->cluster != 0 || !op->work) return CFD2D_E_ARG;
+    PcgLaunch L = {};
+    L.op = *op;
+    L.rhs_mode = 0;
+    L.rhs = rhs;
+    L.rtol = rtol;
+    L.maxiter = maxiter;
+    L.p_out = p;
+    L.iters_out = iters_out;
+    L.status_out = status_out;
+    L.snap = snap;
+    L.snap_every = every;
+    L.snap_max = max_snaps;
+    return status_of(pcg_launch(L, as_stream(stream)));
 }
 
 int cfd2d_sim_scalar_fill_ghosts(const cfd2d_sim* sim, int slot, void* stream) {

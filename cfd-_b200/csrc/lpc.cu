@@ -1,0 +1,475 @@
+// lpc.cu - learned Poisson preconditioner: a small convolutional network that maps
+// the pressure residual to an error estimate inside flexible CG.
+//
+// Activations are BF16 in NHWC layout (pixel = MAC cell (i, j) flattened as
+// i*W + j with j contiguous, 32 channels innermost); every product is accumulated
+// in FP32. The 32 -> 32 channel 3x3 convolutions (the FLOP-heavy layers) are
+// implicit GEMMs on the 5th-generation tensor cores: per CTA a tile of 128
+// consecutive pixels of one grid row (M = 128), N = 32 output channels,
+// K = 9 taps x 32 input channels = 288, issued as 18 tcgen05.mma (kind::f16, BF16
+// inputs, FP32 accumulator in tensor memory) by one thread; operands are staged in
+// shared memory in the K-major no-swizzle core-matrix layout (8 rows x 16 bytes
+// per core matrix) described by UMMA shared-memory descriptors; the epilogue reads
+// the accumulator with tcgen05.ld and fuses bias, skip addition, ReLU and the
+// fluid mask. The 1-channel layers, pooling, upsampling and the backward pass run
+// on CUDA cores with FP32 accumulation.
+//
+// This file is compiled without -fmad=false: it is not part of the float64
+// parity path.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "lpc.cuh"
+
+namespace cfd {
+namespace lpc {
+
+namespace {
+
+constexpr int CH = 32;
+constexpr int KDIM = 9 * CH;            // 288
+constexpr int TM = 128;                 // pixels per tile
+constexpr int CORE_BYTES = 128;         // one core matrix: 8 rows x 16 bytes
+constexpr int SBO = (KDIM / 8) * CORE_BYTES;  // 4608 bytes between 8-row groups
+constexpr int A_BYTES = (TM / 8) * SBO;       // 73728
+constexpr int B_BYTES = (CH / 8) * SBO;       // 18432
+constexpr uint32_t kWaitLimit = 1u << 24;
+
+// UMMA instruction descriptor, kind::f16: FP32 accumulator (bits 4-5 = 1), A and B
+// BF16 (bits 7-9, 10-12 = 1), both K-major (bits 15, 16 = 0), N >> 3 at bit 17,
+// M >> 4 at bit 24.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(CH >> 3) << 17) |
+                            ((uint32_t)(TM >> 4) << 24);
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// UMMA shared-memory descriptor: start address >> 4 (bits 0-13), leading byte
+// offset >> 4 (bits 16-29, distance between the two K core matrices of one MMA),
+// stride byte offset >> 4 (bits 32-45, distance between 8-row groups), version 1
+// (bits 46-47), no swizzle (bits 61-63 = 0).
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = (uint64_t)((saddr & 0x3FFFFu) >> 4);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;
+    return d;
+}
+
+__device__ __forceinline__ float bf2f(__nv_bfloat16 x) { return __bfloat162float(x); }
+
+}  // namespace
+
+// ---------------------------------------------------------------- 32 -> 32 conv (tensor cores)
+// y[p][n] = act(bias[n] + sum_{tap, c} w[n][c][tap] * x[p + tap][c] (+ skip[p][n])), masked.
+// wpack is the B operand image (N = 32 rows, K = 288) in the shared-memory layout.
+__global__ void __launch_bounds__(TM) k_conv32_tc(const __nv_bfloat16* __restrict__ x,
+                                                  const uint4* __restrict__ wpack,
+                                                  const float* __restrict__ bias,
+                                                  const __nv_bfloat16* __restrict__ skip,
+                                                  const uint8_t* __restrict__ mask,
+                                                  __nv_bfloat16* __restrict__ y, int H, int W,
+                                                  int relu, int* __restrict__ err) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint8_t* As = smem;
+    uint8_t* Bs = smem + A_BYTES;
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t tmem_slot;
+    __shared__ int ok;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int i = blockIdx.y;
+    const int j0 = blockIdx.x * TM;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                     "r"(32));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&mbar)), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        ok = 1;
+    }
+    // B operand: a straight copy of the prepacked image
+    for (int q = tid; q < B_BYTES / 16; q += TM) reinterpret_cast<uint4*>(Bs)[q] = wpack[q];
+    // A operand: row m = pixel (i, j0 + m); K index k = tap * 32 + c, tap = (di+1)*3 + (dj+1)
+    {
+        const int m = tid;
+        const int j = j0 + m;
+        uint8_t* rowbase = As + (m >> 3) * SBO + (m & 7) * 16;
+#pragma unroll
+        for (int tap = 0; tap < 9; ++tap) {
+            const int ii = i + tap / 3 - 1, jj = j + tap % 3 - 1;
+            const bool in = (j < W) && ii >= 0 && ii < H && jj >= 0 && jj < W;
+            const uint4* src = reinterpret_cast<const uint4*>(x + ((size_t)ii * W + jj) * CH);
+#pragma unroll
+            for (int c8 = 0; c8 < 4; ++c8) {
+                uint4 v = make_uint4(0u, 0u, 0u, 0u);
+                if (in) v = src[c8];
+                *reinterpret_cast<uint4*>(rowbase + (tap * 4 + c8) * CORE_BYTES) = v;
+            }
+        }
+    }
+    // generic-proxy shared-memory writes become visible to the tensor cores
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_slot;
+    if (tid == 0) {
+        const uint32_t a0 = smem_u32(As), b0 = smem_u32(Bs);
+#pragma unroll
+        for (int s = 0; s < KDIM / 16; ++s) {
+            const uint64_t ad = umma_desc(a0 + s * 2 * CORE_BYTES, CORE_BYTES, SBO);
+            const uint64_t bd = umma_desc(b0 + s * 2 * CORE_BYTES, CORE_BYTES, SBO);
+            const uint32_t acc = s > 0 ? 1u : 0u;
+            asm volatile(
+                "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+                "l"(ad), "l"(bd), "r"(kIdesc), "r"(acc));
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_u32(&mbar))
+                     : "memory");
+    }
+    // bounded wait for the accumulator
+    {
+        uint32_t done = 0;
+        for (uint32_t spin = 0; spin < kWaitLimit && !done; ++spin) {
+            asm volatile(
+                "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+                "selp.b32 %0, 1, 0, P1;\n\t}\n"
+                : "=r"(done)
+                : "r"(smem_u32(&mbar)), "r"(0));
+        }
+        if (!done) {
+            ok = 0;
+            if (err) atomicExch(err, 1);
+        }
+    }
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (ok) {
+        float acc[CH];
+#pragma unroll
+        for (int c0 = 0; c0 < CH; c0 += 8) {
+            uint32_t r[8];
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+                           "=r"(r[6]), "=r"(r[7])
+                         : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int q = 0; q < 8; ++q) acc[c0 + q] = __uint_as_float(r[q]);
+        }
+        const int m = warp * 32 + lane;
+        const int j = j0 + m;
+        if (j < W) {
+            const size_t p = (size_t)i * W + j;
+            const bool fl = mask ? (mask[p] != 0) : true;
+            __align__(16) __nv_bfloat16 out[CH];
+#pragma unroll
+            for (int n = 0; n < CH; ++n) {
+                float v = acc[n] + bias[n];
+                if (skip) v += bf2f(skip[p * CH + n]);
+                if (relu) v = fmaxf(v, 0.0f);
+                out[n] = __float2bfloat16(fl ? v : 0.0f);
+            }
+            uint4* dst = reinterpret_cast<uint4*>(y + p * CH);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) dst[q] = reinterpret_cast<const uint4*>(out)[q];
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(32));
+    }
+}
+
+// Pack w[n][c][3][3] (float, PyTorch OIHW) into the B operand image.
+__global__ void k_pack_w32(const float* __restrict__ w, __nv_bfloat16* __restrict__ img) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;  // over n * 288
+    if (e >= CH * KDIM) return;
+    const int n = e / KDIM, k = e % KDIM;
+    const int tap = k / CH, c = k % CH;
+    const float v = w[(n * CH + c) * 9 + tap];
+    const int off = (n >> 3) * SBO + (k >> 3) * CORE_BYTES + (n & 7) * 16 + (k & 7) * 2;
+    img[off / 2] = __float2bfloat16(v);
+}
+
+// ---------------------------------------------------------------- generic conv (CUDA cores)
+// cin, cout in {1, 32}. Forward: y[p][o] = bias[o] + sum w[o][c][tap] x[p + tap][c].
+// transposed (backward data): y[p][c] = sum w[o][c][tap] x[p - tap][o] (x = dy, cin = cout of
+// the forward layer). Inputs and outputs are FP32 or BF16 (xbf/ybf).
+template <int CIN, int COUT>
+__global__ void k_conv_generic(const void* __restrict__ x, int xbf, const float* __restrict__ w,
+                               const float* __restrict__ bias, const uint8_t* __restrict__ mask,
+                               void* __restrict__ y, int ybf, int H, int W, int relu, int transposed) {
+    __shared__ float ws[CIN * COUT * 9];
+    for (int e = threadIdx.x; e < CIN * COUT * 9; e += blockDim.x) ws[e] = w[e];
+    __syncthreads();
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= H * W) return;
+    const int i = p / W, j = p % W;
+    float acc[COUT];
+#pragma unroll
+    for (int o = 0; o < COUT; ++o) acc[o] = (bias && !transposed) ? bias[o] : 0.0f;
+    for (int tap = 0; tap < 9; ++tap) {
+        const int di = tap / 3 - 1, dj = tap % 3 - 1;
+        const int ii = transposed ? i - di : i + di, jj = transposed ? j - dj : j + dj;
+        if (ii < 0 || ii >= H || jj < 0 || jj >= W) continue;
+        const size_t q = (size_t)ii * W + jj;
+#pragma unroll 4
+        for (int c = 0; c < CIN; ++c) {
+            const float xv = xbf ? bf2f(reinterpret_cast<const __nv_bfloat16*>(x)[q * CIN + c])
+                                 : reinterpret_cast<const float*>(x)[q * CIN + c];
+#pragma unroll
+            for (int o = 0; o < COUT; ++o) {
+                // forward: w[o][c][tap]; transposed: the forward layer had (cin = COUT, cout = CIN)
+                const float wv = transposed ? ws[(c * COUT + o) * 9 + tap] : ws[(o * CIN + c) * 9 + tap];
+                acc[o] += wv * xv;
+            }
+        }
+    }
+    const bool fl = mask ? (mask[p] != 0) : true;
+#pragma unroll
+    for (int o = 0; o < COUT; ++o) {
+        float v = acc[o];
+        if (relu) v = fmaxf(v, 0.0f);
+        if (!fl) v = 0.0f;
+        if (ybf) reinterpret_cast<__nv_bfloat16*>(y)[(size_t)p * COUT + o] = __float2bfloat16(v);
+        else reinterpret_cast<float*>(y)[(size_t)p * COUT + o] = v;
+    }
+}
+
+// ---------------------------------------------------------------- pooling, upsampling
+// coarse (Hc, Wc) = (ceil(H/2), ceil(W/2)): mean of the in-range children
+__global__ void k_pool2(const __nv_bfloat16* __restrict__ x, __nv_bfloat16* __restrict__ y, int H, int W) {
+    const int Hc = (H + 1) / 2, Wc = (W + 1) / 2;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= Hc * Wc * CH) return;
+    const int c = e % CH, q = e / CH;
+    const int ic = q / Wc, jc = q % Wc;
+    float s = 0.0f;
+    int n = 0;
+    for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b) {
+            const int i = 2 * ic + a, j = 2 * jc + b;
+            if (i < H && j < W) { s += bf2f(x[((size_t)i * W + j) * CH + c]); ++n; }
+        }
+    y[e] = __float2bfloat16(s / (float)n);
+}
+
+// y[p] = coarse[parent(p)] + skip[p]
+__global__ void k_upadd(const __nv_bfloat16* __restrict__ coarse, const __nv_bfloat16* __restrict__ skip,
+                        __nv_bfloat16* __restrict__ y, int H, int W) {
+    const int Wc = (W + 1) / 2;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= H * W * CH) return;
+    const int c = e % CH, p = e / CH;
+    const int i = p / W, j = p % W;
+    const float v = bf2f(coarse[((size_t)(i / 2) * Wc + j / 2) * CH + c]) + bf2f(skip[e]);
+    y[e] = __float2bfloat16(v);
+}
+
+// coarse mask: any child fluid
+__global__ void k_pool_mask(const uint8_t* __restrict__ m, uint8_t* __restrict__ mc, int H, int W) {
+    const int Hc = (H + 1) / 2, Wc = (W + 1) / 2;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= Hc * Wc) return;
+    const int ic = q / Wc, jc = q % Wc;
+    uint8_t v = 0;
+    for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b) {
+            const int i = 2 * ic + a, j = 2 * jc + b;
+            if (i < H && j < W) v |= m[(size_t)i * W + j];
+        }
+    mc[q] = v ? 1 : 0;
+}
+
+// ---------------------------------------------------------------- backward helpers
+// g = dy * (y > 0) * mask  (ReLU layers) in FP32
+__global__ void k_relu_bwd(const float* __restrict__ dy, const __nv_bfloat16* __restrict__ y,
+                           const uint8_t* __restrict__ mask, float* __restrict__ g, int npix, int ch,
+                           int relu) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= npix * ch) return;
+    const int p = e / ch;
+    float v = dy[e];
+    if (relu && !(bf2f(y[e]) > 0.0f)) v = 0.0f;
+    if (mask && !mask[p]) v = 0.0f;
+    g[e] = v;
+}
+
+// dcoarse[q] = sum over children of dfine[p]  (upsample backward), dfine given FP32
+__global__ void k_upadd_bwd(const float* __restrict__ dy, float* __restrict__ dcoarse, int H, int W) {
+    const int Hc = (H + 1) / 2, Wc = (W + 1) / 2;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= Hc * Wc * CH) return;
+    const int c = e % CH, q = e / CH;
+    const int ic = q / Wc, jc = q % Wc;
+    float s = 0.0f;
+    for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b) {
+            const int i = 2 * ic + a, j = 2 * jc + b;
+            if (i < H && j < W) s += dy[((size_t)i * W + j) * CH + c];
+        }
+    dcoarse[e] = s;
+}
+
+// dfine[p] += dcoarse[parent(p)] / n_children(parent)   (pool backward, accumulating)
+__global__ void k_pool_bwd(const float* __restrict__ dcoarse, float* __restrict__ dfine, int H, int W) {
+    const int Wc = (W + 1) / 2;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= H * W * CH) return;
+    const int c = e % CH, p = e / CH;
+    const int i = p / W, j = p % W;
+    const int ic = i / 2, jc = j / 2;
+    const int na = (2 * ic + 1 < H) ? 2 : 1, nb = (2 * jc + 1 < W) ? 2 : 1;
+    dfine[e] += dcoarse[((size_t)ic * Wc + jc) * CH + c] / (float)(na * nb);
+}
+
+// Weight gradient of a 3x3 conv: dw[o][c][tap] = sum_p g[p][o] x[p + tap][c], db[o] = sum_p g[p][o].
+// Each block reduces a contiguous pixel range into partial sums (deterministic order);
+// k_reduce_partials adds the blocks in index order.
+template <int CIN, int COUT>
+__global__ void k_conv_dw(const void* __restrict__ x, int xbf, const float* __restrict__ g, int H, int W,
+                          int pix_per_block, float* __restrict__ partial) {
+    constexpr int NW = COUT * CIN * 9;
+    const int p0 = blockIdx.x * pix_per_block;
+    const int p1 = min(H * W, p0 + pix_per_block);
+    for (int e = threadIdx.x; e < NW + COUT; e += blockDim.x) {
+        float s = 0.0f;
+        if (e < NW) {
+            const int o = e / (CIN * 9), c = (e / 9) % CIN, tap = e % 9;
+            const int di = tap / 3 - 1, dj = tap % 3 - 1;
+            for (int p = p0; p < p1; ++p) {
+                const int i = p / W, j = p % W;
+                const int ii = i + di, jj = j + dj;
+                if (ii < 0 || ii >= H || jj < 0 || jj >= W) continue;
+                const size_t q = (size_t)ii * W + jj;
+                const float xv = xbf ? bf2f(reinterpret_cast<const __nv_bfloat16*>(x)[q * CIN + c])
+                                     : reinterpret_cast<const float*>(x)[q * CIN + c];
+                s += g[(size_t)p * COUT + o] * xv;
+            }
+        } else {
+            const int o = e - NW;
+            for (int p = p0; p < p1; ++p) s += g[(size_t)p * COUT + o];
+        }
+        partial[(size_t)blockIdx.x * (NW + COUT) + e] = s;
+    }
+}
+
+__global__ void k_reduce_partials(const float* __restrict__ partial, int nblocks, int n, float* __restrict__ out) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    float s = 0.0f;
+    for (int b = 0; b < nblocks; ++b) s += partial[(size_t)b * n + e];
+    out[e] = s;
+}
+
+// ---------------------------------------------------------------- host launchers
+namespace {
+inline int cdiv(long long a, int b) { return (int)((a + b - 1) / b); }
+}  // namespace
+
+size_t conv32_smem_bytes() { return (size_t)A_BYTES + B_BYTES; }
+
+cudaError_t conv32_tc(const __nv_bfloat16* x, const __nv_bfloat16* wpack, const float* bias,
+                      const __nv_bfloat16* skip, const uint8_t* mask, __nv_bfloat16* y, int H, int W, int relu,
+                      int* err, cudaStream_t s) {
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(k_conv32_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)conv32_smem_bytes());
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    dim3 grid(cdiv(W, TM), H);
+    k_conv32_tc<<<grid, TM, conv32_smem_bytes(), s>>>(x, reinterpret_cast<const uint4*>(wpack), bias, skip,
+                                                      mask, y, H, W, relu, err);
+    return cudaGetLastError();
+}
+
+cudaError_t pack_w32(const float* w, __nv_bfloat16* img, cudaStream_t s) {
+    k_pack_w32<<<cdiv(CH * KDIM, 256), 256, 0, s>>>(w, img);
+    return cudaGetLastError();
+}
+
+cudaError_t conv_generic(int cin, int cout, const void* x, int xbf, const float* w, const float* bias,
+                         const uint8_t* mask, void* y, int ybf, int H, int W, int relu, int transposed,
+                         cudaStream_t s) {
+    const int n = H * W;
+    const int blk = 128;
+    if (cin == 1 && cout == 32)
+        k_conv_generic<1, 32><<<cdiv(n, blk), blk, 0, s>>>(x, xbf, w, bias, mask, y, ybf, H, W, relu, transposed);
+    else if (cin == 32 && cout == 1)
+        k_conv_generic<32, 1><<<cdiv(n, blk), blk, 0, s>>>(x, xbf, w, bias, mask, y, ybf, H, W, relu, transposed);
+    else if (cin == 32 && cout == 32)
+        k_conv_generic<32, 32><<<cdiv(n, blk), blk, 0, s>>>(x, xbf, w, bias, mask, y, ybf, H, W, relu, transposed);
+    else
+        return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+cudaError_t pool2(const __nv_bfloat16* x, __nv_bfloat16* y, int H, int W, cudaStream_t s) {
+    const int n = ((H + 1) / 2) * ((W + 1) / 2) * CH;
+    k_pool2<<<cdiv(n, 256), 256, 0, s>>>(x, y, H, W);
+    return cudaGetLastError();
+}
+
+cudaError_t pool_mask(const uint8_t* m, uint8_t* mc, int H, int W, cudaStream_t s) {
+    const int n = ((H + 1) / 2) * ((W + 1) / 2);
+    k_pool_mask<<<cdiv(n, 256), 256, 0, s>>>(m, mc, H, W);
+    return cudaGetLastError();
+}
+
+cudaError_t upadd(const __nv_bfloat16* coarse, const __nv_bfloat16* skip, __nv_bfloat16* y, int H, int W,
+                  cudaStream_t s) {
+    k_upadd<<<cdiv((long long)H * W * CH, 256), 256, 0, s>>>(coarse, skip, y, H, W);
+    return cudaGetLastError();
+}
+
+cudaError_t relu_bwd(const float* dy, const __nv_bfloat16* y, const uint8_t* mask, float* g, int npix, int ch,
+                     int relu, cudaStream_t s) {
+    k_relu_bwd<<<cdiv((long long)npix * ch, 256), 256, 0, s>>>(dy, y, mask, g, npix, ch, relu);
+    return cudaGetLastError();
+}
+
+cudaError_t upadd_bwd(const float* dy, float* dcoarse, int H, int W, cudaStream_t s) {
+    const int n = ((H + 1) / 2) * ((W + 1) / 2) * CH;
+    k_upadd_bwd<<<cdiv(n, 256), 256, 0, s>>>(dy, dcoarse, H, W);
+    return cudaGetLastError();
+}
+
+cudaError_t pool_bwd(const float* dcoarse, float* dfine, int H, int W, cudaStream_t s) {
+    k_pool_bwd<<<cdiv((long long)H * W * CH, 256), 256, 0, s>>>(dcoarse, dfine, H, W);
+    return cudaGetLastError();
+}
+
+size_t conv_dw_partial_floats(int cin, int cout, int H, int W, int pix_per_block) {
+    return (size_t)cdiv((long long)H * W, pix_per_block) * (cin * cout * 9 + cout);
+}
+
+cudaError_t conv_dw(int cin, int cout, const void* x, int xbf, const float* g, int H, int W, int pix_per_block,
+                    float* partial, float* out, cudaStream_t s) {
+    const int nb = cdiv((long long)H * W, pix_per_block);
+    const int n = cin * cout * 9 + cout;
+    if (cin == 1 && cout == 32)
+        k_conv_dw<1, 32><<<nb, 256, 0, s>>>(x, xbf, g, H, W, pix_per_block, partial);
+    else if (cin == 32 && cout == 1)
+        k_conv_dw<32, 1><<<nb, 256, 0, s>>>(x, xbf, g, H, W, pix_per_block, partial);
+    else if (cin == 32 && cout == 32)
+        k_conv_dw<32, 32><<<nb, 256, 0, s>>>(x, xbf, g, H, W, pix_per_block, partial);
+    else
+        return cudaErrorInvalidValue;
+    k_reduce_partials<<<cdiv(n, 256), 256, 0, s>>>(partial, nb, n, out);
+    return cudaGetLastError();
+}
+
+}  // namespace lpc
+}  // namespace cfd

@@ -595,6 +595,11 @@ __global__ void __launch_bounds__(kGridThreads) k_pcg_grid(PcgLaunch L) {
                 v2[0] += r * r;
                 v2[1] += r * (op.dinv[c] * r);
             }
+            if (L.snap) {
+                const int k = (it + 1) / L.snap_every;
+                if ((it + 1) % L.snap_every == 0 && k <= L.snap_max)
+                    for (int c = c0 + tid; c < c1; c += kGridThreads) L.snap[(size_t)(k - 1) * n + c] = X[c];
+            }
             if (!grid_sum<2>(v2, red_smem, W.partB, W.bar, status)) return;
             rr = v2[0];
             beta = v2[1] / rho;
@@ -674,6 +679,20 @@ int grid_blocks_for(int n) {
 }
 
 }  // namespace
+
+__global__ void k_matvec(cfd2d_poisson op, const double* x, double* y) {
+    const int n = op.nx * op.ny;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        const uint8_t nb = op.nbr[c];
+        y[c] = (nb & 0x80) ? apply_A(op, x, c / op.ny, c % op.ny, nb, op.diag[c]) : 0.0;
+    }
+}
+
+cudaError_t pcg_matvec(const cfd2d_poisson& op, const double* x, double* y, cudaStream_t s) {
+    const int n = op.nx * op.ny;
+    k_matvec<<<(n + 255) / 256, 256, 0, s>>>(op, x, y);
+    return cudaGetLastError();
+}
 
 size_t pcg_grid_workspace_doubles(int nx, int ny) {
     // R, P0, P1 + three partial arrays for up to 148 * 32 CTAs + barrier words

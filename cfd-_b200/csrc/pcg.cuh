@@ -26,10 +26,13 @@ struct PcgLaunch {
     int32_t* status_out;       // device, may be null (atomicOr of CFD2D_S_* bits)
     const int32_t* active;     // device, may be null: skip when *active == 0
     int cap_cells;             // set by pcg_launch
+    double* snap;              // grid solver: iterate snapshots (nullable)
+    int snap_every, snap_max;
 };
 
 int pcg_cluster_plan(int nx, int ny);
 size_t pcg_grid_workspace_doubles(int nx, int ny);
 cudaError_t pcg_launch(const PcgLaunch& L, cudaStream_t s);
+cudaError_t pcg_matvec(const cfd2d_poisson& op, const double* x, double* y, cudaStream_t s);
 
 }  // namespace cfd

@@ -281,6 +281,82 @@ int cfd2d_events_create(int n, void** events);
 int cfd2d_events_destroy(int n, void** events);
 int cfd2d_event_elapsed_ms(void* start, void* end, float* ms);
 
+/* ---- split step, for an external pressure solver ------------------------ */
+
+/* First part of cfd2d_sim_step: boundary conditions, model pre-momentum hooks,
+ * time step and predictor F, G (cfd2d/solver.py:326-368). */
+int cfd2d_sim_step_begin(const cfd2d_sim* sim, void* stream);
+
+/* Second part: with sim->p holding the pressure of this step, the correction,
+ * boundary conditions, flow-rate control, scalar transport and the end-of-step
+ * record (cfd2d/solver.py:277-403). */
+int cfd2d_sim_step_finish(const cfd2d_sim* sim, void* stream);
+
+/* y = A x for the pressure operator (nx*ny vectors, solid entries 0), rows summed
+ * in increasing column order. No reference counterpart (scipy's A @ x). */
+int cfd2d_poisson_matvec(const cfd2d_poisson* op, const double* x, double* y, void* stream);
+
+/* Pressure solve that also records the iterate x every `every` iterations into
+ * snap (up to max_snaps vectors of nx*ny), for harvesting training pairs of the
+ * learned preconditioner; otherwise as cfd2d_pressure_solve. Grid-persistent
+ * solver only (op->cluster == 0). No reference counterpart. */
+int cfd2d_pressure_solve_snapshots(const cfd2d_poisson* op, const double* rhs, double* p, double rtol,
+                                   int maxiter, double* snap, int every, int max_snaps, int32_t* iters_out,
+                                   int32_t* status_out, void* stream);
+
+/* ---- learned Poisson preconditioner (no counterpart in the reference) ---- */
+/* Activations: BF16, NHWC with 32 channels, pixel = cell (i, j) at i*W + j. */
+
+/* Bytes of the packed weight image of one 32->32 3x3 convolution. */
+size_t cfd2d_lpc_w32_bytes(void);
+/* Pack w[32][32][3][3] (float32, out x in x kh x kw) into the tensor-core image. */
+int cfd2d_lpc_pack_w32(const float* w, void* image, void* stream);
+/* y = act(conv3x3(x, w) + bias (+ skip)) masked; tcgen05 implicit GEMM. err: device
+ * int set to 1 if the bounded wait for the accumulator gave up (may be NULL). */
+int cfd2d_lpc_conv32(const void* x, const void* image, const float* bias, const void* skip,
+                     const uint8_t* mask, void* y, int H, int W, int relu, int32_t* err, void* stream);
+/* CUDA-core 3x3 convolution for cin, cout in {1, 32}: x and y FP32 or BF16
+ * (x_bf16, y_bf16 flags); transposed != 0 applies the adjoint (data gradient). */
+int cfd2d_lpc_conv(int cin, int cout, const void* x, int x_bf16, const float* w, const float* bias,
+                   const uint8_t* mask, void* y, int y_bf16, int H, int W, int relu, int transposed,
+                   void* stream);
+int cfd2d_lpc_pool2(const void* x, void* y, int H, int W, void* stream);
+int cfd2d_lpc_pool_mask(const uint8_t* m, uint8_t* mc, int H, int W, void* stream);
+int cfd2d_lpc_upadd(const void* coarse, const void* skip, void* y, int H, int W, void* stream);
+int cfd2d_lpc_relu_bwd(const float* dy, const void* y, const uint8_t* mask, float* g, int npix, int ch,
+                       int relu, void* stream);
+int cfd2d_lpc_upadd_bwd(const float* dy, float* dcoarse, int H, int W, void* stream);
+int cfd2d_lpc_pool_bwd(const float* dcoarse, float* dfine, int H, int W, void* stream);
+size_t cfd2d_lpc_conv_dw_partial_floats(int cin, int cout, int H, int W, int pix_per_block);
+/* weight and bias gradient: out = [dw (cout*cin*9), db (cout)] */
+int cfd2d_lpc_conv_dw(int cin, int cout, const void* x, int x_bf16, const float* g, int H, int W,
+                      int pix_per_block, float* partial, float* out, void* stream);
+
+/* ---- flexible CG around a variable preconditioner (no reference counterpart) */
+typedef struct cfd2d_fcg_scalars {
+    double alpha, beta, rz, pq, rr, bb;
+    int32_t iters;
+    uint32_t ticket;
+} cfd2d_fcg_scalars;
+
+size_t cfd2d_fcg_partial_doubles(int n);
+/* b = -(div(F,G)/dt) (or -rhs when rhs != NULL), r = b - A x */
+int cfd2d_fcg_init(const cfd2d_poisson* op, const double* F, const double* G, const double* rhs, double dx,
+                   double dy, const double* dt, double* b, double* x, double* r, cfd2d_fcg_scalars* s,
+                   double* partial, void* stream);
+int cfd2d_fcg_pq(const cfd2d_poisson* op, const double* p, double* q, cfd2d_fcg_scalars* s, double* partial,
+                 void* stream);
+int cfd2d_fcg_update(int n, double* x, double* r, double* r_old, const double* p, const double* q,
+                     cfd2d_fcg_scalars* s, double* partial, void* stream);
+int cfd2d_fcg_zr(int n, const double* z, const double* r, const double* r_old, int first, cfd2d_fcg_scalars* s,
+                 double* partial, void* stream);
+int cfd2d_fcg_dir(int n, const double* z, double* p, const cfd2d_fcg_scalars* s, void* stream);
+int cfd2d_fcg_net_in(int n, const double* r, const cfd2d_fcg_scalars* s, const uint8_t* mask, float* in,
+                     void* stream);
+int cfd2d_fcg_net_out(int n, const float* out, const double* r, const double* dinv, const uint8_t* mask,
+                      const cfd2d_fcg_scalars* s, double jacobi, double* z, void* stream);
+int cfd2d_fcg_scatter_p(const cfd2d_poisson* op, const double* x, double* p_padded, void* stream);
+
 /* Library version string (host memory, static). */
 const char* cfd2d_version(void);
 
