@@ -99,14 +99,26 @@ class _Clocks:
         try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                                          "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+                                          "-lms", "50"], stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return self
+        # nvidia-smi takes a moment to start: the timed region begins after its
+        # first sample, and only later samples are summarised
+        self.skip = 0
+        t_end = time.time() + 5.0
+        while time.time() < t_end and self.proc.poll() is None:
+            self.f.flush()
+            n = len(Path(self.path).read_text().splitlines())
+            if n >= 1:
+                self.skip = n
+                break
+            time.sleep(0.02)
         return self
 
     def __exit__(self, *a):
         if self.proc is not None:
-            time.sleep(0.25)
+            time.sleep(0.06)
             self.proc.terminate()
             self.proc.wait(timeout=5)
             self.f.close()
@@ -116,7 +128,7 @@ class _Clocks:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in Path(self.path).read_text().splitlines():
+        for line in Path(self.path).read_text().splitlines()[self.skip:]:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) < 9 or parts[0] != str(dev_index):
                 continue

@@ -255,7 +255,9 @@ def torch_reference_forward(net: LPCNet, x_in, masks):
         return a.to(t.bfloat16).float()
 
     def conv(name, a, relu, lvl, round_out=True):
-        y = F.conv2d(a, net.wq(name).cpu(), net.b[name].detach().cpu(), padding=1)
+        bias = net.b[name]
+        bias = bias.detach().cpu() if bias.is_cuda else bias
+        y = F.conv2d(a, net.wq(name).cpu(), bias, padding=1)
         if relu:
             y = t.relu(y)
         y = y * masks[lvl]

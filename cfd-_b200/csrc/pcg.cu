@@ -88,7 +88,7 @@ __device__ __forceinline__ void cluster_sum(cg::cluster_group& cluster, double (
 
 }  // namespace
 
-template <int CPT>
+template <int CPT, bool PAIR>
 __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cluster(PcgLaunch L) {
     cg::cluster_group cluster = cg::this_cluster();
     const int C = (int)cluster.num_blocks();
@@ -240,7 +240,7 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cluster(PcgLaunch L) {
     } else {
         double beta = 0.0;
         int cur = 0;  // p of this iteration goes to buffer cur (P0 or P1)
-        double q[CPT];
+        double q[PAIR ? 2 * CPT : CPT];
         for (it = 0; it < L.maxiter; ++it) {
             if (sqrt(rr) < atol) { converged = true; break; }
             double* Pn = cur ? P1 : P0;
@@ -248,6 +248,68 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cluster(PcgLaunch L) {
             const int po = cur ? 2 * cap : 3 * cap;  // offset of the previous p from X
             const bool first = (it == 0);
             double pq = 0.0;
+            if constexpr (PAIR) {
+                // two cells (c, c+1) of one row per slot; ny is even, so c is even and
+                // every 16-byte pair load is aligned
+#pragma unroll
+                for (int k = 0; k < CPT; ++k) {
+                    q[2 * k] = 0.0;
+                    q[2 * k + 1] = 0.0;
+                    const int c = 2 * (tid + k * kPcgThreads);
+                    if (c >= nloc) continue;
+                    const unsigned nb2 = *reinterpret_cast<const uint16_t*>(NB + c);
+                    const unsigned nb0 = nb2 & 0xFFu, nb1 = nb2 >> 8;
+                    if (!((nb0 | nb1) & 0x80u)) continue;
+                    const int li = (int)__umulhi((unsigned)c, magic);
+                    const int j = c - li * ny;
+                    const double2 z2 = *reinterpret_cast<const double2*>(Z + c);
+                    double pC0 = z2.x, pC1 = z2.y;
+                    if (!first) {
+                        const double2 o2 = *reinterpret_cast<const double2*>(Po + c);
+                        pC0 = o2.x * beta + z2.x;
+                        pC1 = o2.y * beta + z2.y;
+                    }
+                    // solid cells carry p = z = 0 and no coupling bits, so their terms vanish
+                    double tW0 = 0.0, tW1 = 0.0, tE0 = 0.0, tE1 = 0.0;
+                    const double tS0 = (nb0 & 2) ? mdy2 * (first ? Z[c - 1] : Po[c - 1] * beta + Z[c - 1]) : 0.0;
+                    const double tN0 = (nb0 & 4) ? mdy2 * pC1 : 0.0;
+                    const double tS1 = (nb1 & 2) ? mdy2 * pC0 : 0.0;
+                    const double tN1 = (nb1 & 4) ? mdy2 * (first ? Z[c + 2] : Po[c + 2] * beta + Z[c + 2]) : 0.0;
+                    if ((nb0 | nb1) & 1) {
+                        const double* g = (li > 0) ? (X + c - ny) : (baseW + j);
+                        const double2 gz = *reinterpret_cast<const double2*>(g + 6 * cap);
+                        double w0 = gz.x, w1 = gz.y;
+                        if (!first) {
+                            const double2 go = *reinterpret_cast<const double2*>(g + po);
+                            w0 = go.x * beta + gz.x;
+                            w1 = go.y * beta + gz.y;
+                        }
+                        if (nb0 & 1) tW0 = mdx2 * w0;
+                        if (nb1 & 1) tW1 = mdx2 * w1;
+                    }
+                    if ((nb0 | nb1) & 8) {
+                        const double* g = (li < rows - 1) ? (X + c + ny) : (baseE + j);
+                        const double2 gz = *reinterpret_cast<const double2*>(g + 6 * cap);
+                        double e0 = gz.x, e1 = gz.y;
+                        if (!first) {
+                            const double2 go = *reinterpret_cast<const double2*>(g + po);
+                            e0 = go.x * beta + gz.x;
+                            e1 = go.y * beta + gz.y;
+                        }
+                        if (nb0 & 8) tE0 = mdx2 * e0;
+                        if (nb1 & 8) tE1 = mdx2 * e1;
+                    }
+                    const double2 dg = *reinterpret_cast<const double2*>(DG + c);
+                    const int i = r0 + li;
+                    const double q0 = row_sum(periodic, i, nx, tW0, tS0, dg.x * pC0, tN0, tE0);
+                    const double q1 = row_sum(periodic, i, nx, tW1, tS1, dg.y * pC1, tN1, tE1);
+                    *reinterpret_cast<double2*>(Pn + c) = make_double2(pC0, pC1);
+                    q[2 * k] = q0;
+                    q[2 * k + 1] = q1;
+                    pq += pC0 * q0;
+                    pq += pC1 * q1;
+                }
+            } else {
 #pragma unroll
             for (int k = 0; k < CPT; ++k) {
                 q[k] = 0.0;
@@ -276,6 +338,7 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cluster(PcgLaunch L) {
                 q[k] = qq;
                 pq += pC * qq;
             }
+            }
             {
                 double v[1] = {pq};
                 cluster_sum<1>(cluster, v, red_smem, SLOTS(), C, me);
@@ -283,6 +346,38 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cluster(PcgLaunch L) {
             }
             const double alpha = rho / pq;
             double v2[2] = {0.0, 0.0};
+            if constexpr (PAIR) {
+#pragma unroll
+                for (int k = 0; k < CPT; ++k) {
+                    const int c = 2 * (tid + k * kPcgThreads);
+                    if (c >= nloc) continue;
+                    const unsigned nb2 = *reinterpret_cast<const uint16_t*>(NB + c);
+                    const bool f0 = nb2 & 0x80u, f1 = (nb2 >> 8) & 0x80u;
+                    if (!(f0 || f1)) continue;
+                    double2 x2 = *reinterpret_cast<const double2*>(X + c);
+                    double2 r2 = *reinterpret_cast<const double2*>(R + c);
+                    double2 z2 = *reinterpret_cast<const double2*>(Z + c);
+                    const double2 p2 = *reinterpret_cast<const double2*>(Pn + c);
+                    const double2 d2 = *reinterpret_cast<const double2*>(DI + c);
+                    if (f0) {
+                        x2.x = x2.x + alpha * p2.x;
+                        r2.x = r2.x - alpha * q[2 * k];
+                        z2.x = d2.x * r2.x;
+                        v2[0] += r2.x * r2.x;
+                        v2[1] += r2.x * z2.x;
+                    }
+                    if (f1) {
+                        x2.y = x2.y + alpha * p2.y;
+                        r2.y = r2.y - alpha * q[2 * k + 1];
+                        z2.y = d2.y * r2.y;
+                        v2[0] += r2.y * r2.y;
+                        v2[1] += r2.y * z2.y;
+                    }
+                    *reinterpret_cast<double2*>(X + c) = x2;
+                    *reinterpret_cast<double2*>(R + c) = r2;
+                    *reinterpret_cast<double2*>(Z + c) = z2;
+                }
+            } else {
 #pragma unroll
             for (int k = 0; k < CPT; ++k) {
                 const int c = tid + k * kPcgThreads;
@@ -295,6 +390,7 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cluster(PcgLaunch L) {
                 Z[c] = z;
                 v2[0] += r * r;
                 v2[1] += r * z;
+            }
             }
             cluster_sum<2>(cluster, v2, red_smem, SLOTS(), C, me);
             rr = v2[0];
@@ -723,7 +819,7 @@ size_t smem_bytes(int cap) { return (size_t)cap * (kArrays * sizeof(double) + 1)
 // Kernel attributes are set once per instantiation, outside any stream capture
 // (cfd2d_pcg_plan runs before the first launch): the maximum dynamic shared
 // memory the hardware allows and permission for 16-CTA clusters.
-template <int CPT>
+template <int CPT, bool PAIR>
 cudaError_t configure_cpt() {
     static bool done = false;
     if (done) return cudaSuccess;
@@ -733,19 +829,19 @@ cudaError_t configure_cpt() {
     e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     if (e != cudaSuccess) return e;
     const int dyn = optin - (int)((32 * kMaxK + 2 * 16 * kMaxK + CFD2D_MAX_COMPONENTS) * sizeof(double)) - 1024;
-    e = cudaFuncSetAttribute(k_pcg_cluster<CPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+    e = cudaFuncSetAttribute(k_pcg_cluster<CPT, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_pcg_cluster<CPT>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    e = cudaFuncSetAttribute(k_pcg_cluster<CPT, PAIR>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     if (e != cudaSuccess) return e;
     done = true;
     return cudaSuccess;
 }
 
-template <int CPT>
+template <int CPT, bool PAIR>
 cudaError_t launch_cpt(const PcgLaunch& L, int C, cudaStream_t s) {
-    auto kern = k_pcg_cluster<CPT>;
+    auto kern = k_pcg_cluster<CPT, PAIR>;
     const size_t bytes = smem_bytes(L.cap_cells);
-    cudaError_t e = configure_cpt<CPT>();
+    cudaError_t e = configure_cpt<CPT, PAIR>();
     if (e != cudaSuccess) return e;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(C, 1, 1);
@@ -817,10 +913,19 @@ int pcg_cluster_plan(int nx, int ny) {
         cudaError_t e = cudaSuccess;
         const void* f = nullptr;
         switch (cpt) {
-            case 1: e = configure_cpt<1>(); f = (const void*)k_pcg_cluster<1>; break;
-            case 2: e = configure_cpt<2>(); f = (const void*)k_pcg_cluster<2>; break;
-            case 4: e = configure_cpt<4>(); f = (const void*)k_pcg_cluster<4>; break;
-            default: e = configure_cpt<8>(); f = (const void*)k_pcg_cluster<8>; break;
+            case 1: e = configure_cpt<1, false>(); f = (const void*)k_pcg_cluster<1, false>; break;
+            case 2: e = configure_cpt<2, false>(); f = (const void*)k_pcg_cluster<2, false>; break;
+            case 4: e = configure_cpt<4, false>(); f = (const void*)k_pcg_cluster<4, false>; break;
+            default: e = configure_cpt<8, false>(); f = (const void*)k_pcg_cluster<8, false>; break;
+        }
+        // the paired variant (even ny) has the same block size and shared memory
+        if (e == cudaSuccess) {
+            switch (cpt_for((int)((cells + 1) / 2))) {
+                case 1: e = configure_cpt<1, true>(); break;
+                case 2: e = configure_cpt<2, true>(); break;
+                case 4: e = configure_cpt<4, true>(); break;
+                default: e = configure_cpt<8, true>(); break;
+            }
         }
         if (e != cudaSuccess) { cudaGetLastError(); continue; }
         e = cudaOccupancyMaxActiveClusters(&nclusters, f, &cfg);
@@ -838,11 +943,20 @@ cudaError_t pcg_launch(const PcgLaunch& L0, cudaStream_t s) {
     if (C < 1 || C > 16) return cudaErrorInvalidValue;
     const int rows = (L.op.nx + C - 1) / C;
     L.cap_cells = rows * L.op.ny;
+    if (L.op.ny % 2 == 0) {
+        switch (cpt_for((L.cap_cells + 1) / 2)) {
+            case 1: return launch_cpt<1, true>(L, C, s);
+            case 2: return launch_cpt<2, true>(L, C, s);
+            case 4: return launch_cpt<4, true>(L, C, s);
+            case 8: return launch_cpt<8, true>(L, C, s);
+            default: return cudaErrorInvalidValue;
+        }
+    }
     switch (cpt_for(L.cap_cells)) {
-        case 1: return launch_cpt<1>(L, C, s);
-        case 2: return launch_cpt<2>(L, C, s);
-        case 4: return launch_cpt<4>(L, C, s);
-        case 8: return launch_cpt<8>(L, C, s);
+        case 1: return launch_cpt<1, false>(L, C, s);
+        case 2: return launch_cpt<2, false>(L, C, s);
+        case 4: return launch_cpt<4, false>(L, C, s);
+        case 8: return launch_cpt<8, false>(L, C, s);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -1,0 +1,186 @@
+"""Learned Poisson preconditioner: kernels against PyTorch CPU, training, flexible CG (GPU).
+
+The CPU checker is PyTorch on the same BF16-rounded weights and activations: the
+forward pass must agree to BF16 resolution and every weight gradient of the
+hand-written backward kernels to a few percent (the kernels keep activations in
+BF16 and accumulate in FP32, the checker in FP32 throughout).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = [pytest.mark.gpu]
+
+
+@pytest.fixture(scope="module")
+def L(cuda_lib):
+    import torch
+
+    from cfd2d_b200 import _lib, learned
+
+    torch.manual_seed(0)
+    return torch, _lib, learned
+
+
+def relerr(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-30)
+
+
+def test_conv32_tensor_cores_match_torch(L):
+    torch, _lib, learned = L
+    F = torch.nn.functional
+    H, W = 7, 200  # one full and one partial 128-pixel tile per row
+    g = torch.Generator().manual_seed(1)
+    x = torch.randn((H, W, 32), generator=g).to(torch.bfloat16)
+    w = torch.randn((32, 32, 3, 3), generator=g) * 0.1
+    b = torch.randn(32, generator=g) * 0.1
+    skip = torch.randn((H, W, 32), generator=g).to(torch.bfloat16)
+    mask = (torch.rand((H, W), generator=g) > 0.2).to(torch.uint8)
+    dev = _lib.device()
+    img = torch.zeros(int(_lib.lib().cfd2d_lpc_w32_bytes()) // 2, dtype=torch.bfloat16, device=dev)
+    wd = w.to(dev).contiguous()
+    _lib.check(_lib.lib().cfd2d_lpc_pack_w32(_lib.ptr(wd), _lib.ptr(img), _lib.stream_ptr()), "pack")
+    xd, sd, md = x.to(dev), skip.to(dev), mask.to(dev)
+    y = torch.zeros((H, W, 32), dtype=torch.bfloat16, device=dev)
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    bd = b.to(dev)
+    _lib.check(_lib.lib().cfd2d_lpc_conv32(_lib.ptr(xd), _lib.ptr(img), _lib.ptr(bd), _lib.ptr(sd), _lib.ptr(md),
+                                           _lib.ptr(y), H, W, 1, _lib.ptr(err), _lib.stream_ptr()), "conv32")
+    assert int(err.item()) == 0
+    xin = x.float().permute(2, 0, 1)[None]
+    ref = F.conv2d(xin, w.to(torch.bfloat16).float(), b, padding=1)[0].permute(1, 2, 0)
+    ref = torch.relu(ref + skip.float()) * mask[..., None]
+    assert relerr(y.float().cpu(), ref.to(torch.bfloat16).float()) < 1e-2
+
+
+@pytest.mark.parametrize("cin,cout", [(1, 32), (32, 1), (32, 32)])
+def test_cuda_core_conv_and_adjoint(L, cin, cout):
+    torch, _lib, learned = L
+    F = torch.nn.functional
+    H, W = 9, 13
+    g = torch.Generator().manual_seed(cin * 100 + cout)
+    x = torch.randn((H, W, cin), generator=g)
+    w = torch.randn((cout, cin, 3, 3), generator=g) * 0.2
+    b = torch.randn(cout, generator=g)
+    dev = _lib.device()
+    y = torch.zeros((H, W, cout), device=dev)
+    xd, wd, bd = x.to(dev).contiguous(), w.to(dev).contiguous(), b.to(dev)
+    _lib.check(_lib.lib().cfd2d_lpc_conv(cin, cout, _lib.ptr(xd), 0, _lib.ptr(wd), _lib.ptr(bd), None, _lib.ptr(y), 0,
+                                         H, W, 0, 0, _lib.stream_ptr()), "conv")
+    ref = F.conv2d(x.permute(2, 0, 1)[None], w, b, padding=1)[0].permute(1, 2, 0)
+    assert relerr(y.cpu(), ref) < 1e-5
+    # adjoint: <conv(x), d> == <x, conv^T(d)>
+    d = torch.randn((H, W, cout), generator=g)
+    dx = torch.zeros((H, W, cin), device=dev)
+    dd = d.to(dev).contiguous()
+    _lib.check(_lib.lib().cfd2d_lpc_conv(cout, cin, _lib.ptr(dd), 0, _lib.ptr(wd), None, None, _lib.ptr(dx), 0,
+                                         H, W, 0, 1, _lib.stream_ptr()), "conv^T")
+    lhs = float(((ref - b) * d).sum())
+    rhs = float((x * dx.cpu()).sum())
+    assert abs(lhs - rhs) <= 1e-4 * max(abs(lhs), 1.0)
+
+
+def _random_mask(H, W, seed):
+    rng = np.random.default_rng(seed)
+    m = np.ones((H, W), dtype=np.uint8)
+    for _ in range(4):
+        i, j = rng.integers(0, H - 4), rng.integers(0, W - 4)
+        m[i:i + 4, j:j + 3] = 0
+    return m
+
+
+def test_network_forward_matches_torch(L):
+    torch, _lib, learned = L
+    H, W = 40, 37
+    net = learned.LPCNet(seed=3)
+    for name in net.b:
+        net.b[name].copy_(torch.randn_like(net.b[name]) * 0.05)
+    net.repack()
+    mask = _random_mask(H, W, 0)
+    ws = learned.Workspace(H, W, mask)
+    g = torch.Generator().manual_seed(4)
+    x = (torch.randn((H, W), generator=g) * torch.from_numpy(mask)).float()
+    out = learned.net_forward(net, ws, x.to(_lib.device()).contiguous()).cpu()
+    masks = [m.cpu().float()[None, None] for m in ws.masks]
+    ref = learned.torch_reference_forward(net, x, masks)
+    assert relerr(out, ref) < 3e-2
+
+
+def test_backward_kernels_match_autograd(L):
+    torch, _lib, learned = L
+    H, W = 24, 21
+    net = learned.LPCNet(seed=5)
+    mask = _random_mask(H, W, 1)
+    ws = learned.Workspace(H, W, mask)
+    g = torch.Generator().manual_seed(6)
+    x = (torch.randn((H, W), generator=g) * torch.from_numpy(mask)).float()
+    dout = torch.randn((H, W), generator=g) * torch.from_numpy(mask)
+    learned.net_forward(net, ws, x.to(_lib.device()).contiguous())
+    grads = learned.net_backward(net, ws, x.to(_lib.device()).contiguous(), dout.to(_lib.device()).contiguous())
+    # autograd on the CPU reference with leaf copies of the BF16-rounded weights
+    masks = [m.cpu().float()[None, None] for m in ws.masks]
+    saved = {k: (v.clone(), net.b[k].clone()) for k, v in net.w.items()}
+    leaf_w = {k: net.wq(k).cpu().requires_grad_(True) for k in net.w}
+    leaf_b = {k: net.b[k].detach().cpu().clone().requires_grad_(True) for k in net.b}
+
+    class Shim:
+        w = leaf_w
+        b = leaf_b
+
+        @staticmethod
+        def wq(name):
+            return leaf_w[name]
+
+    out = learned.torch_reference_forward(Shim, x, masks)
+    (out * dout).sum().backward()
+    for name in net.w:
+        gw, gb = grads[name]
+        assert relerr(gw.cpu(), leaf_w[name].grad) < 5e-2, name
+        if leaf_b[name].grad.abs().max() > 0:
+            assert relerr(gb.cpu(), leaf_b[name].grad) < 5e-2, name
+    for k, (w_, b_) in saved.items():
+        assert torch.equal(net.w[k], w_) and torch.equal(net.b[k], b_)
+
+
+def test_flexible_cg_reaches_tolerance_and_matches_plain_cg(L):
+    torch, _lib, learned = L
+    rng = np.random.default_rng(7)
+    case = learned.obstacle_case(rng, 256, 128)
+    sim = case.sim
+    sim.advance(2)
+    g = sim.grid
+    F, G = sim.F, sim.G
+    rhs = ((F[1:, 1:-1] - F[:-1, 1:-1]) / g.dx + (G[1:-1, 1:] - G[1:-1, :-1]) / g.dy) / sim.dt
+    ps = sim.pressure
+    # both solvers from a cold start (the warm start after a step already solves
+    # this right-hand side) to a tight relative residual
+    ps.tol = 1e-9
+    zero = np.zeros(int(ps.fluid.sum()))
+    ps._x0 = zero
+    p_plain = ps.solve(rhs)
+    assert ps.last_iterations > 0
+    ps._x0 = zero
+    net = learned.LPCNet(seed=0)
+    fcg = learned.LearnedPCG(ps, net)
+    p_fcg = fcg.solve(rhs)
+    assert fcg.last_total_iterations > 0
+    assert relerr(p_fcg, p_plain) < 1e-4
+    # the stop test is the plain solver's, ||r|| < tol ||b|| on the recursively
+    # updated residual; the true residual of the final iterate is within 2x of it
+    A = ps.A
+    b = -rhs[ps.fluid]
+    x = ps._x0
+    assert np.linalg.norm(b - A @ x) <= 2e-9 * np.linalg.norm(b)
+
+
+def test_training_reduces_the_loss(L):
+    torch, _lib, learned = L
+    R, E, M = learned.harvest_pairs(n_cases=3, nx=128, ny=64, seed=1, every=6, max_snaps=40)
+    assert R.shape[0] >= 20 and R.shape[1:] == (128, 64)
+    net = learned.LPCNet(seed=1)
+    log = learned.train(net, R, E, M, steps=120, batch=2, lr=2e-3, log_every=0)
+    assert np.mean(log[-20:]) < 0.8 * np.mean(log[:20])
