@@ -128,6 +128,7 @@ def lib():
         "cfd2d_pcg_workspace_bytes": ([i, i], sz),
         "cfd2d_pcg_plan": ([i, i, C.POINTER(C.c_int)], i),
         "cfd2d_pressure_solve": ([vp, vp, vp, d, i, vp, vp, vp], i),
+        "cfd2d_pressure_solve_static": ([vp, vp, vp, d, i, vp, vp, vp], i),
         "cfd2d_sim_scratch_doubles": ([i, i], sz),
         "cfd2d_sim_apply_bc": ([vp, vp], i),
         "cfd2d_sim_project_initial": ([vp, vp], i),
@@ -191,6 +192,7 @@ def exported_symbols():
         "cfd2d_lpc_upadd_bwd", "cfd2d_lpc_pool_bwd", "cfd2d_lpc_conv_dw_partial_floats", "cfd2d_lpc_conv_dw",
         "cfd2d_fcg_partial_doubles", "cfd2d_fcg_init", "cfd2d_fcg_pq", "cfd2d_fcg_update", "cfd2d_fcg_zr",
         "cfd2d_fcg_dir", "cfd2d_fcg_net_in", "cfd2d_fcg_net_out", "cfd2d_fcg_scatter_p",
+        "cfd2d_pressure_solve_static",
     ]
 
 

@@ -304,6 +304,27 @@ int cfd2d_pressure_solve_snapshots(const cfd2d_poisson* op, const double* rhs, d
                                    int maxiter, double* snap, int every, int max_snaps, int32_t* iters_out,
                                    int32_t* status_out, void* stream);
 
+/* ---- pressure solve without device allocation (no counterpart in the reference)
+ *
+ * For callers that cannot provide cfd2d_poisson.work: a C or ctypes host that owns
+ * no device allocator, or a time loop that must not call cudaMalloc/cudaFree
+ * between steps (both can synchronise the device). Same arguments, results and
+ * error codes as cfd2d_pressure_solve, always on the grid-persistent solver
+ * (op->cluster and op->work are ignored); its scratch is a static device array of
+ * the library (8.2 MiB per device), so nothing is allocated.
+ *  - Grids above CFD2D_STATIC_MAX_CELLS cells return CFD2D_E_CAPACITY.
+ *  - The first call on each device looks the array up (cudaGetSymbolAddress, which
+ *    can load the library's module on that device): make it outside any stream
+ *    capture, with that device current.
+ *  - Nothing has to start at zero: each call clears the solver's barrier words on
+ *    `stream` before its launch, and the solver writes the rest before reading it.
+ *  - All calls on one device share the array: two calls whose kernels can overlap
+ *    (different streams with no ordering between them) race on it and give wrong
+ *    results. Order them on one stream or with events. */
+#define CFD2D_STATIC_MAX_CELLS 262144 /* e.g. 512 x 512 */
+int cfd2d_pressure_solve_static(const cfd2d_poisson* op, const double* rhs, double* p, double rtol,
+                                int maxiter, int32_t* iters_out, int32_t* status_out, void* stream);
+
 /* ---- learned Poisson preconditioner (no counterpart in the reference) ---- */
 /* Activations: BF16, NHWC with 32 channels, pixel = cell (i, j) at i*W + j. */
 
