@@ -211,6 +211,74 @@ def run_reference(args, dist, rank, world):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------------ stencil roofline
+STENCIL_NX, STENCIL_NY = 4096, 2048
+# compulsory FP64 traffic per cell (each array read or written once; flags 1 B)
+STENCIL_BYTES = {
+    "momentum_tendencies": 8 + 8 + 1 + 8 + 8,          # R u, v, fluid; W hu, hv (constant nu)
+    "scalar_transport": 8 + 8 + 8 + 8 + 1 + 8,         # R phi, u, v, D, fluid; W out
+}
+
+
+def stencil_roofline(peak: float, reps: int = 10) -> dict:
+    """The kernel-level drop-ins (cfd2d/kernels.py entry points; van Leer for the
+    scalar) on a 4096 x 2048 grid with random solid cells: event-timed per launch
+    with L2 flushed before each launch, achieved GB/s from the compulsory bytes
+    above."""
+    import numpy as np
+    import torch
+
+    from cfd2d_b200 import _lib
+
+    L = _lib.lib()
+    nx, ny = STENCIL_NX, STENCIL_NY
+    dev = _lib.device()
+    g = torch.Generator(device=dev).manual_seed(0)
+    u = torch.rand((nx + 1, ny + 2), dtype=torch.float64, device=dev, generator=g)
+    v = torch.rand((nx + 2, ny + 1), dtype=torch.float64, device=dev, generator=g) - 0.5
+    fluid = (torch.rand((nx + 2, ny + 2), device=dev, generator=g) > 0.05).to(torch.uint8)
+    fluid[0, :] = 0
+    fluid[-1, :] = 0
+    fluid[:, 0] = 0
+    fluid[:, -1] = 0
+    phi = torch.rand((nx + 2, ny + 2), dtype=torch.float64, device=dev, generator=g)
+    diff = torch.full((nx + 2, ny + 2), 1e-3, dtype=torch.float64, device=dev)
+    out = torch.zeros_like(phi)
+    hu, hv = torch.zeros_like(u), torch.zeros_like(v)
+    nu = torch.full((1,), 1e-3, dtype=torch.float64, device=dev)
+    bt = {k: torch.zeros(n, dtype=torch.int64, device=dev) for k, n in (("l", ny), ("r", ny), ("b", nx), ("t", nx))}
+    bv = {k: torch.zeros(n, dtype=torch.float64, device=dev) for k, n in (("l", ny), ("r", ny), ("b", nx), ("t", nx))}
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    P = _lib.ptr
+    sp = _lib.stream_ptr()
+    dx, dy = 1.0 / nx, 0.5 / ny
+    calls = {
+        "momentum_tendencies": lambda: L.cfd2d_momentum_tendencies(
+            P(u), P(v), P(fluid), nx, ny, dx, dy, P(nu), 0, 0.1, 0, P(hu), P(hv), None, 0, sp),
+        "scalar_transport": lambda: L.cfd2d_scalar_transport(
+            P(phi), P(u), P(v), P(fluid), nx, ny, dx, dy, P(diff), 1, 0, P(bt["l"]), P(bv["l"]), P(bt["r"]),
+            P(bv["r"]), P(bt["b"]), P(bv["b"]), P(bt["t"]), P(bv["t"]), 0, 0.0, P(out), sp),
+    }
+    res = {}
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    for name, fn in calls.items():
+        _lib.check(fn(), name)
+        ms = []
+        for _ in range(reps):
+            flush.fill_(1.0)
+            ev[0].record()
+            _lib.check(fn(), name)
+            ev[1].record()
+            torch.cuda.synchronize()
+            ms.append(ev[0].elapsed_time(ev[1]))
+        med = float(np.median(ms))
+        gbs = STENCIL_BYTES[name] * nx * ny / (med * 1e-3) / 1e9
+        res[name] = {"ms": med, "bytes_per_cell": STENCIL_BYTES[name], "achieved_gbs": gbs, "frac": gbs / peak}
+    del u, v, fluid, phi, diff, out, hu, hv, flush
+    torch.cuda.empty_cache()
+    return {"grid": [nx, ny], "l2": "flushed before each launch", **res}
+
+
 # ------------------------------------------------------------------ GPU arm
 def run_b200(args, dist, rank, world):
     import numpy as np
@@ -316,6 +384,7 @@ def run_b200(args, dist, rank, world):
 
     if rank != 0:
         return
+    stencils = stencil_roofline(peak) if not args.no_stencils else None
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         d = cpu_oracle_rate(3, 1, 1)
@@ -341,6 +410,7 @@ def run_b200(args, dist, rank, world):
                      "kernel": "k_pcg_cluster (on-chip FP64 Jacobi-PCG)", "peak_kind": peak_kind},
         "cpu_baseline": cpu,
         "clocks": clocks,
+        "stencils": stencils,
     }
     print(json.dumps(line), flush=True)
 
@@ -352,6 +422,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-stencils", action="store_true", help="skip the stencil-kernel roofline section")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -98,6 +98,15 @@ class FcgScalars(C.Structure):
                 ("rr", C.c_double), ("bb", C.c_double), ("iters", C.c_int32), ("ticket", C.c_uint32)]
 
 
+class FcgControl(C.Structure):
+    _fields_ = [("rtol", C.c_double), ("stall_factor", C.c_double), ("stall_window", C.c_int32),
+                ("maxiter", C.c_int32), ("reason", C.c_int32), ("iters", C.c_int32), ("calls", C.c_int32),
+                ("pad", C.c_int32), ("hist", C.c_void_p)]
+
+
+FCG_RUNNING, FCG_CONVERGED, FCG_MAXITER, FCG_STALLED, FCG_NONFINITE = 0, 1, 2, 3, 4
+
+
 _LIB = None
 
 
@@ -159,13 +168,21 @@ def lib():
         "cfd2d_lpc_conv_dw_partial_floats": ([i, i, i, i, i], sz),
         "cfd2d_lpc_conv_dw": ([i, i, vp, i, vp, i, i, i, vp, vp, vp], i),
         "cfd2d_fcg_partial_doubles": ([i], sz),
-        "cfd2d_fcg_init": ([vp, vp, vp, vp, d, d, vp, vp, vp, vp, vp, vp, vp], i),
+        "cfd2d_fcg_init": ([vp, vp, vp, vp, d, d, vp, vp, vp, vp, vp, vp, vp, vp], i),
         "cfd2d_fcg_pq": ([vp, vp, vp, vp, vp, vp], i),
         "cfd2d_fcg_update": ([i, vp, vp, vp, vp, vp, vp, vp, vp], i),
         "cfd2d_fcg_zr": ([i, vp, vp, vp, i, vp, vp, vp], i),
         "cfd2d_fcg_dir": ([i, vp, vp, vp, vp], i),
         "cfd2d_fcg_net_in": ([i, vp, vp, vp, vp, vp], i),
-        "cfd2d_fcg_net_out": ([i, vp, vp, vp, vp, vp, d, vp, vp], i),
+        "cfd2d_fcg_net_out": ([i, vp, vp, vp, vp, vp, d, d, vp, vp], i),
+        "cfd2d_fcg_gate": ([vp, vp, C.c_uint64, vp], i),
+        "cfd2d_fcg_zero_rhs": ([i, vp, vp, vp, vp], i),
+        "cfd2d_capture_begin": ([vp], i),
+        "cfd2d_capture_condition": ([vp, vp], i),
+        "cfd2d_capture_while_begin": ([vp, vp, C.c_uint64], i),
+        "cfd2d_capture_while_end": ([vp], i),
+        "cfd2d_capture_end": ([vp, vp], i),
+        "cfd2d_capture_abort": ([vp], i),
         "cfd2d_fcg_scatter_p": ([vp, vp, vp, vp], i),
     }
     for name, (args, res) in sig.items():
@@ -192,7 +209,9 @@ def exported_symbols():
         "cfd2d_lpc_upadd_bwd", "cfd2d_lpc_pool_bwd", "cfd2d_lpc_conv_dw_partial_floats", "cfd2d_lpc_conv_dw",
         "cfd2d_fcg_partial_doubles", "cfd2d_fcg_init", "cfd2d_fcg_pq", "cfd2d_fcg_update", "cfd2d_fcg_zr",
         "cfd2d_fcg_dir", "cfd2d_fcg_net_in", "cfd2d_fcg_net_out", "cfd2d_fcg_scatter_p",
-        "cfd2d_pressure_solve_static",
+        "cfd2d_pressure_solve_static", "cfd2d_fcg_gate", "cfd2d_fcg_zero_rhs", "cfd2d_capture_begin",
+        "cfd2d_capture_condition", "cfd2d_capture_while_begin", "cfd2d_capture_while_end", "cfd2d_capture_end",
+        "cfd2d_capture_abort",
     ]
 
 

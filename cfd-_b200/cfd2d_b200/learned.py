@@ -16,10 +16,18 @@ FP32 accumulation, 65,025 parameters):
 Every layer output is multiplied by the fluid mask of its level. The 32->32
 layers run on tcgen05 (``cfd2d_lpc_conv32``); the 1-channel layers, pooling,
 upsampling and the whole backward pass are hand-written CUDA-core kernels of the
-same library. Training uses these kernels through ``torch.autograd.Function``; the
-optimiser (Adam) is PyTorch's. The preconditioner applied inside flexible CG is
-M(r) = ||r|| * net(r / ||r||) + omega * D^-1 r; flexible CG (Polak-Ribiere) falls
-back to the plain Jacobi-PCG when it stalls.
+same library (``net_forward`` / ``net_backward``); the optimiser (Adam) is
+PyTorch's, on FP32 master weights.
+
+The network works on the dimensionless operator Ah = h^2 A (h^2 = 2 / (1/dx^2 +
+1/dy^2)), so one set of weights serves every grid spacing: for a residual r it
+approximates Ah^-1 (r / ||r||). Training minimises the energy-norm error of that
+approximation, (e - o)^T Ah (e - o) with e = Ah^-1 r_hat, i.e. o^T Ah o - 2 o.r_hat
+(the constant e^T Ah e dropped), over residuals harvested from the plain solver's
+own iterations. Inside flexible CG (Polak-Ribiere) the preconditioner is
+M(r) = h^2 ||r|| net(r / ||r||) + omega D^-1 r; the loop runs on the device inside
+one CUDA graph (a WHILE node) and falls back to the plain Jacobi-PCG from the
+current iterate when it stalls.
 """
 
 from __future__ import annotations
@@ -66,6 +74,7 @@ class LPCNet:
             self.w[name] = (t.randn((cout, cin, 3, 3), generator=g) * std).to(_lib.device())
             self.b[name] = t.zeros(cout, device=_lib.device())
         self._images = {}
+        self._wq = {}
         self.repack()
 
     @property
@@ -79,11 +88,19 @@ class LPCNet:
         return out
 
     def repack(self):
-        """BF16 weights: round the masters and pack the tensor-core images."""
+        """BF16 weights: round the masters and pack the tensor-core images. The
+        images and the rounded CUDA-core weights are updated in place, so graphs
+        captured with them stay valid."""
         t = _t()
         L = _lib.lib()
         nbytes = int(L.cfd2d_lpc_w32_bytes())
         for name, cin, cout, _lvl, _relu in LAYERS:
+            if not (cin == CH and cout == CH):
+                q = self.wq(name)
+                if name in self._wq:
+                    self._wq[name].copy_(q)
+                else:
+                    self._wq[name] = q
             if cin == CH and cout == CH:
                 img = self._images.get(name)
                 if img is None:
@@ -157,7 +174,7 @@ def net_forward(net: LPCNet, ws: Workspace, x_in):
         _lib.check(rc, "lpc_conv32")
 
     H, W = sh[0]
-    _lib.check(L.cfd2d_lpc_conv(1, CH, P(x_in), 0, P(net.wq("a0")), P(net.b["a0"]), P(ws.masks[0]), P(ws.a["a0"]),
+    _lib.check(L.cfd2d_lpc_conv(1, CH, P(x_in), 0, P(net._wq["a0"]), P(net.b["a0"]), P(ws.masks[0]), P(ws.a["a0"]),
                                 1, H, W, 1, 0, s), "lpc_conv a0")
     conv32("a0b", ws.a["a0"], 0)
     prev = ws.a["a0b"]
@@ -171,7 +188,7 @@ def net_forward(net: LPCNet, ws: Workspace, x_in):
         _lib.check(L.cfd2d_lpc_upadd(P(prev), P(ws.a[skip]), P(ws.up[lvl]), h, w, s), "upadd")
         conv32(name, ws.up[lvl], lvl)
         prev = ws.a[name]
-    _lib.check(L.cfd2d_lpc_conv(CH, 1, P(prev), 1, P(net.wq("out")), P(net.b["out"]), P(ws.masks[0]), P(ws.out),
+    _lib.check(L.cfd2d_lpc_conv(CH, 1, P(prev), 1, P(net._wq["out"]), P(net.b["out"]), P(ws.masks[0]), P(ws.out),
                                 0, H, W, 0, 0, s), "lpc_conv out")
     return ws.out
 
@@ -288,39 +305,53 @@ def torch_reference_forward(net: LPCNet, x_in, masks):
 
 
 # ------------------------------------------------------------------ flexible CG
+def h2_of(pressure) -> float:
+    """h^2 of the dimensionless operator: 2 / (1/dx^2 + 1/dy^2)."""
+    return 2.0 / (pressure.dx2 + pressure.dy2)
+
+
 class LearnedPCG:
     """Flexible CG with the learned preconditioner for one PressureSolver's operator.
 
     solve(rhs) mirrors PressureSolver.solve on domains with an outflow (Dirichlet)
-    boundary: same operator, warm start, stop test ||r|| < tol ||b||. If the
-    residual fails to fall by ``stall_factor`` over ``stall_window`` iterations,
-    the solve continues with the plain Jacobi-PCG from the current iterate.
+    boundary: same operator, warm start (the solver's x0, updated in place), stop
+    test ||r|| < tol ||b||. If the residual fails to fall by ``stall_factor`` over
+    ``stall_window`` iterations, the solve continues with the plain Jacobi-PCG from
+    the current iterate.
     """
 
-    def __init__(self, pressure, net: LPCNet, omega: float = 0.6, stall_window: int = 20,
-                 stall_factor: float = 0.5, maxiter: int = 2000):
+    def __init__(self, pressure, net: LPCNet, omega: float = 0.5, stall_window: int = 30,
+                 stall_factor: float = 0.7, maxiter: int = 2000):
         t = _t()
         if pressure.neumann_components:
             raise ValueError("the learned preconditioner path needs an outflow (Dirichlet) boundary")
         self.ps, self.net = pressure, net
         self.omega, self.stall_window, self.stall_factor = omega, stall_window, stall_factor
         self.maxiter = maxiter
+        self.h2 = h2_of(pressure)
         g = pressure.grid
         self.nx, self.ny = g.nx, g.ny
         n = self.nx * self.ny
         dev = _lib.device()
         z = lambda: t.zeros(n, dtype=t.float64, device=dev)  # noqa: E731
         self.b, self.r, self.r_old, self.p, self.q, self.z = z(), z(), z(), z(), z(), z()
+        self.rhs_buf = z()
         self.net_in = t.zeros((self.nx, self.ny), dtype=t.float32, device=dev)
         self.partial = t.zeros(int(_lib.lib().cfd2d_fcg_partial_doubles(n)), dtype=t.float64, device=dev)
         self.scal = t.zeros(C.sizeof(_lib.FcgScalars) // 8, dtype=t.float64, device=dev)
         self.mask = pressure._d_nbr.view(self.nx, self.ny) >= 0x80
         self.mask_u8 = self.mask.to(t.uint8).contiguous()
         self.ws = Workspace(self.nx, self.ny, self.mask_u8)
+        self.hist = t.zeros(maxiter + 1, dtype=t.float64, device=dev)
+        self.ctl = t.zeros(C.sizeof(_lib.FcgControl), dtype=t.uint8, device=dev)
+        self._graphs = {}
         self.last_iterations = 0
+        self.last_total_iterations = 0
         self.last_fallback = False
+        self.last_reason = 0
         self.history = []
 
+    # ---------------------------------------------------------------- pieces
     def _scalars(self):
         raw = self.scal.cpu().numpy().tobytes()
         return _lib.FcgScalars.from_buffer_copy(raw)
@@ -333,62 +364,114 @@ class LearnedPCG:
         _lib.check(L.cfd2d_fcg_net_in(n, P(self.r), P(self.scal), P(self.mask_u8), P(self.net_in), s), "net_in")
         out = net_forward(self.net, self.ws, self.net_in)
         _lib.check(L.cfd2d_fcg_net_out(n, P(out), P(self.r), P(self.ps._d_dinv), P(self.mask_u8), P(self.scal),
-                                       self.omega, P(self.z), s), "net_out")
+                                       self.h2, self.omega, P(self.z), s), "net_out")
 
-    def solve_into_x(self, rhs=None, F=None, G=None, dx=1.0, dy=1.0, dt_ptr=None, tol=None):
-        """Run FCG on x = pressure x0 (in place). Returns the iteration count."""
+    def _init(self, rhs=None, F=None, G=None, dx=1.0, dy=1.0, dt_ptr=None):
+        P = _lib.ptr
+        _lib.check(_lib.lib().cfd2d_fcg_init(C.byref(self.ps.op), P(F), P(G), P(rhs), dx, dy, dt_ptr, P(self.b),
+                                             P(self.ps._d_x0.view(-1)), P(self.r), P(self.p), P(self.scal),
+                                             P(self.partial), _lib.stream_ptr()), "fcg_init")
+
+    def _body(self, handle: int):
+        """One iteration: z = M(r), beta, p = z + beta p, q = A p, x and r update, gate."""
         L = _lib.lib()
         s = _lib.stream_ptr()
         P = _lib.ptr
         n = self.nx * self.ny
         op = C.byref(self.ps.op)
-        x = self.ps._d_x0.view(-1)
-        tol = self.ps.rtol if tol is None else tol
-        _lib.check(L.cfd2d_fcg_init(op, P(F), P(G), P(rhs), dx, dy, dt_ptr, P(self.b), P(x), P(self.r),
-                                    P(self.scal), P(self.partial), s), "fcg_init")
-        st = self._scalars()
-        atol = tol * math.sqrt(st.bb)
-        self.history = [math.sqrt(st.rr)]
-        self.last_fallback = False
-        if st.bb == 0.0:
-            x.copy_(self.b)
-            self.last_iterations = 0
-            return 0
-        it = 0
         self.precondition()
-        _lib.check(L.cfd2d_fcg_zr(n, P(self.z), P(self.r), P(self.r_old), 1, P(self.scal), P(self.partial), s), "zr")
-        self.p.copy_(self.z)
-        while math.sqrt(st.rr) >= atol and it < self.maxiter:
-            _lib.check(L.cfd2d_fcg_pq(op, P(self.p), P(self.q), P(self.scal), P(self.partial), s), "pq")
-            _lib.check(L.cfd2d_fcg_update(n, P(x), P(self.r), P(self.r_old), P(self.p), P(self.q), P(self.scal),
-                                          P(self.partial), s), "update")
-            it += 1
-            st = self._scalars()
-            res = math.sqrt(st.rr)
-            self.history.append(res)
-            if not math.isfinite(res):
-                raise FloatingPointError("flexible CG produced a non-finite residual")
-            if res < atol:
-                break
-            k = len(self.history) - 1
-            if k >= self.stall_window and res > self.stall_factor * self.history[k - self.stall_window]:
-                self.last_fallback = True
-                break
-            self.precondition()
-            _lib.check(L.cfd2d_fcg_zr(n, P(self.z), P(self.r), P(self.r_old), 0, P(self.scal), P(self.partial), s),
-                       "zr")
-            _lib.check(L.cfd2d_fcg_dir(n, P(self.z), P(self.p), P(self.scal), s), "dir")
-        self.last_iterations = it
-        return it
+        _lib.check(L.cfd2d_fcg_zr(n, P(self.z), P(self.r), P(self.r_old), -1, P(self.scal), P(self.partial), s), "zr")
+        _lib.check(L.cfd2d_fcg_dir(n, P(self.z), P(self.p), P(self.scal), s), "dir")
+        _lib.check(L.cfd2d_fcg_pq(op, P(self.p), P(self.q), P(self.scal), P(self.partial), s), "pq")
+        _lib.check(L.cfd2d_fcg_update(n, P(self.ps._d_x0.view(-1)), P(self.r), P(self.r_old), P(self.p), P(self.q),
+                                      P(self.scal), P(self.partial), s), "update")
+        _lib.check(L.cfd2d_fcg_gate(P(self.scal), P(self.ctl), handle, s), "gate")
 
-    def solve(self, rhs):
+    def _set_control(self, tol):
+        t = _t()
+        c = _lib.FcgControl(rtol=tol, stall_factor=self.stall_factor, stall_window=self.stall_window,
+                            maxiter=self.maxiter, reason=0, iters=0, calls=0, pad=0, hist=self.hist.data_ptr())
+        host = t.frombuffer(bytearray(bytes(c)), dtype=t.uint8)
+        self.ctl.copy_(host)
+
+    def _control(self):
+        return _lib.FcgControl.from_buffer_copy(self.ctl.cpu().numpy().tobytes())
+
+    # ---------------------------------------------------------------- solves
+    def solve_into_x_host(self, rhs=None, F=None, G=None, dx=1.0, dy=1.0, dt_ptr=None, tol=None):
+        """The same iteration driven from the host (one launch sequence and one scalar
+        read per iteration); kept as the reference for the graph-driven loop."""
+        tol = self.ps.rtol if tol is None else tol
+        self._set_control(tol)
+        self._init(rhs, F, G, dx, dy, dt_ptr)
+        _lib.check(_lib.lib().cfd2d_fcg_gate(_lib.ptr(self.scal), _lib.ptr(self.ctl), 0, _lib.stream_ptr()), "gate")
+        while self._control().reason == _lib.FCG_RUNNING:
+            self._body(0)
+        return self._finish()
+
+    def _graph(self, key, rhs=None, F=None, G=None, dx=1.0, dy=1.0, dt_ptr=None):
+        """Graph of one whole solve: init, gate, WHILE(body), zero-rhs fix."""
+        g = self._graphs.get(key)
+        if g is not None:
+            return g
+        t = _t()
+        L = _lib.lib()
+        main, body = t.cuda.Stream(), t.cuda.Stream()
+        main.wait_stream(t.cuda.current_stream())
+        n = self.nx * self.ny
+        graph = C.c_void_p()
+        with t.cuda.stream(main):
+            mp = C.c_void_p(main.cuda_stream)
+            _lib.check(L.cfd2d_capture_begin(mp), "capture_begin")
+            try:
+                self._init(rhs, F, G, dx, dy, dt_ptr)
+                h = C.c_uint64()
+                _lib.check(L.cfd2d_capture_condition(mp, C.byref(h)), "capture_condition")
+                _lib.check(L.cfd2d_fcg_gate(_lib.ptr(self.scal), _lib.ptr(self.ctl), h.value, mp), "gate")
+                _lib.check(L.cfd2d_capture_while_begin(mp, C.c_void_p(body.cuda_stream), h.value), "while_begin")
+                with t.cuda.stream(body):
+                    self._body(h.value)
+                _lib.check(L.cfd2d_capture_while_end(C.c_void_p(body.cuda_stream)), "while_end")
+                _lib.check(L.cfd2d_fcg_zero_rhs(n, _lib.ptr(self.b), _lib.ptr(self.ps._d_x0.view(-1)),
+                                                _lib.ptr(self.scal), mp), "zero_rhs")
+                _lib.check(L.cfd2d_capture_end(mp, C.byref(graph)), "capture_end")
+            except Exception:
+                L.cfd2d_capture_abort(C.c_void_p(body.cuda_stream))
+                L.cfd2d_capture_abort(mp)
+                raise
+        self._graphs[key] = graph
+        return graph
+
+    def solve_into_x(self, rhs=None, F=None, G=None, dx=1.0, dy=1.0, dt_ptr=None, tol=None, key=None):
+        """Run the graph-driven FCG on x = pressure x0 (in place). Returns the iteration count."""
+        tol = self.ps.rtol if tol is None else tol
+        self._set_control(tol)
+        graph = self._graph(key if key is not None else ("rhs", _lib.ptr(rhs).value if rhs is not None else 0),
+                            rhs, F, G, dx, dy, dt_ptr)
+        _lib.check(_lib.lib().cfd2d_graph_launch(graph, _lib.stream_ptr()), "graph_launch")
+        return self._finish()
+
+    def _finish(self):
+        c = self._control()
+        self.last_reason = c.reason
+        self.last_iterations = c.iters
+        self.last_fallback = c.reason == _lib.FCG_STALLED
+        self.history = self.hist[: c.iters + 1].cpu().numpy().tolist()
+        if c.reason == _lib.FCG_NONFINITE:
+            raise FloatingPointError("flexible CG produced a non-finite residual")
+        return c.iters
+
+    def solve(self, rhs, graph: bool = True):
         """Lap(p) = rhs (same conventions as PressureSolver.solve); host or device rhs."""
         t = _t()
         host = not isinstance(rhs, t.Tensor)
-        r = _lib.to_dev(rhs, t.float64).reshape(-1)
-        self.solve_into_x(rhs=r)
+        self.rhs_buf.copy_(_lib.to_dev(rhs, t.float64).reshape(-1))
+        if graph:
+            self.solve_into_x(rhs=self.rhs_buf)
+        else:
+            self.solve_into_x_host(rhs=self.rhs_buf)
         extra = 0
-        if self.last_fallback:
+        if self.last_reason in (_lib.FCG_STALLED, _lib.FCG_MAXITER):
             # continue with the plain Jacobi-PCG from the current iterate
             self.ps.solve(rhs)
             extra = self.ps.last_iterations
@@ -396,6 +479,11 @@ class LearnedPCG:
         out[~self.mask] = 0.0
         self.last_total_iterations = self.last_iterations + extra
         return out.cpu().numpy() if host else out
+
+    def close(self):
+        for g in self._graphs.values():
+            _lib.lib().cfd2d_graph_destroy(g)
+        self._graphs.clear()
 
 
 # ------------------------------------------------------------------ data and training
@@ -427,14 +515,28 @@ def obstacle_case(rng, nx: int, ny: int, pressure_solver: str = "cg"):
                                   inflow_profile="uniform", walls="slip", pressure_solver=pressure_solver)
 
 
-def harvest_pairs(n_cases: int = 100, nx: int = 256, ny: int = 128, seed: int = 0, steps: int = 3,
-                  every: int = 8, max_snaps: int = 100, rtol: float = 1e-11):
-    """Residual -> error pairs from the solver's own runs.
+class TrainingSet:
+    """Normalised residuals r_k / ||r_k|| (FP32, (N, H, W), on the device), the case
+    each one belongs to, and per case the pressure operator (for Ah o in the loss),
+    its h^2 and its fluid mask."""
+
+    def __init__(self, R, case_of, solvers, masks):
+        self.R, self.case_of, self.solvers, self.masks = R, case_of, solvers, masks
+        self.h2 = [h2_of(ps) for ps in solvers]
+
+    def __len__(self):
+        return int(self.R.shape[0])
+
+
+def harvest_residuals(n_cases: int = 24, nx: int = 256, ny: int = 128, seed: int = 0, steps: int = 3,
+                      every: int = 8, max_snaps: int = 100, rtol: float = 1e-11) -> TrainingSet:
+    """Residuals from the solver's own runs.
 
     For each seeded obstacle case: a few projection steps, then the pressure system
-    of the next predictor solved from zero by the plain Jacobi-PCG with iterate
-    snapshots; each snapshot x_k gives e_k = x* - x_k and r_k = A e_k. Returns FP32
-    tensors R, E (normalised by ||r_k||) and the fluid masks, on the device.
+    of the next predictor solved from zero by the plain Jacobi-PCG (grid solver) with
+    iterate snapshots; each snapshot x_k gives the residual r_k = A (x* - x_k) of an
+    iterate the preconditioner will meet. Later snapshots are dominated by the smooth
+    error modes Jacobi-PCG is slow on.
     """
     import os
 
@@ -443,8 +545,8 @@ def harvest_pairs(n_cases: int = 100, nx: int = 256, ny: int = 128, seed: int = 
     t = _t()
     L = _lib.lib()
     rng = np.random.default_rng(seed)
-    Rs, Es, Ms = [], [], []
-    for _ in range(n_cases):
+    Rs, case_of, solvers, masks = [], [], [], []
+    for ci in range(n_cases):
         case = obstacle_case(rng, nx, ny)
         sim = case.sim
         sim.pressure.tol = 1e-8
@@ -470,8 +572,8 @@ def harvest_pairs(n_cases: int = 100, nx: int = 256, ny: int = 128, seed: int = 
                                                     _lib.ptr(snap), every, max_snaps, _lib.ptr(ps._d_iters),
                                                     _lib.ptr(st), _lib.stream_ptr()), "snapshots")
         its = int(ps._d_iters[0].item())
-        xstar = ps._d_x0.view(-1)
-        mask = (ps._d_nbr >= 0x80).to(t.uint8).contiguous()
+        xstar = ps._d_x0.view(-1).clone()
+        mask = (ps._d_nbr >= 0x80).to(t.uint8).contiguous().view(nx, ny)
         k = min(max_snaps, its // every)
         for s_ in range(k):
             e = xstar - snap[s_]
@@ -482,40 +584,64 @@ def harvest_pairs(n_cases: int = 100, nx: int = 256, ny: int = 128, seed: int = 
             if rn == 0.0 or not math.isfinite(rn):
                 continue
             Rs.append((r / rn).float().view(nx, ny))
-            Es.append((e / rn).float().view(nx, ny))
-            Ms.append(mask)
-    return t.stack(Rs), t.stack(Es), Ms
+            case_of.append(ci)
+        solvers.append(ps)
+        masks.append(mask)
+    return TrainingSet(t.stack(Rs), case_of, solvers, masks)
 
 
-def train(net: LPCNet, R, E, masks, steps: int = 1000, batch: int = 4, lr: float = 1e-3, seed: int = 0,
-          log_every: int = 100, time_budget_s: float | None = None):
-    """Fit net(r) ~ e (relative L2 over the fluid cells) with the project's forward and
-    backward kernels; Adam on FP32 master weights, BF16 copies repacked every step."""
+def energy_loss_grad(ps, h2: float, out, r_hat):
+    """Energy-norm loss o^T Ah o - 2 o.r_hat of one sample and its gradient
+    2 (Ah o - r_hat), with Ah = h^2 A applied by the solver's FP64 operator."""
+    t = _t()
+    o = out.reshape(-1).double()
+    Ao = t.empty_like(o)
+    _lib.check(_lib.lib().cfd2d_poisson_matvec(C.byref(ps.op), _lib.ptr(o), _lib.ptr(Ao), _lib.stream_ptr()),
+               "matvec")
+    Ao.mul_(h2)
+    rh = r_hat.reshape(-1).double()
+    loss = t.dot(o, Ao) - 2.0 * t.dot(o, rh)
+    grad = (2.0 * (Ao - rh)).float().view_as(out)
+    return loss, grad
+
+
+def train(net: LPCNet, data: TrainingSet, steps: int = 1000, batch: int = 4, lr: float = 1e-3, seed: int = 0,
+          log_every: int = 100, time_budget_s: float | None = None, clip: float = 1.0):
+    """Minimise the energy-norm error of net(r_hat) ~ Ah^-1 r_hat with the project's
+    forward and backward kernels; Adam with a cosine learning-rate decay on FP32
+    master weights, gradient-norm clipping, BF16 copies repacked every step.
+    Returns the per-step mean loss."""
     t = _t()
     params = net.parameters()
     for p_ in params:
         p_.requires_grad_(False)
     opt = t.optim.Adam(params, lr=lr)
-    H, W = R.shape[1:]
-    ws = Workspace(H, W, masks[0])
+    H, W = data.R.shape[1:]
+    ws = Workspace(H, W, data.masks[0])
+    cur_mask = 0
     gen = np.random.default_rng(seed)
     log = []
     t0 = time.time()
     for step in range(steps):
-        idx = gen.integers(0, R.shape[0], batch)
+        # cosine decay over the step count or the time budget, whichever ends first
+        frac = step / max(1, steps)
+        if time_budget_s:
+            frac = max(frac, (time.time() - t0) / time_budget_s)
+        for grp in opt.param_groups:
+            grp["lr"] = lr * 0.5 * (1.0 + math.cos(math.pi * min(1.0, frac)))
+        idx = gen.integers(0, len(data), batch)
         acc = {name: (t.zeros_like(net.w[name]), t.zeros_like(net.b[name])) for name, *_ in LAYERS}
-        loss = 0.0
+        loss = t.zeros((), dtype=t.float64, device=_lib.device())
         for k in idx:
-            if ws.mask_src is not masks[k]:
-                ws.set_mask(masks[k])
-            x = R[k].contiguous()
+            ci = data.case_of[k]
+            if ci != cur_mask:
+                ws.set_mask(data.masks[ci])
+                cur_mask = ci
+            x = data.R[k].contiguous()
             out = net_forward(net, ws, x)
-            e = E[k]
-            den = float((e * e).sum()) + 1e-30
-            diff = out - e
-            loss += float((diff * diff).sum()) / den / batch
-            dout = (2.0 / den / batch) * diff
-            grads = net_backward(net, ws, x, dout)
+            lk, g = energy_loss_grad(data.solvers[ci], data.h2[ci], out, x)
+            loss += lk / batch
+            grads = net_backward(net, ws, x, (g / batch).contiguous())
             for name in grads:
                 acc[name][0].add_(grads[name][0])
                 acc[name][1].add_(grads[name][1])
@@ -523,11 +649,60 @@ def train(net: LPCNet, R, E, masks, steps: int = 1000, batch: int = 4, lr: float
         for name, *_ in LAYERS:
             net.w[name].grad = acc[name][0]
             net.b[name].grad = acc[name][1]
+        if clip:
+            t.nn.utils.clip_grad_norm_(params, clip)
         opt.step()
         net.repack()
-        log.append(loss)
+        log.append(float(loss))
         if log_every and step % log_every == 0:
             print(f"train step {step}: loss {np.mean(log[-log_every:]):.4f}", flush=True)
         if time_budget_s is not None and time.time() - t0 > time_budget_s:
             break
     return log
+
+
+def save_weights(net: LPCNet, path) -> None:
+    np.savez(path, **{k: v.numpy() for k, v in net.state_dict().items()})
+
+
+def load_weights(path, net: LPCNet | None = None) -> LPCNet:
+    t = _t()
+    net = net or LPCNet()
+    d = np.load(path)
+    net.load_state_dict({k: t.from_numpy(d[k]) for k in d.files})
+    return net
+
+
+def pretrained():
+    """The network trained by ``python -m cfd2d_b200.learned`` (shipped weights)."""
+    from pathlib import Path
+
+    return load_weights(Path(__file__).resolve().parent / "data" / "lpc_weights.npz")
+
+
+def main(argv=None):
+    """Harvest residuals, train, save the weights: python -m cfd2d_b200.learned OUT.npz"""
+    import argparse
+
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument("out")
+    ap.add_argument("--cases", type=int, default=24)
+    ap.add_argument("--nx", type=int, default=256)
+    ap.add_argument("--ny", type=int, default=128)
+    ap.add_argument("--seconds", type=float, default=600.0)
+    ap.add_argument("--steps", type=int, default=100000)
+    ap.add_argument("--batch", type=int, default=4)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--seed", type=int, default=0)
+    a = ap.parse_args(argv)
+    data = harvest_residuals(n_cases=a.cases, nx=a.nx, ny=a.ny, seed=a.seed, every=8, max_snaps=80)
+    print(f"residuals {tuple(data.R.shape)}", flush=True)
+    net = LPCNet(seed=a.seed)
+    log = train(net, data, steps=a.steps, batch=a.batch, lr=a.lr, seed=a.seed, log_every=200,
+                time_budget_s=a.seconds)
+    print(f"steps {len(log)} loss first {np.mean(log[:50]):.4f} last {np.mean(log[-50:]):.4f}", flush=True)
+    save_weights(net, a.out)
+
+
+if __name__ == "__main__":
+    main()

@@ -85,10 +85,10 @@ int cfd2d_lpc_conv_dw(int cin, int cout, const void* x, int x_bf16, const float*
 size_t cfd2d_fcg_partial_doubles(int n) { return fcg::partial_doubles(n); }
 
 int cfd2d_fcg_init(const cfd2d_poisson* op, const double* F, const double* G, const double* rhs, double dx,
-                   double dy, const double* dt, double* b, double* x, double* r, cfd2d_fcg_scalars* s,
-                   double* partial, void* stream) {
+                   double dy, const double* dt, double* b, double* x, double* r, double* p_zero,
+                   cfd2d_fcg_scalars* s, double* partial, void* stream) {
     if (!op || !b || !x || !r || !s || !partial || (!rhs && (!F || !G))) return CFD2D_E_ARG;
-    return status_of(fcg::init(*op, F, G, rhs, dx, dy, dt, b, x, r, s, partial, as_stream(stream)));
+    return status_of(fcg::init(*op, F, G, rhs, dx, dy, dt, b, x, r, p_zero, s, partial, as_stream(stream)));
 }
 
 int cfd2d_fcg_pq(const cfd2d_poisson* op, const double* p, double* q, cfd2d_fcg_scalars* s, double* partial,
@@ -121,14 +121,102 @@ int cfd2d_fcg_net_in(int n, const double* r, const cfd2d_fcg_scalars* s, const u
 }
 
 int cfd2d_fcg_net_out(int n, const float* out, const double* r, const double* dinv, const uint8_t* mask,
-                      const cfd2d_fcg_scalars* s, double jacobi, double* z, void* stream) {
+                      const cfd2d_fcg_scalars* s, double scale, double jacobi, double* z, void* stream) {
     if (n < 1 || !out || !r || !dinv || !mask || !s || !z) return CFD2D_E_ARG;
-    return status_of(fcg::net_out(n, out, r, dinv, mask, s, jacobi, z, as_stream(stream)));
+    return status_of(fcg::net_out(n, out, r, dinv, mask, s, scale, jacobi, z, as_stream(stream)));
 }
 
 int cfd2d_fcg_scatter_p(const cfd2d_poisson* op, const double* x, double* p_padded, void* stream) {
     if (!op || !x || !p_padded) return CFD2D_E_ARG;
     return status_of(fcg::scatter_p(*op, x, p_padded, as_stream(stream)));
+}
+
+int cfd2d_fcg_gate(const cfd2d_fcg_scalars* s, cfd2d_fcg_control* ctl, uint64_t handle, void* stream) {
+    if (!s || !ctl) return CFD2D_E_ARG;
+    return status_of(fcg::gate(s, ctl, (unsigned long long)handle, as_stream(stream)));
+}
+
+int cfd2d_fcg_zero_rhs(int n, const double* b, double* x, const cfd2d_fcg_scalars* s, void* stream) {
+    if (n < 1 || !b || !x || !s) return CFD2D_E_ARG;
+    return status_of(fcg::zero_rhs(n, b, x, s, as_stream(stream)));
+}
+
+int cfd2d_capture_begin(void* stream) {
+    if (!stream) return CFD2D_E_ARG;  // the legacy default stream cannot be captured
+    return status_of(cudaStreamBeginCapture(as_stream(stream), cudaStreamCaptureModeRelaxed));
+}
+
+int cfd2d_capture_condition(void* stream, uint64_t* handle_out) {
+    if (!stream || !handle_out) return CFD2D_E_ARG;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamGetCaptureInfo(as_stream(stream), &cs, nullptr, &g, nullptr, nullptr);
+    if (e != cudaSuccess) return status_of(e);
+    if (cs != cudaStreamCaptureStatusActive || !g) return CFD2D_E_ARG;
+    cudaGraphConditionalHandle h = 0;
+    e = cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault);
+    if (e != cudaSuccess) return status_of(e);
+    *handle_out = (uint64_t)h;
+    return CFD2D_OK;
+}
+
+int cfd2d_capture_while_begin(void* stream, void* body_stream, uint64_t handle) {
+    if (!stream || !body_stream || !handle || stream == body_stream) return CFD2D_E_ARG;
+    cudaStream_t s = as_stream(stream);
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    cudaError_t e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &ndeps);
+    if (e != cudaSuccess) return status_of(e);
+    if (cs != cudaStreamCaptureStatusActive || !g) return CFD2D_E_ARG;
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = (cudaGraphConditionalHandle)handle;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node = nullptr;
+    e = cudaGraphAddNode(&node, g, deps, ndeps, &np);
+    if (e != cudaSuccess) return status_of(e);
+    e = cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies);
+    if (e != cudaSuccess) return status_of(e);
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    return status_of(cudaStreamBeginCaptureToGraph(as_stream(body_stream), body, nullptr, nullptr, 0,
+                                                   cudaStreamCaptureModeRelaxed));
+}
+
+int cfd2d_capture_while_end(void* body_stream) {
+    if (!body_stream) return CFD2D_E_ARG;
+    cudaGraph_t body = nullptr;
+    return status_of(cudaStreamEndCapture(as_stream(body_stream), &body));
+}
+
+int cfd2d_capture_end(void* stream, void** graph_out) {
+    if (!stream || !graph_out) return CFD2D_E_ARG;
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(as_stream(stream), &g);
+    if (e != cudaSuccess) return status_of(e);
+    cudaGraphExec_t x = nullptr;
+    e = cudaGraphInstantiate(&x, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return status_of(e);
+    *graph_out = (void*)x;
+    return CFD2D_OK;
+}
+
+int cfd2d_capture_abort(void* stream) {
+    if (!stream) return CFD2D_E_ARG;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(as_stream(stream), &cs) != cudaSuccess) {
+        cudaGetLastError();
+        return CFD2D_E_CUDA;
+    }
+    if (cs == cudaStreamCaptureStatusNone) return CFD2D_OK;
+    cudaGraph_t g = nullptr;
+    cudaStreamEndCapture(as_stream(stream), &g);
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    return CFD2D_OK;
 }
 
 }  // extern "C"

@@ -62,8 +62,8 @@ __device__ __forceinline__ bool reduce_last(double (&v)[K], double* partial, uns
 // b = -(div(F, G) / dt) on fluid cells (no Neumann component: the learned path runs
 // on domains with an outflow boundary), r = b - A x, ||b||^2, ||r||^2
 __global__ void k_init(cfd2d_poisson op, const double* F, const double* G, const double* rhs, double dx,
-                       double dy, const double* dt_ptr, double* b, double* x, double* r, FcgScalars* s,
-                       double* partial) {
+                       double dy, const double* dt_ptr, double* b, double* x, double* r, double* p_zero,
+                       FcgScalars* s, double* partial) {
     const int n = op.nx * op.ny;
     const int ny = op.ny;
     double v[2] = {0.0, 0.0};
@@ -82,6 +82,7 @@ __global__ void k_init(cfd2d_poisson op, const double* F, const double* G, const
             }
         }
         b[c] = bb;
+        if (p_zero) p_zero[c] = 0.0;  // the first direction is z + 0 * p
         v[0] += bb * bb;
     }
     double tot[2];
@@ -136,8 +137,10 @@ __global__ void k_update(int n, double* x, double* r, double* r_old, const doubl
 }
 
 // beta = z.(r - r_old) / rz_old (0 on the first direction), rz = z.r
-__global__ void k_zr(int n, const double* z, const double* r, const double* r_old, int first, FcgScalars* s,
+__global__ void k_zr(int n, const double* z, const double* r, const double* r_old, int first_flag, FcgScalars* s,
                      double* partial) {
+    // first_flag < 0: the first direction is the one taken before any update (iters == 0)
+    const int first = first_flag < 0 ? (s->iters == 0) : first_flag;
     double v[2] = {0.0, 0.0};
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
         v[0] += z[c] * r[c];
@@ -164,13 +167,44 @@ __global__ void k_net_in(int n, const double* r, const FcgScalars* s, const uint
         in[c] = mask[c] ? (float)(r[c] * inv) : 0.0f;
 }
 
-// z = scale * out + jacobi * r / diag (the Jacobi term keeps the high frequencies the
-// network does not resolve), masked
+// z = ||r|| * scale * out + jacobi * r / diag, masked. The network works on the
+// dimensionless operator h^2 A, so scale = h^2 maps its output back to A^-1 r; the
+// Jacobi term keeps the high frequencies the network does not resolve.
 __global__ void k_net_out(int n, const float* out, const double* r, const double* dinv, const uint8_t* mask,
-                          const FcgScalars* s, double jacobi, double* z) {
-    const double sc = sqrt(s->rr > 0.0 ? s->rr : 1.0);
+                          const FcgScalars* s, double scale, double jacobi, double* z) {
+    const double sc = sqrt(s->rr > 0.0 ? s->rr : 1.0) * scale;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
         z[c] = mask[c] ? ((double)out[c] * sc + jacobi * dinv[c] * r[c]) : 0.0;
+}
+
+// Stop tests of the device-driven loop, one thread: records ||r|| of this iterate,
+// decides whether another iteration runs and sets the loop's graph condition.
+__global__ void k_gate(const FcgScalars* s, cfd2d_fcg_control* ctl, cudaGraphConditionalHandle h) {
+    const int it = s->iters;
+    const int calls = ctl->calls + 1;
+    ctl->calls = calls;
+    const double res = sqrt(s->rr);
+    if (it >= 0 && it <= ctl->maxiter) ctl->hist[it] = res;
+    const double atol = ctl->rtol * sqrt(s->bb);
+    int reason = CFD2D_FCG_RUNNING;
+    if (!isfinite(res)) {
+        reason = CFD2D_FCG_NONFINITE;
+    } else if (res < atol || s->bb == 0.0) {
+        reason = CFD2D_FCG_CONVERGED;
+    } else if (it >= ctl->maxiter || calls > ctl->maxiter + 1) {
+        reason = CFD2D_FCG_MAXITER;
+    } else if (it >= ctl->stall_window && res > ctl->stall_factor * ctl->hist[it - ctl->stall_window]) {
+        reason = CFD2D_FCG_STALLED;
+    }
+    ctl->reason = reason;
+    ctl->iters = it;
+    if (h) cudaGraphSetConditional(h, reason == CFD2D_FCG_RUNNING ? 1u : 0u);
+}
+
+// x = b where ||b|| = 0 (scipy returns b for a zero right-hand side)
+__global__ void k_zero_rhs(int n, const double* b, double* x, const FcgScalars* s) {
+    if (s->bb != 0.0) return;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) x[c] = b[c];
 }
 
 // padded pressure output p[(i+1)(ny+2) + j+1] = x (no Neumann component to remove)
@@ -198,10 +232,10 @@ int blocks(int n) {
 size_t partial_doubles(int n) { return (size_t)2 * blocks(n) + 8; }
 
 cudaError_t init(const cfd2d_poisson& op, const double* F, const double* G, const double* rhs, double dx,
-                 double dy, const double* dt_ptr, double* b, double* x, double* r, FcgScalars* s,
+                 double dy, const double* dt_ptr, double* b, double* x, double* r, double* p_zero, FcgScalars* s,
                  double* partial, cudaStream_t st) {
     const int n = op.nx * op.ny;
-    k_init<<<blocks(n), T, 0, st>>>(op, F, G, rhs, dx, dy, dt_ptr, b, x, r, s, partial);
+    k_init<<<blocks(n), T, 0, st>>>(op, F, G, rhs, dx, dy, dt_ptr, b, x, r, p_zero, s, partial);
     return cudaGetLastError();
 }
 
@@ -235,8 +269,18 @@ cudaError_t net_in(int n, const double* r, const FcgScalars* s, const uint8_t* m
 }
 
 cudaError_t net_out(int n, const float* out, const double* r, const double* dinv, const uint8_t* mask,
-                    const FcgScalars* s, double jacobi, double* z, cudaStream_t st) {
-    k_net_out<<<blocks(n), T, 0, st>>>(n, out, r, dinv, mask, s, jacobi, z);
+                    const FcgScalars* s, double scale, double jacobi, double* z, cudaStream_t st) {
+    k_net_out<<<blocks(n), T, 0, st>>>(n, out, r, dinv, mask, s, scale, jacobi, z);
+    return cudaGetLastError();
+}
+
+cudaError_t gate(const FcgScalars* s, cfd2d_fcg_control* ctl, unsigned long long handle, cudaStream_t st) {
+    k_gate<<<1, 1, 0, st>>>(s, ctl, (cudaGraphConditionalHandle)handle);
+    return cudaGetLastError();
+}
+
+cudaError_t zero_rhs(int n, const double* b, double* x, const FcgScalars* s, cudaStream_t st) {
+    k_zero_rhs<<<blocks(n), T, 0, st>>>(n, b, x, s);
     return cudaGetLastError();
 }
 

@@ -38,7 +38,7 @@ using FcgScalars = cfd2d_fcg_scalars;
 
 size_t partial_doubles(int n);
 cudaError_t init(const cfd2d_poisson& op, const double* F, const double* G, const double* rhs, double dx,
-                 double dy, const double* dt_ptr, double* b, double* x, double* r, FcgScalars* s,
+                 double dy, const double* dt_ptr, double* b, double* x, double* r, double* p_zero, FcgScalars* s,
                  double* partial, cudaStream_t st);
 cudaError_t pq(const cfd2d_poisson& op, const double* p, double* q, FcgScalars* s, double* partial,
                cudaStream_t st);
@@ -49,8 +49,10 @@ cudaError_t zr(int n, const double* z, const double* r, const double* r_old, int
 cudaError_t dir(int n, const double* z, double* p, const FcgScalars* s, cudaStream_t st);
 cudaError_t net_in(int n, const double* r, const FcgScalars* s, const uint8_t* mask, float* in, cudaStream_t st);
 cudaError_t net_out(int n, const float* out, const double* r, const double* dinv, const uint8_t* mask,
-                    const FcgScalars* s, double jacobi, double* z, cudaStream_t st);
+                    const FcgScalars* s, double scale, double jacobi, double* z, cudaStream_t st);
 cudaError_t scatter_p(const cfd2d_poisson& op, const double* x, double* p_pad, cudaStream_t st);
+cudaError_t gate(const FcgScalars* s, cfd2d_fcg_control* ctl, unsigned long long handle, cudaStream_t st);
+cudaError_t zero_rhs(int n, const double* b, double* x, const FcgScalars* s, cudaStream_t st);
 
 }  // namespace fcg
 }  // namespace cfd

@@ -361,10 +361,10 @@ typedef struct cfd2d_fcg_scalars {
 } cfd2d_fcg_scalars;
 
 size_t cfd2d_fcg_partial_doubles(int n);
-/* b = -(div(F,G)/dt) (or -rhs when rhs != NULL), r = b - A x */
+/* b = -(div(F,G)/dt) (or -rhs when rhs != NULL), r = b - A x, p_zero (may be NULL) = 0 */
 int cfd2d_fcg_init(const cfd2d_poisson* op, const double* F, const double* G, const double* rhs, double dx,
-                   double dy, const double* dt, double* b, double* x, double* r, cfd2d_fcg_scalars* s,
-                   double* partial, void* stream);
+                   double dy, const double* dt, double* b, double* x, double* r, double* p_zero,
+                   cfd2d_fcg_scalars* s, double* partial, void* stream);
 int cfd2d_fcg_pq(const cfd2d_poisson* op, const double* p, double* q, cfd2d_fcg_scalars* s, double* partial,
                  void* stream);
 int cfd2d_fcg_update(int n, double* x, double* r, double* r_old, const double* p, const double* q,
@@ -374,9 +374,55 @@ int cfd2d_fcg_zr(int n, const double* z, const double* r, const double* r_old, i
 int cfd2d_fcg_dir(int n, const double* z, double* p, const cfd2d_fcg_scalars* s, void* stream);
 int cfd2d_fcg_net_in(int n, const double* r, const cfd2d_fcg_scalars* s, const uint8_t* mask, float* in,
                      void* stream);
+/* z = ||r|| * scale * out + jacobi * r / diag (scale = h^2 of the dimensionless operator) */
 int cfd2d_fcg_net_out(int n, const float* out, const double* r, const double* dinv, const uint8_t* mask,
-                      const cfd2d_fcg_scalars* s, double jacobi, double* z, void* stream);
+                      const cfd2d_fcg_scalars* s, double scale, double jacobi, double* z, void* stream);
 int cfd2d_fcg_scatter_p(const cfd2d_poisson* op, const double* x, double* p_padded, void* stream);
+
+/* Device-driven flexible CG: the whole iteration runs inside one CUDA graph whose
+ * WHILE node repeats the loop body (preconditioner, r.z, direction, A p, update,
+ * gate) until the gate kernel stops it, so a solve needs no host round trip per
+ * iteration. The control block lives in device memory. */
+#define CFD2D_FCG_RUNNING 0
+#define CFD2D_FCG_CONVERGED 1
+#define CFD2D_FCG_MAXITER 2
+#define CFD2D_FCG_STALLED 3   /* ||r|| > stall_factor * ||r|| of stall_window iterations ago */
+#define CFD2D_FCG_NONFINITE 4
+typedef struct cfd2d_fcg_control {
+    double rtol;              /* stop when ||r|| < rtol ||b|| */
+    double stall_factor;
+    int32_t stall_window;
+    int32_t maxiter;
+    int32_t reason;           /* CFD2D_FCG_*, written by the gate */
+    int32_t iters;            /* iterations done, written by the gate */
+    int32_t calls;            /* gate invocations (set 0 before a solve); a hard bound
+                                 on the loop independent of the iteration counter */
+    int32_t pad;
+    double* hist;             /* device, maxiter + 1 residual norms */
+} cfd2d_fcg_control;
+
+/* One thread: record ||r||, apply the stop tests, set the WHILE condition `handle`
+ * (0 = no graph, only the tests). */
+int cfd2d_fcg_gate(const cfd2d_fcg_scalars* s, cfd2d_fcg_control* ctl, uint64_t handle, void* stream);
+/* x = b when ||b|| = 0 (read on the device). */
+int cfd2d_fcg_zero_rhs(int n, const double* b, double* x, const cfd2d_fcg_scalars* s, void* stream);
+
+/* Stream capture of a graph with one WHILE loop (no reference counterpart):
+ * capture_begin starts a relaxed-mode capture of `stream`; capture_condition
+ * creates the loop's condition (0 at every launch; a kernel captured before the
+ * loop, such as cfd2d_fcg_gate, sets it); while_begin appends the WHILE node after
+ * the work captured so far and starts capturing `body_stream` into the loop body,
+ * which must end with a kernel that sets the condition again; while_end ends the
+ * body; capture_end instantiates the graph (launch with cfd2d_graph_launch, free
+ * with cfd2d_graph_destroy). No device memory may be allocated or freed while a
+ * capture is open. */
+int cfd2d_capture_begin(void* stream);
+int cfd2d_capture_condition(void* stream, uint64_t* handle_out);
+int cfd2d_capture_while_begin(void* stream, void* body_stream, uint64_t handle);
+int cfd2d_capture_while_end(void* body_stream);
+int cfd2d_capture_end(void* stream, void** graph_out);
+/* Abandon a capture after an error (ends it and frees the partial graph). */
+int cfd2d_capture_abort(void* stream);
 
 /* Library version string (host memory, static). */
 const char* cfd2d_version(void);

@@ -163,11 +163,18 @@ def test_flexible_cg_reaches_tolerance_and_matches_plain_cg(L):
     ps._x0 = zero
     p_plain = ps.solve(rhs)
     assert ps.last_iterations > 0
-    ps._x0 = zero
     net = learned.LPCNet(seed=0)
     fcg = learned.LearnedPCG(ps, net)
+    # the graph-driven loop and the host-driven loop run the same kernels in the
+    # same order: identical iterates
+    ps._x0 = zero
+    p_host = fcg.solve(rhs, graph=False)
+    its_host, hist_host = fcg.last_total_iterations, list(fcg.history)
+    ps._x0 = zero
     p_fcg = fcg.solve(rhs)
     assert fcg.last_total_iterations > 0
+    assert fcg.last_total_iterations == its_host and fcg.history == hist_host
+    assert np.array_equal(p_fcg, p_host)
     assert relerr(p_fcg, p_plain) < 1e-4
     # the stop test is the plain solver's, ||r|| < tol ||b|| on the recursively
     # updated residual; the true residual of the final iterate is within 2x of it
@@ -175,12 +182,14 @@ def test_flexible_cg_reaches_tolerance_and_matches_plain_cg(L):
     b = -rhs[ps.fluid]
     x = ps._x0
     assert np.linalg.norm(b - A @ x) <= 2e-9 * np.linalg.norm(b)
+    fcg.close()
 
 
-def test_training_reduces_the_loss(L):
+def test_training_lowers_the_energy_loss(L):
     torch, _lib, learned = L
-    R, E, M = learned.harvest_pairs(n_cases=3, nx=128, ny=64, seed=1, every=6, max_snaps=40)
-    assert R.shape[0] >= 20 and R.shape[1:] == (128, 64)
+    data = learned.harvest_residuals(n_cases=3, nx=128, ny=64, seed=1, every=6, max_snaps=40)
+    assert len(data) >= 20 and tuple(data.R.shape[1:]) == (128, 64)
     net = learned.LPCNet(seed=1)
-    log = learned.train(net, R, E, M, steps=120, batch=2, lr=2e-3, log_every=0)
-    assert np.mean(log[-20:]) < 0.8 * np.mean(log[:20])
+    log = learned.train(net, data, steps=150, batch=2, lr=2e-3, log_every=0)
+    assert np.all(np.isfinite(log))
+    assert np.mean(log[-20:]) < np.mean(log[:20]) and np.mean(log[-20:]) < 0.0
