@@ -62,10 +62,17 @@ def level_shapes(H, W):
 
 
 class LPCNet:
-    """Weights (FP32 masters) and the packed BF16 tensor-core images of the 32->32 layers."""
+    """Weights (FP32 masters) and the packed BF16 tensor-core images of the 32->32 layers.
 
-    def __init__(self, seed: int = 0):
+    With ``bias=False`` (the default) the biases stay zero and are not trained: the
+    network is then positively homogeneous, net(a r) = a net(r) for a > 0, and with
+    sign-flipped training samples close to odd, as a preconditioner inside CG must
+    be (a trained bias adds a fixed field to every preconditioned residual, and the
+    flexible CG stalls on it)."""
+
+    def __init__(self, seed: int = 0, bias: bool = False):
         t = _t()
+        self.bias = bias
         g = t.Generator().manual_seed(seed)
         self.w, self.b = {}, {}
         for name, cin, cout, _lvl, relu in LAYERS:
@@ -84,7 +91,7 @@ class LPCNet:
     def parameters(self):
         out = []
         for name, *_ in LAYERS:
-            out += [self.w[name], self.b[name]]
+            out += [self.w[name], self.b[name]] if self.bias else [self.w[name]]
         return out
 
     def repack(self):
@@ -118,6 +125,7 @@ class LPCNet:
                {f"{k}.b": v.detach().cpu() for k, v in self.b.items()}
 
     def load_state_dict(self, d):
+        self.bias = any(float(d[f"{name}.b"].abs().max()) > 0.0 for name, *_ in LAYERS)
         for name, *_ in LAYERS:
             self.w[name].copy_(d[f"{name}.w"].to(self.w[name].device))
             self.b[name].copy_(d[f"{name}.b"].to(self.b[name].device))
@@ -638,6 +646,8 @@ def train(net: LPCNet, data: TrainingSet, steps: int = 1000, batch: int = 4, lr:
                 ws.set_mask(data.masks[ci])
                 cur_mask = ci
             x = data.R[k].contiguous()
+            if gen.random() < 0.5:
+                x = -x  # residuals of both signs: the target is odd in r
             out = net_forward(net, ws, x)
             lk, g = energy_loss_grad(data.solvers[ci], data.h2[ci], out, x)
             loss += lk / batch
@@ -648,7 +658,8 @@ def train(net: LPCNet, data: TrainingSet, steps: int = 1000, batch: int = 4, lr:
         opt.zero_grad(set_to_none=False)
         for name, *_ in LAYERS:
             net.w[name].grad = acc[name][0]
-            net.b[name].grad = acc[name][1]
+            if net.bias:
+                net.b[name].grad = acc[name][1]
         if clip:
             t.nn.utils.clip_grad_norm_(params, clip)
         opt.step()

@@ -31,8 +31,8 @@ __global__ void k_momentum(const double* u, const double* v, const uint8_t* fl, 
                            int var_density) {
     const Grid2 g{nx, ny};
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = blockIdx.y;
-    if (j >= ny + 2) return;
+    const int i = (blockIdx.y * blockDim.y + threadIdx.y);
+    if (j >= ny + 2 || i >= nx + 2) return;
     const MomCoef m = mom_coef(dx, dy, gamma, nu[g.c(1, 1)]);
     const int imax = periodic ? nx : nx - 1;
     if (i <= nx) {
@@ -54,8 +54,8 @@ __global__ void k_obstacle_bc(double* u, double* v, const uint8_t* fl, int nx, i
     if (!is_active(st)) return;
     const Grid2 g{nx, ny};
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = blockIdx.y;
-    if (j >= ny + 2) return;
+    const int i = (blockIdx.y * blockDim.y + threadIdx.y);
+    if (j >= ny + 2 || i >= nx + 1) return;
     const int imax = periodic ? nx : nx - 1;
     if (i >= 1 && i <= imax) {
         double nu_ = u[g.u(i, j)];
@@ -76,8 +76,8 @@ __global__ void k_scalar_transport(const double* phi, const double* u, const dou
     if (!is_active(st)) return;
     const Grid2 g{nx, ny};
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = blockIdx.y;
-    if (j >= ny + 2) return;
+    const int i = (blockIdx.y * blockDim.y + threadIdx.y);
+    if (j >= ny + 2 || i >= nx + 2) return;
     double r = 0.0;
     if (i >= 1 && i <= nx && j >= 1 && j <= ny)
         r = transport_cell(phi, u, v, fl, diff, g, dx, dy, limiter, periodic != 0, bc, obs_t, obs_v, i, j);
@@ -87,8 +87,8 @@ __global__ void k_scalar_transport(const double* phi, const double* u, const dou
 // cfd2d/geometry.py:17-22: (X - xc)**2 + (Y - yc)**2 <= r**2, X = (i + 0.5) * dx
 __global__ void k_mask_circle(int nx, int ny, double dx, double dy, double xc, double yc, double r,
                               uint8_t* mask) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
-    if (j >= ny) return;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y * blockDim.y + threadIdx.y;
+    if (j >= ny || i >= nx) return;
     const double X = ((double)i + 0.5) * dx, Y = ((double)j + 0.5) * dy;
     const double a = X - xc, b = Y - yc;
     mask[i * ny + j] = (a * a + b * b <= r * r) ? 1 : 0;
@@ -97,8 +97,8 @@ __global__ void k_mask_circle(int nx, int ny, double dx, double dy, double xc, d
 // cfd2d/geometry.py:25-32
 __global__ void k_mask_ellipse(int nx, int ny, double dx, double dy, double xc, double yc, double a,
                                double b, double cp, double sp, uint8_t* mask) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
-    if (j >= ny) return;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y * blockDim.y + threadIdx.y;
+    if (j >= ny || i >= nx) return;
     const double X = ((double)i + 0.5) * dx, Y = ((double)j + 0.5) * dy;
     const double xr = (X - xc) * cp + (Y - yc) * sp;
     const double yr = -(X - xc) * sp + (Y - yc) * cp;
@@ -109,8 +109,8 @@ __global__ void k_mask_ellipse(int nx, int ny, double dx, double dy, double xc, 
 // cfd2d/geometry.py:35-40
 __global__ void k_mask_rect(int nx, int ny, double dx, double dy, double xa, double ya, double xb,
                             double yb, uint8_t* mask) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
-    if (j >= ny) return;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y * blockDim.y + threadIdx.y;
+    if (j >= ny || i >= nx) return;
     const double X = ((double)i + 0.5) * dx, Y = ((double)j + 0.5) * dy;
     mask[i * ny + j] = (X >= xa && X <= xb && Y >= ya && Y <= yb) ? 1 : 0;
 }
@@ -215,8 +215,8 @@ __global__ void k_sst_pre(cfd2d_sim S) {
     const int nx = S.nx, ny = S.ny;
     const Grid2 g{nx, ny};
     const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    const int i = blockIdx.y + 1;
-    if (j > ny) return;
+    const int i = (blockIdx.y * blockDim.y + threadIdx.y) + 1;
+    if (j > ny || i > nx) return;
     const SSTConst K = sst_const();
     const cfd2d_scalar& ks = S.scalars[S.sst.k_index];
     const cfd2d_scalar& ws = S.scalars[S.sst.w_index];
@@ -272,8 +272,8 @@ __global__ void k_sst_ghosts(cfd2d_sim S) {
     const int nx = S.nx, ny = S.ny;
     const Grid2 g{nx, ny};
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = blockIdx.y;
-    if (j >= ny + 2) return;
+    const int i = (blockIdx.y * blockDim.y + threadIdx.y);
+    if (j >= ny + 2 || i >= nx + 2) return;
     const int c = g.c(i, j);
     const bool ghost = (i == 0 || i == nx + 1 || j == 0 || j == ny + 1);
     double nut;
@@ -411,8 +411,8 @@ __global__ void k_predictor(cfd2d_sim S, int copy_only) {
     const int nx = S.nx, ny = S.ny;
     const Grid2 g{nx, ny};
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = blockIdx.y;
-    if (j >= ny + 2) return;
+    const int i = (blockIdx.y * blockDim.y + threadIdx.y);
+    if (j >= ny + 2 || i >= nx + 2) return;
     const double dt = copy_only ? 0.0 : st->dt;
     const bool ab2 = S.scheme_ab2 && st->have_old;
     const double a = st->ab_a, b = st->ab_b;
@@ -491,8 +491,8 @@ __global__ void k_correct(cfd2d_sim S, const double* p, int unit_dt) {
     const int nx = S.nx, ny = S.ny;
     const Grid2 g{nx, ny};
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = blockIdx.y;
-    if (j >= ny + 2) return;
+    const int i = (blockIdx.y * blockDim.y + threadIdx.y);
+    if (j >= ny + 2 || i >= nx + 2) return;
     const double dt = unit_dt ? 1.0 : st->dt;
     const double dx = S.dx, dy = S.dy;
     const int pc = ny + 2;
@@ -580,7 +580,7 @@ __global__ void k_shift_u(cfd2d_sim S) {
     const int nx = S.nx, ny = S.ny;
     const Grid2 g{nx, ny};
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = blockIdx.y;
+    const int i = (blockIdx.y * blockDim.y + threadIdx.y);
     if (j >= ny + 2 || i > nx) return;
     const double du = st->bulk_du;
     double val = S.u[g.u(i, j)];
@@ -606,8 +606,8 @@ __global__ void k_scalar_rhs(cfd2d_sim S, int s) {
     const int nx = S.nx, ny = S.ny;
     const Grid2 g{nx, ny};
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = blockIdx.y;
-    if (j >= ny + 2) return;
+    const int i = (blockIdx.y * blockDim.y + threadIdx.y);
+    if (j >= ny + 2 || i >= nx + 2) return;
     const cfd2d_scalar& sc = S.scalars[s];
     ScalarBCView bc;
     for (int k = 0; k < 4; ++k) { bc.bt[k] = sc.bt[k]; bc.bv[k] = sc.bv[k]; }
@@ -626,8 +626,8 @@ __global__ void k_scalar_update(cfd2d_sim S, int s) {
     const int nx = S.nx, ny = S.ny;
     const Grid2 g{nx, ny};
     const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    const int i = blockIdx.y + 1;
-    if (j > ny) return;
+    const int i = (blockIdx.y * blockDim.y + threadIdx.y) + 1;
+    if (j > ny || i > nx) return;
     const cfd2d_scalar& sc = S.scalars[s];
     const int c = g.c(i, j);
     const int ci = (i - 1) * ny + (j - 1);
@@ -677,8 +677,8 @@ __global__ void k_sst_wall_omega(cfd2d_sim S) {
     const int nx = S.nx, ny = S.ny;
     const Grid2 g{nx, ny};
     const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    const int i = blockIdx.y + 1;
-    if (j > ny) return;
+    const int i = (blockIdx.y * blockDim.y + threadIdx.y) + 1;
+    if (j > ny || i > nx) return;
     const int ci = (i - 1) * ny + (j - 1);
     if (S.sst.wall_adj[ci]) S.scalars[S.sst.w_index].phi[g.c(i, j)] = S.sst.w_wall[ci];
 }
@@ -734,8 +734,8 @@ __global__ void k_scalar_ghost_solid(cfd2d_sim S, int s, int obs_fixed, double o
     const int nx = S.nx, ny = S.ny;
     const Grid2 g{nx, ny};
     const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    const int i = blockIdx.y + 1;
-    if (j > ny) return;
+    const int i = (blockIdx.y * blockDim.y + threadIdx.y) + 1;
+    if (j > ny || i > nx) return;
     const int c = g.c(i, j);
     if (S.fluid[c]) return;
     const cfd2d_scalar& sc = S.scalars[s];
@@ -869,7 +869,13 @@ __global__ void k_end_step(cfd2d_sim S) {
 
 // ================================================================ host launchers
 namespace {
-inline dim3 grid_rows(int width, int rows) { return dim3((width + kBlock - 1) / kBlock, rows, 1); }
+// row kernels: 2D tiles of kTileX (along j, contiguous) x kTileY (along i) threads, so
+// that the stencil rows a block reads are shared through L1 by its warps
+constexpr int kTileX = 32, kTileY = 8;
+const dim3 kTile(kTileX, kTileY, 1);
+inline dim3 grid_rows(int width, int rows) {
+    return dim3((width + kTileX - 1) / kTileX, (rows + kTileY - 1) / kTileY, 1);
+}
 inline cudaError_t last() { return cudaGetLastError(); }
 }  // namespace
 
@@ -884,14 +890,14 @@ cudaError_t launch_momentum(const double* u, const double* v, const uint8_t* fl,
                             double dx, double dy, const double* nu, int variable, double gamma,
                             int periodic, double* hu, double* hv, const double* rho, int var_density,
                             cudaStream_t s) {
-    k_momentum<<<grid_rows(ny + 2, nx + 2), kBlock, 0, s>>>(u, v, fl, nx, ny, dx, dy, nu, variable, gamma,
+    k_momentum<<<grid_rows(ny + 2, nx + 2), kTile, 0, s>>>(u, v, fl, nx, ny, dx, dy, nu, variable, gamma,
                                                            periodic, hu, hv, rho, var_density);
     return last();
 }
 
 cudaError_t launch_obstacle_bc(double* u, double* v, const uint8_t* fl, int nx, int ny, int periodic,
                                const cfd2d_state* st, cudaStream_t s) {
-    k_obstacle_bc<<<grid_rows(ny + 2, nx + 1), kBlock, 0, s>>>(u, v, fl, nx, ny, periodic, st);
+    k_obstacle_bc<<<grid_rows(ny + 2, nx + 1), kTile, 0, s>>>(u, v, fl, nx, ny, periodic, st);
     return last();
 }
 
@@ -900,7 +906,7 @@ cudaError_t launch_scalar_transport(const double* phi, const double* u, const do
                                     const double* diff, int limiter, int periodic,
                                     const ScalarBCView& bc, int obs_t, double obs_v, double* out,
                                     cudaStream_t s) {
-    k_scalar_transport<<<grid_rows(ny + 2, nx + 2), kBlock, 0, s>>>(phi, u, v, fl, nx, ny, dx, dy, diff,
+    k_scalar_transport<<<grid_rows(ny + 2, nx + 2), kTile, 0, s>>>(phi, u, v, fl, nx, ny, dx, dy, diff,
                                                                    limiter, periodic, bc, obs_t, obs_v,
                                                                    out, nullptr);
     return last();
@@ -909,9 +915,9 @@ cudaError_t launch_scalar_transport(const double* phi, const double* u, const do
 cudaError_t launch_mask(int kind, int nx, int ny, double dx, double dy, const double* q,
                         uint8_t* mask, cudaStream_t s) {
     const dim3 grd = grid_rows(ny, nx);
-    if (kind == 0) k_mask_circle<<<grd, kBlock, 0, s>>>(nx, ny, dx, dy, q[0], q[1], q[2], mask);
-    else if (kind == 1) k_mask_ellipse<<<grd, kBlock, 0, s>>>(nx, ny, dx, dy, q[0], q[1], q[2], q[3], q[4], q[5], mask);
-    else k_mask_rect<<<grd, kBlock, 0, s>>>(nx, ny, dx, dy, q[0], q[1], q[2], q[3], mask);
+    if (kind == 0) k_mask_circle<<<grd, kTile, 0, s>>>(nx, ny, dx, dy, q[0], q[1], q[2], mask);
+    else if (kind == 1) k_mask_ellipse<<<grd, kTile, 0, s>>>(nx, ny, dx, dy, q[0], q[1], q[2], q[3], q[4], q[5], mask);
+    else k_mask_rect<<<grd, kTile, 0, s>>>(nx, ny, dx, dy, q[0], q[1], q[2], q[3], mask);
     return last();
 }
 
@@ -927,8 +933,8 @@ cudaError_t stage_apply_bc(const cfd2d_sim& S, int begin, cudaStream_t s) {
 }
 
 cudaError_t stage_sst_pre(const cfd2d_sim& S, cudaStream_t s) {
-    k_sst_pre<<<grid_rows(S.ny, S.nx), kBlock, 0, s>>>(S);
-    k_sst_ghosts<<<grid_rows(S.ny + 2, S.nx + 2), kBlock, 0, s>>>(S);
+    k_sst_pre<<<grid_rows(S.ny, S.nx), kTile, 0, s>>>(S);
+    k_sst_ghosts<<<grid_rows(S.ny + 2, S.nx + 2), kTile, 0, s>>>(S);
     return last();
 }
 
@@ -938,18 +944,18 @@ cudaError_t stage_dt(const cfd2d_sim& S, cudaStream_t s) {
 }
 
 cudaError_t stage_predictor(const cfd2d_sim& S, int copy_only, cudaStream_t s) {
-    k_predictor<<<grid_rows(S.ny + 2, S.nx + 2), kBlock, 0, s>>>(S, copy_only);
+    k_predictor<<<grid_rows(S.ny + 2, S.nx + 2), kTile, 0, s>>>(S, copy_only);
     return last();
 }
 
 cudaError_t stage_correct(const cfd2d_sim& S, const double* p, int unit_dt, cudaStream_t s) {
-    k_correct<<<grid_rows(S.ny + 2, S.nx + 2), kBlock, 0, s>>>(S, p, unit_dt);
+    k_correct<<<grid_rows(S.ny + 2, S.nx + 2), kTile, 0, s>>>(S, p, unit_dt);
     return last();
 }
 
 cudaError_t stage_flow_shift(const cfd2d_sim& S, cudaStream_t s) {
     k_bulk<<<reduction_blocks(S.nx * S.ny), kBlock, 0, s>>>(S, S.red);
-    k_shift_u<<<grid_rows(S.ny + 2, S.nx + 1), kBlock, 0, s>>>(S);
+    k_shift_u<<<grid_rows(S.ny + 2, S.nx + 1), kTile, 0, s>>>(S);
     return last();
 }
 
@@ -957,11 +963,11 @@ cudaError_t stage_scalar(const cfd2d_sim& S, int slot, cudaStream_t s) {
     const cfd2d_scalar& sc = S.scalars[slot];
     if (sc.turb_div > 0.0 && S.variable_viscosity)
         k_scalar_turb_diff<<<reduction_blocks((S.nx + 2) * (S.ny + 2)), kBlock, 0, s>>>(S, slot);
-    k_scalar_rhs<<<grid_rows(S.ny + 2, S.nx + 2), kBlock, 0, s>>>(S, slot);
-    k_scalar_update<<<grid_rows(S.ny, S.nx), kBlock, 0, s>>>(S, slot);
+    k_scalar_rhs<<<grid_rows(S.ny + 2, S.nx + 2), kTile, 0, s>>>(S, slot);
+    k_scalar_update<<<grid_rows(S.ny, S.nx), kTile, 0, s>>>(S, slot);
     cudaError_t e = stage_scalar_ghosts(S, slot, s);
     if (e != cudaSuccess || sc.source != 2) return e;
-    k_sst_wall_omega<<<grid_rows(S.ny, S.nx), kBlock, 0, s>>>(S);
+    k_sst_wall_omega<<<grid_rows(S.ny, S.nx), kTile, 0, s>>>(S);
     return stage_scalar_ghosts(S, slot, s);
 }
 
@@ -970,7 +976,7 @@ cudaError_t stage_scalar_ghosts(const cfd2d_sim& S, int slot, cudaStream_t s) {
     const int n = S.nx + S.ny;
     k_scalar_ghost_domain<<<(n + kBlock - 1) / kBlock, kBlock, 0, s>>>(S, slot);
     if (S.has_solid)
-        k_scalar_ghost_solid<<<grid_rows(S.ny, S.nx), kBlock, 0, s>>>(S, slot, sc.obs_t == 1 ? 1 : 0, sc.obs_v);
+        k_scalar_ghost_solid<<<grid_rows(S.ny, S.nx), kTile, 0, s>>>(S, slot, sc.obs_t == 1 ? 1 : 0, sc.obs_v);
     return last();
 }
 
