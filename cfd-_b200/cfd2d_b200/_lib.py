@@ -169,9 +169,9 @@ def lib():
         "cfd2d_lpc_conv_dw": ([i, i, vp, i, vp, i, i, i, vp, vp, vp], i),
         "cfd2d_fcg_partial_doubles": ([i], sz),
         "cfd2d_fcg_init": ([vp, vp, vp, vp, d, d, vp, vp, vp, vp, vp, vp, vp, vp], i),
-        "cfd2d_fcg_pq": ([vp, vp, vp, vp, vp, vp], i),
-        "cfd2d_fcg_update": ([i, vp, vp, vp, vp, vp, vp, vp, vp], i),
-        "cfd2d_fcg_zr": ([i, vp, vp, vp, i, vp, vp, vp], i),
+        "cfd2d_fcg_pq": ([vp, vp, vp, vp, vp, vp, vp], i),
+        "cfd2d_fcg_update": ([i, vp, vp, vp, vp, vp, vp, vp], i),
+        "cfd2d_fcg_zr": ([i, vp, vp, i, vp, vp, vp], i),
         "cfd2d_fcg_dir": ([i, vp, vp, vp, vp], i),
         "cfd2d_fcg_net_in": ([i, vp, vp, vp, vp, vp], i),
         "cfd2d_fcg_net_out": ([i, vp, vp, vp, vp, vp, d, d, vp, vp], i),

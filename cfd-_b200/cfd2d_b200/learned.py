@@ -24,7 +24,7 @@ The network works on the dimensionless operator Ah = h^2 A (h^2 = 2 / (1/dx^2 +
 approximates Ah^-1 (r / ||r||). Training minimises the energy-norm error of that
 approximation, (e - o)^T Ah (e - o) with e = Ah^-1 r_hat, i.e. o^T Ah o - 2 o.r_hat
 (the constant e^T Ah e dropped), over residuals harvested from the plain solver's
-own iterations. Inside flexible CG (Polak-Ribiere) the preconditioner is
+own iterations. Inside flexible CG (Notay's form, one stored direction) the preconditioner is
 M(r) = h^2 ||r|| net(r / ||r||) + omega D^-1 r; the loop runs on the device inside
 one CUDA graph (a WHILE node) and falls back to the plain Jacobi-PCG from the
 current iterate when it stalls.
@@ -342,7 +342,7 @@ class LearnedPCG:
         n = self.nx * self.ny
         dev = _lib.device()
         z = lambda: t.zeros(n, dtype=t.float64, device=dev)  # noqa: E731
-        self.b, self.r, self.r_old, self.p, self.q, self.z = z(), z(), z(), z(), z(), z()
+        self.b, self.r, self.p, self.q, self.z = z(), z(), z(), z(), z()
         self.rhs_buf = z()
         self.net_in = t.zeros((self.nx, self.ny), dtype=t.float32, device=dev)
         self.partial = t.zeros(int(_lib.lib().cfd2d_fcg_partial_doubles(n)), dtype=t.float64, device=dev)
@@ -381,18 +381,19 @@ class LearnedPCG:
                                              P(self.partial), _lib.stream_ptr()), "fcg_init")
 
     def _body(self, handle: int):
-        """One iteration: z = M(r), beta, p = z + beta p, q = A p, x and r update, gate."""
+        """One iteration: z = M(r), beta = -(z . A p_old) / (p_old . A p_old), p = z + beta p,
+        q = A p, alpha = (p . r) / (p . q), x and r update, gate."""
         L = _lib.lib()
         s = _lib.stream_ptr()
         P = _lib.ptr
         n = self.nx * self.ny
         op = C.byref(self.ps.op)
         self.precondition()
-        _lib.check(L.cfd2d_fcg_zr(n, P(self.z), P(self.r), P(self.r_old), -1, P(self.scal), P(self.partial), s), "zr")
+        _lib.check(L.cfd2d_fcg_zr(n, P(self.z), P(self.q), -1, P(self.scal), P(self.partial), s), "zr")
         _lib.check(L.cfd2d_fcg_dir(n, P(self.z), P(self.p), P(self.scal), s), "dir")
-        _lib.check(L.cfd2d_fcg_pq(op, P(self.p), P(self.q), P(self.scal), P(self.partial), s), "pq")
-        _lib.check(L.cfd2d_fcg_update(n, P(self.ps._d_x0.view(-1)), P(self.r), P(self.r_old), P(self.p), P(self.q),
-                                      P(self.scal), P(self.partial), s), "update")
+        _lib.check(L.cfd2d_fcg_pq(op, P(self.p), P(self.q), P(self.r), P(self.scal), P(self.partial), s), "pq")
+        _lib.check(L.cfd2d_fcg_update(n, P(self.ps._d_x0.view(-1)), P(self.r), P(self.p), P(self.q), P(self.scal),
+                                      P(self.partial), s), "update")
         _lib.check(L.cfd2d_fcg_gate(P(self.scal), P(self.ctl), handle, s), "gate")
 
     def _set_control(self, tol):

@@ -91,22 +91,22 @@ int cfd2d_fcg_init(const cfd2d_poisson* op, const double* F, const double* G, co
     return status_of(fcg::init(*op, F, G, rhs, dx, dy, dt, b, x, r, p_zero, s, partial, as_stream(stream)));
 }
 
-int cfd2d_fcg_pq(const cfd2d_poisson* op, const double* p, double* q, cfd2d_fcg_scalars* s, double* partial,
-                 void* stream) {
-    if (!op || !p || !q || !s || !partial) return CFD2D_E_ARG;
-    return status_of(fcg::pq(*op, p, q, s, partial, as_stream(stream)));
-}
-
-int cfd2d_fcg_update(int n, double* x, double* r, double* r_old, const double* p, const double* q,
-                     cfd2d_fcg_scalars* s, double* partial, void* stream) {
-    if (n < 1 || !x || !r || !r_old || !p || !q || !s || !partial) return CFD2D_E_ARG;
-    return status_of(fcg::update(n, x, r, r_old, p, q, s, partial, as_stream(stream)));
-}
-
-int cfd2d_fcg_zr(int n, const double* z, const double* r, const double* r_old, int first, cfd2d_fcg_scalars* s,
+int cfd2d_fcg_pq(const cfd2d_poisson* op, const double* p, double* q, const double* r, cfd2d_fcg_scalars* s,
                  double* partial, void* stream) {
-    if (n < 1 || !z || !r || !r_old || !s || !partial) return CFD2D_E_ARG;
-    return status_of(fcg::zr(n, z, r, r_old, first, s, partial, as_stream(stream)));
+    if (!op || !p || !q || !r || !s || !partial) return CFD2D_E_ARG;
+    return status_of(fcg::pq(*op, p, q, r, s, partial, as_stream(stream)));
+}
+
+int cfd2d_fcg_update(int n, double* x, double* r, const double* p, const double* q, cfd2d_fcg_scalars* s,
+                     double* partial, void* stream) {
+    if (n < 1 || !x || !r || !p || !q || !s || !partial) return CFD2D_E_ARG;
+    return status_of(fcg::update(n, x, r, p, q, s, partial, as_stream(stream)));
+}
+
+int cfd2d_fcg_zr(int n, const double* z, const double* q, int first, cfd2d_fcg_scalars* s, double* partial,
+                 void* stream) {
+    if (n < 1 || !z || !q || !s || !partial) return CFD2D_E_ARG;
+    return status_of(fcg::zr(n, z, q, first, s, partial, as_stream(stream)));
 }
 
 int cfd2d_fcg_dir(int n, const double* z, double* p, const cfd2d_fcg_scalars* s, void* stream) {

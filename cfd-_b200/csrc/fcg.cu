@@ -1,5 +1,8 @@
-// fcg.cu - flexible conjugate gradients (Polak-Ribiere form) around a variable
-// preconditioner, for the learned Poisson preconditioner. Vectors are FP64 over the
+// fcg.cu - flexible conjugate gradients around a variable preconditioner, for the
+// learned Poisson preconditioner. The form is Notay's FCG with one stored
+// direction: beta = -(z . A p_old) / (p_old . A p_old), alpha = (p . r) / (p . A p).
+// Unlike the Polak-Ribiere form it relies on no positivity of r . M(r): every step
+// is an exact line search along p, so the A-norm of the error never grows. Vectors are FP64 over the
 // nx*ny interior cells; the operator is the matrix-free 5-point A of the
 // pressure solver (same data as cfd2d_poisson, same row summation order). Every
 // scalar (alpha, beta, r.z, ||r||^2) stays on the device: each reduction kernel
@@ -100,32 +103,33 @@ __global__ void k_init(cfd2d_poisson op, const double* F, const double* G, const
     }
 }
 
-// q = A p, alpha = rz / (p . q)
-__global__ void k_pq(cfd2d_poisson op, const double* p, double* q, FcgScalars* s, double* partial) {
+// q = A p, alpha = (p . r) / (p . q)
+__global__ void k_pq(cfd2d_poisson op, const double* p, double* q, const double* r, FcgScalars* s,
+                     double* partial) {
     const int n = op.nx * op.ny;
-    double v[1] = {0.0};
+    double v[2] = {0.0, 0.0};
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
         const double qq = apply_A(op, p, c);
         q[c] = qq;
         v[0] += p[c] * qq;
+        v[1] += p[c] * r[c];
     }
-    double tot[1];
-    if (reduce_last<1>(v, partial, &s->ticket, tot) && threadIdx.x == 0) {
+    double tot[2];
+    if (reduce_last<2>(v, partial, &s->ticket, tot) && threadIdx.x == 0) {
         s->pq = tot[0];
-        s->alpha = s->rz / tot[0];
+        s->rz = tot[1];
+        s->alpha = tot[1] / tot[0];
     }
 }
 
-// x += alpha p, r_old = r, r -= alpha q, ||r||^2
-__global__ void k_update(int n, double* x, double* r, double* r_old, const double* p, const double* q,
-                         FcgScalars* s, double* partial) {
+// x += alpha p, r -= alpha q, ||r||^2
+__global__ void k_update(int n, double* x, double* r, const double* p, const double* q, FcgScalars* s,
+                         double* partial) {
     const double alpha = s->alpha;
     double v[1] = {0.0};
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
         x[c] = x[c] + alpha * p[c];
-        const double ro = r[c];
-        r_old[c] = ro;
-        const double rn = ro - alpha * q[c];
+        const double rn = r[c] - alpha * q[c];
         r[c] = rn;
         v[0] += rn * rn;
     }
@@ -136,21 +140,15 @@ __global__ void k_update(int n, double* x, double* r, double* r_old, const doubl
     }
 }
 
-// beta = z.(r - r_old) / rz_old (0 on the first direction), rz = z.r
-__global__ void k_zr(int n, const double* z, const double* r, const double* r_old, int first_flag, FcgScalars* s,
-                     double* partial) {
+// beta = -(z . q_old) / (p_old . q_old) with q_old = A p_old (0 on the first direction)
+__global__ void k_zr(int n, const double* z, const double* q, int first_flag, FcgScalars* s, double* partial) {
     // first_flag < 0: the first direction is the one taken before any update (iters == 0)
     const int first = first_flag < 0 ? (s->iters == 0) : first_flag;
-    double v[2] = {0.0, 0.0};
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
-        v[0] += z[c] * r[c];
-        if (!first) v[1] += z[c] * (r[c] - r_old[c]);
-    }
-    double tot[2];
-    if (reduce_last<2>(v, partial, &s->ticket, tot) && threadIdx.x == 0) {
-        s->beta = first ? 0.0 : tot[1] / s->rz;
-        s->rz = tot[0];
-    }
+    double v[1] = {0.0};
+    if (!first)
+        for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) v[0] += z[c] * q[c];
+    double tot[1];
+    if (reduce_last<1>(v, partial, &s->ticket, tot) && threadIdx.x == 0) s->beta = first ? 0.0 : -tot[0] / s->pq;
 }
 
 // p = z + beta p
@@ -239,22 +237,22 @@ cudaError_t init(const cfd2d_poisson& op, const double* F, const double* G, cons
     return cudaGetLastError();
 }
 
-cudaError_t pq(const cfd2d_poisson& op, const double* p, double* q, FcgScalars* s, double* partial,
-               cudaStream_t st) {
-    const int n = op.nx * op.ny;
-    k_pq<<<blocks(n), T, 0, st>>>(op, p, q, s, partial);
-    return cudaGetLastError();
-}
-
-cudaError_t update(int n, double* x, double* r, double* r_old, const double* p, const double* q, FcgScalars* s,
-                   double* partial, cudaStream_t st) {
-    k_update<<<blocks(n), T, 0, st>>>(n, x, r, r_old, p, q, s, partial);
-    return cudaGetLastError();
-}
-
-cudaError_t zr(int n, const double* z, const double* r, const double* r_old, int first, FcgScalars* s,
+cudaError_t pq(const cfd2d_poisson& op, const double* p, double* q, const double* r, FcgScalars* s,
                double* partial, cudaStream_t st) {
-    k_zr<<<blocks(n), T, 0, st>>>(n, z, r, r_old, first, s, partial);
+    const int n = op.nx * op.ny;
+    k_pq<<<blocks(n), T, 0, st>>>(op, p, q, r, s, partial);
+    return cudaGetLastError();
+}
+
+cudaError_t update(int n, double* x, double* r, const double* p, const double* q, FcgScalars* s, double* partial,
+                   cudaStream_t st) {
+    k_update<<<blocks(n), T, 0, st>>>(n, x, r, p, q, s, partial);
+    return cudaGetLastError();
+}
+
+cudaError_t zr(int n, const double* z, const double* q, int first, FcgScalars* s, double* partial,
+               cudaStream_t st) {
+    k_zr<<<blocks(n), T, 0, st>>>(n, z, q, first, s, partial);
     return cudaGetLastError();
 }
 

@@ -40,12 +40,12 @@ size_t partial_doubles(int n);
 cudaError_t init(const cfd2d_poisson& op, const double* F, const double* G, const double* rhs, double dx,
                  double dy, const double* dt_ptr, double* b, double* x, double* r, double* p_zero, FcgScalars* s,
                  double* partial, cudaStream_t st);
-cudaError_t pq(const cfd2d_poisson& op, const double* p, double* q, FcgScalars* s, double* partial,
-               cudaStream_t st);
-cudaError_t update(int n, double* x, double* r, double* r_old, const double* p, const double* q, FcgScalars* s,
-                   double* partial, cudaStream_t st);
-cudaError_t zr(int n, const double* z, const double* r, const double* r_old, int first, FcgScalars* s,
+cudaError_t pq(const cfd2d_poisson& op, const double* p, double* q, const double* r, FcgScalars* s,
                double* partial, cudaStream_t st);
+cudaError_t update(int n, double* x, double* r, const double* p, const double* q, FcgScalars* s, double* partial,
+                   cudaStream_t st);
+cudaError_t zr(int n, const double* z, const double* q, int first, FcgScalars* s, double* partial,
+               cudaStream_t st);
 cudaError_t dir(int n, const double* z, double* p, const FcgScalars* s, cudaStream_t st);
 cudaError_t net_in(int n, const double* r, const FcgScalars* s, const uint8_t* mask, float* in, cudaStream_t st);
 cudaError_t net_out(int n, const float* out, const double* r, const double* dinv, const uint8_t* mask,

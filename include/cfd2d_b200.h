@@ -365,12 +365,16 @@ size_t cfd2d_fcg_partial_doubles(int n);
 int cfd2d_fcg_init(const cfd2d_poisson* op, const double* F, const double* G, const double* rhs, double dx,
                    double dy, const double* dt, double* b, double* x, double* r, double* p_zero,
                    cfd2d_fcg_scalars* s, double* partial, void* stream);
-int cfd2d_fcg_pq(const cfd2d_poisson* op, const double* p, double* q, cfd2d_fcg_scalars* s, double* partial,
-                 void* stream);
-int cfd2d_fcg_update(int n, double* x, double* r, double* r_old, const double* p, const double* q,
-                     cfd2d_fcg_scalars* s, double* partial, void* stream);
-int cfd2d_fcg_zr(int n, const double* z, const double* r, const double* r_old, int first, cfd2d_fcg_scalars* s,
+/* Notay's flexible CG with one stored direction (no reliance on r . M(r) > 0):
+ * pq: q = A p, pq = p . q, alpha = (p . r) / pq;  update: x += alpha p, r -= alpha q,
+ * rr = ||r||^2, iters += 1;  zr: beta = -(z . q) / pq with q = A p_old (0 when
+ * first != 0, or when first < 0 and iters == 0);  dir: p = z + beta p. */
+int cfd2d_fcg_pq(const cfd2d_poisson* op, const double* p, double* q, const double* r, cfd2d_fcg_scalars* s,
                  double* partial, void* stream);
+int cfd2d_fcg_update(int n, double* x, double* r, const double* p, const double* q, cfd2d_fcg_scalars* s,
+                     double* partial, void* stream);
+int cfd2d_fcg_zr(int n, const double* z, const double* q, int first, cfd2d_fcg_scalars* s, double* partial,
+                 void* stream);
 int cfd2d_fcg_dir(int n, const double* z, double* p, const cfd2d_fcg_scalars* s, void* stream);
 int cfd2d_fcg_net_in(int n, const double* r, const cfd2d_fcg_scalars* s, const uint8_t* mask, float* in,
                      void* stream);
