@@ -101,7 +101,7 @@ class FcgScalars(C.Structure):
 class FcgControl(C.Structure):
     _fields_ = [("rtol", C.c_double), ("stall_factor", C.c_double), ("stall_window", C.c_int32),
                 ("maxiter", C.c_int32), ("reason", C.c_int32), ("iters", C.c_int32), ("calls", C.c_int32),
-                ("pad", C.c_int32), ("hist", C.c_void_p)]
+                ("pad", C.c_int32), ("hist", C.c_void_p), ("iters_out", C.c_void_p)]
 
 
 FCG_RUNNING, FCG_CONVERGED, FCG_MAXITER, FCG_STALLED, FCG_NONFINITE = 0, 1, 2, 3, 4

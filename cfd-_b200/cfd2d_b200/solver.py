@@ -105,6 +105,7 @@ class Simulation:
         self._thermal = None
         self._sst = None
         self._graphs: dict = {}
+        self._learned = None
         self._mirrors: dict = {}
         self._hist_seen = 0
         self.history = History()
@@ -437,6 +438,10 @@ class Simulation:
         return g
 
     def _launch_steps(self, nsteps: int) -> None:
+        if self._learned is not None:
+            for _ in range(int(nsteps)):
+                self._learned_step()
+            return
         left = int(nsteps)
         for size in GRAPH_SIZES:
             while left >= size:
@@ -444,6 +449,39 @@ class Simulation:
                                                    _lib.stream_ptr(self._stream))
                 _lib.check(rc, "cfd2d_graph_launch")
                 left -= size
+
+    # ================================================================ learned pressure preconditioner
+    def set_pressure_preconditioner(self, net=None, **kw) -> None:
+        """Solve each step's pressure system by flexible CG with the learned
+        preconditioner ``net`` (cfd2d_b200.learned; keyword arguments go to
+        LearnedPCG), or with the plain Jacobi-PCG again when net is None. Needs an
+        outflow (Dirichlet) boundary. No counterpart in the reference."""
+        if self._learned is not None:
+            self._learned.close()
+            self._learned = None
+        if net is not None:
+            from .learned import LearnedPCG
+
+            with self._on_stream():
+                lp = LearnedPCG(self.pressure, net, **kw)
+            lp.iters_out = self._d_state.data_ptr() + _lib.State.cg_iters_step.offset
+            self._learned = lp
+
+    def _learned_step(self) -> None:
+        """step_begin, flexible CG on div(F, G)/dt inside one graph, the Jacobi-PCG
+        fallback if it stalled, p scattered into the padded field, step_finish."""
+        lp = self._learned
+        L = _lib.lib()
+        s = _lib.stream_ptr(self._stream)
+        self._call("cfd2d_sim_step_begin")
+        dt_ptr = C.c_void_p(self._d_state.data_ptr() + _lib.State.dt.offset)
+        lp.solve_into_x(F=self._F, G=self._G, dx=self.grid.dx, dy=self.grid.dy, dt_ptr=dt_ptr, key="sim")
+        if lp.last_reason in (_lib.FCG_STALLED, _lib.FCG_MAXITER):
+            # the plain solver continues from the flexible CG's iterate
+            self.pressure.solve((-lp.b).view(self.grid.nx, self.grid.ny))
+        _lib.check(L.cfd2d_fcg_scatter_p(C.byref(self.pressure.op), _lib.ptr(self.pressure._d_x0),
+                                         _lib.ptr(self._p), s), "fcg_scatter_p")
+        self._call("cfd2d_sim_step_finish")
 
     def _set_run_limits(self, t_end=math.inf, max_steps=-1, steady_tol=0.0):
         st = self._pull()

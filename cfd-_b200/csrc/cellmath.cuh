@@ -42,12 +42,20 @@ struct MomCoef {
     double idx, idy, idx2, idy2, nu0, gx, gy;  // gx = gamma*idx, gy = gamma*idy
 };
 
-CFD_HD MomCoef mom_coef(double dx, double dy, double gamma, double nu0) {
+// Reciprocal spacings, computed once on the host: the kernels then divide by
+// nothing per cell. Same IEEE operations as the reference's 1/dx, 1/dx**2.
+struct InvSpacing {
+    double idx, idy, idx2, idy2;
+};
+inline InvSpacing inv_spacing(double dx, double dy) {
+    return InvSpacing{1.0 / dx, 1.0 / dy, 1.0 / (dx * dx), 1.0 / (dy * dy)};
+}
+CFD_HD MomCoef mom_coef_inv(const InvSpacing& s, double gamma, double nu0) {
     MomCoef m;
-    m.idx2 = 1.0 / (dx * dx);
-    m.idy2 = 1.0 / (dy * dy);
-    m.idx = 1.0 / dx;
-    m.idy = 1.0 / dy;
+    m.idx2 = s.idx2;
+    m.idy2 = s.idy2;
+    m.idx = s.idx;
+    m.idy = s.idy;
     m.nu0 = nu0;
     m.gx = gamma * m.idx;
     m.gy = gamma * m.idy;

@@ -196,6 +196,7 @@ __global__ void k_gate(const FcgScalars* s, cfd2d_fcg_control* ctl, cudaGraphCon
     }
     ctl->reason = reason;
     ctl->iters = it;
+    if (ctl->iters_out) *ctl->iters_out = it;
     if (h) cudaGraphSetConditional(h, reason == CFD2D_FCG_RUNNING ? 1u : 0u);
 }
 

@@ -26,14 +26,14 @@ __device__ __forceinline__ bool v_fluid(const cfd2d_sim& S, Grid2 g, int i, int 
 
 // ================================================================ drop-in kernels
 __global__ void k_momentum(const double* u, const double* v, const uint8_t* fl, int nx, int ny,
-                           double dx, double dy, const double* nu, int variable, double gamma,
+                           InvSpacing inv, const double* nu, int variable, double gamma,
                            int periodic, double* hu, double* hv, const double* rho,
                            int var_density) {
     const Grid2 g{nx, ny};
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = (blockIdx.y * blockDim.y + threadIdx.y);
     if (j >= ny + 2 || i >= nx + 2) return;
-    const MomCoef m = mom_coef(dx, dy, gamma, nu[g.c(1, 1)]);
+    const MomCoef m = mom_coef_inv(inv, gamma, nu[g.c(1, 1)]);
     const int imax = periodic ? nx : nx - 1;
     if (i <= nx) {
         double h = 0.0;
@@ -405,7 +405,7 @@ __global__ void k_dt(cfd2d_sim S) {
 // force), the outflow extrapolation of F, G and u_prev, v_prev
 // (cfd2d/solver.py:338-368, cfd2d/models.py:386-396, cfd2d/boundary.py:225-245).
 // With copy_only, F = u and G = v plus the extrapolation (solver.py:199-201, 417-419).
-__global__ void k_predictor(cfd2d_sim S, int copy_only) {
+__global__ void k_predictor(cfd2d_sim S, int copy_only, InvSpacing inv) {
     cfd2d_state* st = S.state;
     if (!is_active(st)) return;
     const int nx = S.nx, ny = S.ny;
@@ -418,7 +418,7 @@ __global__ void k_predictor(cfd2d_sim S, int copy_only) {
     const double a = st->ab_a, b = st->ab_b;
     const double fx = S.body_fx + st->flow_force;
     const double fy = S.body_fy;
-    const MomCoef m = mom_coef(S.dx, S.dy, st->gamma, S.nu_eff[g.c(1, 1)]);
+    const MomCoef m = mom_coef_inv(inv, st->gamma, S.nu_eff[g.c(1, 1)]);
     const bool var = S.variable_viscosity != 0;
     const double* T = (S.thermal_index >= 0) ? S.scalars[S.thermal_index].phi : nullptr;
     const bool lo = S.bc_kind[0] == CFD2D_BC_OUTFLOW, ro = S.bc_kind[1] == CFD2D_BC_OUTFLOW;
@@ -890,8 +890,8 @@ cudaError_t launch_momentum(const double* u, const double* v, const uint8_t* fl,
                             double dx, double dy, const double* nu, int variable, double gamma,
                             int periodic, double* hu, double* hv, const double* rho, int var_density,
                             cudaStream_t s) {
-    k_momentum<<<grid_rows(ny + 2, nx + 2), kTile, 0, s>>>(u, v, fl, nx, ny, dx, dy, nu, variable, gamma,
-                                                           periodic, hu, hv, rho, var_density);
+    k_momentum<<<grid_rows(ny + 2, nx + 2), kTile, 0, s>>>(u, v, fl, nx, ny, inv_spacing(dx, dy), nu, variable,
+                                                           gamma, periodic, hu, hv, rho, var_density);
     return last();
 }
 
@@ -944,7 +944,7 @@ cudaError_t stage_dt(const cfd2d_sim& S, cudaStream_t s) {
 }
 
 cudaError_t stage_predictor(const cfd2d_sim& S, int copy_only, cudaStream_t s) {
-    k_predictor<<<grid_rows(S.ny + 2, S.nx + 2), kTile, 0, s>>>(S, copy_only);
+    k_predictor<<<grid_rows(S.ny + 2, S.nx + 2), kTile, 0, s>>>(S, copy_only, inv_spacing(S.dx, S.dy));
     return last();
 }
 

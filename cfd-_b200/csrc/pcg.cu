@@ -49,14 +49,21 @@ __device__ __forceinline__ double row_sum(bool periodic, int i, int nx, double t
     return (((tW + tS) + tC) + tN) + tE;
 }
 
-// Cluster-wide sum of K per-thread values. Block tree first; then lane r of warp 0
-// pushes this CTA's K partials into slot[me*K + k] of CTA r, so that after the
-// cluster barrier every CTA holds all C partials in its own shared memory and each
-// thread adds them in rank order: all threads of all CTAs get the same value.
+// Cluster-wide sum of K per-thread values. Block tree first: warp sums, then the
+// 16 warp partials combined by a 16-lane butterfly in warp 0, whose lane 0 stores
+// the CTA partial in this CTA's own slot. After the cluster barrier lanes 0..C-1 of
+// warp 0 each load one CTA's partial through DSMEM and a second butterfly adds
+// them; lane 0 leaves the sum in shared memory for the whole CTA. Every CTA adds
+// the same C values in the same lane positions, so all threads of all CTAs get the
+// same bits. Only local stores precede the barrier (remote stores there would
+// lengthen it); consecutive reductions alternate slot buffers, so a CTA rewrites a
+// slot only after the next barrier, which every reader passes after reading.
 template <int K>
 __device__ __forceinline__ void cluster_sum(cg::cluster_group& cluster, double (&v)[K],
                                             double* red_smem, double* slots, int C, int me) {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    static_assert(kPcgThreads == 512, "16 warps: the block stage is a 16-lane butterfly");
+    (void)me;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
     for (int k = 0; k < K; ++k) v[k] = warp_sum(v[k]);
     if (lane == 0) {
@@ -67,23 +74,38 @@ __device__ __forceinline__ void cluster_sum(cg::cluster_group& cluster, double (
     if (w == 0) {
         double x[K];
 #pragma unroll
-        for (int k = 0; k < K; ++k) {
-            x[k] = warp_sum((lane < nw) ? red_smem[k * 32 + lane] : 0.0);
-            x[k] = __shfl_sync(0xffffffffu, x[k], 0);
-        }
-        if (lane < C) {
-            double* dst = cluster.map_shared_rank(slots, lane);
+        for (int k = 0; k < K; ++k) x[k] = (lane < 16) ? red_smem[k * 32 + lane] : 0.0;
 #pragma unroll
-            for (int k = 0; k < K; ++k) dst[me * K + k] = x[k];
+        for (int o = 8; o > 0; o >>= 1) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) x[k] += __shfl_xor_sync(0xffffffffu, x[k], o);
+        }
+        if (lane == 0) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) slots[k] = x[k];
         }
     }
     cluster.sync();
+    // the result slots sit above the block-stage slots (k * 32 + w < 3 * 32 + 16)
+    double* result = red_smem + 32 * kMaxK - kMaxK;
+    if (w == 0) {
+        double y[K];
+        const double* src = cluster.map_shared_rank(slots, lane < C ? lane : 0);
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-        double s = slots[k];
-        for (int r = 1; r < C; ++r) s = s + slots[r * K + k];
-        v[k] = s;
+        for (int k = 0; k < K; ++k) y[k] = (lane < C) ? src[k] : 0.0;
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) y[k] += __shfl_xor_sync(0xffffffffu, y[k], o);
+        }
+        if (lane == 0) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) result[k] = y[k];
+        }
     }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = result[k];
 }
 
 }  // namespace

@@ -193,3 +193,54 @@ def test_training_lowers_the_energy_loss(L):
     log = learned.train(net, data, steps=150, batch=2, lr=2e-3, log_every=0)
     assert np.all(np.isfinite(log))
     assert np.mean(log[-20:]) < np.mean(log[:20]) and np.mean(log[-20:]) < 0.0
+
+
+def test_trained_network_reduces_iterations(L):
+    """What the shipped network gains over the method without it: the same solve
+    from zero to 1e-8 by flexible CG with the learned preconditioner against the
+    plain Jacobi-PCG, on held-out obstacle flows (seeds not in the training set)."""
+    torch, _lib, learned = L
+    net = learned.pretrained()
+    for seed in (11, 12):
+        rng = np.random.default_rng(seed)
+        case = learned.obstacle_case(rng, 256, 128)
+        sim = case.sim
+        sim.pressure.tol = 1e-8
+        sim.advance(2)
+        g = sim.grid
+        F, G = sim.F, sim.G
+        rhs = ((F[1:, 1:-1] - F[:-1, 1:-1]) / g.dx + (G[1:-1, 1:] - G[1:-1, :-1]) / g.dy) / sim.dt
+        ps = sim.pressure
+        zero = np.zeros(int(ps.fluid.sum()))
+        ps._x0 = zero
+        p_plain = ps.solve(rhs)
+        its_plain = ps.last_iterations
+        fcg = learned.LearnedPCG(ps, net)
+        ps._x0 = zero
+        p = fcg.solve(rhs)
+        assert fcg.last_reason == _lib.FCG_CONVERGED, (seed, fcg.last_reason, fcg.last_iterations)
+        assert fcg.last_total_iterations <= 0.7 * its_plain, (seed, fcg.last_total_iterations, its_plain)
+        assert relerr(p, p_plain) < 1e-4
+        fcg.close()
+
+
+def test_learned_pressure_solve_inside_the_step(L):
+    """Simulation.set_pressure_preconditioner: the same steps from the same state
+    with the plain and the learned pressure solve agree to the solver tolerance."""
+    torch, _lib, learned = L
+    net = learned.pretrained()
+    out = {}
+    for mode in ("plain", "learned"):
+        rng = np.random.default_rng(31)
+        case = learned.obstacle_case(rng, 256, 128)
+        sim = case.sim
+        sim.pressure.tol = 1e-8
+        sim.advance(20)
+        if mode == "learned":
+            sim.set_pressure_preconditioner(net)
+        sim.advance(4)
+        out[mode] = (sim.u.copy(), sim.v.copy(), list(sim.history.extra["cg_iterationen"][-4:]))
+        sim.set_pressure_preconditioner(None)
+    (up, vp, ip), (ul, vl, il) = out["plain"], out["learned"]
+    assert relerr(ul, up) < 1e-6 and relerr(vl, vp) < 1e-6
+    assert all(a > 0 for a in il) and sum(il) < sum(ip), (il, ip)
