@@ -15,6 +15,11 @@ e2e       = the same metric through the public API (``sim.step()``) with the sta
 roofline  = the pressure solver kernel: algorithmic bytes 88 B per cell per CG
             iteration (FP64 x, r, p, q, z traffic of a streaming implementation)
             over its event-timed duration.
+stencils  = the kernel-level stencil drop-ins on a 4096 x 2048 grid against the
+            measured HBM peak (compulsory bytes per cell over event time).
+learned_pc = Poisson ms and iterations at 1e-8 on a seeded 1024 x 512 obstacle flow:
+            plain Jacobi-PCG against flexible CG with the shipped learned
+            preconditioner.
 --impl reference times the CPU restatement of the reference (the oracle: NumPy
 stencils and scipy's CG iteration) on the same workload.
 """
@@ -279,6 +284,51 @@ def stencil_roofline(peak: float, reps: int = 10) -> dict:
     return {"grid": [nx, ny], "l2": "flushed before each launch", **res}
 
 
+# ------------------------------------------------------------------ learned preconditioner
+def learned_section() -> dict:
+    """Pressure solve of a seeded 1024 x 512 obstacle flow (2-12 obstacles, uniform
+    inflow, outflow p = 0) to 1e-8: plain Jacobi-PCG against flexible CG with the
+    shipped learned preconditioner, from the same warm start (the previous step's
+    pressure), event-timed on the device after one untimed warm-up solve each."""
+    import numpy as np
+    import torch
+
+    from cfd2d_b200 import learned
+
+    rng = np.random.default_rng(13)
+    case = learned.obstacle_case(rng, 1024, 512)
+    sim = case.sim
+    sim.pressure.tol = CG_RTOL
+    sim.advance(1)
+    ps = sim.pressure
+    xprev = ps._d_x0.clone()
+    sim.advance(1)
+    g = sim.grid
+    F, G = sim.F, sim.G
+    rhs = torch.from_numpy(((F[1:, 1:-1] - F[:-1, 1:-1]) / g.dx + (G[1:-1, 1:] - G[1:-1, :-1]) / g.dy)
+                           / sim.dt).cuda()
+    fcg = learned.LearnedPCG(ps, learned.pretrained(), maxiter=6000)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    out = {"workload": "obstacles 1024x512 (seed 13), warm start, FP64, rtol 1e-8"}
+    for name, solve in (("plain", lambda: ps.solve(rhs)), ("learned", lambda: fcg.solve(rhs))):
+        for timed in (False, True):
+            ps._d_x0.copy_(xprev)
+            torch.cuda.synchronize()
+            ev[0].record()
+            solve()
+            ev[1].record()
+            torch.cuda.synchronize()
+        its = ps.last_iterations if name == "plain" else fcg.last_total_iterations
+        out[name] = {"poisson_ms": ev[0].elapsed_time(ev[1]), "iterations": int(its)}
+        if name == "learned":
+            out[name]["fcg_iterations"] = int(fcg.last_iterations)
+            out[name]["fell_back"] = bool(fcg.last_reason != 1)
+    fcg.close()
+    del sim, case
+    torch.cuda.empty_cache()
+    return out
+
+
 # ------------------------------------------------------------------ GPU arm
 def run_b200(args, dist, rank, world):
     import numpy as np
@@ -385,6 +435,12 @@ def run_b200(args, dist, rank, world):
     if rank != 0:
         return
     stencils = stencil_roofline(peak) if not args.no_stencils else None
+    learned_pc = None
+    if not args.no_learned:
+        try:
+            learned_pc = learned_section()
+        except Exception as exc:  # an optional section never costs the bench line
+            learned_pc = {"error": f"{type(exc).__name__}: {exc}"}
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         d = cpu_oracle_rate(3, 1, 1)
@@ -411,6 +467,7 @@ def run_b200(args, dist, rank, world):
         "cpu_baseline": cpu,
         "clocks": clocks,
         "stencils": stencils,
+        "learned_pc": learned_pc,
     }
     print(json.dumps(line), flush=True)
 
@@ -423,6 +480,7 @@ def main():
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-stencils", action="store_true", help="skip the stencil-kernel roofline section")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner section")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -25,10 +25,97 @@ __device__ __forceinline__ bool v_fluid(const cfd2d_sim& S, Grid2 g, int i, int 
 }
 
 // ================================================================ drop-in kernels
-__global__ void k_momentum(const double* u, const double* v, const uint8_t* fl, int nx, int ny,
-                           InvSpacing inv, const double* nu, int variable, double gamma,
-                           int periodic, double* hu, double* hv, const double* rho,
-                           int var_density) {
+// row kernels: 2D tiles of kTileX (along j, contiguous) x kTileY (along i) threads, so
+// that the stencil rows a block reads are shared through L1 by its warps
+constexpr int kTileX = 32, kTileY = 8;
+
+// TVD transport (cfd2d/kernels.py:271-391) of the kTileY x kTileX cells of one block,
+// every interior face flux computed once and shared by its two cells. FX[r][c] holds
+// xflux/dx of the west face of cell (i0 + r, j0 + c) (row kTileY: the east face of
+// the tile's last row, which is also the periodic face nx -> 1); FY[r][c] holds
+// yflux/dy of the south face of cell (i0 + r, j0 + c). The cell then assembles
+// ((west + east) + south) + north exactly as transport_cell does, with -FX / -FY for
+// its east and north faces, so the result is bit-identical. Every thread of the
+// block must call it (it synchronises the block).
+__device__ __forceinline__ double transport_tile(const double* __restrict__ phi, const double* __restrict__ u,
+                                                 const double* __restrict__ v, const uint8_t* __restrict__ fl,
+                                                 const double* __restrict__ diff, Grid2 g, double dx, double dy,
+                                                 int lim, bool periodic, const ScalarBCView& bc, int obs_t,
+                                                 double obs_v) {
+    __shared__ double FX[kTileY + 1][kTileX];
+    __shared__ double FY[kTileY][kTileX + 1];
+    const int nx = g.nx, ny = g.ny;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int j = blockIdx.x * kTileX + tx;
+    const int i = blockIdx.y * kTileY + ty;
+    const bool jin = (j >= 1 && j <= ny);
+    // west face of cell ii (1 <= ii <= nx + 1); the domain faces are not shared
+    auto west = [&](int ii) -> double {
+        int L, R, fi;
+        if (ii == 1 || ii == nx + 1) {
+            if (!periodic) return 0.0;
+            L = nx; R = 1; fi = nx;
+        } else {
+            L = ii - 1; R = ii; fi = ii - 1;
+        }
+        if (!(fl[g.c(L, j)] && fl[g.c(R, j)])) return 0.0;
+        return xflux(phi, u, fl, diff, g, dx, lim, periodic, fi, L, R, j) / dx;
+    };
+    // south face of cell jj (2 <= jj <= ny)
+    auto south = [&](int jj) -> double {
+        if (!(fl[g.c(i, jj - 1)] && fl[g.c(i, jj)])) return 0.0;
+        return yflux(phi, v, fl, diff, g, dy, lim, i, jj - 1) / dy;
+    };
+    if (jin && i >= 1 && i <= nx + 1) {
+        FX[ty][tx] = west(i);
+        if (ty == kTileY - 1 && i + 1 <= nx + 1) FX[kTileY][tx] = west(i + 1);
+    }
+    if (i >= 1 && i <= nx && j >= 2 && j <= ny) FY[ty][tx] = south(j);
+    if (tx == kTileX - 1 && i >= 1 && i <= nx && j + 1 >= 2 && j + 1 <= ny) FY[ty][kTileX] = south(j + 1);
+    __syncthreads();
+    if (!(jin && i >= 1 && i <= nx) || !fl[g.c(i, j)]) return 0.0;
+    const double phP = phi[g.c(i, j)];
+    const double DP = diff[g.c(i, j)];
+    double xw = 0.0, xe = 0.0, ys = 0.0, yn = 0.0;
+    if (i == 1 && !periodic) {
+        xw = boundary_term(u[g.u(0, j)], phP, DP, bc.bt[0][j - 1], bc.bv[0][j - 1], dx);
+    } else {
+        const int L = (i == 1) ? nx : i - 1;
+        if (fl[g.c(L, j)]) xw = FX[ty][tx];
+        else if (obs_t == 1) xw = ((DP * (obs_v - phP)) / (0.5 * dx)) / dx;
+    }
+    if (i == nx && !periodic) {
+        xe = boundary_term(-u[g.u(nx, j)], phP, DP, bc.bt[1][j - 1], bc.bv[1][j - 1], dx);
+    } else {
+        const int R = (i == nx) ? 1 : i + 1;
+        if (fl[g.c(R, j)]) xe = -FX[ty + 1][tx];
+        else if (obs_t == 1) xe = ((DP * (obs_v - phP)) / (0.5 * dx)) / dx;
+    }
+    if (j == 1) {
+        ys = boundary_term(v[g.v(i, 0)], phP, DP, bc.bt[2][i - 1], bc.bv[2][i - 1], dy);
+    } else {
+        if (fl[g.c(i, j - 1)]) ys = FY[ty][tx];
+        else if (obs_t == 1) ys = ((DP * (obs_v - phP)) / (0.5 * dy)) / dy;
+    }
+    if (j == ny) {
+        yn = boundary_term(-v[g.v(i, ny)], phP, DP, bc.bt[3][i - 1], bc.bv[3][i - 1], dy);
+    } else {
+        if (fl[g.c(i, j + 1)]) yn = -FY[ty][tx + 1];
+        else if (obs_t == 1) yn = ((DP * (obs_v - phP)) / (0.5 * dy)) / dy;
+    }
+    return ((xw + xe) + ys) + yn;
+}
+
+// Inputs and outputs never alias (the C ABI requires it): __restrict__ lets the
+// compiler issue every stencil load of a thread before its stores.
+// The viscosity and density forms are template parameters, so each instance carries
+// only the arithmetic it needs.
+template <bool VARIABLE, bool VAR_DENSITY>
+__global__ void __launch_bounds__(256) k_momentum(const double* __restrict__ u, const double* __restrict__ v,
+                                                  const uint8_t* __restrict__ fl, int nx, int ny, InvSpacing inv,
+                                                  const double* __restrict__ nu, double gamma, int periodic,
+                                                  double* __restrict__ hu, double* __restrict__ hv,
+                                                  const double* __restrict__ rho) {
     const Grid2 g{nx, ny};
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = (blockIdx.y * blockDim.y + threadIdx.y);
@@ -38,13 +125,13 @@ __global__ void k_momentum(const double* u, const double* v, const uint8_t* fl, 
     if (i <= nx) {
         double h = 0.0;
         if (i >= 1 && i <= imax && j >= 1 && j <= ny)
-            h = mom_u(u, v, fl, nu, rho, g, m, variable != 0, var_density != 0, i, j);
+            h = mom_u(u, v, fl, nu, rho, g, m, VARIABLE, VAR_DENSITY, i, j);
         hu[g.u(i, j)] = h;
     }
     if (j <= ny) {
         double h = 0.0;
         if (i >= 1 && i <= nx && j >= 1 && j <= ny - 1)
-            h = mom_v(u, v, fl, nu, rho, g, m, variable != 0, var_density != 0, i, j);
+            h = mom_v(u, v, fl, nu, rho, g, m, VARIABLE, VAR_DENSITY, i, j);
         hv[g.v(i, j)] = h;
     }
 }
@@ -69,19 +156,20 @@ __global__ void k_obstacle_bc(double* u, double* v, const uint8_t* fl, int nx, i
     if (i >= 1 && i <= nx && j >= 1 && j <= ny - 1) v[g.v(i, j)] = obc_v(v, fl, g, i, j);
 }
 
-__global__ void k_scalar_transport(const double* phi, const double* u, const double* v,
-                                   const uint8_t* fl, int nx, int ny, double dx, double dy,
-                                   const double* diff, int limiter, int periodic, ScalarBCView bc,
-                                   int obs_t, double obs_v, double* out, const cfd2d_state* st) {
-    if (!is_active(st)) return;
+__global__ void __launch_bounds__(256) k_scalar_transport(const double* __restrict__ phi,
+                                                          const double* __restrict__ u,
+                                                          const double* __restrict__ v,
+                                                          const uint8_t* __restrict__ fl, int nx, int ny,
+                                                          double dx, double dy, const double* __restrict__ diff,
+                                                          int limiter, int periodic, ScalarBCView bc, int obs_t,
+                                                          double obs_v, double* __restrict__ out,
+                                                          const cfd2d_state* st) {
+    if (!is_active(st)) return;  // uniform over the grid
     const Grid2 g{nx, ny};
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = (blockIdx.y * blockDim.y + threadIdx.y);
-    if (j >= ny + 2 || i >= nx + 2) return;
-    double r = 0.0;
-    if (i >= 1 && i <= nx && j >= 1 && j <= ny)
-        r = transport_cell(phi, u, v, fl, diff, g, dx, dy, limiter, periodic != 0, bc, obs_t, obs_v, i, j);
-    out[g.c(i, j)] = r;
+    const double r = transport_tile(phi, u, v, fl, diff, g, dx, dy, limiter, periodic != 0, bc, obs_t, obs_v);
+    if (j < ny + 2 && i < nx + 2) out[g.c(i, j)] = r;
 }
 
 // cfd2d/geometry.py:17-22: (X - xc)**2 + (Y - yc)**2 <= r**2, X = (i + 0.5) * dx
@@ -607,15 +695,13 @@ __global__ void k_scalar_rhs(cfd2d_sim S, int s) {
     const Grid2 g{nx, ny};
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = (blockIdx.y * blockDim.y + threadIdx.y);
-    if (j >= ny + 2 || i >= nx + 2) return;
     const cfd2d_scalar& sc = S.scalars[s];
     ScalarBCView bc;
     for (int k = 0; k < 4; ++k) { bc.bt[k] = sc.bt[k]; bc.bv[k] = sc.bv[k]; }
-    double r = 0.0;
-    if (i >= 1 && i <= nx && j >= 1 && j <= ny)
-        r = transport_cell(sc.phi, S.u, S.v, S.fluid, sc.diff, g, S.dx, S.dy, sc.limiter,
-                           S.periodic != 0, bc, sc.obs_t, sc.obs_v, i, j);
-    sc.rhs[g.c(i, j)] = r;
+    // rhs does not overlap phi, u, v, diff or the flags
+    const double r = transport_tile(sc.phi, S.u, S.v, S.fluid, sc.diff, g, S.dx, S.dy, sc.limiter,
+                                    S.periodic != 0, bc, sc.obs_t, sc.obs_v);
+    if (j < ny + 2 && i < nx + 2) sc.rhs[g.c(i, j)] = r;
 }
 
 // Euler update with point-implicit source and clipping (cfd2d/models.py:196-207);
@@ -869,9 +955,6 @@ __global__ void k_end_step(cfd2d_sim S) {
 
 // ================================================================ host launchers
 namespace {
-// row kernels: 2D tiles of kTileX (along j, contiguous) x kTileY (along i) threads, so
-// that the stencil rows a block reads are shared through L1 by its warps
-constexpr int kTileX = 32, kTileY = 8;
 const dim3 kTile(kTileX, kTileY, 1);
 inline dim3 grid_rows(int width, int rows) {
     return dim3((width + kTileX - 1) / kTileX, (rows + kTileY - 1) / kTileY, 1);
@@ -890,8 +973,16 @@ cudaError_t launch_momentum(const double* u, const double* v, const uint8_t* fl,
                             double dx, double dy, const double* nu, int variable, double gamma,
                             int periodic, double* hu, double* hv, const double* rho, int var_density,
                             cudaStream_t s) {
-    k_momentum<<<grid_rows(ny + 2, nx + 2), kTile, 0, s>>>(u, v, fl, nx, ny, inv_spacing(dx, dy), nu, variable,
-                                                           gamma, periodic, hu, hv, rho, var_density);
+    const InvSpacing inv = inv_spacing(dx, dy);
+    const dim3 grd = grid_rows(ny + 2, nx + 2);
+    if (variable && var_density)
+        k_momentum<true, true><<<grd, kTile, 0, s>>>(u, v, fl, nx, ny, inv, nu, gamma, periodic, hu, hv, rho);
+    else if (variable)
+        k_momentum<true, false><<<grd, kTile, 0, s>>>(u, v, fl, nx, ny, inv, nu, gamma, periodic, hu, hv, rho);
+    else if (var_density)
+        k_momentum<false, true><<<grd, kTile, 0, s>>>(u, v, fl, nx, ny, inv, nu, gamma, periodic, hu, hv, rho);
+    else
+        k_momentum<false, false><<<grd, kTile, 0, s>>>(u, v, fl, nx, ny, inv, nu, gamma, periodic, hu, hv, rho);
     return last();
 }
 

@@ -542,7 +542,7 @@ __device__ bool grid_barrier(unsigned int* bar, int* status) {
                     ok = 0;
                     break;
                 }
-                __nanosleep(64);
+                __nanosleep(16);
             }
         }
         __threadfence();
@@ -552,26 +552,37 @@ __device__ bool grid_barrier(unsigned int* bar, int* status) {
 }
 
 // grid-wide sum of K values: block tree, partials to part[b*kSlot + k], barrier,
-// then every warp adds the G partials in the same fixed order.
+// then warp 0 of every block adds the G partials in one fixed order (lane-strided,
+// then a butterfly, so every block gets the same bits) and shares the sums through
+// shared memory. (Having every warp read all G partials cost a third of an
+// iteration at 1024 x 512.)
 template <int K>
 __device__ __forceinline__ bool grid_sum(double (&v)[K], double* red_smem, double* part,
                                          unsigned int* bar, int* status) {
+    static_assert(K <= CFD2D_MAX_COMPONENTS + 1, "gsum holds at most MAX_COMPONENTS + 1 values");
     block_sum<K>(v, red_smem);
     if (threadIdx.x == 0) {
 #pragma unroll
         for (int k = 0; k < K; ++k) part[(size_t)blockIdx.x * kSlot + k] = v[k];
     }
     if (!grid_barrier(bar, status)) return false;
-    const int lane = threadIdx.x & 31;
-    const int G = gridDim.x;
+    __shared__ double gsum[CFD2D_MAX_COMPONENTS + 1];
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        const int G = gridDim.x;
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-        double x = 0.0;
-        for (int b = lane; b < G; b += 32) x += __ldcg(&part[(size_t)b * kSlot + k]);
+        for (int k = 0; k < K; ++k) {
+            double x = 0.0;
+            for (int b = lane; b < G; b += 32) x += __ldcg(&part[(size_t)b * kSlot + k]);
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-        v[k] = x;
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+            if (lane == 0) gsum[k] = x;
+        }
     }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = gsum[k];
+    // gsum is rewritten by the next reduction only after its block tree and barrier
     return true;
 }
 

@@ -172,7 +172,8 @@ typedef struct cfd2d_sim {
 
 /* ---- kernel-level entry points (drop-in for cfd2d/kernels.py) ------------ */
 
-/* hu, hv = diffusion - convection on fluid faces; zero elsewhere.
+/* hu, hv = diffusion - convection on fluid faces; zero elsewhere. hu and hv must
+ * not overlap any input array.
  * Replaces cfd2d/kernels.py:44-46 momentum_tendencies(u, v, fluid, nx, ny, dx,
  * dy, nu, variable, gamma, periodic, hu, hv, rho, var_density). */
 int cfd2d_momentum_tendencies(const double* u, const double* v, const uint8_t* fluid, int nx,
@@ -185,7 +186,8 @@ int cfd2d_momentum_tendencies(const double* u, const double* v, const uint8_t* f
 int cfd2d_obstacle_bc(double* u, double* v, const uint8_t* fluid, int nx, int ny, int periodic,
                       void* stream);
 
-/* out = -div(u phi) + div(D grad phi) on fluid cells (TVD faces).
+/* out = -div(u phi) + div(D grad phi) on fluid cells (TVD faces); out must not
+ * overlap any input array.
  * Replaces cfd2d/kernels.py:254-256 scalar_transport(phi, u, v, fluid, nx, ny,
  * dx, dy, diff, limiter, periodic, bt_l, bv_l, bt_r, bv_r, bt_b, bv_b, bt_t,
  * bv_t, obs_t, obs_v, out). bt_* are int64 arrays, bv_* float64 arrays of
@@ -403,6 +405,7 @@ typedef struct cfd2d_fcg_control {
                                  on the loop independent of the iteration counter */
     int32_t pad;
     double* hist;             /* device, maxiter + 1 residual norms */
+    int32_t* iters_out;       /* device, may be NULL: also receives the iteration count */
 } cfd2d_fcg_control;
 
 /* One thread: record ||r||, apply the stop tests, set the WHILE condition `handle`
