@@ -17,6 +17,8 @@ roofline  = the pressure solver kernel: algorithmic bytes 88 B per cell per CG
             over its event-timed duration.
 stencils  = the kernel-level stencil drop-ins on a 4096 x 2048 grid against the
             measured HBM peak (compulsory bytes per cell over event time).
+mixed_precision = the workload with FP32 solver iterations and FP64 refinement against
+            the FP64 solver: ms per step and the per-field error of the end state.
 learned_pc = Poisson ms and iterations at 1e-8 on a seeded 1024 x 512 obstacle flow:
             plain Jacobi-PCG against flexible CG with the shipped learned
             preconditioner.
@@ -329,6 +331,47 @@ def learned_section() -> dict:
     return out
 
 
+# ------------------------------------------------------------------ mixed precision
+def mixed_section(steps: int = 300) -> dict:
+    """The bench workload from rest, `steps` steps with the FP64 solver and with the
+    mixed one (FP32 iterations, FP64 refinement and reductions): ms per step from
+    events around the run, and the end state of the mixed run against the FP64 one
+    (max-norm of the difference over the max-norm of the FP64 field; the drag and
+    lift series over the last 100 steps)."""
+    import numpy as np
+    import torch
+
+    from cfd2d_b200 import cases
+
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    res = {}
+    for prec in ("fp64", "mixed"):
+        case = cases.build_case(SPEC)
+        sim = case.sim
+        sim.pressure.tol = CG_RTOL
+        sim.pressure.precision = prec
+        sim.advance(5)
+        torch.cuda.synchronize()
+        ev[0].record(torch.cuda.current_stream())
+        sim.advance(steps)
+        ev[1].record(torch.cuda.current_stream())
+        torch.cuda.synchronize()
+        its = sim.history.extra["cg_iterationen"][-steps:]
+        res[prec] = dict(ms_per_step=ev[0].elapsed_time(ev[1]) / steps, iters=float(np.mean(its)),
+                         fields=(sim.u.copy(), sim.v.copy(), sim.p.copy(), sim.scalars["c"].phi.copy()),
+                         fx=np.array(sim.history.fx[-100:]), fy=np.array(sim.history.fy[-100:]))
+    e = lambda a, b: float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))  # noqa: E731
+    f64, mx = res["fp64"], res["mixed"]
+    return {
+        "workload": f"{WORKLOAD}, {steps} steps after 5 from rest",
+        "fp64": {"ms_per_step": f64["ms_per_step"], "poisson_iters_per_step": f64["iters"]},
+        "mixed": {"ms_per_step": mx["ms_per_step"], "poisson_iters_per_step": mx["iters"]},
+        "rel_err_vs_fp64": {"u": e(mx["fields"][0], f64["fields"][0]), "v": e(mx["fields"][1], f64["fields"][1]),
+                            "p": e(mx["fields"][2], f64["fields"][2]), "c": e(mx["fields"][3], f64["fields"][3]),
+                            "drag_force": e(mx["fx"], f64["fx"]), "lift_force": e(mx["fy"], f64["fy"])},
+    }
+
+
 # ------------------------------------------------------------------ GPU arm
 def run_b200(args, dist, rank, world):
     import numpy as np
@@ -435,6 +478,12 @@ def run_b200(args, dist, rank, world):
     if rank != 0:
         return
     stencils = stencil_roofline(peak) if not args.no_stencils else None
+    mixed = None
+    if not args.no_mixed:
+        try:
+            mixed = mixed_section()
+        except Exception as exc:  # an optional section never costs the bench line
+            mixed = {"error": f"{type(exc).__name__}: {exc}"}
     learned_pc = None
     if not args.no_learned:
         try:
@@ -468,6 +517,7 @@ def run_b200(args, dist, rank, world):
         "clocks": clocks,
         "stencils": stencils,
         "learned_pc": learned_pc,
+        "mixed_precision": mixed,
     }
     print(json.dumps(line), flush=True)
 
@@ -481,6 +531,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-stencils", action="store_true", help="skip the stencil-kernel roofline section")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner section")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision section")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

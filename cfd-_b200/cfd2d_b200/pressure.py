@@ -153,7 +153,25 @@ class PressureSolver:
         else:
             P.work, P.work_bytes = 0, 0
         P.cluster = self.cluster
+        P.mixed = 0
         self.op = P
+
+    @property
+    def precision(self) -> str:
+        """"fp64": the reference's iteration (scipy's CG form) in FP64; "mixed": FP32
+        iterations with FP64 residual refinement and FP64 reductions, to the same
+        relative residual (on-chip solver only; no counterpart in the reference)."""
+        return "mixed" if self.op.mixed else "fp64"
+
+    @precision.setter
+    def precision(self, value: str) -> None:
+        if value not in ("fp64", "mixed"):
+            raise ValueError(f"precision must be 'fp64' or 'mixed', not {value!r}")
+        if value == "mixed" and self.cluster == 0:
+            raise ValueError("the mixed-precision solver runs on the on-chip (cluster) solver only")
+        self.op.mixed = int(value == "mixed")
+        if self.on_change is not None:
+            self.on_change()
 
     @property
     def tol(self) -> float:

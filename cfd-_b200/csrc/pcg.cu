@@ -479,6 +479,302 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cluster(PcgLaunch L) {
 #undef SLOTS
 }
 
+// ---------------------------------------------------------------- mixed precision
+// Ordered row sum in FP32 (the inner iterations of the mixed solver).
+__device__ __forceinline__ float row_sum_f(bool periodic, int i, int nx, float tW, float tS, float tC, float tN,
+                                           float tE) {
+    if (periodic && i == 0) return (((tS + tC) + tN) + tE) + tW;
+    if (periodic && i == nx - 1) return (((tE + tW) + tS) + tC) + tN;
+    return (((tW + tS) + tC) + tN) + tE;
+}
+
+// Jacobi-PCG with FP32 iterations and FP64 iterative refinement, cluster-resident
+// (an upgrade beside the scipy-form solver above; no reference counterpart).
+// Outer loop in FP64: r = b - A x, stop when ||r|| < rtol ||b||; otherwise an FP32
+// Jacobi-PCG solves A d = r from d = 0 until its recursive residual falls below
+// kInnerTol ||r||, and x += d in FP64. Every dot product is accumulated and reduced
+// in FP64. Shared memory per cell: x and b in FP64, d, r, p (two buffers), z,
+// 1/diag and diag in FP32, the coupling bits: 45 bytes.
+constexpr float kInnerTol = 1e-4f;
+
+template <int CPT>
+__global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cluster_mixed(PcgLaunch L) {
+    cg::cluster_group cluster = cg::this_cluster();
+    const int C = (int)cluster.num_blocks();
+    const int me = (int)cluster.block_rank();
+    if (L.active && *L.active == 0) return;  // uniform over the cluster
+
+    const cfd2d_poisson& op = L.op;
+    const int nx = op.nx, ny = op.ny;
+    const bool periodic = op.periodic != 0;
+    const int r0 = row0_of(me, nx, C), r1 = row0_of(me + 1, nx, C);
+    const int rows = r1 - r0;
+    const int nloc = rows * ny;
+    const int cap = L.cap_cells;
+    const int tid = threadIdx.x;
+    const double mdx2 = -op.dx2, mdy2 = -op.dy2;
+    const float fdx2 = (float)mdx2, fdy2 = (float)mdy2;
+    const int goff = r0 * ny;
+
+    extern __shared__ __align__(16) double sm[];
+    double* X = sm;
+    double* B = X + cap;
+    float* D = reinterpret_cast<float*>(B + cap);
+    float* R = D + cap;
+    float* P0 = R + cap;
+    float* P1 = P0 + cap;
+    float* Z = P1 + cap;
+    float* DI = Z + cap;
+    float* DG = DI + cap;
+    uint8_t* NB = reinterpret_cast<uint8_t*>(DG + cap);
+    __shared__ double red_smem[32 * kMaxK];
+    __shared__ double slotsA[16 * kMaxK];
+    __shared__ double slotsB[16 * kMaxK];
+    __shared__ double cmean[CFD2D_MAX_COMPONENTS];
+    int nred = 0;
+#define SLOTS() ((nred++ & 1) ? slotsB : slotsA)
+
+    const unsigned magic = (unsigned)(((1ull << 32) + (unsigned)ny - 1) / (unsigned)ny);
+    // neighbouring rows in other CTAs: their x (FP64) and their FP32 arrays at j = 0
+    const double* baseWx = nullptr;
+    const double* baseEx = nullptr;
+    const float* baseWf = nullptr;
+    const float* baseEf = nullptr;
+    {
+        const int iw = (r0 == 0) ? (periodic ? nx - 1 : -1) : r0 - 1;
+        const int ie = (r1 == nx) ? (periodic ? 0 : -1) : r1;
+        if (iw >= 0) {
+            const int o = owner_of(iw, nx, C);
+            const int off = (iw - row0_of(o, nx, C)) * ny;
+            baseWx = cluster.map_shared_rank(X, o) + off;
+            baseWf = cluster.map_shared_rank(D, o) + off;
+        }
+        if (ie >= 0) {
+            const int o = owner_of(ie, nx, C);
+            const int off = (ie - row0_of(o, nx, C)) * ny;
+            baseEx = cluster.map_shared_rank(X, o) + off;
+            baseEf = cluster.map_shared_rank(D, o) + off;
+        }
+    }
+
+    // ------------------------------------------------------------ prologue
+    double dt = 1.0;
+    if (L.rhs_mode == 1) dt = L.dt_ptr ? *L.dt_ptr : L.dt_const;
+    for (int c = tid; c < nloc; c += kPcgThreads) {
+        const int gidx = goff + c;
+        const uint8_t nb = op.nbr[gidx];
+        NB[c] = nb;
+        X[c] = op.x0[gidx];
+        DI[c] = (float)op.dinv[gidx];
+        DG[c] = (float)op.diag[gidx];
+        P0[c] = 0.0f;
+        P1[c] = 0.0f;
+        double braw = 0.0;
+        if (nb & 0x80) {
+            if (L.rhs_mode == 0) {
+                braw = L.rhs[gidx];
+            } else {
+                const int li = (int)__umulhi((unsigned)c, magic);
+                const int j = c - li * ny;
+                const int pu = ny + 2, pv = ny + 1;
+                const int ig = r0 + li + 1, jg = j + 1;
+                const double div = (L.F[ig * pu + jg] - L.F[(ig - 1) * pu + jg]) / L.dx +
+                                   (L.G[ig * pv + jg] - L.G[ig * pv + jg - 1]) / L.dy;
+                braw = div / dt;
+            }
+        }
+        B[c] = braw;
+    }
+    const int ncomp = op.ncomp;
+    for (int k = 0; k < ncomp; ++k) {
+        double v[1] = {0.0};
+        for (int c = tid; c < nloc; c += kPcgThreads)
+            if ((NB[c] & 0x80) && op.label[goff + c] == k) v[0] += B[c];
+        cluster_sum<1>(cluster, v, red_smem, SLOTS(), C, me);
+        if (tid == 0) cmean[k] = v[0] / op.comp_count[k];
+    }
+    __syncthreads();
+    double bb = 0.0;
+    for (int c = tid; c < nloc; c += kPcgThreads) {
+        double b = 0.0;
+        if (NB[c] & 0x80) {
+            b = B[c];
+            if (ncomp > 0) {
+                const int lab = op.label[goff + c];
+                if (lab >= 0) b = b - cmean[lab];
+            }
+            b = -b;
+        }
+        B[c] = b;
+        bb += b * b;
+    }
+    {
+        // also the barrier after which other CTAs read this CTA's x
+        double v[1] = {bb};
+        cluster_sum<1>(cluster, v, red_smem, SLOTS(), C, me);
+        bb = v[0];
+    }
+    const double bnrm2 = sqrt(bb);
+    const double atol = L.rtol * bnrm2;
+    int total = 0;
+    bool converged = false;
+    if (bnrm2 == 0.0) {
+        for (int c = tid; c < nloc; c += kPcgThreads) X[c] = B[c];
+        converged = true;
+    } else {
+        for (int outer = 0; outer < 64 && !converged; ++outer) {
+            // true residual in FP64; the inner iteration starts from d = 0
+            double part[2] = {0.0, 0.0};
+            for (int c = tid; c < nloc; c += kPcgThreads) {
+                const uint8_t nb = NB[c];
+                D[c] = 0.0f;
+                if (!(nb & 0x80)) { R[c] = 0.0f; Z[c] = 0.0f; continue; }
+                const int li = (int)__umulhi((unsigned)c, magic);
+                const int j = c - li * ny;
+                double tW = 0.0, tS = 0.0, tN = 0.0, tE = 0.0;
+                if (nb & 2) tS = mdy2 * X[c - 1];
+                if (nb & 4) tN = mdy2 * X[c + 1];
+                if (nb & 1) tW = mdx2 * ((li > 0) ? X[c - ny] : baseWx[j]);
+                if (nb & 8) tE = mdx2 * ((li < rows - 1) ? X[c + ny] : baseEx[j]);
+                const double r = B[c] - row_sum(periodic, r0 + li, nx, tW, tS, op.diag[goff + c] * X[c], tN, tE);
+                const float rf = (float)r;
+                const float zf = DI[c] * rf;
+                R[c] = rf;
+                Z[c] = zf;
+                part[0] += r * r;
+                part[1] += (double)rf * (double)zf;
+            }
+            cluster_sum<2>(cluster, part, red_smem, SLOTS(), C, me);
+            const double rnorm = sqrt(part[0]);
+            if (rnorm < atol) { converged = true; break; }
+            if (total >= L.maxiter) break;
+            // FP32 Jacobi-PCG on A d = r (the p recompute and halo scheme of the FP64 solver)
+            const double tol_in = (double)kInnerTol * rnorm;
+            double rr = part[0], rho = part[1], beta = 0.0;
+            int cur = 0;
+            float q[CPT];
+            for (int k = 0; total < L.maxiter; ++k, ++total) {
+                if (k > 0 && sqrt(rr) < tol_in) break;
+                float* Pn = cur ? P1 : P0;
+                const float* Po = cur ? P0 : P1;
+                const int po = cur ? 2 * cap : 3 * cap;  // previous p from D
+                const bool first = (k == 0);
+                const float fb = (float)beta;
+                double pq = 0.0;
+#pragma unroll
+                for (int s = 0; s < CPT; ++s) {
+                    q[s] = 0.0f;
+                    const int c = tid + s * kPcgThreads;
+                    if (c >= nloc) continue;
+                    const uint8_t nb = NB[c];
+                    if (!(nb & 0x80)) continue;
+                    const int li = (int)__umulhi((unsigned)c, magic);
+                    const int j = c - li * ny;
+                    const float pC = first ? Z[c] : Po[c] * fb + Z[c];
+                    float tW = 0.0f, tS = 0.0f, tN = 0.0f, tE = 0.0f;
+                    if (nb & 2) tS = fdy2 * (first ? Z[c - 1] : Po[c - 1] * fb + Z[c - 1]);
+                    if (nb & 4) tN = fdy2 * (first ? Z[c + 1] : Po[c + 1] * fb + Z[c + 1]);
+                    if (nb & 1) {
+                        const float* g = (li > 0) ? (D + c - ny) : (baseWf + j);
+                        tW = fdx2 * (first ? g[4 * cap] : g[po] * fb + g[4 * cap]);
+                    }
+                    if (nb & 8) {
+                        const float* g = (li < rows - 1) ? (D + c + ny) : (baseEf + j);
+                        tE = fdx2 * (first ? g[4 * cap] : g[po] * fb + g[4 * cap]);
+                    }
+                    const float qq = row_sum_f(periodic, r0 + li, nx, tW, tS, DG[c] * pC, tN, tE);
+                    Pn[c] = pC;
+                    q[s] = qq;
+                    pq += (double)pC * (double)qq;
+                }
+                {
+                    double v[1] = {pq};
+                    cluster_sum<1>(cluster, v, red_smem, SLOTS(), C, me);
+                    pq = v[0];
+                }
+                const float alpha = (float)(rho / pq);
+                double v2[2] = {0.0, 0.0};
+#pragma unroll
+                for (int s = 0; s < CPT; ++s) {
+                    const int c = tid + s * kPcgThreads;
+                    if (c >= nloc) continue;
+                    if (!(NB[c] & 0x80)) continue;
+                    D[c] = D[c] + alpha * Pn[c];
+                    const float r = R[c] - alpha * q[s];
+                    R[c] = r;
+                    const float z = DI[c] * r;
+                    Z[c] = z;
+                    v2[0] += (double)r * (double)r;
+                    v2[1] += (double)r * (double)z;
+                }
+                cluster_sum<2>(cluster, v2, red_smem, SLOTS(), C, me);
+                rr = v2[0];
+                beta = v2[1] / rho;
+                rho = v2[1];
+                cur ^= 1;
+            }
+            // x += d in FP64; the barrier makes the new x visible to the neighbours'
+            // residual rows (and ends every read of this CTA's d, r, z)
+            for (int c = tid; c < nloc; c += kPcgThreads)
+                if (NB[c] & 0x80) X[c] = X[c] + (double)D[c];
+            cluster.sync();
+        }
+    }
+    // ------------------------------------------------------------ epilogue
+    __syncthreads();
+    for (int c = tid; c < nloc; c += kPcgThreads) op.x0[goff + c] = X[c];
+    for (int k = 0; k < ncomp; ++k) {
+        double v[1] = {0.0};
+        for (int c = tid; c < nloc; c += kPcgThreads)
+            if ((NB[c] & 0x80) && op.label[goff + c] == k) v[0] += X[c];
+        cluster_sum<1>(cluster, v, red_smem, SLOTS(), C, me);
+        if (tid == 0) cmean[k] = v[0] / op.comp_count[k];
+    }
+    __syncthreads();
+    const int pp = ny + 2;
+    for (int c = tid; c < nloc; c += kPcgThreads) {
+        const int li = (int)__umulhi((unsigned)c, magic);
+        const int j = c - li * ny;
+        const int i = r0 + li;
+        double pv = 0.0;
+        if (NB[c] & 0x80) {
+            pv = X[c];
+            if (ncomp > 0) {
+                const int lab = op.label[goff + c];
+                if (lab >= 0) pv = pv - cmean[lab];
+            }
+        }
+        if (!L.p_padded) {
+            L.p_out[goff + c] = pv;
+        } else {
+            L.p_out[(i + 1) * pp + j + 1] = pv;
+            if (periodic && i == nx - 1) L.p_out[j + 1] = pv;
+            if (periodic && i == 0) L.p_out[(nx + 1) * pp + j + 1] = pv;
+        }
+    }
+    if (L.p_padded) {
+        for (int i = r0 + tid; i < r1; i += kPcgThreads) {
+            L.p_out[(i + 1) * pp] = 0.0;
+            L.p_out[(i + 1) * pp + ny + 1] = 0.0;
+        }
+        if (me == 0) {
+            for (int j = tid; j < pp; j += kPcgThreads)
+                if (!periodic || j == 0 || j == ny + 1) L.p_out[j] = 0.0;
+        }
+        if (me == C - 1) {
+            for (int j = tid; j < pp; j += kPcgThreads)
+                if (!periodic || j == 0 || j == ny + 1) L.p_out[(nx + 1) * pp + j] = 0.0;
+        }
+    }
+    if (me == 0 && tid == 0) {
+        if (L.iters_out) *L.iters_out = total;
+        if (L.iters_out2) *L.iters_out2 = total;
+        if (L.status_out && !converged) atomicOr(L.status_out, CFD2D_S_CG_MAXITER);
+    }
+    cluster.sync();
+#undef SLOTS
+}
+
 // ---------------------------------------------------------------- grid-persistent variant
 // For grids beyond the on-chip capacity of one cluster: a cooperative launch of
 // G co-resident CTAs over all SMs, vectors in global memory (the workspace),
@@ -891,6 +1187,40 @@ cudaError_t launch_cpt(const PcgLaunch& L, int C, cudaStream_t s) {
     return cudaLaunchKernelEx(&cfg, kern, L);
 }
 
+// the mixed-precision solver: x and b in FP64, seven FP32 arrays, the coupling bits
+size_t smem_bytes_mixed(int cap) { return (size_t)cap * (2 * sizeof(double) + 7 * sizeof(float) + 1) + 16; }
+
+template <int CPT>
+cudaError_t launch_mixed(const PcgLaunch& L, int C, cudaStream_t s) {
+    static bool done = false;
+    if (!done) {
+        int dev = 0, optin = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return e;
+        e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        if (e != cudaSuccess) return e;
+        const int dyn = optin - (int)((32 * kMaxK + 2 * 16 * kMaxK + CFD2D_MAX_COMPONENTS) * sizeof(double)) - 1024;
+        e = cudaFuncSetAttribute(k_pcg_cluster_mixed<CPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+        if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(k_pcg_cluster_mixed<CPT>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        if (e != cudaSuccess) return e;
+        done = true;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(C, 1, 1);
+    cfg.blockDim = dim3(kPcgThreads, 1, 1);
+    cfg.dynamicSmemBytes = smem_bytes_mixed(L.cap_cells);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_pcg_cluster_mixed<CPT>, L);
+}
+
 int cpt_for(int cap) {
     const int need = (cap + kPcgThreads - 1) / kPcgThreads;
     if (need <= 1) return 1;
@@ -976,6 +1306,16 @@ cudaError_t pcg_launch(const PcgLaunch& L0, cudaStream_t s) {
     if (C < 1 || C > 16) return cudaErrorInvalidValue;
     const int rows = (L.op.nx + C - 1) / C;
     L.cap_cells = rows * L.op.ny;
+    if (L.op.mixed) {
+        // the cluster planned for the FP64 solver holds the 45-byte cells as well
+        switch (cpt_for(L.cap_cells)) {
+            case 1: return launch_mixed<1>(L, C, s);
+            case 2: return launch_mixed<2>(L, C, s);
+            case 4: return launch_mixed<4>(L, C, s);
+            case 8: return launch_mixed<8>(L, C, s);
+            default: return cudaErrorInvalidValue;
+        }
+    }
     if (L.op.ny % 2 == 0) {
         switch (cpt_for((L.cap_cells + 1) / 2)) {
             case 1: return launch_cpt<1, true>(L, C, s);

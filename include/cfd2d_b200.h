@@ -95,6 +95,9 @@ typedef struct cfd2d_poisson {
     double* work;             /* scratch, cfd2d_pcg_workspace_bytes() */
     size_t work_bytes;
     int cluster;              /* CTAs of the on-chip solver (0 = grid-persistent solver) */
+    int mixed;                /* 1: FP32 iterations with FP64 residual refinement and FP64
+                                 reductions (on-chip solver only; no reference counterpart);
+                                 0: the FP64 scipy-form iteration */
 } cfd2d_poisson;
 
 /* One scalar transport equation (cfd2d/models.py:73-250). */
