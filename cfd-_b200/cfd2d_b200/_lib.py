@@ -53,6 +53,7 @@ class Poisson(C.Structure):
         ("diag", _vp), ("dinv", _vp), ("nbr", _vp), ("label", _vp),
         ("ncomp", C.c_int), ("comp_count", _vp), ("x0", _vp), ("work", _vp),
         ("work_bytes", C.c_size_t), ("cluster", C.c_int), ("mixed", C.c_int),
+        ("grid_ctas", C.c_int),
     ]
 
 

@@ -524,6 +524,28 @@ class Simulation:
             self.wall_time += time.perf_counter() - t0
             self._after_steps()
 
+    def launch_steps(self, nsteps: int) -> None:
+        """Queue nsteps projection steps on this simulation's stream and return at
+        once; finish_steps() waits for them and reads the results. Lets several
+        simulations run side by side (cfd2d_b200.batch)."""
+        with self._on_stream():
+            self._flush_mirrors()
+            self._set_run_limits()
+            self._t_launch = time.perf_counter()
+            self._launch_steps(nsteps)
+
+    def finish_steps(self) -> None:
+        """Wait for the steps queued by launch_steps() and report their results."""
+        with self._on_stream():
+            self._sync()
+            self.wall_time += time.perf_counter() - getattr(self, "_t_launch", time.perf_counter())
+            self._after_steps()
+
+    @property
+    def stream(self):
+        """The CUDA stream (torch.cuda.Stream) this simulation's work runs on."""
+        return self._stream
+
     def advance(self, nsteps: int) -> None:
         """nsteps projection steps with a single host synchronisation at the end."""
         t0 = time.perf_counter()

@@ -788,6 +788,7 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cluster_mixed(PcgLaunch 
 namespace {
 
 constexpr int kGridThreads = 256;
+constexpr int kClusterL2Threads = 512;  // one 16-CTA cluster, vectors in global memory
 
 struct GridWork {
     double* R;
@@ -897,7 +898,66 @@ __device__ __forceinline__ double apply_A(const cfd2d_poisson& op, const double*
 
 }  // namespace
 
-__global__ void __launch_bounds__(kGridThreads) k_pcg_grid(PcgLaunch L) {
+// Sum of K values over one thread-block cluster (any K <= kSlot, any block size that
+// is a multiple of 32), pull form: warp sums, block partial stored in this CTA's own
+// slot, cluster barrier, warp 0 loads the C partials through DSMEM (one per lane) and
+// adds them by a butterfly, the CTA reads the sum from shared memory. Consecutive
+// calls alternate two slot buffers (a slot is rewritten only after the next barrier).
+template <int K>
+__device__ __forceinline__ void cluster_sum_any(double (&v)[K], double* red_smem, double* slot) {
+    static_assert(K <= kSlot, "slot capacity");
+    cg::cluster_group cluster = cg::this_cluster();
+    const int C = (int)cluster.num_blocks();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    __shared__ double res[kSlot];
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = warp_sum(v[k]);
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) red_smem[k * 32 + w] = v[k];
+    }
+    __syncthreads();
+    if (w == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            double x = (lane < nw) ? red_smem[k * 32 + lane] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+            if (lane == 0) slot[k] = x;
+        }
+    }
+    cluster.sync();
+    if (w == 0) {
+        const double* src = cluster.map_shared_rank(slot, lane < C ? lane : 0);
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            double y = (lane < C) ? src[k] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) y += __shfl_xor_sync(0xffffffffu, y, o);
+            if (lane == 0) res[k] = y;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = res[k];
+}
+
+// The reduction of the grid-persistent solver: over the whole cooperative grid (CL =
+// false, counting barrier, may give up) or over one cluster (CL = true).
+template <bool CL, int K>
+__device__ __forceinline__ bool sync_sum(double (&v)[K], double* red_smem, double* part, unsigned int* bar,
+                                         int* status, double* slotA, double* slotB, int& nred) {
+    if constexpr (CL) {
+        cluster_sum_any<K>(v, red_smem, (nred++ & 1) ? slotB : slotA);
+        return true;
+    } else {
+        return grid_sum<K>(v, red_smem, part, bar, status);
+    }
+}
+
+template <bool CL>
+__global__ void __launch_bounds__(CL ? kClusterL2Threads : kGridThreads, 1) k_pcg_grid(PcgLaunch L) {
+    constexpr int TPB = CL ? kClusterL2Threads : kGridThreads;
     if (L.active && *L.active == 0) return;
     const cfd2d_poisson& op = L.op;
     const int nx = op.nx, ny = op.ny;
@@ -912,14 +972,17 @@ __global__ void __launch_bounds__(kGridThreads) k_pcg_grid(PcgLaunch L) {
     const int tid = threadIdx.x;
     const double mdx2 = -op.dx2, mdy2 = -op.dy2;
     __shared__ double red_smem[32 * kSlot];
+    __shared__ double slotA[kSlot], slotB[kSlot];  // cluster mode: this CTA's partials
+    int nred = 0;
     int* status = L.status_out;
+#define SSUM(K, v, part) sync_sum<CL, K>(v, red_smem, part, W.bar, status, slotA, slotB, nred)
 
     double dt = 1.0;
     if (L.rhs_mode == 1) dt = L.dt_ptr ? *L.dt_ptr : L.dt_const;
     double csum[CFD2D_MAX_COMPONENTS + 1];
 #pragma unroll
     for (int k = 0; k <= CFD2D_MAX_COMPONENTS; ++k) csum[k] = 0.0;
-    for (int c = c0 + tid; c < c1; c += kGridThreads) {
+    for (int c = c0 + tid; c < c1; c += TPB) {
         const uint8_t nb = op.nbr[c];
         double braw = 0.0;
         if (nb & 0x80) {
@@ -941,10 +1004,10 @@ __global__ void __launch_bounds__(kGridThreads) k_pcg_grid(PcgLaunch L) {
         }
         R[c] = braw;
     }
-    if (!grid_sum<CFD2D_MAX_COMPONENTS + 1>(csum, red_smem, W.partA, W.bar, status)) return;
+    if (!SSUM(CFD2D_MAX_COMPONENTS + 1, csum, W.partA)) return;
     const bool x_any = csum[CFD2D_MAX_COMPONENTS] > 0.0;
     double part[3] = {0.0, 0.0, 0.0};
-    for (int c = c0 + tid; c < c1; c += kGridThreads) {
+    for (int c = c0 + tid; c < c1; c += TPB) {
         const uint8_t nb = op.nbr[c];
         if (!(nb & 0x80)) { W.P1[c] = 0.0; W.P0[c] = 0.0; R[c] = 0.0; continue; }
         const int i = c / ny, j = c % ny;
@@ -967,7 +1030,7 @@ __global__ void __launch_bounds__(kGridThreads) k_pcg_grid(PcgLaunch L) {
         part[1] += r * r;
         part[2] += r * (op.dinv[c] * r);
     }
-    if (!grid_sum<3>(part, red_smem, W.partB, W.bar, status)) return;
+    if (!SSUM(3, part, W.partB)) return;
     const double bnrm2 = sqrt(part[0]);
     double rr = part[1];
     double rho = part[2];
@@ -975,7 +1038,7 @@ __global__ void __launch_bounds__(kGridThreads) k_pcg_grid(PcgLaunch L) {
     int it = 0;
     bool converged = false;
     if (bnrm2 == 0.0) {
-        for (int c = c0 + tid; c < c1; c += kGridThreads) X[c] = W.P1[c];
+        for (int c = c0 + tid; c < c1; c += TPB) X[c] = W.P1[c];
         converged = true;
     } else {
         double beta = 0.0;
@@ -986,7 +1049,7 @@ __global__ void __launch_bounds__(kGridThreads) k_pcg_grid(PcgLaunch L) {
             const double* Po = cur ? W.P0 : W.P1;
             const bool first = (it == 0);
             double pq = 0.0;
-            for (int c = c0 + tid; c < c1; c += kGridThreads) {
+            for (int c = c0 + tid; c < c1; c += TPB) {
                 const uint8_t nb = op.nbr[c];
                 if (!(nb & 0x80)) continue;
                 const int i = c / ny, j = c % ny;
@@ -1004,12 +1067,12 @@ __global__ void __launch_bounds__(kGridThreads) k_pcg_grid(PcgLaunch L) {
             }
             {
                 double v[1] = {pq};
-                if (!grid_sum<1>(v, red_smem, W.partA, W.bar, status)) return;
+                if (!SSUM(1, v, W.partA)) return;
                 pq = v[0];
             }
             const double alpha = rho / pq;
             double v2[2] = {0.0, 0.0};
-            for (int c = c0 + tid; c < c1; c += kGridThreads) {
+            for (int c = c0 + tid; c < c1; c += TPB) {
                 const uint8_t nb = op.nbr[c];
                 if (!(nb & 0x80)) continue;
                 const int i = c / ny, j = c % ny;
@@ -1023,9 +1086,9 @@ __global__ void __launch_bounds__(kGridThreads) k_pcg_grid(PcgLaunch L) {
             if (L.snap) {
                 const int k = (it + 1) / L.snap_every;
                 if ((it + 1) % L.snap_every == 0 && k <= L.snap_max)
-                    for (int c = c0 + tid; c < c1; c += kGridThreads) L.snap[(size_t)(k - 1) * n + c] = X[c];
+                    for (int c = c0 + tid; c < c1; c += TPB) L.snap[(size_t)(k - 1) * n + c] = X[c];
             }
-            if (!grid_sum<2>(v2, red_smem, W.partB, W.bar, status)) return;
+            if (!SSUM(2, v2, W.partB)) return;
             rr = v2[0];
             beta = v2[1] / rho;
             rho = v2[1];
@@ -1036,17 +1099,17 @@ __global__ void __launch_bounds__(kGridThreads) k_pcg_grid(PcgLaunch L) {
 #pragma unroll
     for (int k = 0; k < CFD2D_MAX_COMPONENTS; ++k) xs[k] = 0.0;
     if (op.ncomp > 0) {
-        for (int c = c0 + tid; c < c1; c += kGridThreads) {
+        for (int c = c0 + tid; c < c1; c += TPB) {
             if (!(op.nbr[c] & 0x80)) continue;
             const int lab = op.label[c];
 #pragma unroll
             for (int k = 0; k < CFD2D_MAX_COMPONENTS; ++k)
                 if (k == lab) xs[k] += X[c];
         }
-        if (!grid_sum<CFD2D_MAX_COMPONENTS>(xs, red_smem, W.partC, W.bar, status)) return;
+        if (!SSUM(CFD2D_MAX_COMPONENTS, xs, W.partC)) return;
     }
     const int pp = ny + 2;
-    for (int c = c0 + tid; c < c1; c += kGridThreads) {
+    for (int c = c0 + tid; c < c1; c += TPB) {
         const int i = c / ny, j = c % ny;
         double pv = 0.0;
         if (op.nbr[c] & 0x80) {
@@ -1071,7 +1134,7 @@ __global__ void __launch_bounds__(kGridThreads) k_pcg_grid(PcgLaunch L) {
         }
     }
     if (L.p_padded && blockIdx.x == 0) {
-        for (int j = tid; j < pp; j += kGridThreads) {
+        for (int j = tid; j < pp; j += TPB) {
             if (!op.periodic || j == 0 || j == ny + 1) {
                 L.p_out[j] = 0.0;
                 L.p_out[(nx + 1) * pp + j] = 0.0;
@@ -1083,6 +1146,8 @@ __global__ void __launch_bounds__(kGridThreads) k_pcg_grid(PcgLaunch L) {
         if (L.iters_out2) *L.iters_out2 = it;
         if (L.status_out && !converged) atomicOr(L.status_out, CFD2D_S_CG_MAXITER);
     }
+    if constexpr (CL) cg::this_cluster().sync();
+#undef SSUM
 }
 
 namespace {
@@ -1093,7 +1158,7 @@ int grid_blocks_for(int n) {
         int dev = 0;
         if (cudaGetDevice(&dev) != cudaSuccess) return 0;
         if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_grid, kGridThreads, 0) != cudaSuccess)
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_grid<false>, kGridThreads, 0) != cudaSuccess)
             return 0;
     }
     long long g = (long long)per_sm * sms;
@@ -1126,8 +1191,10 @@ size_t pcg_grid_workspace_doubles(int nx, int ny) {
 
 cudaError_t pcg_grid_launch(const PcgLaunch& L, cudaStream_t s) {
     const int n = L.op.nx * L.op.ny;
-    const int G = grid_blocks_for(n);
+    const bool cl = L.op.grid_ctas == 16;
+    const int G = cl ? 16 : grid_blocks_for(n);
     if (G < 1 || G > 148 * 32) return cudaErrorInvalidConfiguration;
+    if (L.op.grid_ctas != 0 && !cl) return cudaErrorInvalidValue;
     if (L.op.work == nullptr || L.op.work_bytes < pcg_grid_workspace_doubles(L.op.nx, L.op.ny) * sizeof(double))
         return cudaErrorInvalidValue;
     PcgLaunch Lc = L;
@@ -1136,8 +1203,31 @@ cudaError_t pcg_grid_launch(const PcgLaunch& L, cudaStream_t s) {
     const size_t n3 = (size_t)3 * n + (size_t)3 * G * kSlot;
     cudaError_t e = cudaMemsetAsync(L.op.work + n3, 0, 2 * sizeof(unsigned int), s);
     if (e != cudaSuccess) return e;
+    if (cl) {
+        // one 16-CTA cluster: its reductions use cluster barriers, so several such
+        // solves (of different cases) can run side by side on the other SMs
+        static bool configured = false;
+        if (!configured) {
+            e = cudaFuncSetAttribute(k_pcg_grid<true>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+            if (e != cudaSuccess) return e;
+            configured = true;
+        }
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(16, 1, 1);
+        cfg.blockDim = dim3(kClusterL2Threads, 1, 1);
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = 16;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        return cudaLaunchKernelEx(&cfg, k_pcg_grid<true>, Lc);
+    }
     void* args[] = {&Lc};
-    return cudaLaunchCooperativeKernel((const void*)k_pcg_grid, dim3(G), dim3(kGridThreads), args, 0, s);
+    return cudaLaunchCooperativeKernel((const void*)k_pcg_grid<false>, dim3(G), dim3(kGridThreads), args, 0, s);
 }
 
 // ---------------------------------------------------------------- launch

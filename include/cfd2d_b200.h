@@ -98,6 +98,9 @@ typedef struct cfd2d_poisson {
     int mixed;                /* 1: FP32 iterations with FP64 residual refinement and FP64
                                  reductions (on-chip solver only; no reference counterpart);
                                  0: the FP64 scipy-form iteration */
+    int grid_ctas;            /* cluster == 0 only: 0 = cooperative launch over every SM;
+                                 16 = one 16-CTA cluster (vectors in the workspace, cluster
+                                 barriers), which leaves the other SMs to other solves */
 } cfd2d_poisson;
 
 /* One scalar transport equation (cfd2d/models.py:73-250). */

@@ -254,14 +254,16 @@ def test_misc_runs(pkg):
 
 
 # ---------------------------------------------------------------- grid-persistent solver
+@pytest.mark.parametrize("variant", ["grid", "cluster-l2"])
 @pytest.mark.parametrize("name", ["cav", "cyl", "per", "two"])
-def test_pressure_solve_grid_variant(pkg, name, monkeypatch):
-    """The grid-persistent CG (used beyond on-chip capacity) on the same fixtures."""
-    monkeypatch.setenv("CFD2D_PCG_VARIANT", "grid")
+def test_pressure_solve_grid_variant(pkg, name, variant, monkeypatch):
+    """The workspace CG (used beyond on-chip capacity), over every SM or on one 16-CTA
+    cluster, on the same fixtures."""
+    monkeypatch.setenv("CFD2D_PCG_VARIANT", variant)
     g = golden("golden_pressure")
     sim = _pressure_sim(pkg, name)
     ps = sim.pressure
-    assert ps.cluster == 0
+    assert ps.cluster == 0 and ps.grid_ctas == (16 if variant == "cluster-l2" else 0)
     ps.tol = 1e-10
     for key in ("", "2"):
         p = ps.solve(g[name + "_rhs" + key])
@@ -270,7 +272,8 @@ def test_pressure_solve_grid_variant(pkg, name, monkeypatch):
         assert rel(p, g[name + "_p" + key]) < 1e-7
 
 
-def test_large_grid_uses_grid_variant_and_matches_oracle(pkg):
+@pytest.mark.parametrize("grid_ctas", [0, 16])
+def test_large_grid_uses_grid_variant_and_matches_oracle(pkg, grid_ctas):
     """A grid beyond one cluster's shared memory: solve against the oracle's CG."""
     import oracle as O
 
@@ -279,6 +282,7 @@ def test_large_grid_uses_grid_variant_and_matches_oracle(pkg):
     case = cases.custom_obstacles(obst, lx=2.0, ly=1.0, nx=512, ny=256, re=200.0, pressure_solver="cg")
     ps = case.sim.pressure
     assert ps.cluster == 0
+    ps.grid_ctas = grid_ctas
     ref = O.custom_obstacles(obst, lx=2.0, ly=1.0, nx=512, ny=256, re=200.0, tol=None)
     rng = np.random.default_rng(3)
     rhs = rng.standard_normal((512, 256))
@@ -291,9 +295,10 @@ def test_large_grid_uses_grid_variant_and_matches_oracle(pkg):
     assert abs(ps.last_iterations - ref.pressure.last_iterations) <= max(3, ref.pressure.last_iterations // 20)
 
 
-def test_cavity_step_with_grid_variant(pkg, monkeypatch):
-    """Whole steps with the grid-persistent solver agree with the golden run."""
-    monkeypatch.setenv("CFD2D_PCG_VARIANT", "grid")
+@pytest.mark.parametrize("variant", ["grid", "cluster-l2"])
+def test_cavity_step_with_grid_variant(pkg, variant, monkeypatch):
+    """Whole steps with the workspace solver agree with the golden run."""
+    monkeypatch.setenv("CFD2D_PCG_VARIANT", variant)
     _, cases, _, _ = pkg
     g = golden("golden_cavity64")
     case = cases.lid_driven_cavity(re=100, n=64, scheme="ab2", gamma=0.1, tau=0.5, pressure_solver="cg")
