@@ -120,20 +120,15 @@ __global__ void __launch_bounds__(256) k_momentum(const double* __restrict__ u, 
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = (blockIdx.y * blockDim.y + threadIdx.y);
     if (j >= ny + 2 || i >= nx + 2) return;
-    const MomCoef m = mom_coef_inv(inv, gamma, nu[g.c(1, 1)]);
+    const MomCoef m = mom_coef_inv(inv, gamma, __ldg(&nu[g.c(1, 1)]));
     const int imax = periodic ? nx : nx - 1;
-    if (i <= nx) {
-        double h = 0.0;
-        if (i >= 1 && i <= imax && j >= 1 && j <= ny)
-            h = mom_u(u, v, fl, nu, rho, g, m, VARIABLE, VAR_DENSITY, i, j);
-        hu[g.u(i, j)] = h;
-    }
-    if (j <= ny) {
-        double h = 0.0;
-        if (i >= 1 && i <= nx && j >= 1 && j <= ny - 1)
-            h = mom_v(u, v, fl, nu, rho, g, m, VARIABLE, VAR_DENSITY, i, j);
-        hv[g.v(i, j)] = h;
-    }
+    // both tendencies first, then both stores: every load of the thread can be in
+    // flight together
+    double hU = 0.0, hV = 0.0;
+    if (i >= 1 && i <= imax && j >= 1 && j <= ny) hU = mom_u(u, v, fl, nu, rho, g, m, VARIABLE, VAR_DENSITY, i, j);
+    if (i >= 1 && i <= nx && j >= 1 && j <= ny - 1) hV = mom_v(u, v, fl, nu, rho, g, m, VARIABLE, VAR_DENSITY, i, j);
+    if (i <= nx) hu[g.u(i, j)] = hU;
+    if (j <= ny) hv[g.v(i, j)] = hV;
 }
 
 __global__ void k_obstacle_bc(double* u, double* v, const uint8_t* fl, int nx, int ny,
