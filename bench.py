@@ -325,6 +325,23 @@ def learned_section() -> dict:
         if name == "learned":
             out[name]["fcg_iterations"] = int(fcg.last_iterations)
             out[name]["fell_back"] = bool(fcg.last_reason != 1)
+    # one application of the network alone, launched directly (outside the solve's
+    # graph, whose conditional node keeps profilers from seeing its kernels)
+    fcg.precondition()
+    torch.cuda.synchronize()
+    reps = 5
+    ev[0].record()
+    for _ in range(reps):
+        fcg.precondition()
+    ev[1].record()
+    torch.cuda.synchronize()
+    net_ms = ev[0].elapsed_time(ev[1]) / reps
+    # 2 * pixels * 9 * 32 * 32 for the seven 32 -> 32 layers on the tensor cores
+    # (two per level on levels 0-2, one on level 3; pixels per level H*W / 4^level)
+    px = [1024 * 512 // (4 ** lvl) for lvl in range(4)]
+    tc_flops = 2 * 9 * 32 * 32 * (px[0] * 2 + px[1] * 2 + px[2] * 2 + px[3])
+    out["network"] = {"ms_per_application": net_ms, "tensor_core_flops": tc_flops,
+                      "tensor_core_tflops_over_whole_application": tc_flops / (net_ms * 1e-3) / 1e12}
     fcg.close()
     del sim, case
     torch.cuda.empty_cache()

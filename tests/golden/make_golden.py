@@ -283,8 +283,42 @@ def gen_misc():
     _save("golden_misc", out)
 
 
+def gen_checkpoint():
+    """A checkpoint written by the reference itself (cfd2d/functions.py:326) after 40
+    steps of the 88 x 17 cylinder with a passive scalar, and the reference's state
+    after 80 steps (tests/test_functions.py:48-70 setting, CG at 1e-12 so that the
+    iterative GPU solve can be compared)."""
+    import tempfile
+
+    from cfd2d import functions
+
+    spec = {"fall": "cylinder", "parameter": {"re": 100, "nx": 88, "ny": 17, "t_end": 0.2},
+            "numerik": {"pressure_solver": "cg"},
+            "skalar": {"name": "c", "diffusivity": 1e-3, "inflow_band": [0.15, 0.25]}}
+    ref = cases.build_case(spec)
+    ref.sim.pressure.tol = 1e-12
+    for _ in range(80):
+        ref.sim.step()
+    a = cases.build_case(spec)
+    a.sim.pressure.tol = 1e-12
+    for _ in range(40):
+        a.sim.step()
+    with tempfile.TemporaryDirectory() as td:
+        path = Path(td) / "cp.npz"
+        functions.save_checkpoint(a.sim, path)
+        cp = dict(np.load(path, allow_pickle=False))
+    out = {f"cp_{k}": v for k, v in cp.items()}
+    out["ref80_u"] = ref.sim.u.copy()
+    out["ref80_v"] = ref.sim.v.copy()
+    out["ref80_p"] = ref.sim.p.copy()
+    out["ref80_c"] = ref.sim.scalars["c"].phi.copy()
+    out["ref80_t"] = np.array(ref.sim.t)
+    _save("golden_checkpoint", out)
+
+
 GROUPS = {"kernels": gen_kernels, "geometry": gen_geometry, "pressure": gen_pressure,
-          "cavity": gen_cavity, "cylinder": gen_cylinder, "sst": gen_sst, "misc": gen_misc}
+          "cavity": gen_cavity, "cylinder": gen_cylinder, "sst": gen_sst, "misc": gen_misc,
+          "checkpoint": gen_checkpoint}
 
 if __name__ == "__main__":
     import warnings
