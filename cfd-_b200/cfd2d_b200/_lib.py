@@ -73,6 +73,10 @@ class SST(C.Structure):
     ]
 
 
+class Smagorinsky(C.Structure):
+    _fields_ = [("l2", _vp)]
+
+
 class Sim(C.Structure):
     _fields_ = [
         ("nx", C.c_int), ("ny", C.c_int), ("dx", C.c_double), ("dy", C.c_double),
@@ -89,7 +93,7 @@ class Sim(C.Structure):
         ("nscalars", C.c_int), ("scalars", Scalar * MAX_SCALARS),
         ("scalar_dtlim_const", C.c_double * MAX_SCALARS), ("thermal_index", C.c_int),
         ("gx", C.c_double), ("gy", C.c_double), ("T_ref", C.c_double), ("sst_on", C.c_int),
-        ("sst", SST), ("state", _vp), ("red", _vp), ("hist", _vp), ("hist_cap", C.c_int),
+        ("sst", SST), ("smag_on", C.c_int), ("smag", Smagorinsky), ("state", _vp), ("red", _vp), ("hist", _vp), ("hist_cap", C.c_int),
         ("p_tmp", _vp),
     ]
 
@@ -145,6 +149,7 @@ def lib():
         "cfd2d_sim_step": ([vp, vp], i),
         "cfd2d_sim_scalar_fill_ghosts": ([vp, i, vp], i),
         "cfd2d_sim_sst_pre_momentum": ([vp, vp], i),
+        "cfd2d_sim_smagorinsky_pre_momentum": ([vp, vp], i),
         "cfd2d_graph_capture_steps": ([vp, i, vp, C.POINTER(C.c_void_p)], i),
         "cfd2d_graph_launch": ([vp, vp], i),
         "cfd2d_graph_destroy": ([vp], i),
@@ -202,7 +207,7 @@ def exported_symbols():
         "cfd2d_pcg_workspace_bytes", "cfd2d_pcg_plan", "cfd2d_pressure_solve",
         "cfd2d_sim_scratch_doubles", "cfd2d_sim_apply_bc", "cfd2d_sim_project_initial",
         "cfd2d_sim_step", "cfd2d_sim_scalar_fill_ghosts", "cfd2d_sim_sst_pre_momentum",
-        "cfd2d_graph_capture_steps", "cfd2d_graph_launch", "cfd2d_graph_destroy",
+        "cfd2d_sim_smagorinsky_pre_momentum", "cfd2d_graph_capture_steps", "cfd2d_graph_launch", "cfd2d_graph_destroy",
         "cfd2d_graph_capture_steps_ex", "cfd2d_events_create", "cfd2d_events_destroy",
         "cfd2d_event_elapsed_ms", "cfd2d_sim_step_begin", "cfd2d_sim_step_finish", "cfd2d_poisson_matvec",
         "cfd2d_pressure_solve_snapshots", "cfd2d_lpc_w32_bytes", "cfd2d_lpc_pack_w32", "cfd2d_lpc_conv32",

@@ -104,6 +104,7 @@ class Simulation:
         self._slots: list = []
         self._thermal = None
         self._sst = None
+        self._smag = None
         self._graphs: dict = {}
         self._learned = None
         self._mirrors: dict = {}
@@ -220,6 +221,8 @@ class Simulation:
         S.sst_on = int(self._sst is not None)
         if self._sst is not None:
             self._sst.fill_struct(S.sst)
+        S.smag_on = int(self._smag is not None)
+        S.smag.l2 = self._smag.l2_ptr() if self._smag is not None else None
         S.state = self._d_state.data_ptr()
         S.red = self._red.data_ptr()
         S.hist = self._hist.data_ptr()
@@ -245,6 +248,16 @@ class Simulation:
     def _set_sst(self, sst):
         self._sst = sst
         self._invalidate()
+
+    def _set_smagorinsky(self, model):
+        self._smag = model
+        self._invalidate()
+
+    def _smagorinsky_pre_momentum(self):
+        with self._on_stream():
+            self._flush_mirrors()
+            self._call("cfd2d_sim_smagorinsky_pre_momentum")
+            self._device_changed()
 
     def _scalar_fill_ghosts(self, slot):
         with self._on_stream():

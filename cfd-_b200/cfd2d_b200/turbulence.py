@@ -1,11 +1,14 @@
-"""k-omega SST on the device path (drop-in for cfd2d/turbulence.py).
+"""Turbulence models on the device path (drop-in for cfd2d/turbulence.py):
+k-omega SST and LES Smagorinsky.
 
 Setup on the host (cfd2d/turbulence.py:199-236): inlet/initial k and omega, the
 wall distance (exact Euclidean distance transform, scipy.ndimage, as the
 reference), the wall-adjacent cells and their viscous omega. Every step, the
 CUDA kernels evaluate the blending functions, nu_t and the blended diffusivities
 before the momentum update and transport k and omega with their sources after
-the projection.
+the projection. Smagorinsky keeps only its squared length scale on the device; its
+kernel evaluates nu_t before each momentum update. One turbulence model per
+simulation: attaching a second raises ValueError.
 """
 
 from __future__ import annotations
@@ -93,6 +96,8 @@ class KOmegaSST(Model):
 
     def attach(self, sim) -> None:
         super().attach(sim)
+        if sim._smag is not None:
+            raise ValueError("nur ein Turbulenzmodell je Simulation")
         sim.variable_viscosity = True
         nu = sim.nu
         k0 = 1.5 * (self.I * self.U_ref) ** 2
@@ -166,15 +171,43 @@ class KOmegaSST(Model):
 
 
 class Smagorinsky(Model):
-    """LES Smagorinsky (cfd2d/turbulence.py:130-160): not on the B200 path yet."""
+    """LES Smagorinsky, nu_t = l^2 |S| (cfd2d/turbulence.py:130-160).
+
+    The squared length l^2 = min(C_s sqrt(dx dy), kappa d)^2 (wall damping with the
+    same wall distance as SST) is computed once on the host when the model attaches;
+    every step a CUDA kernel evaluates the strain rate, nu_t, its ghost values and
+    nu_eff before the momentum update."""
 
     kind = "turbulence"
 
     def __init__(self, cs: float = 0.17, wall_damping: bool = True):
-        self.cs, self.wall_damping = float(cs), wall_damping
+        self.cs = float(cs)
+        self.wall_damping = wall_damping
+        self.title = f"LES Smagorinsky (C_s = {cs:g}" + (", Wanddämpfung" if wall_damping else "") + ")"
 
     def attach(self, sim) -> None:
-        raise NotImplementedError("Smagorinsky ist nicht Teil des B200-Pfads (nur k-ω SST)")
+        super().attach(sim)
+        if sim._sst is not None:
+            raise ValueError("nur ein Turbulenzmodell je Simulation")
+        sim.variable_viscosity = True
+        g = sim.grid
+        length = np.full((g.nx, g.ny), self.cs * np.sqrt(g.dx * g.dy))
+        if self.wall_damping:
+            length = np.minimum(length, KAPPA * wall_distance(sim)[1:-1, 1:-1])
+        self.l2 = length ** 2
+        self._l2 = _lib.to_dev(self.l2)
+        sim._set_smagorinsky(self)
+        sim._smagorinsky_pre_momentum()
+
+    def l2_ptr(self) -> int:
+        return self._l2.data_ptr()
+
+    def monitors(self, sim) -> dict:
+        return {"nu_t_max": float(sim.nu_t.max())}
+
+    def fields(self, sim) -> dict:
+        return {"nu_t": ("Turbulente Viskosität ν_t",
+                         np.where(sim.grid.solid, np.nan, sim.nu_t[1:-1, 1:-1]))}
 
 
 TURBULENCE_MODELS = {"laminar": None, "kOmegaSST": KOmegaSST, "Smagorinsky": Smagorinsky}

@@ -204,8 +204,9 @@ int sim_step_impl(const cfd2d_sim* sim, cudaStream_t s, cudaEvent_t* ev) {
 int step_begin(const cfd2d_sim& S, cudaStream_t s) {
     // 1. boundary conditions (and the run() stop decision for this step)
     CFD_TRY(stage_apply_bc(S, 1, s));
-    // 2. model pre-momentum hooks: k-omega SST blending, nu_t, nu_eff
+    // 2. model pre-momentum hooks: k-omega SST blending or Smagorinsky, nu_t, nu_eff
     if (S.sst_on) CFD_TRY(stage_sst_pre(S, s));
+    if (S.smag_on) CFD_TRY(stage_smag_pre(S, s));
     // 3. time step and upwind fraction
     CFD_TRY(stage_dt(S, s));
     // 4. tendencies, AB2, predictor, outflow extrapolation
@@ -288,6 +289,11 @@ int cfd2d_sim_scalar_fill_ghosts(const cfd2d_sim* sim, int slot, void* stream) {
 int cfd2d_sim_sst_pre_momentum(const cfd2d_sim* sim, void* stream) {
     if (!sim || !sim->sst_on) return CFD2D_E_ARG;
     return status_of(stage_sst_pre(*sim, as_stream(stream)));
+}
+
+int cfd2d_sim_smagorinsky_pre_momentum(const cfd2d_sim* sim, void* stream) {
+    if (!sim || !sim->smag_on || !sim->smag.l2) return CFD2D_E_ARG;
+    return status_of(stage_smag_pre(*sim, as_stream(stream)));
 }
 
 int cfd2d_graph_capture_steps_ex(const cfd2d_sim* sim, int nsteps, void* stream, void* const* events,

@@ -335,9 +335,25 @@ __global__ void k_sst_pre(cfd2d_sim S) {
     S.sst.cross[ci] = cross;
 }
 
-// nu_t ghost values (cfd2d/turbulence.py:110-124), clamped ghost copies of the
-// k and omega diffusivities (turbulence.py:278-282) and nu_eff = nu + nu_t
-// (cfd2d/solver.py:332-333) over every cell.
+// ================================================================ Smagorinsky
+// cfd2d/turbulence.py:149-152 per interior cell: nu_t = l^2 sqrt(S^2) on fluid
+// cells, 0 on solids (l^2 fixed at attach time, turbulence.py:137-147).
+__global__ void k_smag_pre(cfd2d_sim S) {
+    if (!is_active(S.state)) return;
+    const int nx = S.nx, ny = S.ny;
+    const Grid2 g{nx, ny};
+    const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int i = (blockIdx.y * blockDim.y + threadIdx.y) + 1;
+    if (j > ny || i > nx) return;
+    const int c = g.c(i, j);
+    const double S2 = strain2(S.u, S.v, g, S.dx, S.dy, i, j);
+    const double nut = S.smag.l2[(i - 1) * ny + (j - 1)] * sqrt(S2);
+    S.nu_t[c] = S.fluid[c] ? nut : 0.0;
+}
+
+// nu_t ghost values (cfd2d/turbulence.py:110-124) and nu_eff = nu + nu_t
+// (cfd2d/solver.py:332-333) over every cell; with SST also the clamped ghost
+// copies of the k and omega diffusivities (turbulence.py:278-282).
 __device__ __forceinline__ double nut_col(const cfd2d_sim& S, Grid2 g, int i, int j) {
     // value of column i (0..nx+1) at row j (1..ny) after the column step
     const int nx = S.nx;
@@ -350,7 +366,8 @@ __device__ __forceinline__ double nut_col(const cfd2d_sim& S, Grid2 g, int i, in
     return S.bc_kind[1] == CFD2D_BC_NOSLIP ? 0.0 : S.nu_t[g.c(nx, j)];
 }
 
-__global__ void k_sst_ghosts(cfd2d_sim S) {
+template <bool SST>
+__global__ void k_nut_ghosts(cfd2d_sim S) {
     if (!is_active(S.state)) return;
     const int nx = S.nx, ny = S.ny;
     const Grid2 g{nx, ny};
@@ -366,13 +383,15 @@ __global__ void k_sst_ghosts(cfd2d_sim S) {
         if (j == 0) nut = S.bc_kind[2] == CFD2D_BC_NOSLIP ? 0.0 : nut_col(S, g, i, 1);
         else if (j == ny + 1) nut = S.bc_kind[3] == CFD2D_BC_NOSLIP ? 0.0 : nut_col(S, g, i, ny);
         else nut = nut_col(S, g, i, j);
-        // diffusivity ghosts: diff[i, j] = diff[clamp(i), clamp(j)]
-        const int ii = i < 1 ? 1 : (i > nx ? nx : i);
-        const int jj = j < 1 ? 1 : (j > ny ? ny : j);
-        const cfd2d_scalar& ks = S.scalars[S.sst.k_index];
-        const cfd2d_scalar& ws = S.scalars[S.sst.w_index];
-        ks.diff[c] = ks.diff[g.c(ii, jj)];
-        ws.diff[c] = ws.diff[g.c(ii, jj)];
+        if (SST) {
+            // diffusivity ghosts: diff[i, j] = diff[clamp(i), clamp(j)]
+            const int ii = i < 1 ? 1 : (i > nx ? nx : i);
+            const int jj = j < 1 ? 1 : (j > ny ? ny : j);
+            const cfd2d_scalar& ks = S.scalars[S.sst.k_index];
+            const cfd2d_scalar& ws = S.scalars[S.sst.w_index];
+            ks.diff[c] = ks.diff[g.c(ii, jj)];
+            ws.diff[c] = ws.diff[g.c(ii, jj)];
+        }
     }
     __syncwarp();
     if (ghost) S.nu_t[c] = nut;
@@ -1020,7 +1039,13 @@ cudaError_t stage_apply_bc(const cfd2d_sim& S, int begin, cudaStream_t s) {
 
 cudaError_t stage_sst_pre(const cfd2d_sim& S, cudaStream_t s) {
     k_sst_pre<<<grid_rows(S.ny, S.nx), kTile, 0, s>>>(S);
-    k_sst_ghosts<<<grid_rows(S.ny + 2, S.nx + 2), kTile, 0, s>>>(S);
+    k_nut_ghosts<true><<<grid_rows(S.ny + 2, S.nx + 2), kTile, 0, s>>>(S);
+    return last();
+}
+
+cudaError_t stage_smag_pre(const cfd2d_sim& S, cudaStream_t s) {
+    k_smag_pre<<<grid_rows(S.ny, S.nx), kTile, 0, s>>>(S);
+    k_nut_ghosts<false><<<grid_rows(S.ny + 2, S.nx + 2), kTile, 0, s>>>(S);
     return last();
 }
 

@@ -133,6 +133,12 @@ typedef struct cfd2d_sst {
     int k_index, w_index;     /* scalar slots of k and omega */
 } cfd2d_sst;
 
+/* LES Smagorinsky model data (cfd2d/turbulence.py:130-160): nu_t = l^2 |S| on fluid
+ * cells, l = min(C_s sqrt(dx dy), kappa d) fixed when the model attaches. */
+typedef struct cfd2d_smagorinsky {
+    const double* l2;         /* nx*ny squared length scale l^2 */
+} cfd2d_smagorinsky;
+
 /* A whole simulation: geometry, boundary data, device fields and parameters.
  * Filled by the host once; every pointer is a device pointer. */
 typedef struct cfd2d_sim {
@@ -167,6 +173,8 @@ typedef struct cfd2d_sim {
     double gx, gy, T_ref;     /* buoyancy beta*g and reference temperature */
     int sst_on;
     cfd2d_sst sst;
+    int smag_on;              /* Smagorinsky nu_t before the momentum update */
+    cfd2d_smagorinsky smag;
     cfd2d_state* state;
     double* red;              /* reduction scratch, cfd2d_sim_scratch_doubles() */
     double* hist;             /* history ring: hist_cap records of CFD2D_HIST_FIELDS doubles:
@@ -267,6 +275,10 @@ int cfd2d_sim_scalar_fill_ghosts(const cfd2d_sim* sim, int slot, void* stream);
 /* k-omega SST blending functions, nu_t, blended diffusivities and nu_eff.
  * Replaces cfd2d/turbulence.py:262 KOmegaSST.pre_momentum(sim). */
 int cfd2d_sim_sst_pre_momentum(const cfd2d_sim* sim, void* stream);
+
+/* Smagorinsky nu_t = l^2 sqrt(S^2) on fluid cells, its ghost values and nu_eff.
+ * Replaces cfd2d/turbulence.py:149 Smagorinsky.pre_momentum(sim). */
+int cfd2d_sim_smagorinsky_pre_momentum(const cfd2d_sim* sim, void* stream);
 
 /* Capture nsteps consecutive calls of cfd2d_sim_step on `stream` (a created,
  * non-default stream) into an instantiated CUDA graph returned as an opaque

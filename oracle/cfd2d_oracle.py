@@ -24,11 +24,13 @@ __all__ = [
     "SIDES", "LIMITERS", "OGrid", "circle_mask", "ellipse_mask", "rectangle_mask",
     "obstacle_mask", "OBC", "OBoundary", "momentum_tendencies", "obstacle_bc",
     "scalar_transport", "OPressure", "pcg_scipy_trajectory", "OScalarBC", "OScalarField",
-    "OPassiveScalar", "OBoussinesq", "OKOmegaSST", "OSimulation", "cavity", "cylinder",
+    "OPassiveScalar", "OBoussinesq", "OSmagorinsky", "OKOmegaSST", "OSimulation", "cavity", "cylinder",
     "custom_obstacles", "heated_cavity", "sst_channel", "add_scalar",
 ]
 
 SIDES = ("left", "right", "bottom", "top")
+# von Karman constant of the Smagorinsky wall damping, cfd2d/turbulence.py:21
+KAPPA = 0.41
 # limiter codes, cfd2d/kernels.py:33
 LIMITERS = {"upwind": 0, "vanleer": 1, "minmod": 2, "superbee": 3, "linear": 4, "mc": 5}
 
@@ -1074,6 +1076,32 @@ def _set_nut_ghosts(sim, nut):
     nut[:, 0] = 0.0 if sim.bcs["bottom"].kind == "noslip" else nut[:, 1]
     nut[:, ny + 1] = 0.0 if sim.bcs["top"].kind == "noslip" else nut[:, ny]
     nut[g.interior_solid_padded()] = 0.0
+
+
+class OSmagorinsky(OModel):
+    """LES Smagorinsky, nu_t = l^2 |S| with l = min(C_s sqrt(dx dy), kappa d)
+    (cfd2d/turbulence.py:130-160)."""
+    kind = "turbulence"
+
+    def __init__(self, cs=0.17, wall_damping=True):
+        self.cs, self.wall_damping = float(cs), wall_damping
+
+    def attach(self, sim):
+        # cfd2d/turbulence.py:137-147: the squared length is fixed at attach time
+        super().attach(sim)
+        sim.variable_viscosity = True
+        g = sim.grid
+        length = np.full((g.nx, g.ny), self.cs * np.sqrt(g.dx * g.dy))
+        if self.wall_damping:
+            length = np.minimum(length, KAPPA * wall_distance(sim)[1:-1, 1:-1])
+        self.l2 = length ** 2
+        self.pre_momentum(sim)
+
+    def pre_momentum(self, sim):
+        # cfd2d/turbulence.py:149-152
+        rate = np.sqrt(strain_rate_squared(sim))
+        sim.nu_t[1:-1, 1:-1] = np.where(sim.grid.fluid[1:-1, 1:-1], self.l2 * rate, 0.0)
+        _set_nut_ghosts(sim, sim.nu_t)
 
 
 class OKOmegaSST(OModel):

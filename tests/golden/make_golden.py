@@ -5,7 +5,8 @@ Run in a container that holds the reference checkout (default
 
     python tests/golden/make_golden.py [group ...]
 
-Groups: kernels geometry pressure cavity cylinder sst misc (default: all).
+Groups: kernels geometry pressure cavity cylinder sst misc checkpoint smagorinsky
+(default: all).
 The reference imports matplotlib at module load; ``mplstub/`` stands in for it
 (no fixture case needs plotting or polygon masks). Every pressure solve uses the
 reference's own ``PressureSolver`` (scipy CG or SuperLU) with
@@ -283,6 +284,39 @@ def gen_misc():
     _save("golden_misc", out)
 
 
+def gen_smagorinsky():
+    """The Smagorinsky model (cfd2d/turbulence.py:130-160) on three cases: the
+    reference's own test setting (tests/test_models.py:116-122, cavity Re 1000 on
+    32 x 32, 100 steps), a periodic channel around a cylinder (periodic nu_t ghosts,
+    interior solid, flow-rate control) and the 110 x 21 cylinder without wall
+    damping carrying a scalar whose diffusivity takes nu_t / Sc_t."""
+    out = {}
+    f = dict(UVP)
+    f["nut"] = lambda s: s.nu_t
+    case = cases.add_turbulence(cases.lid_driven_cavity(re=1000, n=32, pressure_solver="cg"),
+                                "Smagorinsky")
+    case.sim.pressure.tol = TOL
+    _run(case.sim, 100, {1, 100}, f, out, "smc")
+    g = Grid(32, 32, 1.0, 1.0)
+    g.add_obstacle(geometry.circle(g, 0.5, 0.5, 0.15))
+    bcs = dict(left=BC("periodic"), right=BC("periodic"), bottom=BC("noslip"), top=BC("noslip"))
+    from cfd2d.turbulence import Smagorinsky
+
+    sim = Simulation(g, bcs, nu=0.002, flow_rate=1.0, models=[Smagorinsky(cs=0.2)],
+                     pressure_solver="cg")
+    sim.pressure.tol = TOL
+    _run(sim, 50, {50}, f, out, "smp")
+    out["smp_flow_force"] = np.array(sim.flow_force)
+    case = cases.cylinder_flow(re=1000, nx=110, ny=21, pressure_solver="cg")
+    cases.add_turbulence(case, "Smagorinsky", cs=0.1, wall_damping=False)
+    cases.add_scalar(case, "c", 1e-4, inflow_band=(0.15, 0.25))
+    case.sim.pressure.tol = TOL
+    fc = dict(f)
+    fc["c"] = lambda s: s.scalars["c"].phi
+    _run(case.sim, 30, {30}, fc, out, "smy")
+    _save("golden_smagorinsky", out)
+
+
 def gen_checkpoint():
     """A checkpoint written by the reference itself (cfd2d/functions.py:326) after 40
     steps of the 88 x 17 cylinder with a passive scalar, and the reference's state
@@ -318,7 +352,7 @@ def gen_checkpoint():
 
 GROUPS = {"kernels": gen_kernels, "geometry": gen_geometry, "pressure": gen_pressure,
           "cavity": gen_cavity, "cylinder": gen_cylinder, "sst": gen_sst, "misc": gen_misc,
-          "checkpoint": gen_checkpoint}
+          "checkpoint": gen_checkpoint, "smagorinsky": gen_smagorinsky}
 
 if __name__ == "__main__":
     import warnings

@@ -204,6 +204,85 @@ def test_sst_channel_20_steps(pkg):
     assert sim.flow_force == pytest.approx(float(g["sst_flow_force"]), rel=1e-9)
 
 
+def test_smagorinsky_pre_momentum_bitwise(pkg):
+    """nu_t, its ghosts and nu_eff of the Smagorinsky kernel equal the oracle's
+    restatement of cfd2d/turbulence.py:149-152 bit for bit on the same velocities."""
+    _, cases, _, _ = pkg
+    import oracle as O
+
+    case = cases.add_turbulence(cases.lid_driven_cavity(re=1000, n=32, pressure_solver="cg"), "Smagorinsky")
+    sim = case.sim
+    sim.advance(20)
+    osim = O.cavity(re=1000, n=32, tol=1e-8)
+    om = O.OSmagorinsky()
+    osim.add_model(om)
+    assert np.array_equal(om.l2, sim.model("turbulence").l2)
+    osim.u, osim.v = sim.u.copy(), sim.v.copy()
+    sim._smagorinsky_pre_momentum()
+    om.pre_momentum(osim)
+    assert np.abs(osim.nu_t).max() > 0
+    assert np.array_equal(sim.nu_t, osim.nu_t)
+    assert np.array_equal(sim.nu_eff, sim.nu + osim.nu_t)
+
+
+@pytest.mark.parametrize("name", ["smc", "smp", "smy"])
+def test_smagorinsky_runs(pkg, name):
+    """LES Smagorinsky against the reference's own runs (tests/golden/make_golden.py
+    gen_smagorinsky): the reference test's cavity (tests/test_models.py:116-122),
+    a periodic channel around a cylinder, and the cylinder with a scalar."""
+    _, cases, G, _ = pkg
+    from cfd2d_b200.boundary import BoundaryCondition as BC
+    from cfd2d_b200.grid import Grid
+    from cfd2d_b200.solver import Simulation
+    from cfd2d_b200.turbulence import Smagorinsky
+
+    g = golden("golden_smagorinsky")
+    if name == "smc":
+        sim = cases.add_turbulence(cases.lid_driven_cavity(re=1000, n=32, pressure_solver="cg"),
+                                   "Smagorinsky").sim
+        keep = (1, 100)
+    elif name == "smp":
+        grid = Grid(32, 32, 1.0, 1.0)
+        grid.add_obstacle(G.circle(grid, 0.5, 0.5, 0.15))
+        bcs = dict(left=BC("periodic"), right=BC("periodic"), bottom=BC("noslip"), top=BC("noslip"))
+        sim = Simulation(grid, bcs, nu=0.002, flow_rate=1.0, models=[Smagorinsky(cs=0.2)],
+                         pressure_solver="cg")
+        keep = (50,)
+    else:
+        case = cases.cylinder_flow(re=1000, nx=110, ny=21, pressure_solver="cg")
+        cases.add_turbulence(case, "Smagorinsky", cs=0.1, wall_damping=False)
+        cases.add_scalar(case, "c", 1e-4, inflow_band=(0.15, 0.25))
+        sim = case.sim
+        keep = (30,)
+    sim.pressure.tol = 1e-8
+    n = 0
+    for k in keep:
+        sim.advance(k - n)
+        n = k
+        for f in "uvp":
+            assert rel(getattr(sim, f), g[f"{name}_{f}_{k}"]) < TOL, (f, k)
+        assert rel(sim.nu_t, g[f"{name}_nut_{k}"]) < TOL, k
+    assert sim.nu_t[1:-1, 1:-1].max() > 0
+    if name == "smp":
+        assert sim.flow_force == pytest.approx(float(g["smp_flow_force"]), rel=1e-9)
+    if name == "smy":
+        assert rel(sim.scalars["c"].phi, g["smy_c_30"]) < TOL
+
+
+def test_smagorinsky_runs_and_vanishes_at_walls(pkg):
+    """The reference's own test (tests/test_models.py:116-122) with its default
+    (direct) pressure solve, plus nu_t = 0 in the no-slip ghost cells."""
+    _, cases, _, _ = pkg
+    case = cases.add_turbulence(cases.lid_driven_cavity(re=1000, n=32), "Smagorinsky")
+    case.sim.advance(100)
+    nut = case.sim.nu_t
+    assert nut[1:-1, 1:-1].max() > 0
+    assert case.sim.max_divergence() < 1e-10
+    assert not nut[0, :].any() and not nut[-1, :].any() and not nut[:, 0].any() and not nut[:, -1].any()
+    with pytest.raises(ValueError):
+        cases.add_turbulence(case, "kOmegaSST")
+
+
 def test_misc_runs(pkg):
     _, cases, G, _ = pkg
     from cfd2d_b200.boundary import BoundaryCondition as BC

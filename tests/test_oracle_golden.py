@@ -192,3 +192,43 @@ def test_misc_runs():
         sim.step()
     for f in "uvp":
         assert rel(getattr(sim, f), g[f"eul_{f}_30"]) < 1e-12
+
+
+def test_smagorinsky_runs():
+    """LES Smagorinsky (cfd2d/turbulence.py:130-160): the reference's own test case
+    (tests/test_models.py:116-122), a periodic channel around a cylinder with wall
+    damping and the cylinder without it, carrying a scalar."""
+    g = golden("golden_smagorinsky")
+    sim = O.cavity(re=1000, n=32, tol=1e-8)
+    sim.add_model(O.OSmagorinsky())
+    for n in range(1, 101):
+        sim.step()
+        if n in (1, 100):
+            for f in "uvp":
+                assert rel(getattr(sim, f), g[f"smc_{f}_{n}"]) < 1e-12, (f, n)
+            assert rel(sim.nu_t, g[f"smc_nut_{n}"]) < 1e-12
+    assert np.array_equal(np.array(sim.iterations), g["smc_its"])
+    assert sim.nu_t[1:-1, 1:-1].max() > 0  # the reference test's own check
+
+    grid = O.OGrid(32, 32, 1.0, 1.0)
+    grid.add_obstacle(O.circle_mask(grid, 0.5, 0.5, 0.15))
+    bcs = {"left": O.OBC("periodic"), "right": O.OBC("periodic"), "bottom": O.OBC("noslip"),
+           "top": O.OBC("noslip")}
+    sim = O.OSimulation(grid, bcs, nu=0.002, flow_rate=1.0, models=[O.OSmagorinsky(cs=0.2)],
+                        pressure_solver="cg", tol=1e-8)
+    for _ in range(50):
+        sim.step()
+    for f in ("u", "v", "p", "nu_t"):
+        key = "nut" if f == "nu_t" else f
+        assert rel(getattr(sim, f), g[f"smp_{key}_50"]) < 1e-12, f
+    assert sim.flow_force == pytest.approx(float(g["smp_flow_force"]), rel=1e-12)
+
+    sim = O.cylinder(re=1000, nx=110, ny=21, tol=1e-8)
+    sim.add_model(O.OSmagorinsky(cs=0.1, wall_damping=False))
+    O.add_scalar(sim, "c", 1e-4, inflow_band=(0.15, 0.25))
+    for _ in range(30):
+        sim.step()
+    for f in ("u", "v", "p", "nu_t"):
+        key = "nut" if f == "nu_t" else f
+        assert rel(getattr(sim, f), g[f"smy_{key}_30"]) < 1e-12, f
+    assert rel(sim.scalars["c"].phi, g["smy_c_30"]) < 1e-12
