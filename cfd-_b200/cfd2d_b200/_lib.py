@@ -150,6 +150,8 @@ def lib():
         "cfd2d_sim_scalar_fill_ghosts": ([vp, i, vp], i),
         "cfd2d_sim_sst_pre_momentum": ([vp, vp], i),
         "cfd2d_sim_smagorinsky_pre_momentum": ([vp, vp], i),
+        "cfd2d_wall_distance_workspace_bytes": ([i, i], sz),
+        "cfd2d_sim_wall_distance": ([vp, vp, vp, sz, vp], i),
         "cfd2d_graph_capture_steps": ([vp, i, vp, C.POINTER(C.c_void_p)], i),
         "cfd2d_graph_launch": ([vp, vp], i),
         "cfd2d_graph_destroy": ([vp], i),
@@ -207,7 +209,8 @@ def exported_symbols():
         "cfd2d_pcg_workspace_bytes", "cfd2d_pcg_plan", "cfd2d_pressure_solve",
         "cfd2d_sim_scratch_doubles", "cfd2d_sim_apply_bc", "cfd2d_sim_project_initial",
         "cfd2d_sim_step", "cfd2d_sim_scalar_fill_ghosts", "cfd2d_sim_sst_pre_momentum",
-        "cfd2d_sim_smagorinsky_pre_momentum", "cfd2d_graph_capture_steps", "cfd2d_graph_launch", "cfd2d_graph_destroy",
+        "cfd2d_sim_smagorinsky_pre_momentum", "cfd2d_wall_distance_workspace_bytes",
+        "cfd2d_sim_wall_distance", "cfd2d_graph_capture_steps", "cfd2d_graph_launch", "cfd2d_graph_destroy",
         "cfd2d_graph_capture_steps_ex", "cfd2d_events_create", "cfd2d_events_destroy",
         "cfd2d_event_elapsed_ms", "cfd2d_sim_step_begin", "cfd2d_sim_step_finish", "cfd2d_poisson_matvec",
         "cfd2d_pressure_solve_snapshots", "cfd2d_lpc_w32_bytes", "cfd2d_lpc_pack_w32", "cfd2d_lpc_conv32",

@@ -1,9 +1,9 @@
 """Turbulence models on the device path (drop-in for cfd2d/turbulence.py):
 k-omega SST and LES Smagorinsky.
 
-Setup on the host (cfd2d/turbulence.py:199-236): inlet/initial k and omega, the
-wall distance (exact Euclidean distance transform, scipy.ndimage, as the
-reference), the wall-adjacent cells and their viscous omega. Every step, the
+Setup (cfd2d/turbulence.py:199-236): inlet/initial k and omega, the wall-adjacent
+cells and their viscous omega on the host; the wall distance (exact Euclidean
+distance transform of the wall cells) on the device. Every step, the
 CUDA kernels evaluate the blending functions, nu_t and the blended diffusivities
 before the momentum update and transport k and omega with their sources after
 the projection. Smagorinsky keeps only its squared length scale on the device; its
@@ -14,7 +14,6 @@ simulation: attaching a second raises ValueError.
 from __future__ import annotations
 
 import numpy as np
-from scipy import ndimage
 
 from . import _lib
 from .boundary import SIDES
@@ -39,27 +38,22 @@ def wall_mask_padded(sim) -> np.ndarray:
 
 
 def wall_distance(sim) -> np.ndarray:
-    """Cell-centre distance to the nearest wall face, (nx+2, ny+2) (turbulence.py:43-70)."""
+    """Cell-centre distance to the nearest wall face, (nx+2, ny+2) (turbulence.py:43-70).
+
+    Computed on the device (``cfd2d_sim_wall_distance``: exact separable Euclidean
+    distance transform of the wall cells, periodic in x when the case is)."""
     g = sim.grid
-    wall = wall_mask_padded(sim)
-    if not wall.any():
-        return np.full(wall.shape, 1e6)
-    if sim.periodic:
-        core = wall[1:-1, :]
-        tiled = np.concatenate([core, core, core], axis=0)
-        d = ndimage.distance_transform_edt(~tiled, sampling=(g.dx, g.dy))
-        n = core.shape[0]
-        mid = d[n:2 * n, :]
-        dist = np.empty(wall.shape)
-        dist[1:-1, :] = mid
-        dist[0, :] = mid[-1, :]
-        dist[-1, :] = mid[0, :]
-    else:
-        dist = ndimage.distance_transform_edt(~wall, sampling=(g.dx, g.dy))
-    half = 0.5 * min(g.dx, g.dy)
-    dist = np.maximum(dist - half, 0.5 * min(g.dx, g.dy))
-    dist[~g.fluid] = 0.0
-    return dist
+    t = _lib.torch()
+    dev = _lib.device()
+    lib = _lib.lib()
+    nbytes = int(lib.cfd2d_wall_distance_workspace_bytes(g.nx, g.ny))
+    work = t.empty(nbytes, dtype=t.uint8, device=dev)
+    dist = t.empty((g.nx + 2, g.ny + 2), dtype=t.float64, device=dev)
+    with sim._on_stream():
+        sim._flush_mirrors()
+        sim._call("cfd2d_sim_wall_distance", _lib.ptr(dist), _lib.ptr(work), nbytes)
+        out = dist.cpu().numpy()
+    return out
 
 
 def wall_adjacent_cells(sim):

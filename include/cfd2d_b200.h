@@ -280,6 +280,18 @@ int cfd2d_sim_sst_pre_momentum(const cfd2d_sim* sim, void* stream);
  * Replaces cfd2d/turbulence.py:149 Smagorinsky.pre_momentum(sim). */
 int cfd2d_sim_smagorinsky_pre_momentum(const cfd2d_sim* sim, void* stream);
 
+/* Bytes of device workspace cfd2d_sim_wall_distance needs for an nx x ny grid. */
+size_t cfd2d_wall_distance_workspace_bytes(int nx, int ny);
+
+/* Distance of every cell centre to the nearest wall face, (nx+2)(ny+2) doubles into
+ * `dist`: the exact Euclidean distance transform of the wall cells (interior solids
+ * and the ghost layer of no-slip sides; periodic in x when sim->periodic) minus half
+ * a cell, at least half a cell, 0 on non-fluid cells, 1e6 everywhere when the grid
+ * has no wall. Reads sim->nx, ny, dx, dy, periodic, bc_kind and fluid only.
+ * Replaces cfd2d/turbulence.py:43 wall_distance(sim) (scipy.ndimage
+ * distance_transform_edt). */
+int cfd2d_sim_wall_distance(const cfd2d_sim* sim, double* dist, void* work, size_t work_bytes, void* stream);
+
 /* Capture nsteps consecutive calls of cfd2d_sim_step on `stream` (a created,
  * non-default stream) into an instantiated CUDA graph returned as an opaque
  * handle; cfd2d_graph_launch replays it, cfd2d_graph_destroy frees it. The

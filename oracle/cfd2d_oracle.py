@@ -25,7 +25,8 @@ __all__ = [
     "obstacle_mask", "OBC", "OBoundary", "momentum_tendencies", "obstacle_bc",
     "scalar_transport", "OPressure", "pcg_scipy_trajectory", "OScalarBC", "OScalarField",
     "OPassiveScalar", "OBoussinesq", "OSmagorinsky", "OKOmegaSST", "OSimulation", "cavity", "cylinder",
-    "custom_obstacles", "heated_cavity", "sst_channel", "add_scalar",
+    "custom_obstacles", "heated_cavity", "sst_channel", "add_scalar", "wall_distance",
+    "wall_adjacent_cells", "strain_rate_squared", "KAPPA",
 ]
 
 SIDES = ("left", "right", "bottom", "top")
