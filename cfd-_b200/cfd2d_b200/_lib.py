@@ -73,6 +73,24 @@ class SST(C.Structure):
     ]
 
 
+# field selectors of the device function objects
+FIELD_U, FIELD_V, FIELD_PRESSURE, FIELD_UC, FIELD_VC, FIELD_SPEED, FIELD_VORTICITY = range(7)
+FIELD_CELL, FIELD_CELL_LOG10, FIELD_NODE, FIELD_FLUID = 7, 8, 9, 10
+MAX_FIELDS = 16
+
+
+class Field(C.Structure):
+    _fields_ = [("kind", C.c_int), ("pad", C.c_int), ("data", _vp)]
+
+
+class ProbeSeries(C.Structure):
+    _fields_ = [("t", _vp), ("values", _vp), ("count", _vp), ("cap", C.c_int), ("every", C.c_int)]
+
+
+class FieldAverage(C.Structure):
+    _fields_ = [("t_start", C.c_double), ("sum", _vp), ("sum2", _vp), ("T", _vp)]
+
+
 class Smagorinsky(C.Structure):
     _fields_ = [("l2", _vp)]
 
@@ -152,6 +170,12 @@ def lib():
         "cfd2d_sim_smagorinsky_pre_momentum": ([vp, vp], i),
         "cfd2d_wall_distance_workspace_bytes": ([i, i], sz),
         "cfd2d_sim_wall_distance": ([vp, vp, vp, sz, vp], i),
+        "cfd2d_sample": ([vp, vp, i, vp, vp, i, vp, vp], i),
+        "cfd2d_cell_values": ([vp, vp, vp, vp], i),
+        "cfd2d_probe_record": ([vp, vp, i, vp, vp, i, vp, vp], i),
+        "cfd2d_field_average_accumulate": ([vp, vp, vp], i),
+        "cfd2d_streamfunction": ([vp, vp, vp], i),
+        "cfd2d_vtk_pack": ([vp, vp, i, vp, vp], i),
         "cfd2d_graph_capture_steps": ([vp, i, vp, C.POINTER(C.c_void_p)], i),
         "cfd2d_graph_launch": ([vp, vp], i),
         "cfd2d_graph_destroy": ([vp], i),
@@ -210,7 +234,8 @@ def exported_symbols():
         "cfd2d_sim_scratch_doubles", "cfd2d_sim_apply_bc", "cfd2d_sim_project_initial",
         "cfd2d_sim_step", "cfd2d_sim_scalar_fill_ghosts", "cfd2d_sim_sst_pre_momentum",
         "cfd2d_sim_smagorinsky_pre_momentum", "cfd2d_wall_distance_workspace_bytes",
-        "cfd2d_sim_wall_distance", "cfd2d_graph_capture_steps", "cfd2d_graph_launch", "cfd2d_graph_destroy",
+        "cfd2d_sim_wall_distance", "cfd2d_sample", "cfd2d_cell_values", "cfd2d_probe_record", "cfd2d_field_average_accumulate",
+        "cfd2d_streamfunction", "cfd2d_vtk_pack", "cfd2d_graph_capture_steps", "cfd2d_graph_launch", "cfd2d_graph_destroy",
         "cfd2d_graph_capture_steps_ex", "cfd2d_events_create", "cfd2d_events_destroy",
         "cfd2d_event_elapsed_ms", "cfd2d_sim_step_begin", "cfd2d_sim_step_finish", "cfd2d_poisson_matvec",
         "cfd2d_pressure_solve_snapshots", "cfd2d_lpc_w32_bytes", "cfd2d_lpc_pack_w32", "cfd2d_lpc_conv32",

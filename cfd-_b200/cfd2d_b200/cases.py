@@ -287,8 +287,6 @@ def build_case(spec: dict) -> Case:
         if sk.get("inflow_band") is not None:
             sk["inflow_band"] = tuple(sk["inflow_band"])
         add_scalar(case, **sk)
-    if spec.get("function_objects"):
-        raise NotImplementedError("function_objects sind nicht Teil des B200-Pfads")
     case.spec = spec
     return case
 

@@ -213,6 +213,12 @@ class Model:
     def fields(self, sim) -> dict:
         return {}
 
+    def device_fields(self, sim):
+        """{key: (label, CFD2D_FIELD_* kind, device tensor)} of the fields() this model
+        offers, read on the device by the function objects; None when the model has
+        only host fields (they are then uploaded when sampled)."""
+        return None
+
     def state(self) -> dict:
         return {}
 
@@ -252,6 +258,9 @@ class PassiveScalar(Model):
 
     def fields(self, sim) -> dict:
         return {self.name: (self.field.label, self.field.cell())}
+
+    def device_fields(self, sim):
+        return {self.name: (self.field.label, _lib.FIELD_CELL, self.field._phi)}
 
 
 class BoussinesqTemperature(Model):
@@ -306,3 +315,6 @@ class BoussinesqTemperature(Model):
 
     def fields(self, sim) -> dict:
         return {"T": ("Temperatur T", self.field.cell())}
+
+    def device_fields(self, sim):
+        return {"T": ("Temperatur T", _lib.FIELD_CELL, self.field._phi)}

@@ -451,6 +451,9 @@ class Simulation:
         return g
 
     def _launch_steps(self, nsteps: int) -> None:
+        if self.function_objects:
+            self._steps_with_functions(int(nsteps))
+            return
         if self._learned is not None:
             for _ in range(int(nsteps)):
                 self._learned_step()
@@ -462,6 +465,32 @@ class Simulation:
                                                    _lib.stream_ptr(self._stream))
                 _lib.check(rc, "cfd2d_graph_launch")
                 left -= size
+
+    def _steps_with_functions(self, nsteps: int) -> None:
+        """Steps one at a time with the function objects after each (cfd2d/solver.py:401-403).
+        Device function objects only queue kernels behind the step; host ones (and
+        user-defined ones) run after a synchronisation, with the state read back,
+        and only when the step ran."""
+        fos = list(self.function_objects)
+        host = [fo for fo in fos if not getattr(fo, "device", False)]
+        saved, self.function_objects = self.function_objects, []
+        try:
+            for _ in range(nsteps):
+                n0 = int(self._st.n)
+                self._launch_steps(1)
+                for fo in fos:
+                    if getattr(fo, "device", False):
+                        fo.execute(self)
+                if host:
+                    self._sync()
+                    self._after_steps()
+                    if int(self._st.n) == n0:
+                        break
+                    for fo in host:
+                        fo.execute(self)
+                    self._flush_mirrors()
+        finally:
+            self.function_objects = saved
 
     # ================================================================ learned pressure preconditioner
     def set_pressure_preconditioner(self, net=None, **kw) -> None:
@@ -762,22 +791,17 @@ class Simulation:
         return psi
 
     def sample_u(self, x, y) -> np.ndarray:
-        from scipy.interpolate import RegularGridInterpolator
+        """u interpolated bilinearly at arbitrary points, wall values through the ghost
+        cells (cfd2d/solver.py:598-606); evaluated on the device."""
+        from .functions import sample_field
 
-        g = self.grid
-        xs = np.arange(g.nx + 1) * g.dx
-        ys = (np.arange(g.ny + 2) - 0.5) * g.dy
-        f = RegularGridInterpolator((xs, ys), self.u, bounds_error=False, fill_value=None)
-        return f(np.column_stack([np.ravel(x), np.ravel(y)]))
+        return sample_field(self, "u", x, y)
 
     def sample_v(self, x, y) -> np.ndarray:
-        from scipy.interpolate import RegularGridInterpolator
+        """v at arbitrary points (cfd2d/solver.py:608-615); evaluated on the device."""
+        from .functions import sample_field
 
-        g = self.grid
-        xs = (np.arange(g.nx + 2) - 0.5) * g.dx
-        ys = np.arange(g.ny + 1) * g.dy
-        f = RegularGridInterpolator((xs, ys), self.v, bounds_error=False, fill_value=None)
-        return f(np.column_stack([np.ravel(x), np.ravel(y)]))
+        return sample_field(self, "v", x, y)
 
     def summary(self) -> str:
         g = self.grid

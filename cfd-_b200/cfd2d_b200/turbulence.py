@@ -157,6 +157,11 @@ class KOmegaSST(Model):
     def monitors(self, sim) -> dict:
         return {"k_mittel": float(np.nanmean(self.k.cell())), "nu_t_max": float(sim.nu_t.max())}
 
+    def device_fields(self, sim):
+        return {"k": (self.k.label, _lib.FIELD_CELL, self.k._phi),
+                "omega": ("log10 ω (spez. Dissipationsrate)", _lib.FIELD_CELL_LOG10, self.w._phi),
+                "nu_t": ("Turbulente Viskosität ν_t", _lib.FIELD_CELL, sim._nu_t)}
+
     def fields(self, sim) -> dict:
         solid = sim.grid.solid
         return {"k": (self.k.label, self.k.cell()),
@@ -202,6 +207,9 @@ class Smagorinsky(Model):
     def fields(self, sim) -> dict:
         return {"nu_t": ("Turbulente Viskosität ν_t",
                          np.where(sim.grid.solid, np.nan, sim.nu_t[1:-1, 1:-1]))}
+
+    def device_fields(self, sim):
+        return {"nu_t": ("Turbulente Viskosität ν_t", _lib.FIELD_CELL, sim._nu_t)}
 
 
 TURBULENCE_MODELS = {"laminar": None, "kOmegaSST": KOmegaSST, "Smagorinsky": Smagorinsky}

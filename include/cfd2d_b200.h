@@ -461,6 +461,82 @@ int cfd2d_capture_end(void* stream, void** graph_out);
 /* Abandon a capture after an error (ends it and frees the partial graph). */
 int cfd2d_capture_abort(void* stream);
 
+/* ---- function objects fed from the device (drop-in for cfd2d/functions.py) ----
+ * Probes, line samples, time averages and the VTK export read the device fields
+ * directly: nothing copies a whole field to the host per step. */
+
+/* Field selectors (cfd2d/visualization.py:50-73 field_data; cfd2d/solver.py:598-615
+ * sample_u / sample_v). Face fields are interpolated on their own staggered grid and
+ * extrapolated outside it; cell fields are NaN on solid cells and their sample
+ * points are clipped to the first and last cell centre (cfd2d/functions.py:24-39). */
+#define CFD2D_FIELD_U 0           /* face u, (nx+1)(ny+2) at (i dx, (j - 1/2) dy) */
+#define CFD2D_FIELD_V 1           /* face v, (nx+2)(ny+1) at ((i - 1/2) dx, j dy) */
+#define CFD2D_FIELD_PRESSURE 2    /* p of the cell */
+#define CFD2D_FIELD_UC 3          /* mean of the two u faces (cfd2d/solver.py:526-533) */
+#define CFD2D_FIELD_VC 4
+#define CFD2D_FIELD_SPEED 5       /* sqrt(uc^2 + vc^2) */
+#define CFD2D_FIELD_VORTICITY 6   /* mean of the 4 node vorticities (cfd2d/solver.py:569-578) */
+#define CFD2D_FIELD_CELL 7        /* `data`: a padded (nx+2)(ny+2) cell array (scalar, nu_t) */
+#define CFD2D_FIELD_CELL_LOG10 8  /* log10(max(data, 1e-30)) of a padded cell array */
+#define CFD2D_FIELD_NODE 9        /* mean of the 4 corners of a (nx+1)(ny+1) node array (psi) */
+#define CFD2D_FIELD_FLUID 10      /* 1 on fluid cells, 0 on solids (not NaN) */
+#define CFD2D_MAX_FIELDS 16
+
+typedef struct cfd2d_field {
+    int kind;                 /* CFD2D_FIELD_* */
+    int pad;
+    const double* data;       /* CELL, CELL_LOG10, NODE: the device array; else NULL */
+} cfd2d_field;
+
+/* out[f * npts + k] = field f at (px[k], py[k]) (device arrays), bilinear
+ * interpolation as scipy's RegularGridInterpolator(method="linear",
+ * bounds_error=False, fill_value=None). `fields` is a host array of nfields <=
+ * CFD2D_MAX_FIELDS. Replaces cfd2d/functions.py:24 sample_field(sim, field, x, y). */
+int cfd2d_sample(const cfd2d_sim* sim, const cfd2d_field* fields, int nfields, const double* px,
+                 const double* py, int npts, double* out, void* stream);
+
+/* out[i ny + j] = field at interior cell (i, j), NaN on solids (FLUID: 1 or 0).
+ * Replaces cfd2d/visualization.py:50 field_data(sim, field). */
+int cfd2d_cell_values(const cfd2d_sim* sim, const cfd2d_field* field, double* out, void* stream);
+
+/* Time series of a Probes object (cfd2d/functions.py:59-80): device buffers. */
+typedef struct cfd2d_probe_series {
+    double* t;                /* cap sample times */
+    double* values;           /* cap rows of nfields * npts values (row, field, point) */
+    int64_t* count;           /* [0] rows written, [1] step number of the last row,
+                                 [2] 1 when a row did not fit (the host sizes cap ahead) */
+    int cap;
+    int every;                /* record when n % every == 0 */
+} cfd2d_probe_series;
+
+/* Append one row after a step: skipped when no step ran since the last row or
+ * n % every != 0 (reads t and n from sim->state). One block, no host sync.
+ * Replaces cfd2d/functions.py:70 Probes.execute(sim). */
+int cfd2d_probe_record(const cfd2d_sim* sim, const cfd2d_field* fields, int nfields, const double* px,
+                       const double* py, int npts, const cfd2d_probe_series* series, void* stream);
+
+/* Time sums of the cell velocity and pressure (cfd2d/functions.py:180-224). */
+typedef struct cfd2d_field_average {
+    double t_start;           /* accumulate once t >= t_start */
+    double* sum;              /* 3 nx*ny: uc, vc, p (NaN on solids), sum of value * dt */
+    double* sum2;             /* 3 nx*ny: sum of value * value * dt */
+    double* T;                /* device [0] summed time, [1] step number of the last sum (as double) */
+} cfd2d_field_average;
+
+/* Add this step's fields (skipped before t_start or when no step ran since the
+ * last call). Replaces cfd2d/functions.py:189 FieldAverage.execute(sim). */
+int cfd2d_field_average_accumulate(const cfd2d_sim* sim, const cfd2d_field_average* avg, void* stream);
+
+/* Stream function psi, (nx+1)(ny+1) node values (cfd2d/solver.py:580-596, the same
+ * running sums in the same order). */
+int cfd2d_streamfunction(const cfd2d_sim* sim, double* psi, void* stream);
+
+/* VTK payload (cfd2d/functions.py:244-287 write_vtk): big-endian float32, cells in
+ * VTK order (x fastest), NaN written as 0. `out` receives the velocity vectors
+ * (uc, vc, 0 per cell; 12 nx ny bytes) followed by one block of 4 nx ny bytes per
+ * field. The host writes the text header lines around these blocks. */
+int cfd2d_vtk_pack(const cfd2d_sim* sim, const cfd2d_field* fields, int nfields, uint8_t* out, void* stream);
+
 /* Library version string (host memory, static). */
 const char* cfd2d_version(void);
 

@@ -26,7 +26,9 @@ __all__ = [
     "scalar_transport", "OPressure", "pcg_scipy_trajectory", "OScalarBC", "OScalarField",
     "OPassiveScalar", "OBoussinesq", "OSmagorinsky", "OKOmegaSST", "OSimulation", "cavity", "cylinder",
     "custom_obstacles", "heated_cavity", "sst_channel", "add_scalar", "wall_distance",
-    "wall_adjacent_cells", "strain_rate_squared", "KAPPA",
+    "wall_adjacent_cells", "strain_rate_squared", "KAPPA", "cell_velocity", "cell_pressure",
+    "cell_vorticity", "streamfunction", "available_fields", "field_data", "sample_u", "sample_v",
+    "sample_field", "line_points", "OFieldAverage", "write_vtk_bytes",
 ]
 
 SIDES = ("left", "right", "bottom", "top")
@@ -929,6 +931,11 @@ class OPassiveScalar(OModel):
         lim = self.field.dt_limit()
         return lim if np.isfinite(lim) else None
 
+    def fields(self, sim):
+        # cfd2d/models.py:332-333 with ScalarField.cell (models.py:217-219)
+        return {self.name: ("Skalar " + self.name,
+                            np.where(~sim.grid.fluid[1:-1, 1:-1], np.nan, self.field.phi[1:-1, 1:-1]))}
+
 
 class OBoussinesq(OModel):
     """cfd2d/models.py:339-426"""
@@ -1604,3 +1611,202 @@ def sst_channel(nx=128, ny=192, lx=2 * np.pi, ly=2.0, re_b=1e4, seed=0, noise=0.
     sim.apply_bc()
     sim.project_initial()
     return sim
+
+
+# --------------------------------------------------------------------------- #
+# Function objects, VTK export and derived fields (cfd2d/functions.py:24-287,
+# cfd2d/solver.py:526-615, cfd2d/visualization.py:41-89). They take any object
+# with the reference's Simulation attributes (u, v, p, grid, models, t, dt,
+# nu_t, variable_viscosity).
+# --------------------------------------------------------------------------- #
+BASE_FIELDS = {"speed": "Geschwindigkeitsbetrag |u|", "vorticity": "Wirbelstärke ω", "pressure": "Druck p",
+               "u": "Geschwindigkeit u (x-Richtung)", "v": "Geschwindigkeit v (y-Richtung)",
+               "streamfunction": "Stromfunktion ψ"}
+
+
+def _solid(sim):
+    return ~sim.grid.fluid[1:-1, 1:-1]
+
+
+def cell_velocity(sim):
+    # cfd2d/solver.py:526-533
+    uc = 0.5 * (sim.u[:-1, 1:-1] + sim.u[1:, 1:-1])
+    vc = 0.5 * (sim.v[1:-1, :-1] + sim.v[1:-1, 1:])
+    return np.where(_solid(sim), np.nan, uc), np.where(_solid(sim), np.nan, vc)
+
+
+def cell_pressure(sim):
+    # cfd2d/solver.py:535-536
+    return np.where(_solid(sim), np.nan, sim.p[1:-1, 1:-1])
+
+
+def cell_vorticity(sim):
+    # cfd2d/solver.py:569-578
+    g = sim.grid
+    w = (sim.v[1:, :] - sim.v[:-1, :]) / g.dx - (sim.u[:, 1:] - sim.u[:, :-1]) / g.dy
+    wc = 0.25 * (w[:-1, :-1] + w[1:, :-1] + w[:-1, 1:] + w[1:, 1:])
+    return np.where(_solid(sim), np.nan, wc)
+
+
+def streamfunction(sim):
+    # cfd2d/solver.py:580-596
+    g = sim.grid
+    fl = g.fluid
+    u_open = fl[:-1, 1:-1] | fl[1:, 1:-1]
+    v_open = fl[1:-1, 0] | fl[1:-1, 1]
+    u = np.where(u_open, sim.u[:, 1:-1], 0.0)
+    v0 = np.where(v_open, sim.v[1:-1, 0], 0.0)
+    psi = np.zeros((g.nx + 1, g.ny + 1))
+    psi[1:, 0] = -np.cumsum(v0) * g.dx
+    psi[:, 1:] = psi[:, :1] + np.cumsum(u, axis=1) * g.dy
+    return psi
+
+
+def _model_fields(sim):
+    out = {}
+    for m in getattr(sim, "models", []):
+        if hasattr(m, "fields"):
+            out.update(m.fields(sim))
+    return out
+
+
+def available_fields(sim):
+    # cfd2d/visualization.py:80-89
+    out = dict(BASE_FIELDS)
+    for k, (label, _) in _model_fields(sim).items():
+        out[k] = label
+    if getattr(sim, "variable_viscosity", False) and "nu_t" not in out:
+        out["nu_t"] = "Turbulente Viskosität ν_t"
+    return out
+
+
+def field_data(sim, field):
+    # cfd2d/visualization.py:50-73
+    if field == "speed":
+        uc, vc = cell_velocity(sim)
+        return np.sqrt(uc ** 2 + vc ** 2)
+    if field == "vorticity":
+        return cell_vorticity(sim)
+    if field == "pressure":
+        return cell_pressure(sim)
+    if field == "u":
+        return cell_velocity(sim)[0]
+    if field == "v":
+        return cell_velocity(sim)[1]
+    if field == "streamfunction":
+        psi = streamfunction(sim)
+        pc = 0.25 * (psi[:-1, :-1] + psi[1:, :-1] + psi[:-1, 1:] + psi[1:, 1:])
+        return np.where(_solid(sim), np.nan, pc)
+    mf = _model_fields(sim)
+    if field in mf:
+        return mf[field][1]
+    if field == "nu_t" and getattr(sim, "variable_viscosity", False):
+        return np.where(_solid(sim), np.nan, sim.nu_t[1:-1, 1:-1])
+    raise ValueError(field)
+
+
+def _rgi(xs, ys, values, x, y):
+    from scipy.interpolate import RegularGridInterpolator
+
+    f = RegularGridInterpolator((xs, ys), values, bounds_error=False, fill_value=None)
+    return f(np.column_stack([np.ravel(x), np.ravel(y)]))
+
+
+def sample_u(sim, x, y):
+    # cfd2d/solver.py:598-606
+    g = sim.grid
+    return _rgi(np.arange(g.nx + 1) * g.dx, (np.arange(g.ny + 2) - 0.5) * g.dy, sim.u, x, y)
+
+
+def sample_v(sim, x, y):
+    # cfd2d/solver.py:608-615
+    g = sim.grid
+    return _rgi((np.arange(g.nx + 2) - 0.5) * g.dx, np.arange(g.ny + 1) * g.dy, sim.v, x, y)
+
+
+def sample_field(sim, field, x, y):
+    # cfd2d/functions.py:24-39
+    x = np.atleast_1d(np.asarray(x, dtype=float))
+    y = np.atleast_1d(np.asarray(y, dtype=float))
+    if field == "u":
+        return sample_u(sim, x, y)
+    if field == "v":
+        return sample_v(sim, x, y)
+    g = sim.grid
+    xc = (np.arange(g.nx) + 0.5) * g.dx
+    yc = (np.arange(g.ny) + 0.5) * g.dy
+    return _rgi(xc, yc, field_data(sim, field), np.clip(x, xc[0], xc[-1]), np.clip(y, yc[0], yc[-1]))
+
+
+def line_points(p0, p1, n):
+    # cfd2d/functions.py:133-137
+    s = np.linspace(0, 1, n)
+    x = p0[0] + s * (p1[0] - p0[0])
+    y = p0[1] + s * (p1[1] - p0[1])
+    return s * np.hypot(p1[0] - p0[0], p1[1] - p0[1]), x, y
+
+
+class OFieldAverage:
+    """cfd2d/functions.py:180-224"""
+
+    def __init__(self, t_start=0.0):
+        self.t_start, self.T, self.sum, self.sum2 = float(t_start), 0.0, None, None
+
+    def execute(self, sim):
+        if sim.t < self.t_start:
+            return
+        uc, vc = cell_velocity(sim)
+        vals = {"u": uc, "v": vc, "p": cell_pressure(sim)}
+        if self.sum is None:
+            self.sum = {k: np.zeros_like(a) for k, a in vals.items()}
+            self.sum2 = {k: np.zeros_like(a) for k, a in vals.items()}
+        for k, a in vals.items():
+            self.sum[k] += a * sim.dt
+            self.sum2[k] += a * a * sim.dt
+        self.T += sim.dt
+
+    def mean(self, k):
+        return self.sum[k] / max(self.T, 1e-300)
+
+    def rms(self, k):
+        m = self.mean(k)
+        return np.sqrt(np.maximum(self.sum2[k] / max(self.T, 1e-300) - m * m, 0.0))
+
+
+def write_vtk_bytes(sim):
+    """The bytes of cfd2d/functions.py:244-287 write_vtk (legacy binary RECTILINEAR_GRID)."""
+    g = sim.grid
+    nx, ny = g.nx, g.ny
+    out = bytearray()
+
+    def line(s):
+        out.extend((s + "\n").encode("ascii"))
+
+    line("# vtk DataFile Version 3.0")
+    line(f"cfd2d t={sim.t:.8g}")
+    line("BINARY")
+    line("DATASET RECTILINEAR_GRID")
+    line(f"DIMENSIONS {nx + 1} {ny + 1} 1")
+    line(f"X_COORDINATES {nx + 1} float")
+    out.extend((np.arange(nx + 1) * g.dx).astype(">f4").tobytes())
+    line("")
+    line(f"Y_COORDINATES {ny + 1} float")
+    out.extend((np.arange(ny + 1) * g.dy).astype(">f4").tobytes())
+    line("")
+    line("Z_COORDINATES 1 float")
+    out.extend(np.zeros(1, ">f4").tobytes())
+    line("")
+    line(f"CELL_DATA {nx * ny}")
+    uc, vc = cell_velocity(sim)
+    vec = np.stack([np.nan_to_num(uc).T.ravel(), np.nan_to_num(vc).T.ravel(), np.zeros(nx * ny)], axis=1)
+    line("VECTORS U float")
+    out.extend(vec.astype(">f4").tobytes())
+    line("")
+    names = [k for k in available_fields(sim) if k not in ("u", "v")]
+    for k in names + ["fluid"]:
+        d = g.fluid[1:-1, 1:-1].astype(float) if k == "fluid" else field_data(sim, k)
+        line(f"SCALARS {k.replace(' ', '_')} float 1")
+        line("LOOKUP_TABLE default")
+        out.extend(np.nan_to_num(d, nan=0.0).T.astype(">f4").ravel().tobytes())
+        line("")
+    return bytes(out)

@@ -6,7 +6,7 @@ Run in a container that holds the reference checkout (default
     python tests/golden/make_golden.py [group ...]
 
 Groups: kernels geometry pressure cavity cylinder sst misc checkpoint smagorinsky
-(default: all).
+functions (default: all).
 The reference imports matplotlib at module load; ``mplstub/`` stands in for it
 (no fixture case needs plotting or polygon masks). Every pressure solve uses the
 reference's own ``PressureSolver`` (scipy CG or SuperLU) with
@@ -317,6 +317,47 @@ def gen_smagorinsky():
     _save("golden_smagorinsky", out)
 
 
+FO_POINTS = [(0.5, 0.2), (0.2, 0.2), (0.0, 0.0), (2.2, 0.41), (1.0, 0.05), (-0.1, 0.5), (0.31, 0.1337),
+             (0.15, 0.2), (2.5, -0.2)]
+FO_FIELDS = ("u", "v", "pressure", "vorticity", "speed", "streamfunction", "c")
+
+
+def gen_functions():
+    """Function objects of the reference (cfd2d/functions.py) on the 88 x 17 cylinder
+    with a passive scalar: probes of every field kind at points inside, on walls,
+    in the obstacle and outside the domain, a time average started after the first
+    steps, a slanted line sample and the VTK file after 30 steps."""
+    import tempfile
+
+    from cfd2d import functions
+
+    case = cases.cylinder_flow(re=100, nx=88, ny=17, pressure_solver="cg")
+    cases.add_scalar(case, "c", 1e-3, inflow_band=(0.15, 0.25))
+    sim = case.sim
+    sim.pressure.tol = TOL
+    pr = functions.Probes(FO_POINTS, fields=FO_FIELDS)
+    fa = functions.FieldAverage(t_start=0.01)
+    sim.function_objects += [pr, fa]
+    for _ in range(30):
+        sim.step()
+    out = {"fo_u": sim.u.copy(), "fo_v": sim.v.copy(), "fo_p": sim.p.copy(),
+           "fo_c": sim.scalars["c"].phi.copy(), "fo_t": np.array(sim.t), "fo_dt": np.array(sim.dt),
+           "fo_probe_t": np.array(pr.t)}
+    for f in FO_FIELDS:
+        out[f"fo_probe_{f}"] = np.array(pr.data[f])
+    out["fo_avg_T"] = np.array(fa.T)
+    for k in ("u", "v", "p"):
+        out[f"fo_avg_sum_{k}"] = fa.sum[k]
+        out[f"fo_avg_sum2_{k}"] = fa.sum2[k]
+    ls = functions.LineSample((0.0, 0.1), (2.2, 0.3), n=37, fields=["u", "v", "pressure", "c"], label="schraeg")
+    for k, v in ls.sample(sim).items():
+        out[f"fo_line_{k}"] = np.asarray(v)
+    with tempfile.TemporaryDirectory() as td:
+        raw = functions.write_vtk(sim, Path(td) / "f.vtk").read_bytes()
+    out["fo_vtk"] = np.frombuffer(raw, dtype=np.uint8)
+    _save("golden_functions", out)
+
+
 def gen_checkpoint():
     """A checkpoint written by the reference itself (cfd2d/functions.py:326) after 40
     steps of the 88 x 17 cylinder with a passive scalar, and the reference's state
@@ -352,7 +393,7 @@ def gen_checkpoint():
 
 GROUPS = {"kernels": gen_kernels, "geometry": gen_geometry, "pressure": gen_pressure,
           "cavity": gen_cavity, "cylinder": gen_cylinder, "sst": gen_sst, "misc": gen_misc,
-          "checkpoint": gen_checkpoint, "smagorinsky": gen_smagorinsky}
+          "checkpoint": gen_checkpoint, "smagorinsky": gen_smagorinsky, "functions": gen_functions}
 
 if __name__ == "__main__":
     import warnings

@@ -232,3 +232,66 @@ def test_smagorinsky_runs():
         key = "nut" if f == "nu_t" else f
         assert rel(getattr(sim, f), g[f"smy_{key}_30"]) < 1e-12, f
     assert rel(sim.scalars["c"].phi, g["smy_c_30"]) < 1e-12
+
+
+# ---------------------------------------------------------------- function objects
+FO_POINTS = [(0.5, 0.2), (0.2, 0.2), (0.0, 0.0), (2.2, 0.41), (1.0, 0.05), (-0.1, 0.5), (0.31, 0.1337),
+             (0.15, 0.2), (2.5, -0.2)]
+FO_FIELDS = ("u", "v", "pressure", "vorticity", "speed", "streamfunction", "c")
+
+
+def _fo_case():
+    sim = O.cylinder(re=100, nx=88, ny=17, tol=1e-8)
+    O.add_scalar(sim, "c", 1e-3, inflow_band=(0.15, 0.25))
+    return sim
+
+
+def _eq(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return a.shape == b.shape and np.array_equal(a, b, equal_nan=True)
+
+
+def test_function_objects_on_the_reference_state_bitwise():
+    """Sampling, line sample and the VTK bytes of the oracle on the reference's own
+    final state equal the reference's outputs bit for bit (cfd2d/functions.py:24-287)."""
+    g = golden("golden_functions")
+    sim = _fo_case()
+    sim.u, sim.v, sim.p = g["fo_u"], g["fo_v"], g["fo_p"]
+    sim.scalars["c"].phi[:] = g["fo_c"]
+    sim.t, sim.dt = float(g["fo_t"]), float(g["fo_dt"])
+    xs, ys = [p[0] for p in FO_POINTS], [p[1] for p in FO_POINTS]
+    for f in FO_FIELDS:
+        assert _eq(O.sample_field(sim, f, xs, ys), g[f"fo_probe_{f}"][-1]), f
+    s, x, y = O.line_points((0.0, 0.1), (2.2, 0.3), 37)
+    assert _eq(s, g["fo_line_s"]) and _eq(x, g["fo_line_x"]) and _eq(y, g["fo_line_y"])
+    for f in ("u", "v", "pressure", "c"):
+        assert _eq(O.sample_field(sim, f, x, y), g[f"fo_line_{f}"]), f
+    assert O.write_vtk_bytes(sim) == g["fo_vtk"].tobytes()
+
+
+def test_probe_series_and_field_average_runs():
+    """Probes and FieldAverage executed after each of 30 oracle steps match the
+    reference's series and sums (cfd2d/functions.py:59-80, 180-204)."""
+    g = golden("golden_functions")
+    sim = _fo_case()
+    fa = O.OFieldAverage(t_start=0.01)
+    xs, ys = [p[0] for p in FO_POINTS], [p[1] for p in FO_POINTS]
+    rows = {f: [] for f in FO_FIELDS}
+    ts = []
+    for _ in range(30):
+        sim.step()
+        ts.append(sim.t)
+        for f in FO_FIELDS:
+            rows[f].append(O.sample_field(sim, f, xs, ys))
+        fa.execute(sim)
+    assert rel(ts, g["fo_probe_t"]) < 1e-13
+    for f in FO_FIELDS:
+        a, b = np.array(rows[f]), g[f"fo_probe_{f}"]
+        assert np.array_equal(np.isnan(a), np.isnan(b)), f
+        assert rel(np.nan_to_num(a), np.nan_to_num(b)) < 1e-11, f
+    assert fa.T == pytest.approx(float(g["fo_avg_T"]), rel=1e-13)
+    for k in ("u", "v", "p"):
+        for name, mine in (("sum", fa.sum[k]), ("sum2", fa.sum2[k])):
+            ref = g[f"fo_avg_{name}_{k}"]
+            assert np.array_equal(np.isnan(mine), np.isnan(ref))
+            assert rel(np.nan_to_num(mine), np.nan_to_num(ref)) < 1e-11, (name, k)
