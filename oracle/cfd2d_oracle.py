@@ -29,6 +29,7 @@ __all__ = [
     "wall_adjacent_cells", "strain_rate_squared", "KAPPA", "cell_velocity", "cell_pressure",
     "cell_vorticity", "streamfunction", "available_fields", "field_data", "sample_u", "sample_v",
     "sample_field", "line_points", "OFieldAverage", "write_vtk_bytes",
+    "vof_advect", "OVOF", "dam_break", "rectangle_mask",
 ]
 
 SIDES = ("left", "right", "bottom", "top")
@@ -747,6 +748,59 @@ class OPressure:
         return p
 
 
+    def solve_variable(self, rhs, bx, by):
+        """div(b grad p) = rhs with face coefficients b = 1/rho, bx (nx+1, ny), by
+        (nx, ny+1); the matrix is rebuilt and solved directly on every call
+        (cfd2d/pressure.py:187-244)."""
+        from scipy.sparse import csc_matrix
+        from scipy.sparse.linalg import spsolve
+
+        g, f, idx = self.g, self.fluid, self.idx
+        nx, ny = g.nx, g.ny
+        dx2, dy2 = self.dx2, self.dy2
+        bxm, bym, bp = self.both_x, self.both_y, self.both_p
+        diag = np.zeros((nx, ny))
+        cxi = (bx[1:nx, :] * dx2)[bxm]
+        diag[:-1, :][bxm] += cxi
+        diag[1:, :][bxm] += cxi
+        cyi = (by[:, 1:ny] * dy2)[bym]
+        diag[:, :-1][bym] += cyi
+        diag[:, 1:][bym] += cyi
+        cpi = np.zeros(0)
+        if self.periodic:
+            cpi = (bx[nx, :] * dx2)[bp]
+            diag[-1, :][bp] += cpi
+            diag[0, :][bp] += cpi
+        d = self.dirichlet
+        diag[0, :][d["left"]] += 2 * dx2 * bx[0, :][d["left"]]
+        diag[-1, :][d["right"]] += 2 * dx2 * bx[nx, :][d["right"]]
+        diag[:, 0][d["bottom"]] += 2 * dy2 * by[:, 0][d["bottom"]]
+        diag[:, -1][d["top"]] += 2 * dy2 * by[:, ny][d["top"]]
+        for fi, fj in self.pinned:
+            diag[fi, fj] += dx2 * max(float(bx.max()), 1e-30)
+        rows = [idx[:-1, :][bxm], idx[1:, :][bxm], idx[:, :-1][bym], idx[:, 1:][bym],
+                idx[-1, :][bp], idx[0, :][bp], np.arange(self.n)]
+        cols = [idx[1:, :][bxm], idx[:-1, :][bxm], idx[:, 1:][bym], idx[:, :-1][bym],
+                idx[0, :][bp], idx[-1, :][bp], np.arange(self.n)]
+        vals = [-cxi, -cxi, -cyi, -cyi, -cpi, -cpi, diag[f]]
+        A = csc_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                       shape=(self.n, self.n))
+        b = rhs[f].astype(float)
+        if self.neumann_components:
+            lab = self.labels[f]
+            for c in self.neumann_components:
+                m = lab == c
+                b[m] -= b[m].mean()
+        x = spsolve(A, -b)
+        p = np.zeros(f.shape)
+        p[f] = x
+        if self.neumann_components:
+            for c in self.neumann_components:
+                m = self.labels == c
+                p[m] -= p[m].mean()
+        return p
+
+
 # --------------------------------------------------------------------------- #
 # Scalars and models (cfd2d/models.py:28-426, cfd2d/turbulence.py:28-325)
 # --------------------------------------------------------------------------- #
@@ -1267,6 +1321,7 @@ class OSimulation:
         self.nu_t = np.zeros((nx + 2, ny + 2))
         self.nu_eff = np.full((nx + 2, ny + 2), self.nu)
         self.variable_viscosity = False
+        self.variable_density = False
         self.rho = np.ones((nx + 2, ny + 2))
         self.body_force = (float(body_force[0]), float(body_force[1]))
         self.flow_rate = flow_rate
@@ -1327,7 +1382,10 @@ class OSimulation:
         g = self.grid
         umax = max(np.abs(self.u).max(), 1e-12)
         vmax = max(np.abs(self.v).max(), 1e-12)
-        nu_max = float(self.nu_eff.max()) if self.variable_viscosity else self.nu
+        if self.variable_density:
+            nu_max = float((self.nu_eff / self.rho)[g.fluid].max())
+        else:
+            nu_max = float(self.nu_eff.max()) if self.variable_viscosity else self.nu
         dt_visc = 0.5 / (nu_max * (1.0 / g.dx ** 2 + 1.0 / g.dy ** 2))
         dt_conv = min(g.dx / umax, g.dy / vmax)
         if self.scheme == "ab2":
@@ -1348,18 +1406,30 @@ class OSimulation:
         if self.scheme == "euler":
             cfl = max(umax * dt / g.dx, vmax * dt / g.dy)
             return float(min(1.0, max(0.05, 1.2 * cfl)))
-        nu_ref = float(self.nu_eff[g.fluid].min()) if self.variable_viscosity else self.nu
+        if self.variable_density:
+            nu_ref = float((self.nu_eff / self.rho)[g.fluid].min())
+        else:
+            nu_ref = float(self.nu_eff[g.fluid].min()) if self.variable_viscosity else self.nu
         re_cell = max(umax * g.dx, vmax * g.dy) / nu_ref
         return float(min(1.0, max(0.05, 0.015 * re_cell)))
 
     def solve_pressure_and_correct(self, dt):
-        # cfd2d/solver.py:258-321 (constant density)
+        # cfd2d/solver.py:258-321; with variable density the face coefficients
+        # b = 2 / (rho_L + rho_R) scale the operator and the correction
         g = self.grid
         nx, ny, dx, dy = g.nx, g.ny, g.dx, g.dy
         F, G = self.F, self.G
         if self.periodic:
             F[0, :] = F[nx, :]
         div = (F[1:, 1:-1] - F[:-1, 1:-1]) / dx + (G[1:-1, 1:] - G[1:-1, :-1]) / dy
+        if self.variable_density:
+            bx = 2.0 / (self.rho[:-1, :] + self.rho[1:, :])
+            by = 2.0 / (self.rho[:, :-1] + self.rho[:, 1:])
+            if self.periodic:
+                bx[nx, :] = 2.0 / (self.rho[nx, :] + self.rho[1, :])
+            p_int = self.pressure.solve_variable(div / dt, bx[:, 1:-1], by[1:-1, :])
+            self._solve_correct_variable(dt, p_int, bx, by)
+            return
         p_int = self.pressure.solve(div / dt)
         self.iterations.append(self.pressure.last_iterations)
         p = self.p
@@ -1390,19 +1460,55 @@ class OSimulation:
         self.v[1:nx + 1, ny] = np.where(d["top"], G[1:nx + 1, ny] + 2 * dt * 1.0 * p[1:nx + 1, ny] / dy,
                                         G[1:nx + 1, ny])
 
+    def _solve_correct_variable(self, dt, p_int, bx, by):
+        # cfd2d/solver.py:274-321 with cx = bx, cy = by
+        g = self.grid
+        nx, ny, dx, dy = g.nx, g.ny, g.dx, g.dy
+        F, G = self.F, self.G
+        self.iterations.append(1)
+        p = self.p
+        p[:] = 0.0
+        p[1:-1, 1:-1] = p_int
+        if self.periodic:
+            p[0, :] = p[nx, :]
+            p[nx + 1, :] = p[1, :]
+        uf = self.u_fluid[1:nx, 1:ny + 1]
+        corr = F[1:nx, 1:ny + 1] - dt * bx[1:nx, 1:ny + 1] * (p[2:nx + 1, 1:ny + 1] - p[1:nx, 1:ny + 1]) / dx
+        self.u[1:nx, 1:ny + 1] = np.where(uf, corr, F[1:nx, 1:ny + 1])
+        vf = self.v_fluid[1:nx + 1, 1:ny]
+        corr = G[1:nx + 1, 1:ny] - dt * by[1:nx + 1, 1:ny] * (p[1:nx + 1, 2:ny + 1] - p[1:nx + 1, 1:ny]) / dy
+        self.v[1:nx + 1, 1:ny] = np.where(vf, corr, G[1:nx + 1, 1:ny])
+        if self.periodic:
+            uf = self.u_fluid[nx, 1:ny + 1]
+            corr = F[nx, 1:ny + 1] - dt * bx[nx, 1:ny + 1] * (p[1, 1:ny + 1] - p[nx, 1:ny + 1]) / dx
+            self.u[nx, 1:ny + 1] = np.where(uf, corr, F[nx, 1:ny + 1])
+            self.u[0, :] = self.u[nx, :]
+            return
+        d = self.pressure.dirichlet
+        self.u[0, 1:ny + 1] = np.where(d["left"], F[0, 1:ny + 1] - 2 * dt * bx[0, 1:ny + 1] * p[1, 1:ny + 1] / dx,
+                                       F[0, 1:ny + 1])
+        self.u[nx, 1:ny + 1] = np.where(d["right"],
+                                        F[nx, 1:ny + 1] + 2 * dt * bx[nx, 1:ny + 1] * p[nx, 1:ny + 1] / dx,
+                                        F[nx, 1:ny + 1])
+        self.v[1:nx + 1, 0] = np.where(d["bottom"], G[1:nx + 1, 0] - 2 * dt * by[1:nx + 1, 0] * p[1:nx + 1, 1] / dy,
+                                       G[1:nx + 1, 0])
+        self.v[1:nx + 1, ny] = np.where(d["top"],
+                                        G[1:nx + 1, ny] + 2 * dt * by[1:nx + 1, ny] * p[1:nx + 1, ny] / dy,
+                                        G[1:nx + 1, ny])
+
     def step(self):
         # cfd2d/solver.py:326-403
         g = self.grid
         self.apply_bc()
         for m in self.models:
             m.pre_momentum(self)
-        if self.variable_viscosity:
+        if self.variable_viscosity and not self.variable_density:
             np.add(self.nu, self.nu_t, out=self.nu_eff)
         dt = self.compute_dt()
         self.gamma = self.auto_gamma(dt) if self.gamma_setting == "auto" else float(self.gamma_setting)
         momentum_tendencies(self.u, self.v, g.fluid, g.nx, g.ny, g.dx, g.dy, self.nu_eff,
                             self.variable_viscosity, self.gamma, self.periodic, self.hu, self.hv,
-                            self.rho, False)
+                            self.rho, self.variable_density)
         for m in self.models:
             m.momentum_source(self, self.hu, self.hv)
         if self.scheme == "ab2" and self.hu_old is not None:
@@ -1810,3 +1916,220 @@ def write_vtk_bytes(sim):
         out.extend(np.nan_to_num(d, nan=0.0).T.astype(">f4").ravel().tobytes())
         line("")
     return bytes(out)
+
+
+# --------------------------------------------------------------------------- #
+# Two-phase VOF (cfd2d/vof.py) and the dam break (cfd2d/cases.py:294-320).
+# The advection is restated face by face in the reference's loop order (small
+# grids only): every cell receives its west, east, south and north face terms in
+# that order, and with periodic x the wrapped face nx reaches cell 1 last.
+# --------------------------------------------------------------------------- #
+def _vof_face_value(a_up, a_c, a_d, has_up):
+    # cfd2d/vof.py:23-33: van Leer face value, first order without an upwind cell
+    if not has_up:
+        return a_c
+    den = a_d - a_c
+    if abs(den) < 1e-300:
+        return a_c
+    r = (a_c - a_up) / den
+    lim = 0.0 if r <= 0.0 else 2.0 * r / (1.0 + r)
+    return a_c + 0.5 * lim * den
+
+
+def _vof_face_flux(vel, a_lo, a_hi, a_up, has_up, g_n, g_t, c_alpha):
+    """Flux through one face from its low to its high cell: upwind-bounded
+    advection plus the compression term (cfd2d/vof.py:72-88, 113-124)."""
+    if vel >= 0.0:
+        af = _vof_face_value(a_up, a_lo, a_hi, has_up)
+    else:
+        af = _vof_face_value(a_up, a_hi, a_lo, has_up)
+    flux = vel * af
+    gm = np.sqrt(g_n * g_n + g_t * g_t)
+    if gm > 1e-12 and c_alpha > 0.0:
+        ur = c_alpha * abs(vel) * g_n / gm
+        ac, ad = (a_lo, a_hi) if ur >= 0.0 else (a_hi, a_lo)
+        flux += ur * ac * (1.0 - ad)
+    return flux
+
+
+def vof_advect(a, u, v, fluid, nx, ny, dx, dy, dt, c_alpha, periodic, a_in, out):
+    """One explicit conservative alpha transport step (cfd2d/vof.py:36-137)."""
+    out[:, :] = a
+    for i in range(0, nx + 1):
+        for j in range(1, ny + 1):
+            uf = u[i, j]
+            if i == 0 and periodic:
+                continue
+            if i == 0 or (i == nx and not periodic):
+                P = 1 if i == 0 else nx
+                if fluid[P, j]:
+                    into = uf if i == 0 else -uf
+                    ab = a_in if into > 0 else a[P, j]
+                    out[P, j] += dt * into * ab / dx
+                continue
+            L, R = i, (i + 1 if i < nx else 1)
+            if not (fluid[L, j] and fluid[R, j]):
+                continue
+            if uf >= 0.0:
+                up = L - 1 if L - 1 >= 1 else (nx if periodic else -1)
+            else:
+                up = R + 1 if R + 1 <= nx else (1 if periodic else -1)
+            has_up = up >= 1 and bool(fluid[up, j])
+            gx = (a[R, j] - a[L, j]) / dx
+            jn = j + 1 if j < ny else j
+            js = j - 1 if j > 1 else j
+            gy = 0.25 * ((a[L, jn] - a[L, js]) + (a[R, jn] - a[R, js])) / dy
+            flux = _vof_face_flux(uf, a[L, j], a[R, j], a[up, j] if has_up else 0.0, has_up, gx, gy, c_alpha)
+            out[L, j] -= dt * flux / dx
+            out[R, j] += dt * flux / dx
+    for i in range(1, nx + 1):
+        for j in range(0, ny + 1):
+            vf = v[i, j]
+            if j == 0 or j == ny:
+                P = 1 if j == 0 else ny
+                if fluid[i, P]:
+                    into = vf if j == 0 else -vf
+                    ab = a_in if into > 0 else a[i, P]
+                    out[i, P] += dt * into * ab / dy
+                continue
+            B, T = j, j + 1
+            if not (fluid[i, B] and fluid[i, T]):
+                continue
+            up = B - 1 if vf >= 0.0 else T + 1
+            has_up = 1 <= up <= ny and bool(fluid[i, up])
+            gy = (a[i, T] - a[i, B]) / dy
+            ie = i + 1 if (i < nx or periodic) else i
+            iw = i - 1 if (i > 1 or periodic) else i
+            ie = 1 if ie > nx else ie
+            iw = nx if iw < 1 else iw
+            gx = 0.25 * ((a[ie, B] - a[iw, B]) + (a[ie, T] - a[iw, T])) / dx
+            flux = _vof_face_flux(vf, a[i, B], a[i, T], a[i, up] if has_up else 0.0, has_up, gy, gx, c_alpha)
+            out[i, B] -= dt * flux / dy
+            out[i, T] += dt * flux / dy
+    inner = out[1:-1, 1:-1]
+    f = fluid[1:-1, 1:-1]
+    inner[f] = np.minimum(np.maximum(inner[f], 0.0), 1.0)
+
+
+class OVOF(OModel):
+    """Two-phase VOF, interFoam-like (cfd2d/vof.py:140-306)."""
+    kind = "multiphase"
+
+    def __init__(self, alpha0, rho1=1000.0, rho2=1.0, nu1=1e-6, nu2=1.48e-5, sigma=0.07,
+                 gravity=(0.0, -9.81), c_alpha=1.0, cfl_alpha=0.25, alpha_inflow=0.0):
+        self.alpha0 = np.asarray(alpha0, dtype=float)
+        self.rho1, self.rho2 = float(rho1), float(rho2)
+        self.mu1, self.mu2 = float(nu1 * rho1), float(nu2 * rho2)
+        self.sigma = float(sigma)
+        self.gravity = (float(gravity[0]), float(gravity[1]))
+        self.c_alpha, self.cfl, self.alpha_inflow = float(c_alpha), float(cfl_alpha), float(alpha_inflow)
+
+    def attach(self, sim):
+        # cfd2d/vof.py:184-197
+        super().attach(sim)
+        g = sim.grid
+        self.alpha = np.zeros((g.nx + 2, g.ny + 2))
+        self.alpha[1:-1, 1:-1] = np.where(g.fluid[1:-1, 1:-1], np.clip(self.alpha0, 0, 1), 0.0)
+        self._tmp = np.zeros_like(self.alpha)
+        sim.variable_density = True
+        sim.variable_viscosity = True
+        sim.body_force = (sim.body_force[0] + self.gravity[0], sim.body_force[1] + self.gravity[1])
+        self.update_properties()
+        self.volume0 = self.volume()
+
+    def fill_ghosts(self):
+        # cfd2d/vof.py:200-220: copies at the sides, solids the mean of their fluid neighbours
+        a, g = self.alpha, self.sim.grid
+        nx = g.nx
+        if self.sim.periodic:
+            a[0, :] = a[nx, :]
+            a[nx + 1, :] = a[1, :]
+        else:
+            a[0, :] = a[1, :]
+            a[-1, :] = a[-2, :]
+        a[:, 0] = a[:, 1]
+        a[:, -1] = a[:, -2]
+        solid = ~g.fluid
+        solid[0, :] = solid[-1, :] = solid[:, 0] = solid[:, -1] = False
+        if solid.any():
+            fl = g.fluid.astype(float)
+            af = np.where(g.fluid, a, 0.0)
+            s = np.zeros_like(a)
+            c = np.zeros_like(a)
+            s[1:-1, 1:-1] = af[2:, 1:-1] + af[:-2, 1:-1] + af[1:-1, 2:] + af[1:-1, :-2]
+            c[1:-1, 1:-1] = fl[2:, 1:-1] + fl[:-2, 1:-1] + fl[1:-1, 2:] + fl[1:-1, :-2]
+            a[solid] = np.where(c[solid] > 0, s[solid] / np.maximum(c[solid], 1), 0.0)
+
+    def update_properties(self):
+        # cfd2d/vof.py:222-227: mixture density and dynamic viscosity (held in nu_eff)
+        self.fill_ghosts()
+        a = self.alpha
+        self.sim.rho[:] = a * self.rho1 + (1 - a) * self.rho2
+        self.sim.nu_eff[:] = a * self.mu1 + (1 - a) * self.mu2
+
+    def volume(self):
+        g = self.sim.grid
+        return float(self.alpha[1:-1, 1:-1][g.fluid[1:-1, 1:-1]].sum() * g.dx * g.dy)
+
+    def momentum_source(self, sim, hu, hv):
+        # cfd2d/vof.py:234-258: CSF surface tension sigma kappa grad(alpha) / rho
+        if self.sigma <= 0:
+            return
+        g = sim.grid
+        a = self.alpha
+        As = a.copy()
+        As[1:-1, 1:-1] = (4 * a[1:-1, 1:-1] + a[2:, 1:-1] + a[:-2, 1:-1] + a[1:-1, 2:] + a[1:-1, :-2]) / 8.0
+        gx = 0.5 * ((As[1:, 1:] - As[:-1, 1:]) + (As[1:, :-1] - As[:-1, :-1])) / g.dx
+        gy = 0.5 * ((As[1:, 1:] - As[1:, :-1]) + (As[:-1, 1:] - As[:-1, :-1])) / g.dy
+        gm = np.sqrt(gx ** 2 + gy ** 2) + 1e-8 / g.dx
+        nxn, nyn = gx / gm, gy / gm
+        kappa = np.zeros_like(a)
+        kappa[1:-1, 1:-1] = -(0.5 * ((nxn[1:, 1:] - nxn[:-1, 1:]) + (nxn[1:, :-1] - nxn[:-1, :-1])) / g.dx
+                              + 0.5 * ((nyn[1:, 1:] - nyn[1:, :-1]) + (nyn[:-1, 1:] - nyn[:-1, :-1])) / g.dy)
+        rho = sim.rho
+        fxs = self.sigma * 0.5 * (kappa[:-1, :] + kappa[1:, :]) * (a[1:, :] - a[:-1, :]) / g.dx
+        fys = self.sigma * 0.5 * (kappa[:, :-1] + kappa[:, 1:]) * (a[:, 1:] - a[:, :-1]) / g.dy
+        rx = 0.5 * (rho[:-1, :] + rho[1:, :])
+        ry = 0.5 * (rho[:, :-1] + rho[:, 1:])
+        hu[sim.u_fluid] += (fxs / rx)[sim.u_fluid]
+        hv[sim.v_fluid] += (fys / ry)[sim.v_fluid]
+
+    def post_step(self, sim, dt):
+        # cfd2d/vof.py:260-271: sub-steps at the alpha Courant number cfl
+        g = sim.grid
+        umax = max(np.abs(sim.u).max() / g.dx, np.abs(sim.v).max() / g.dy, 1e-12)
+        nsub = max(1, int(np.ceil(dt * umax / self.cfl)))
+        h = dt / nsub
+        for _ in range(nsub):
+            vof_advect(self.alpha, sim.u, sim.v, g.fluid, g.nx, g.ny, g.dx, g.dy, h, self.c_alpha,
+                       sim.periodic, self.alpha_inflow, self._tmp)
+            self.alpha[:] = self._tmp
+            self.fill_ghosts()
+        self.update_properties()
+
+    def dt_limit(self, sim):
+        # cfd2d/vof.py:273-284
+        g = sim.grid
+        lim = None
+        if self.sigma > 0:
+            h = min(g.dx, g.dy)
+            lim = np.sqrt(0.5 * (self.rho1 + self.rho2) * h ** 3 / (2 * np.pi * self.sigma))
+        gmag = np.hypot(*self.gravity)
+        if gmag > 0:
+            lg = np.sqrt(min(g.dx, g.dy) / gmag)
+            lim = lg if lim is None else min(lim, lg)
+        return lim
+
+
+def dam_break(n=96, size=0.584, column_width=0.1461, column_height=0.292, obstacle=True, sigma=0.07,
+              open_top=True, gamma=0.5, tau=0.5):
+    # cfd2d/cases.py:294-320
+    g = OGrid(n, n, size, size)
+    if obstacle:
+        x0 = 0.5 * size - 0.012
+        g.add_obstacle(rectangle_mask(g, x0, 0.0, x0 + 0.024, 0.048))
+    X, Y = g.centres()
+    alpha0 = ((X <= column_width) & (Y <= column_height)).astype(float)
+    bcs = {"left": OBC("noslip"), "right": OBC("noslip"), "bottom": OBC("noslip"),
+           "top": OBC("outflow") if open_top else OBC("noslip")}
+    return OSimulation(g, bcs, nu=1e-6, models=[OVOF(alpha0, sigma=sigma)], gamma=gamma, tau=tau)

@@ -70,3 +70,36 @@ def scalar_cases():
                     yield dict(nx=nx, ny=ny, dx=1.3 / nx, dy=0.9 / ny, limiter=limiter,
                                periodic=periodic, obs_t=obs_t, obs_v=float(rng.standard_normal()),
                                fluid=fl, u=u, v=v, phi=phi, diff=diff, bt=bt, bv=bv)
+
+
+def vof_cases():
+    """Yield dicts of inputs for vof_advect (cfd2d/vof.py:36-137): a column of
+    phase 1 with a smeared interface, random velocities, random solids."""
+    rng = np.random.default_rng(4321)
+    for nx, ny in SIZES:
+        for periodic in (False, True):
+            for c_alpha in (0.0, 1.0):
+                fluid = rand_fluid(rng, nx, ny, periodic, n_blobs=2)
+                dx, dy = 1.0 / nx, 0.7 / ny
+                a = np.zeros((nx + 2, ny + 2))
+                xs = (np.arange(nx) + 0.5) / nx
+                ys = (np.arange(ny) + 0.5) / ny
+                X, Y = np.meshgrid(xs, ys, indexing="ij")
+                a[1:-1, 1:-1] = np.clip(0.5 - 4.0 * (X - 0.4 - 0.1 * np.sin(6 * Y)), 0.0, 1.0)
+                a[1:-1, 1:-1] += 0.05 * rng.uniform(-1, 1, (nx, ny))
+                a[1:-1, 1:-1] = np.clip(a[1:-1, 1:-1], 0.0, 1.0)
+                a[~fluid] = rng.uniform(0, 1, (~fluid).sum())
+                u = rng.uniform(-1, 1, (nx + 1, ny + 2))
+                v = rng.uniform(-1, 1, (nx + 2, ny + 1))
+                yield dict(a=a, u=u, v=v, fluid=fluid, nx=nx, ny=ny, dx=dx, dy=dy,
+                           dt=0.2 * min(dx, dy), c_alpha=c_alpha, periodic=periodic,
+                           a_in=float(rng.integers(0, 2)))
+
+
+def rho_field(rng, nx, ny, fluid):
+    """Two-phase density (1000 / 1) with a smeared, wavy interface, padded."""
+    xs = (np.arange(nx + 2) - 0.5) / nx
+    ys = (np.arange(ny + 2) - 0.5) / ny
+    X, Y = np.meshgrid(xs, ys, indexing="ij")
+    a = np.clip(0.5 - 5.0 * (Y - 0.45 - 0.1 * np.sin(5 * X + rng.uniform(0, 3))), 0.0, 1.0)
+    return a * 1000.0 + (1 - a) * 1.0

@@ -6,7 +6,7 @@ Run in a container that holds the reference checkout (default
     python tests/golden/make_golden.py [group ...]
 
 Groups: kernels geometry pressure cavity cylinder sst misc checkpoint smagorinsky
-functions (default: all).
+functions vof (default: all).
 The reference imports matplotlib at module load; ``mplstub/`` stands in for it
 (no fixture case needs plotting or polygon masks). Every pressure solve uses the
 reference's own ``PressureSolver`` (scipy CG or SuperLU) with
@@ -358,6 +358,64 @@ def gen_functions():
     _save("golden_functions", out)
 
 
+def _face_coefficients(rho, nx, periodic):
+    # cfd2d/solver.py:267-271
+    bx = 2.0 / (rho[:-1, :] + rho[1:, :])
+    by = 2.0 / (rho[:, :-1] + rho[:, 1:])
+    if periodic:
+        bx[nx, :] = 2.0 / (rho[nx, :] + rho[1, :])
+    return bx, by
+
+
+def gen_vof():
+    """The VOF path of the reference (cfd2d/vof.py, PressureSolver.solve_variable):
+    vof_advect on seeded inputs, solve_variable (sparse direct) on three geometries
+    with a 1000:1 density interface, and a 32 x 32 dam break over 20 steps."""
+    from inputs import rho_field, vof_cases
+
+    from cfd2d.vof import vof_advect
+
+    out = {}
+    k = 0
+    for c in vof_cases():
+        o = np.full_like(c["a"], 5.0)
+        vof_advect(c["a"], c["u"], c["v"], c["fluid"], c["nx"], c["ny"], c["dx"], c["dy"], c["dt"],
+                   c["c_alpha"], c["periodic"], c["a_in"], o)
+        out[f"adv{k}_out"] = o
+        k += 1
+    out["n_adv"] = np.array(k)
+    rng = np.random.default_rng(77)
+    sims = {}
+    g = Grid(30, 20, 1.5, 1.0)
+    g.add_obstacle(geometry.rectangle(g, 0.7, -1.0, 0.8, 2.0))
+    sims["two"] = Simulation(g, {s: BC("noslip") for s in ("left", "right", "bottom", "top")}, nu=0.02)
+    g = Grid(32, 32, 0.584, 0.584)
+    g.add_obstacle(geometry.rectangle(g, 0.28, 0.0, 0.304, 0.048))
+    sims["open"] = Simulation(g, {"left": BC("noslip"), "right": BC("noslip"), "bottom": BC("noslip"),
+                                  "top": BC("outflow")}, nu=1e-6)
+    g = Grid(32, 24, 1.0, 0.75)
+    g.add_obstacle(geometry.circle(g, 0.5, 0.4, 0.12))
+    sims["per"] = Simulation(g, {"left": BC("periodic"), "right": BC("periodic"), "bottom": BC("noslip"),
+                                 "top": BC("slip")}, nu=0.01)
+    for name, sim in sims.items():
+        nx, ny = sim.grid.nx, sim.grid.ny
+        rho = rho_field(rng, nx, ny, sim.grid.fluid)
+        bx, by = _face_coefficients(rho, nx, sim.periodic)
+        rhs = rng.standard_normal((nx, ny))
+        rhs[~sim.pressure.fluid] = 0.0
+        p = sim.pressure.solve_variable(rhs, bx[:, 1:-1], by[1:-1, :])
+        out[f"sv_{name}_rho"] = rho
+        out[f"sv_{name}_rhs"] = rhs
+        out[f"sv_{name}_p"] = p
+    case = cases.dam_break(n=32)
+    f = dict(UVP)
+    vof = case.sim.model("multiphase")
+    f["alpha"] = lambda s: vof.alpha
+    _run(case.sim, 20, {1, 20}, f, out, "dam")
+    out["dam_volume"] = np.array(vof.volume())
+    _save("golden_vof", out)
+
+
 def gen_checkpoint():
     """A checkpoint written by the reference itself (cfd2d/functions.py:326) after 40
     steps of the 88 x 17 cylinder with a passive scalar, and the reference's state
@@ -393,7 +451,8 @@ def gen_checkpoint():
 
 GROUPS = {"kernels": gen_kernels, "geometry": gen_geometry, "pressure": gen_pressure,
           "cavity": gen_cavity, "cylinder": gen_cylinder, "sst": gen_sst, "misc": gen_misc,
-          "checkpoint": gen_checkpoint, "smagorinsky": gen_smagorinsky, "functions": gen_functions}
+          "checkpoint": gen_checkpoint, "smagorinsky": gen_smagorinsky, "functions": gen_functions,
+          "vof": gen_vof}
 
 if __name__ == "__main__":
     import warnings

@@ -295,3 +295,71 @@ def test_probe_series_and_field_average_runs():
             ref = g[f"fo_avg_{name}_{k}"]
             assert np.array_equal(np.isnan(mine), np.isnan(ref))
             assert rel(np.nan_to_num(mine), np.nan_to_num(ref)) < 1e-11, (name, k)
+
+
+# ---------------------------------------------------------------- VOF
+def test_vof_advect_bitwise():
+    """cfd2d/vof.py:36-137 on seeded inputs (periodic or not, with and without
+    compression, random solids): bit for bit."""
+    from inputs import vof_cases
+
+    g = golden("golden_vof")
+    k = 0
+    for c in vof_cases():
+        out = np.full_like(c["a"], 5.0)
+        O.vof_advect(c["a"], c["u"], c["v"], c["fluid"], c["nx"], c["ny"], c["dx"], c["dy"], c["dt"],
+                     c["c_alpha"], c["periodic"], c["a_in"], out)
+        assert np.array_equal(out, g[f"adv{k}_out"]), k
+        k += 1
+    assert k == int(g["n_adv"])
+
+
+def _vof_pressure_sims():
+    sims = {}
+    grid = O.OGrid(30, 20, 1.5, 1.0)
+    grid.add_obstacle(O.rectangle_mask(grid, 0.7, -1.0, 0.8, 2.0))
+    sims["two"] = O.OSimulation(grid, {s: O.OBC("noslip") for s in O.SIDES}, nu=0.02)
+    grid = O.OGrid(32, 32, 0.584, 0.584)
+    grid.add_obstacle(O.rectangle_mask(grid, 0.28, 0.0, 0.304, 0.048))
+    sims["open"] = O.OSimulation(grid, {"left": O.OBC("noslip"), "right": O.OBC("noslip"),
+                                        "bottom": O.OBC("noslip"), "top": O.OBC("outflow")}, nu=1e-6)
+    grid = O.OGrid(32, 24, 1.0, 0.75)
+    grid.add_obstacle(O.circle_mask(grid, 0.5, 0.4, 0.12))
+    sims["per"] = O.OSimulation(grid, {"left": O.OBC("periodic"), "right": O.OBC("periodic"),
+                                       "bottom": O.OBC("noslip"), "top": O.OBC("slip")}, nu=0.01)
+    return sims
+
+
+def face_coefficients(rho, nx, periodic):
+    bx = 2.0 / (rho[:-1, :] + rho[1:, :])
+    by = 2.0 / (rho[:, :-1] + rho[:, 1:])
+    if periodic:
+        bx[nx, :] = 2.0 / (rho[nx, :] + rho[1, :])
+    return bx, by
+
+
+def test_solve_variable():
+    """cfd2d/pressure.py:187-244 (sparse direct) with a 1000:1 density interface:
+    two Neumann components, an open top, periodic x."""
+    g = golden("golden_vof")
+    for name, sim in _vof_pressure_sims().items():
+        rho = g[f"sv_{name}_rho"]
+        bx, by = face_coefficients(rho, sim.grid.nx, sim.periodic)
+        p = sim.pressure.solve_variable(g[f"sv_{name}_rhs"], bx[:, 1:-1], by[1:-1, :])
+        assert rel(p, g[f"sv_{name}_p"]) < 1e-12, name
+
+
+def test_dam_break_20_steps():
+    """The reference's dam break (cfd2d/cases.py:294-320) on 32 x 32: VOF transport,
+    surface tension, variable-density projection."""
+    g = golden("golden_vof")
+    sim = O.dam_break(n=32)
+    vof = sim.model("multiphase")
+    for n in range(1, 21):
+        sim.step()
+        if n in (1, 20):
+            for f in "uvp":
+                assert rel(getattr(sim, f), g[f"dam_{f}_{n}"]) < 1e-10, (f, n)
+            assert rel(vof.alpha, g[f"dam_alpha_{n}"]) < 1e-10, n
+    assert rel(sim.hist["dt"], g["dam_dt"]) < 1e-12
+    assert vof.volume() == pytest.approx(float(g["dam_volume"]), rel=1e-12)
