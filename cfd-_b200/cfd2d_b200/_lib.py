@@ -19,7 +19,7 @@ LIB_PATH = HERE / "lib" / "libcfd2d_b200.so"
 
 OK = 0
 E_ARG, E_CUDA, E_CAPACITY, E_UNSUPPORTED = -1, -2, -3, -4
-S_NONFINITE, S_CG_MAXITER, S_BARRIER_TIMEOUT, S_COMPONENTS = 1, 2, 4, 8
+S_NONFINITE, S_CG_MAXITER, S_BARRIER_TIMEOUT, S_COMPONENTS, S_VOF_SUBSTEPS = 1, 2, 4, 8, 16
 MAX_COMPONENTS = 16
 MAX_SCALARS = 4
 HIST_FIELDS = 10
@@ -53,7 +53,7 @@ class Poisson(C.Structure):
         ("diag", _vp), ("dinv", _vp), ("nbr", _vp), ("label", _vp),
         ("ncomp", C.c_int), ("comp_count", _vp), ("x0", _vp), ("work", _vp),
         ("work_bytes", C.c_size_t), ("cluster", C.c_int), ("mixed", C.c_int),
-        ("grid_ctas", C.c_int),
+        ("grid_ctas", C.c_int), ("bx", _vp), ("by", _vp),
     ]
 
 
@@ -95,6 +95,16 @@ class Smagorinsky(C.Structure):
     _fields_ = [("l2", _vp)]
 
 
+class Vof(C.Structure):
+    _fields_ = [
+        ("alpha", _vp), ("alpha_tmp", _vp), ("rho", _vp), ("smooth", _vp), ("nrm", _vp), ("kappa", _vp),
+        ("bx", _vp), ("by", _vp), ("vdiag", _vp), ("vdinv", _vp), ("scal", _vp), ("vflags", _vp),
+        ("rho1", C.c_double), ("rho2", C.c_double), ("mu1", C.c_double), ("mu2", C.c_double),
+        ("sigma", C.c_double), ("c_alpha", C.c_double), ("cfl", C.c_double), ("alpha_in", C.c_double),
+        ("dt_limit", C.c_double), ("rtol", C.c_double), ("maxiter", C.c_int), ("nsub_max", C.c_int),
+    ]
+
+
 class Sim(C.Structure):
     _fields_ = [
         ("nx", C.c_int), ("ny", C.c_int), ("dx", C.c_double), ("dy", C.c_double),
@@ -111,7 +121,8 @@ class Sim(C.Structure):
         ("nscalars", C.c_int), ("scalars", Scalar * MAX_SCALARS),
         ("scalar_dtlim_const", C.c_double * MAX_SCALARS), ("thermal_index", C.c_int),
         ("gx", C.c_double), ("gy", C.c_double), ("T_ref", C.c_double), ("sst_on", C.c_int),
-        ("sst", SST), ("smag_on", C.c_int), ("smag", Smagorinsky), ("state", _vp), ("red", _vp), ("hist", _vp), ("hist_cap", C.c_int),
+        ("sst", SST), ("smag_on", C.c_int), ("smag", Smagorinsky),
+        ("vof_on", C.c_int), ("vof", Vof), ("state", _vp), ("red", _vp), ("hist", _vp), ("hist_cap", C.c_int),
         ("p_tmp", _vp),
     ]
 
@@ -171,6 +182,8 @@ def lib():
         "cfd2d_wall_distance_workspace_bytes": ([i, i], sz),
         "cfd2d_sim_wall_distance": ([vp, vp, vp, sz, vp], i),
         "cfd2d_sample": ([vp, vp, i, vp, vp, i, vp, vp], i),
+        "cfd2d_vof_advect": ([vp, vp, vp, vp, i, i, d, d, d, d, i, d, vp, vp], i),
+        "cfd2d_sim_vof_properties": ([vp, vp], i),
         "cfd2d_cell_values": ([vp, vp, vp, vp], i),
         "cfd2d_probe_record": ([vp, vp, i, vp, vp, i, vp, vp], i),
         "cfd2d_field_average_accumulate": ([vp, vp, vp], i),
@@ -234,7 +247,7 @@ def exported_symbols():
         "cfd2d_sim_scratch_doubles", "cfd2d_sim_apply_bc", "cfd2d_sim_project_initial",
         "cfd2d_sim_step", "cfd2d_sim_scalar_fill_ghosts", "cfd2d_sim_sst_pre_momentum",
         "cfd2d_sim_smagorinsky_pre_momentum", "cfd2d_wall_distance_workspace_bytes",
-        "cfd2d_sim_wall_distance", "cfd2d_sample", "cfd2d_cell_values", "cfd2d_probe_record", "cfd2d_field_average_accumulate",
+        "cfd2d_sim_wall_distance", "cfd2d_sample", "cfd2d_cell_values", "cfd2d_vof_advect", "cfd2d_sim_vof_properties", "cfd2d_probe_record", "cfd2d_field_average_accumulate",
         "cfd2d_streamfunction", "cfd2d_vtk_pack", "cfd2d_graph_capture_steps", "cfd2d_graph_launch", "cfd2d_graph_destroy",
         "cfd2d_graph_capture_steps_ex", "cfd2d_events_create", "cfd2d_events_destroy",
         "cfd2d_event_elapsed_ms", "cfd2d_sim_step_begin", "cfd2d_sim_step_finish", "cfd2d_poisson_matvec",

@@ -205,8 +205,29 @@ def turbulent_channel(re_tau: float = 180.0, ny: int | None = None, y_plus_1: fl
                 1.0, 2.0, re_b, info)
 
 
-def dam_break(*args, **kwargs) -> Case:
-    raise NotImplementedError("Dammbruch (VOF, variable Dichte) ist nicht Teil des B200-Pfads")
+def dam_break(n: int = 96, size: float = 0.584, column_width: float = 0.1461,
+              column_height: float = 0.292, obstacle: bool = True, sigma: float = 0.07,
+              t_end: float = 1.0, open_top: bool = True, **num) -> Case:
+    """Dam break in a square tank, water and air in SI units (cfd2d/cases.py:294-320):
+    a 0.1461 m x 0.292 m water column at the left wall (Martin & Moyce 1952), an
+    optional 0.024 m x 0.048 m obstacle on the floor, the top open (p = 0) or closed."""
+    from .vof import VOF
+
+    grid = Grid(n, n, size, size)
+    if obstacle:
+        x0 = 0.5 * size - 0.012
+        grid.add_obstacle(geometry.rectangle(grid, x0, 0.0, x0 + 0.024, 0.048))
+    X, Y = grid.cell_centers()
+    alpha0 = ((X <= column_width) & (Y <= column_height)).astype(float)
+    bcs = {"left": BC("noslip"), "right": BC("noslip"), "bottom": BC("noslip"),
+           "top": BC("outflow") if open_top else BC("noslip")}
+    vof = VOF(alpha0, sigma=sigma)
+    num.setdefault("gamma", 0.5)
+    sim = Simulation(grid, bcs, nu=1e-6, models=[vof], **_numerics(num))
+    info = {"a": column_width, "h0": column_height, "g": 9.81}
+    U = np.sqrt(2 * 9.81 * column_height)
+    return Case("dam_break", "Dammbruch (VOF, Wasser/Luft)", sim, t_end, None, U, column_width,
+                float(U * column_width / 1e-6), info)
 
 
 def add_turbulence(case: Case, model: str = "kOmegaSST", **kw) -> Case:

@@ -158,6 +158,18 @@ class PressureSolver:
         P.grid_ctas = 16 if (self.cluster == 0 and os.environ.get("CFD2D_PCG_VARIANT") == "cluster-l2") else 0
         self.op = P
 
+    def ensure_workspace(self) -> None:
+        """Allocate the workspace of the grid-persistent solver (the variable-density
+        solve of the VOF model always runs there)."""
+        if self._work is not None:
+            return
+        t = _lib.torch()
+        nbytes = int(_lib.lib().cfd2d_pcg_workspace_bytes(self.grid.nx, self.grid.ny))
+        self._work = t.zeros(nbytes // 8, dtype=t.float64, device=_lib.device())
+        self.op.work, self.op.work_bytes = self._work.data_ptr(), self._work.numel() * 8
+        if self.on_change is not None:
+            self.on_change()
+
     @property
     def grid_ctas(self) -> int:
         """For grids beyond one on-chip cluster: 0 = the solver spreads over every SM
@@ -258,3 +270,66 @@ class PressureSolver:
         if info[0] & _lib.S_CG_MAXITER:
             warnings.warn(f"CG-Drucklöser nicht konvergiert ({self.maxiter} Iterationen)")
         return p.cpu().numpy() if host else p
+
+    def solve_variable(self, rhs, bx, by):
+        """Solve div(b grad p) = rhs with face coefficients b = 1/rho (cfd2d/pressure.py:187-244):
+        bx (nx+1, ny) on the x faces (face nx couples columns nx-1 and 0 when periodic),
+        by (nx, ny+1). The reference rebuilds the matrix and solves it directly on every
+        call; here the diagonal is assembled in its order on the host and the system is
+        solved by the variable-coefficient PCG on the device to a relative residual of
+        1e-13. The time step itself builds the operator on the device."""
+        t = _lib.torch()
+        g = self.grid
+        nx, ny = g.nx, g.ny
+        bx = np.asarray(bx, dtype=np.float64)
+        by = np.asarray(by, dtype=np.float64)
+        dx2, dy2 = self.dx2, self.dy2
+        f = self.fluid
+        both_x = f[:-1, :] & f[1:, :]
+        both_y = f[:, :-1] & f[:, 1:]
+        diag = np.zeros((nx, ny))
+        cxi = (bx[1:nx, :] * dx2)[both_x]
+        diag[:-1, :][both_x] += cxi
+        diag[1:, :][both_x] += cxi
+        cyi = (by[:, 1:ny] * dy2)[both_y]
+        diag[:, :-1][both_y] += cyi
+        diag[:, 1:][both_y] += cyi
+        if self.periodic:
+            bp = f[-1, :] & f[0, :]
+            cpi = (bx[nx, :] * dx2)[bp]
+            diag[-1, :][bp] += cpi
+            diag[0, :][bp] += cpi
+        d = self.dirichlet
+        diag[0, :][d["left"]] += 2 * dx2 * bx[0, :][d["left"]]
+        diag[-1, :][d["right"]] += 2 * dx2 * bx[nx, :][d["right"]]
+        diag[:, 0][d["bottom"]] += 2 * dy2 * by[:, 0][d["bottom"]]
+        diag[:, -1][d["top"]] += 2 * dy2 * by[:, ny][d["top"]]
+        for fi, fj in self._pinned:
+            diag[fi, fj] += dx2 * max(float(bx.max()), 1e-30)
+        dinv = np.where(f, 1.0 / np.where(f, diag, 1.0), 0.0)
+        self.ensure_workspace()
+        # the solver reads the coefficients on the padded face grids
+        bxp = np.zeros((nx + 1, ny + 2))
+        bxp[:, 1:-1] = bx
+        byp = np.zeros((nx + 2, ny + 1))
+        byp[1:-1, :] = by
+        dev = [_lib.to_dev(a, t.float64) for a in (bxp, byp, np.where(f, diag, 0.0), dinv)]
+        op = _lib.Poisson.from_buffer_copy(self.op)
+        op.bx, op.by, op.diag, op.dinv = (a.data_ptr() for a in dev)
+        x0 = t.zeros((nx, ny), dtype=t.float64, device=_lib.device())  # no warm start, as a direct solve
+        op.x0 = x0.data_ptr()
+        op.cluster, op.mixed = 0, 0
+        op.grid_ctas = 16 if nx * ny <= 262144 else 0
+        r = _lib.to_dev(np.asarray(rhs, dtype=np.float64), t.float64)
+        p = t.empty_like(r)
+        st = t.zeros(1, dtype=t.int32, device=_lib.device())
+        rc = _lib.lib().cfd2d_pressure_solve(C.byref(op), _lib.ptr(r), _lib.ptr(p), 1e-13, 20000,
+                                             _lib.ptr(self._d_iters), _lib.ptr(st), _lib.stream_ptr())
+        _lib.check(rc, "cfd2d_pressure_solve (variable coefficients)")
+        info = st.cpu().numpy()
+        self.last_iterations = int(self._d_iters[0].item())
+        if info[0] & _lib.S_BARRIER_TIMEOUT:
+            raise RuntimeError("pressure solve abandoned: a bounded inter-block wait timed out")
+        if info[0] & _lib.S_CG_MAXITER:
+            warnings.warn("CG-Drucklöser (variable Dichte) nicht konvergiert")
+        return p.cpu().numpy()

@@ -105,6 +105,7 @@ class Simulation:
         self._thermal = None
         self._sst = None
         self._smag = None
+        self._vof = None
         self._graphs: dict = {}
         self._learned = None
         self._mirrors: dict = {}
@@ -126,7 +127,7 @@ class Simulation:
             self._nu_t = z(nx + 2, ny + 2)
             self._nu_eff = t.full((nx + 2, ny + 2), self.nu, dtype=t.float64, device=dev)
             self._p_tmp = z(nx + 2, ny + 2)
-            self.rho = np.ones((nx + 2, ny + 2))
+            self._rho = t.ones((nx + 2, ny + 2), dtype=t.float64, device=dev)
             self.u_fluid = grid.u_fluid_faces()
             self.v_fluid = grid.v_fluid_faces()
             if self.periodic:
@@ -223,6 +224,9 @@ class Simulation:
             self._sst.fill_struct(S.sst)
         S.smag_on = int(self._smag is not None)
         S.smag.l2 = self._smag.l2_ptr() if self._smag is not None else None
+        S.vof_on = int(self._vof is not None)
+        if self._vof is not None:
+            self._vof.fill_struct(S.vof)
         S.state = self._d_state.data_ptr()
         S.red = self._red.data_ptr()
         S.hist = self._hist.data_ptr()
@@ -252,6 +256,16 @@ class Simulation:
     def _set_smagorinsky(self, model):
         self._smag = model
         self._invalidate()
+
+    def _set_vof(self, model):
+        self._vof = model
+        self._invalidate()
+
+    def _vof_properties(self):
+        with self._on_stream():
+            self._flush_mirrors()
+            self._call("cfd2d_sim_vof_properties")
+            self._device_changed()
 
     def _smagorinsky_pre_momentum(self):
         with self._on_stream():
@@ -325,6 +339,7 @@ class Simulation:
     hv = _field("hv")
     nu_t = _field("nu_t")
     nu_eff = _field("nu_eff")
+    rho = _field("rho")
 
     @property
     def hu_old(self):
@@ -546,6 +561,11 @@ class Simulation:
             self._push()
         if st.status & _lib.S_BARRIER_TIMEOUT:
             raise RuntimeError("a bounded device wait timed out; the step was abandoned")
+        if st.status & _lib.S_VOF_SUBSTEPS:
+            st.status &= ~_lib.S_VOF_SUBSTEPS
+            self._push()
+            raise RuntimeError("der VOF-Transport brauchte mehr Unterschritte als vorgesehen "
+                               "(VOF(nsub_max=...) erhöhen oder tau verkleinern)")
         if st.status & _lib.S_NONFINITE:
             n = st.error_step or st.n
             st.status &= ~_lib.S_NONFINITE
@@ -710,7 +730,10 @@ class Simulation:
         g = self.grid
         umax = max(np.abs(self.u).max(), 1e-12)
         vmax = max(np.abs(self.v).max(), 1e-12)
-        nu_max = float(self.nu_eff.max()) if self.variable_viscosity else self.nu
+        if self.variable_density:
+            nu_max = float((self.nu_eff / self.rho)[g.fluid].max())
+        else:
+            nu_max = float(self.nu_eff.max()) if self.variable_viscosity else self.nu
         dt_visc = 0.5 / (nu_max * (1.0 / g.dx ** 2 + 1.0 / g.dy ** 2))
         dt_conv = min(g.dx / umax, g.dy / vmax)
         if self.scheme == "ab2":

@@ -26,6 +26,18 @@ bool grid_ok(int nx, int ny) { return nx >= 4 && ny >= 4 && (long long)(nx + 2) 
 int project(const cfd2d_sim* sim, double* p_out, bool unit_dt, bool main_solve, cudaStream_t s) {
     PcgLaunch L = {};
     L.op = sim->pcg;
+    if (sim->vof_on) {
+        // variable density: div(b grad p) with b = 1/rho on the faces, solved to the
+        // tolerance of a direct solve (cfd2d/pressure.py:187-244 uses spsolve)
+        const cfd2d_vof& V = sim->vof;
+        L.op.bx = V.bx;
+        L.op.by = V.by;
+        L.op.diag = V.vdiag;
+        L.op.dinv = V.vdinv;
+        L.op.cluster = 0;
+        L.op.mixed = 0;
+        if ((long long)sim->nx * sim->ny <= 262144) L.op.grid_ctas = 16;
+    }
     L.rhs_mode = 1;
     L.F = sim->F;
     L.G = sim->G;
@@ -33,8 +45,8 @@ int project(const cfd2d_sim* sim, double* p_out, bool unit_dt, bool main_solve, 
     L.dy = sim->dy;
     L.dt_ptr = unit_dt ? nullptr : &sim->state->dt;
     L.dt_const = 1.0;
-    L.rtol = sim->cg_rtol;
-    L.maxiter = sim->cg_maxiter;
+    L.rtol = sim->vof_on ? sim->vof.rtol : sim->cg_rtol;
+    L.maxiter = sim->vof_on ? sim->vof.maxiter : sim->cg_maxiter;
     L.p_out = p_out;
     L.p_padded = 1;
     L.iters_out = &sim->state->cg_iters;
@@ -157,6 +169,7 @@ int cfd2d_sim_project_initial(const cfd2d_sim* sim, void* stream) {
     // F = u, G = v, outflow extrapolation; solve with dt = 1; correct; p = 0; BCs
     // (cfd2d/solver.py:195-204)
     CFD_TRY(stage_predictor(*sim, 1, s));
+    if (sim->vof_on) CFD_TRY(stage_vof_operator(*sim, s));
     int rc = project(sim, sim->p, true, false, s);
     if (rc) return rc;
     CFD_TRY(stage_correct(*sim, sim->p, 1, s));
@@ -209,8 +222,11 @@ int step_begin(const cfd2d_sim& S, cudaStream_t s) {
     if (S.smag_on) CFD_TRY(stage_smag_pre(S, s));
     // 3. time step and upwind fraction
     CFD_TRY(stage_dt(S, s));
-    // 4. tendencies, AB2, predictor, outflow extrapolation
+    // 4. tendencies (with the VOF surface tension), AB2, predictor, outflow extrapolation
+    if (S.vof_on) CFD_TRY(stage_vof_curvature(S, s));
     CFD_TRY(stage_predictor(S, 0, s));
+    // variable-density operator of this step's projection
+    if (S.vof_on) CFD_TRY(stage_vof_operator(S, s));
     return CFD2D_OK;
 }
 
@@ -230,8 +246,9 @@ int step_finish(const cfd2d_sim* sim, cudaStream_t s) {
         }
         CFD_TRY(stage_apply_bc(S, 0, s));
     }
-    // 7. model post-step hooks: scalar transport (k then omega for SST)
+    // 7. model post-step hooks: scalar transport (k then omega for SST), VOF transport
     for (int k = 0; k < S.nscalars; ++k) CFD_TRY(stage_scalar(S, k, s));
+    if (S.vof_on) CFD_TRY(stage_vof_transport(S, s));
     // 8. residual, counters, history record
     CFD_TRY(stage_end(S, s));
     return CFD2D_OK;
@@ -294,6 +311,30 @@ int cfd2d_sim_sst_pre_momentum(const cfd2d_sim* sim, void* stream) {
 int cfd2d_sim_smagorinsky_pre_momentum(const cfd2d_sim* sim, void* stream) {
     if (!sim || !sim->smag_on || !sim->smag.l2) return CFD2D_E_ARG;
     return status_of(stage_smag_pre(*sim, as_stream(stream)));
+}
+
+int cfd2d_vof_advect(const double* a, const double* u, const double* v, const uint8_t* fluid, int nx, int ny,
+                     double dx, double dy, double dt, double c_alpha, int periodic, double a_in, double* out,
+                     void* stream) {
+    if (!a || !u || !v || !fluid || !out || !grid_ok(nx, ny) || a == out) return CFD2D_E_ARG;
+    cfd2d_sim S = {};
+    S.nx = nx;
+    S.ny = ny;
+    S.dx = dx;
+    S.dy = dy;
+    S.periodic = periodic ? 1 : 0;
+    S.u = const_cast<double*>(u);
+    S.v = const_cast<double*>(v);
+    S.fluid = fluid;
+    S.vof.alpha = const_cast<double*>(a);
+    S.vof.c_alpha = c_alpha;
+    S.vof.alpha_in = a_in;
+    return status_of(launch_vof_advect(S, dt, out, as_stream(stream)));
+}
+
+int cfd2d_sim_vof_properties(const cfd2d_sim* sim, void* stream) {
+    if (!sim || !sim->vof_on || !sim->vof.alpha || !sim->vof.alpha_tmp || !sim->vof.rho) return CFD2D_E_ARG;
+    return status_of(stage_vof_properties(*sim, as_stream(stream)));
 }
 
 int cfd2d_graph_capture_steps_ex(const cfd2d_sim* sim, int nsteps, void* stream, void* const* events,

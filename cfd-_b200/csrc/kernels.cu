@@ -9,6 +9,7 @@
 
 #include "device.cuh"
 #include "kernels.cuh"
+#include "vof.cuh"
 
 namespace cfd {
 
@@ -416,9 +417,18 @@ __global__ void k_dt(cfd2d_sim S) {
         if (i <= nx) m[0] = npmax(m[0], fabs(S.u[g.u(i, j)]));
         if (j <= ny) m[1] = npmax(m[1], fabs(S.v[g.v(i, j)]));
         if (need_nu) {
-            const double ne = S.nu_eff[c];
-            m[2] = npmax(m[2], ne);
-            if (S.fluid[c]) numin = npmin(numin, ne);
+            if (S.vof_on) {
+                // kinematic mixture viscosity over the fluid cells (cfd2d/solver.py:215-216, 248-249)
+                if (S.fluid[c]) {
+                    const double ne = S.nu_eff[c] / S.vof.rho[c];
+                    m[2] = npmax(m[2], ne);
+                    numin = npmin(numin, ne);
+                }
+            } else {
+                const double ne = S.nu_eff[c];
+                m[2] = npmax(m[2], ne);
+                if (S.fluid[c]) numin = npmin(numin, ne);
+            }
         }
         if (S.fluid[c]) {
             for (int s = 0; s < S.nscalars; ++s)
@@ -472,6 +482,7 @@ __global__ void k_dt(cfd2d_sim S) {
             }
             if (isfinite(lim)) dt = pymin(dt, S.tau * lim);
         }
+        if (S.vof_on && S.vof.dt_limit > 0.0) dt = pymin(dt, S.tau * S.vof.dt_limit);
         // run(): shorten the last step to land on t_end (cfd2d/solver.py:470-480)
         if (st->t + dt > st->t_end) dt = st->t_end - st->t;
     }
@@ -522,6 +533,10 @@ __global__ void k_predictor(cfd2d_sim S, int copy_only, InvSpacing inv) {
     const double fy = S.body_fy;
     const MomCoef m = mom_coef_inv(inv, st->gamma, S.nu_eff[g.c(1, 1)]);
     const bool var = S.variable_viscosity != 0;
+    // two-phase VOF: (1/rho) div(mu grad u) and the CSF surface-tension source
+    const bool vd = S.vof_on != 0;
+    const double* rho = vd ? S.vof.rho : nullptr;
+    const bool csf = vd && S.vof.sigma > 0;
     const double* T = (S.thermal_index >= 0) ? S.scalars[S.thermal_index].phi : nullptr;
     const bool lo = S.bc_kind[0] == CFD2D_BC_OUTFLOW, ro = S.bc_kind[1] == CFD2D_BC_OUTFLOW;
     const bool bo = S.bc_kind[2] == CFD2D_BC_OUTFLOW, to = S.bc_kind[3] == CFD2D_BC_OUTFLOW;
@@ -533,11 +548,12 @@ __global__ void k_predictor(cfd2d_sim S, int copy_only, InvSpacing inv) {
         if (!copy_only) {
             double h = 0.0;
             if (u_fluid(S, g, i, j)) {
-                h = mom_u(S.u, S.v, S.fluid, S.nu_eff, nullptr, g, m, var, false, i, j);
+                h = mom_u(S.u, S.v, S.fluid, S.nu_eff, rho, g, m, var, vd, i, j);
                 if (T && S.gx != 0.0) {
                     const double Tf = 0.5 * (T[g.c(i, j)] + T[g.c(i + 1, j)]) - S.T_ref;
                     h = h + (-S.gx) * Tf;
                 }
+                if (csf) h = h + csf_u(S, i, j);
                 const double H = ab2 ? (a * h + b * S.hu[f]) : h;
                 Fv = uij + dt * H;
                 if (fx != 0.0) Fv = Fv + dt * fx;
@@ -562,11 +578,12 @@ __global__ void k_predictor(cfd2d_sim S, int copy_only, InvSpacing inv) {
         if (!copy_only) {
             double h = 0.0;
             if (v_fluid(S, g, i, j)) {
-                h = mom_v(S.u, S.v, S.fluid, S.nu_eff, nullptr, g, m, var, false, i, j);
+                h = mom_v(S.u, S.v, S.fluid, S.nu_eff, rho, g, m, var, vd, i, j);
                 if (T && S.gy != 0.0) {
                     const double Tf = 0.5 * (T[g.c(i, j)] + T[g.c(i, j + 1)]) - S.T_ref;
                     h = h + (-S.gy) * Tf;
                 }
+                if (csf) h = h + csf_v(S, i, j);
                 const double H = ab2 ? (a * h + b * S.hv[f]) : h;
                 Gv = vij + dt * H;
                 if (fy != 0.0) Gv = Gv + dt * fy;
@@ -598,24 +615,28 @@ __global__ void k_correct(cfd2d_sim S, const double* p, int unit_dt) {
     const double dt = unit_dt ? 1.0 : st->dt;
     const double dx = S.dx, dy = S.dy;
     const int pc = ny + 2;
+    // variable density: dt b (dp/dh) with the face coefficient b (cfd2d/solver.py:284-321);
+    // b = 1 gives the constant-density expressions bit for bit
+    const bool vd = S.vof_on != 0;
     if (i <= nx && j >= 1 && j <= ny) {
         const int f = g.u(i, j);
+        const double bu = vd ? S.vof.bx[f] : 1.0;
         if (i >= 1 && i <= nx - 1) {
             const double Fv = S.F[f];
-            S.u[f] = u_fluid(S, g, i, j) ? Fv - (dt * (p[(i + 1) * pc + j] - p[i * pc + j])) / dx : Fv;
+            S.u[f] = u_fluid(S, g, i, j) ? Fv - ((dt * bu) * (p[(i + 1) * pc + j] - p[i * pc + j])) / dx : Fv;
         } else if (S.periodic) {
             if (i == nx) {
                 const double Fv = S.F[f];
-                S.u[f] = u_fluid(S, g, i, j) ? Fv - (dt * (p[1 * pc + j] - p[nx * pc + j])) / dx : Fv;
+                S.u[f] = u_fluid(S, g, i, j) ? Fv - ((dt * bu) * (p[1 * pc + j] - p[nx * pc + j])) / dx : Fv;
             }
         } else if (i == 0) {
             const double Fv = S.F[f];
             const bool d = S.bc_kind[0] == CFD2D_BC_OUTFLOW && S.open[0][j - 1];
-            S.u[f] = d ? Fv - ((2 * dt) * p[1 * pc + j]) / dx : Fv;
+            S.u[f] = d ? Fv - (((2 * dt) * bu) * p[1 * pc + j]) / dx : Fv;
         } else {  // i == nx
             const double Fv = S.F[f];
             const bool d = S.bc_kind[1] == CFD2D_BC_OUTFLOW && S.open[1][j - 1];
-            S.u[f] = d ? Fv + ((2 * dt) * p[nx * pc + j]) / dx : Fv;
+            S.u[f] = d ? Fv + (((2 * dt) * bu) * p[nx * pc + j]) / dx : Fv;
         }
     }
     if (S.periodic && i == nx) {
@@ -624,17 +645,18 @@ __global__ void k_correct(cfd2d_sim S, const double* p, int unit_dt) {
     }
     if (j <= ny && i >= 1 && i <= nx) {
         const int f = g.v(i, j);
+        const double bv = vd ? S.vof.by[f] : 1.0;
         if (j >= 1 && j <= ny - 1) {
             const double Gv = S.G[f];
-            S.v[f] = v_fluid(S, g, i, j) ? Gv - (dt * (p[i * pc + j + 1] - p[i * pc + j])) / dy : Gv;
+            S.v[f] = v_fluid(S, g, i, j) ? Gv - ((dt * bv) * (p[i * pc + j + 1] - p[i * pc + j])) / dy : Gv;
         } else if (!S.periodic) {
             const double Gv = S.G[f];
             if (j == 0) {
                 const bool d = S.bc_kind[2] == CFD2D_BC_OUTFLOW && S.open[2][i - 1];
-                S.v[f] = d ? Gv - ((2 * dt) * p[i * pc + 1]) / dy : Gv;
+                S.v[f] = d ? Gv - (((2 * dt) * bv) * p[i * pc + 1]) / dy : Gv;
             } else {
                 const bool d = S.bc_kind[3] == CFD2D_BC_OUTFLOW && S.open[3][i - 1];
-                S.v[f] = d ? Gv + ((2 * dt) * p[i * pc + ny]) / dy : Gv;
+                S.v[f] = d ? Gv + (((2 * dt) * bv) * p[i * pc + ny]) / dy : Gv;
             }
         }
     }

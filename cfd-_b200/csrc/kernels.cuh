@@ -28,6 +28,11 @@ cudaError_t stage_domain_bc(const cfd2d_sim& S, double* u, double* v, int begin,
 cudaError_t stage_apply_bc(const cfd2d_sim& S, int begin, cudaStream_t s);
 cudaError_t stage_sst_pre(const cfd2d_sim& S, cudaStream_t s);
 cudaError_t stage_smag_pre(const cfd2d_sim& S, cudaStream_t s);
+cudaError_t stage_vof_curvature(const cfd2d_sim& S, cudaStream_t s);
+cudaError_t stage_vof_operator(const cfd2d_sim& S, cudaStream_t s);
+cudaError_t stage_vof_transport(const cfd2d_sim& S, cudaStream_t s);
+cudaError_t stage_vof_properties(const cfd2d_sim& S, cudaStream_t s);
+cudaError_t launch_vof_advect(const cfd2d_sim& S, double dt, double* out, cudaStream_t s);
 cudaError_t stage_dt(const cfd2d_sim& S, cudaStream_t s);
 cudaError_t stage_predictor(const cfd2d_sim& S, int copy_only, cudaStream_t s);
 cudaError_t stage_correct(const cfd2d_sim& S, const double* p, int unit_dt, cudaStream_t s);

@@ -883,16 +883,38 @@ __device__ __forceinline__ bool grid_sum(double (&v)[K], double* red_smem, doubl
     return true;
 }
 
+// Off-diagonal entries of row (i, j): -dx2 and -dy2, or with variable coefficients
+// -(b dx2) of the face (the matrix values of cfd2d/pressure.py:199-216; the west
+// face of column 0 is the periodic face nx)
+template <bool VAR>
+struct Coef {
+    double w, s, n, e;
+    __device__ __forceinline__ Coef(const cfd2d_poisson& op, int i, int j) {
+        if constexpr (VAR) {
+            const int nx = op.nx, ny = op.ny;
+            w = -(op.bx[(size_t)((i == 0) ? nx : i) * (ny + 2) + j + 1] * op.dx2);
+            e = -(op.bx[(size_t)(i + 1) * (ny + 2) + j + 1] * op.dx2);
+            s = -(op.by[(size_t)(i + 1) * (ny + 1) + j] * op.dy2);
+            n = -(op.by[(size_t)(i + 1) * (ny + 1) + j + 1] * op.dy2);
+        } else {
+            w = e = -op.dx2;
+            s = n = -op.dy2;
+        }
+    }
+};
+
 // A x at cell (i, j) from a global vector (csc_matvec order)
+template <bool VAR = false>
 __device__ __forceinline__ double apply_A(const cfd2d_poisson& op, const double* X, int i, int j,
                                           uint8_t nb, double dg) {
     const int nx = op.nx, ny = op.ny;
     const int c = i * ny + j;
+    const Coef<VAR> k(op, i, j);
     double tW = 0.0, tS = 0.0, tN = 0.0, tE = 0.0;
-    if (nb & 2) tS = -op.dy2 * X[c - 1];
-    if (nb & 4) tN = -op.dy2 * X[c + 1];
-    if (nb & 1) tW = -op.dx2 * X[((i == 0) ? nx - 1 : i - 1) * ny + j];
-    if (nb & 8) tE = -op.dx2 * X[((i == nx - 1) ? 0 : i + 1) * ny + j];
+    if (nb & 2) tS = k.s * X[c - 1];
+    if (nb & 4) tN = k.n * X[c + 1];
+    if (nb & 1) tW = k.w * X[((i == 0) ? nx - 1 : i - 1) * ny + j];
+    if (nb & 8) tE = k.e * X[((i == nx - 1) ? 0 : i + 1) * ny + j];
     return row_sum(op.periodic != 0, i, nx, tW, tS, dg * X[c], tN, tE);
 }
 
@@ -955,7 +977,7 @@ __device__ __forceinline__ bool sync_sum(double (&v)[K], double* red_smem, doubl
     }
 }
 
-template <bool CL>
+template <bool CL, bool VAR>
 __global__ void __launch_bounds__(CL ? kClusterL2Threads : kGridThreads, 1) k_pcg_grid(PcgLaunch L) {
     constexpr int TPB = CL ? kClusterL2Threads : kGridThreads;
     if (L.active && *L.active == 0) return;
@@ -1023,7 +1045,7 @@ __global__ void __launch_bounds__(CL ? kClusterL2Threads : kGridThreads, 1) k_pc
         b = -b;
         W.P1[c] = b;
         double r = b;
-        if (x_any) r = b - apply_A(op, X, i, j, nb, op.diag[c]);
+        if (x_any) r = b - apply_A<VAR>(op, X, i, j, nb, op.diag[c]);
         R[c] = r;
         W.P0[c] = 0.0;
         part[0] += b * b;
@@ -1056,10 +1078,15 @@ __global__ void __launch_bounds__(CL ? kClusterL2Threads : kGridThreads, 1) k_pc
 #define PNEWG(idx) (first ? (op.dinv[idx] * R[idx]) : (Po[idx] * beta + op.dinv[idx] * R[idx]))
                 const double pC = PNEWG(c);
                 double tW = 0.0, tS = 0.0, tN = 0.0, tE = 0.0;
-                if (nb & 2) tS = mdy2 * PNEWG(c - 1);
-                if (nb & 4) tN = mdy2 * PNEWG(c + 1);
-                if (nb & 1) { const int o = ((i == 0) ? nx - 1 : i - 1) * ny + j; tW = mdx2 * PNEWG(o); }
-                if (nb & 8) { const int o = ((i == nx - 1) ? 0 : i + 1) * ny + j; tE = mdx2 * PNEWG(o); }
+                double kS = mdy2, kN = mdy2, kW = mdx2, kE = mdx2;
+                if constexpr (VAR) {
+                    const Coef<true> k(op, i, j);
+                    kS = k.s; kN = k.n; kW = k.w; kE = k.e;
+                }
+                if (nb & 2) tS = kS * PNEWG(c - 1);
+                if (nb & 4) tN = kN * PNEWG(c + 1);
+                if (nb & 1) { const int o = ((i == 0) ? nx - 1 : i - 1) * ny + j; tW = kW * PNEWG(o); }
+                if (nb & 8) { const int o = ((i == nx - 1) ? 0 : i + 1) * ny + j; tE = kE * PNEWG(o); }
 #undef PNEWG
                 const double qq = row_sum(op.periodic != 0, i, nx, tW, tS, op.diag[c] * pC, tN, tE);
                 Pn[c] = pC;
@@ -1076,7 +1103,7 @@ __global__ void __launch_bounds__(CL ? kClusterL2Threads : kGridThreads, 1) k_pc
                 const uint8_t nb = op.nbr[c];
                 if (!(nb & 0x80)) continue;
                 const int i = c / ny, j = c % ny;
-                const double qq = apply_A(op, Pn, i, j, nb, op.diag[c]);
+                const double qq = apply_A<VAR>(op, Pn, i, j, nb, op.diag[c]);
                 X[c] = X[c] + alpha * Pn[c];
                 const double r = R[c] - alpha * qq;
                 R[c] = r;
@@ -1152,13 +1179,15 @@ __global__ void __launch_bounds__(CL ? kClusterL2Threads : kGridThreads, 1) k_pc
 
 namespace {
 
+template <bool VAR>
 int grid_blocks_for(int n) {
     static int per_sm = -1, sms = 0;
     if (per_sm < 0) {
         int dev = 0;
         if (cudaGetDevice(&dev) != cudaSuccess) return 0;
         if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_grid<false>, kGridThreads, 0) != cudaSuccess)
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_grid<false, VAR>, kGridThreads, 0) !=
+            cudaSuccess)
             return 0;
     }
     long long g = (long long)per_sm * sms;
@@ -1174,7 +1203,9 @@ __global__ void k_matvec(cfd2d_poisson op, const double* x, double* y) {
     const int n = op.nx * op.ny;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
         const uint8_t nb = op.nbr[c];
-        y[c] = (nb & 0x80) ? apply_A(op, x, c / op.ny, c % op.ny, nb, op.diag[c]) : 0.0;
+        if (!(nb & 0x80)) { y[c] = 0.0; continue; }
+        y[c] = op.bx ? apply_A<true>(op, x, c / op.ny, c % op.ny, nb, op.diag[c])
+                     : apply_A<false>(op, x, c / op.ny, c % op.ny, nb, op.diag[c]);
     }
 }
 
@@ -1189,10 +1220,11 @@ size_t pcg_grid_workspace_doubles(int nx, int ny) {
     return (size_t)3 * nx * ny + (size_t)3 * 148 * 32 * kSlot + 8;
 }
 
-cudaError_t pcg_grid_launch(const PcgLaunch& L, cudaStream_t s) {
+template <bool VAR>
+cudaError_t pcg_grid_launch_t(const PcgLaunch& L, cudaStream_t s) {
     const int n = L.op.nx * L.op.ny;
     const bool cl = L.op.grid_ctas == 16;
-    const int G = cl ? 16 : grid_blocks_for(n);
+    const int G = cl ? 16 : grid_blocks_for<VAR>(n);
     if (G < 1 || G > 148 * 32) return cudaErrorInvalidConfiguration;
     if (L.op.grid_ctas != 0 && !cl) return cudaErrorInvalidValue;
     if (L.op.work == nullptr || L.op.work_bytes < pcg_grid_workspace_doubles(L.op.nx, L.op.ny) * sizeof(double))
@@ -1208,7 +1240,7 @@ cudaError_t pcg_grid_launch(const PcgLaunch& L, cudaStream_t s) {
         // solves (of different cases) can run side by side on the other SMs
         static bool configured = false;
         if (!configured) {
-            e = cudaFuncSetAttribute(k_pcg_grid<true>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+            e = cudaFuncSetAttribute(k_pcg_grid<true, VAR>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
             if (e != cudaSuccess) return e;
             configured = true;
         }
@@ -1224,10 +1256,19 @@ cudaError_t pcg_grid_launch(const PcgLaunch& L, cudaStream_t s) {
         attr[0].val.clusterDim.z = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        return cudaLaunchKernelEx(&cfg, k_pcg_grid<true>, Lc);
+        return cudaLaunchKernelEx(&cfg, k_pcg_grid<true, VAR>, Lc);
     }
     void* args[] = {&Lc};
-    return cudaLaunchCooperativeKernel((const void*)k_pcg_grid<false>, dim3(G), dim3(kGridThreads), args, 0, s);
+    return cudaLaunchCooperativeKernel((const void*)k_pcg_grid<false, VAR>, dim3(G), dim3(kGridThreads), args, 0,
+                                       s);
+}
+
+cudaError_t pcg_grid_launch(const PcgLaunch& L, cudaStream_t s) {
+    if (L.op.bx) {
+        if (!L.op.by) return cudaErrorInvalidValue;
+        return pcg_grid_launch_t<true>(L, s);
+    }
+    return pcg_grid_launch_t<false>(L, s);
 }
 
 // ---------------------------------------------------------------- launch
@@ -1393,6 +1434,7 @@ cudaError_t pcg_launch(const PcgLaunch& L0, cudaStream_t s) {
     PcgLaunch L = L0;
     const int C = L.op.cluster;
     if (C == 0) return pcg_grid_launch(L, s);
+    if (L.op.bx) return cudaErrorInvalidValue;  // variable coefficients: grid solver only
     if (C < 1 || C > 16) return cudaErrorInvalidValue;
     const int rows = (L.op.nx + C - 1) / C;
     L.cap_cells = rows * L.op.ny;

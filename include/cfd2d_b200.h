@@ -34,6 +34,7 @@ extern "C" {
 #define CFD2D_S_CG_MAXITER 2    /* CG stopped at maxiter (reference: warnings.warn) */
 #define CFD2D_S_BARRIER_TIMEOUT 4 /* a bounded inter-block wait gave up */
 #define CFD2D_S_COMPONENTS 8    /* more Neumann components than the solver tracks */
+#define CFD2D_S_VOF_SUBSTEPS 16 /* the VOF transport needed more sub-steps than queued */
 
 /* side order used by every per-side array: left, right, bottom, top */
 #define CFD2D_LEFT 0
@@ -101,6 +102,12 @@ typedef struct cfd2d_poisson {
     int grid_ctas;            /* cluster == 0 only: 0 = cooperative launch over every SM;
                                  16 = one 16-CTA cluster (vectors in the workspace, cluster
                                  barriers), which leaves the other SMs to other solves */
+    const double* bx;         /* NULL: constant coefficients. Else div(b grad p) with face
+                                 coefficients b = 1/rho (cfd2d/pressure.py:187-244):
+                                 bx (nx+1)(ny+2) on the x faces, periodic face nx coupling
+                                 cells nx-1 and 0; needs cluster == 0 and diag/dinv of the
+                                 variable operator */
+    const double* by;         /* (nx+2)(ny+1) on the y faces */
 } cfd2d_poisson;
 
 /* One scalar transport equation (cfd2d/models.py:73-250). */
@@ -139,6 +146,33 @@ typedef struct cfd2d_smagorinsky {
     const double* l2;         /* nx*ny squared length scale l^2 */
 } cfd2d_smagorinsky;
 
+/* Two-phase VOF model data (cfd2d/vof.py:140-306): volume fraction transport with
+ * interface compression, CSF surface tension, mixture density and viscosity, and
+ * the variable-density projection (cfd2d/solver.py:267-321). */
+typedef struct cfd2d_vof {
+    double* alpha;            /* (nx+2)(ny+2) volume fraction of phase 1 */
+    double* alpha_tmp;        /* (nx+2)(ny+2) */
+    double* rho;              /* (nx+2)(ny+2) mixture density; the mixture dynamic viscosity
+                                 is held in sim->nu_eff (cfd2d/vof.py:222-227) */
+    double* smooth;           /* (nx+2)(ny+2) smoothed alpha of the curvature */
+    double* nrm;              /* 2 (nx+1)(ny+1) interface normals at the nodes (x, then y) */
+    double* kappa;            /* (nx+2)(ny+2) curvature, 0 on the ghost layer */
+    double* bx;               /* (nx+1)(ny+2) face coefficients 2 / (rho_L + rho_R) */
+    double* by;               /* (nx+2)(ny+1) */
+    double* vdiag;            /* nx*ny diagonal of the variable-coefficient operator */
+    double* vdinv;            /* nx*ny */
+    double* scal;             /* 4 doubles: largest face coefficient, sub-steps, sub-step length */
+    const uint8_t* vflags;    /* nx*ny: bit0-3 outflow (Dirichlet) at the left/right/bottom/top
+                                 side, bit4 pinned cell of a Neumann component */
+    double rho1, rho2, mu1, mu2;
+    double sigma, c_alpha, cfl, alpha_in;
+    double dt_limit;          /* capillary and gravity-wave limit (cfd2d/vof.py:273-284), 0: none */
+    double rtol;              /* relative residual of the variable-coefficient solve */
+    int maxiter;
+    int nsub_max;             /* transport sub-steps queued per step; more needed sets
+                                 CFD2D_S_VOF_SUBSTEPS */
+} cfd2d_vof;
+
 /* A whole simulation: geometry, boundary data, device fields and parameters.
  * Filled by the host once; every pointer is a device pointer. */
 typedef struct cfd2d_sim {
@@ -175,6 +209,8 @@ typedef struct cfd2d_sim {
     cfd2d_sst sst;
     int smag_on;              /* Smagorinsky nu_t before the momentum update */
     cfd2d_smagorinsky smag;
+    int vof_on;               /* two-phase VOF with variable density */
+    cfd2d_vof vof;
     cfd2d_state* state;
     double* red;              /* reduction scratch, cfd2d_sim_scratch_doubles() */
     double* hist;             /* history ring: hist_cap records of CFD2D_HIST_FIELDS doubles:
@@ -291,6 +327,18 @@ size_t cfd2d_wall_distance_workspace_bytes(int nx, int ny);
  * Replaces cfd2d/turbulence.py:43 wall_distance(sim) (scipy.ndimage
  * distance_transform_edt). */
 int cfd2d_sim_wall_distance(const cfd2d_sim* sim, double* dist, void* work, size_t work_bytes, void* stream);
+
+/* One explicit, conservative transport step of the volume fraction with interface
+ * compression: out = alpha after dt (out must not be alpha). Replaces
+ * cfd2d/vof.py:36 vof_advect(a, u, v, fluid, nx, ny, dx, dy, dt, c_alpha, periodic,
+ * a_in, out) with the same arguments (device arrays). */
+int cfd2d_vof_advect(const double* a, const double* u, const double* v, const uint8_t* fluid, int nx, int ny,
+                     double dx, double dy, double dt, double c_alpha, int periodic, double a_in, double* out,
+                     void* stream);
+
+/* Ghost and solid values of sim->vof.alpha, then the mixture density and viscosity.
+ * Replaces cfd2d/vof.py:222 VOF._update_properties(). */
+int cfd2d_sim_vof_properties(const cfd2d_sim* sim, void* stream);
 
 /* Capture nsteps consecutive calls of cfd2d_sim_step on `stream` (a created,
  * non-default stream) into an instantiated CUDA graph returned as an opaque
