@@ -389,6 +389,52 @@ def mixed_section(steps: int = 300) -> dict:
     }
 
 
+def vof_section(steps: int = 50, n: int = 96) -> dict:
+    """The reference's dam break (two-phase VOF, variable-density projection) at its
+    default 96 x 96 from rest: ms per step from events over `steps` steps after 5,
+    iterations of the variable-coefficient solve, and the reference's own direct
+    solve of the same system (scipy spsolve, as cfd2d/pressure.py:236) timed on the
+    host on the final state for comparison with the device solve."""
+    import numpy as np
+    import torch
+
+    import oracle as O
+    from cfd2d_b200 import cases
+
+    case = cases.dam_break(n=n)
+    sim = case.sim
+    sim.advance(5)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    torch.cuda.synchronize()
+    with torch.cuda.stream(sim.stream):
+        ev[0].record()
+        sim.advance(steps)
+        ev[1].record()
+    torch.cuda.synchronize()
+    ms = ev[0].elapsed_time(ev[1]) / steps
+    its = np.array(sim.history.extra["cg_iterationen"][-steps:], dtype=float)
+    # the same variable-coefficient system on the host: rhs = div(F, G) / dt, b = 1/rho
+    osim = O.dam_break(n=n)
+    g = sim.grid
+    F, G, rho, dt = sim.F, sim.G, sim.rho, sim.dt
+    div = (F[1:, 1:-1] - F[:-1, 1:-1]) / g.dx + (G[1:-1, 1:] - G[1:-1, :-1]) / g.dy
+    bx = 2.0 / (rho[:-1, :] + rho[1:, :])
+    by = 2.0 / (rho[:, :-1] + rho[:, 1:])
+    osim.pressure.solve_variable(div / dt, bx[:, 1:-1], by[1:-1, :])
+    t0 = time.perf_counter()
+    reps = 3
+    for _ in range(reps):
+        osim.pressure.solve_variable(div / dt, bx[:, 1:-1], by[1:-1, :])
+    cpu_ms = 1e3 * (time.perf_counter() - t0) / reps
+    return {"workload": f"dam break {n}x{n} (two-phase VOF, CSF, variable density), {steps} steps after 5",
+            "ms_per_step": ms, "cell_updates_per_s": n * n / (ms / 1e3),
+            "poisson_iters_per_step": float(its.mean()),
+            "volume_error_rel": sim.model("multiphase").monitors(sim)["volumenfehler_rel"],
+            "cpu_direct_solve_ms": cpu_ms,
+            "cpu_direct_solve": "scipy spsolve of the same system on the host (the reference's solver, 1 thread "
+                                "per call as scipy runs it), mean of 3 calls"}
+
+
 # ------------------------------------------------------------------ GPU arm
 def run_b200(args, dist, rank, world):
     import numpy as np
@@ -501,6 +547,12 @@ def run_b200(args, dist, rank, world):
             mixed = mixed_section()
         except Exception as exc:  # an optional section never costs the bench line
             mixed = {"error": f"{type(exc).__name__}: {exc}"}
+    vof = None
+    if not args.no_vof:
+        try:
+            vof = vof_section()
+        except Exception as exc:  # an optional section never costs the bench line
+            vof = {"error": f"{type(exc).__name__}: {exc}"}
     learned_pc = None
     if not args.no_learned:
         try:
@@ -535,6 +587,7 @@ def run_b200(args, dist, rank, world):
         "stencils": stencils,
         "learned_pc": learned_pc,
         "mixed_precision": mixed,
+        "vof_dam_break": vof,
     }
     print(json.dumps(line), flush=True)
 
@@ -617,6 +670,7 @@ def main():
     ap.add_argument("--no-stencils", action="store_true", help="skip the stencil-kernel roofline section")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner section")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision section")
+    ap.add_argument("--no-vof", action="store_true", help="skip the two-phase dam-break section")
     ap.add_argument("--workload", choices=["cylinder", "batch"], default="cylinder",
                     help="cylinder: the headline; batch: 256 uneven cavities stepped together")
     ap.add_argument("--batch-cases", type=int, default=256)
