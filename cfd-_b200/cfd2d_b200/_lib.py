@@ -105,6 +105,15 @@ class Vof(C.Structure):
     ]
 
 
+MAX_MONITORS = 12
+MON_SUM_FLUID, MON_MEAN_FLUID, MON_MAX_ALL, MON_NUSSELT, MON_VOLUME_ERROR, MON_FRONT_X, MON_HEIGHT_LEFT = range(7)
+
+
+class Monitor(C.Structure):
+    _fields_ = [("kind", C.c_int), ("slot", C.c_int), ("side", C.c_int), ("pad", C.c_int), ("data", _vp),
+                ("param", C.c_double)]
+
+
 class Sim(C.Structure):
     _fields_ = [
         ("nx", C.c_int), ("ny", C.c_int), ("dx", C.c_double), ("dy", C.c_double),
@@ -122,7 +131,8 @@ class Sim(C.Structure):
         ("scalar_dtlim_const", C.c_double * MAX_SCALARS), ("thermal_index", C.c_int),
         ("gx", C.c_double), ("gy", C.c_double), ("T_ref", C.c_double), ("sst_on", C.c_int),
         ("sst", SST), ("smag_on", C.c_int), ("smag", Smagorinsky),
-        ("vof_on", C.c_int), ("vof", Vof), ("state", _vp), ("red", _vp), ("hist", _vp), ("hist_cap", C.c_int),
+        ("vof_on", C.c_int), ("vof", Vof), ("nmon", C.c_int), ("mon", Monitor * MAX_MONITORS),
+        ("mon_ring", _vp), ("state", _vp), ("red", _vp), ("hist", _vp), ("hist_cap", C.c_int),
         ("p_tmp", _vp),
     ]
 

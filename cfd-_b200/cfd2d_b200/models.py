@@ -219,6 +219,11 @@ class Model:
         only host fields (they are then uploaded when sampled)."""
         return None
 
+    def device_monitors(self, sim):
+        """[(key, cfd2d_monitor)] of the monitors() this model records in the history
+        after every step, evaluated on the device; None: not recorded per step."""
+        return None
+
     def state(self) -> dict:
         return {}
 
@@ -261,6 +266,9 @@ class PassiveScalar(Model):
 
     def device_fields(self, sim):
         return {self.name: (self.field.label, _lib.FIELD_CELL, self.field._phi)}
+
+    def device_monitors(self, sim):
+        return [(f"{self.name}_integral", _lib.Monitor(_lib.MON_SUM_FLUID, 0, 0, 0, self.field._phi.data_ptr(), 0.0))]
 
 
 class BoussinesqTemperature(Model):
@@ -318,3 +326,11 @@ class BoussinesqTemperature(Model):
 
     def device_fields(self, sim):
         return {"T": ("Temperatur T", _lib.FIELD_CELL, self.field._phi)}
+
+    def device_monitors(self, sim):
+        ptr = self.field._phi.data_ptr()
+        out = [("T_mittel", _lib.Monitor(_lib.MON_MEAN_FLUID, 0, 0, 0, ptr, 0.0))]
+        for k, side in enumerate(SIDES):
+            if np.any(self.field.bt[side] == 1):
+                out.append((f"Nu_{side}", _lib.Monitor(_lib.MON_NUSSELT, self.field.slot, k, 0, ptr, self.alpha)))
+        return out

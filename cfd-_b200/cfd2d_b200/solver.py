@@ -137,6 +137,8 @@ class Simulation:
             self._v_fluid_dev = _lib.to_dev(self.v_fluid)
             self._red = z(int(_lib.lib().cfd2d_sim_scratch_doubles(nx, ny)))
             self._hist = z(HIST_CAP * _lib.HIST_FIELDS)
+            self._mon_ring = z(HIST_CAP * _lib.MAX_MONITORS)
+            self._mon_keys: list = []
             st = _lib.State()
             st.t_end = math.inf
             st.max_steps = -1
@@ -227,6 +229,18 @@ class Simulation:
         S.vof_on = int(self._vof is not None)
         if self._vof is not None:
             self._vof.fill_struct(S.vof)
+        # model monitors recorded after every step (cfd2d/solver.py:441-443), in model order
+        mons = []
+        for m in self.models:
+            dm = m.device_monitors(self) if hasattr(m, "device_monitors") else None
+            mons += list(dm or [])
+        if len(mons) > _lib.MAX_MONITORS:
+            raise ValueError(f"höchstens {_lib.MAX_MONITORS} Monitore auf dem Gerät")
+        self._mon_keys = [key for key, _ in mons]
+        S.nmon = len(mons)
+        for k, (_, mon) in enumerate(mons):
+            S.mon[k] = mon
+        S.mon_ring = self._mon_ring.data_ptr()
         S.state = self._d_state.data_ptr()
         S.red = self._red.data_ptr()
         S.hist = self._hist.data_ptr()
@@ -627,8 +641,11 @@ class Simulation:
             return
         idx = np.arange(first, n) % HIST_CAP
         recs = self._hist.view(HIST_CAP, _lib.HIST_FIELDS).cpu().numpy()[idx]
+        nm = len(self._mon_keys)
+        mrecs = self._mon_ring.view(HIST_CAP, _lib.MAX_MONITORS)[:, :nm].cpu().numpy()[idx] if nm else \
+            np.zeros((len(idx), 0))
         h = self.history
-        for k, r in zip(range(first + 1, n + 1), recs):
+        for k, r, rm in zip(range(first + 1, n + 1), recs, mrecs):
             h.step.append(k)
             h.t.append(float(r[0]))
             h.dt.append(float(r[1]))
@@ -640,6 +657,8 @@ class Simulation:
                 h.fy.append(float(r[6]))
             if self.flow_rate is not None:
                 h.extra.setdefault("antriebskraft", []).append(float(r[7]))
+            for key, val in zip(self._mon_keys, rm):
+                h.extra.setdefault(key, []).append(float(val))
             h.extra.setdefault("cg_iterationen", []).append(int(r[8]))
         self._hist_seen = n
 

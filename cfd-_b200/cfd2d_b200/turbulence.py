@@ -157,6 +157,10 @@ class KOmegaSST(Model):
     def monitors(self, sim) -> dict:
         return {"k_mittel": float(np.nanmean(self.k.cell())), "nu_t_max": float(sim.nu_t.max())}
 
+    def device_monitors(self, sim):
+        return [("k_mittel", _lib.Monitor(_lib.MON_MEAN_FLUID, 0, 0, 0, self.k._phi.data_ptr(), 0.0)),
+                ("nu_t_max", _lib.Monitor(_lib.MON_MAX_ALL, 0, 0, 0, sim._nu_t.data_ptr(), 0.0))]
+
     def device_fields(self, sim):
         return {"k": (self.k.label, _lib.FIELD_CELL, self.k._phi),
                 "omega": ("log10 ω (spez. Dissipationsrate)", _lib.FIELD_CELL_LOG10, self.w._phi),
@@ -210,6 +214,9 @@ class Smagorinsky(Model):
 
     def device_fields(self, sim):
         return {"nu_t": ("Turbulente Viskosität ν_t", _lib.FIELD_CELL, sim._nu_t)}
+
+    def device_monitors(self, sim):
+        return [("nu_t_max", _lib.Monitor(_lib.MON_MAX_ALL, 0, 0, 0, sim._nu_t.data_ptr(), 0.0))]
 
 
 TURBULENCE_MODELS = {"laminar": None, "kOmegaSST": KOmegaSST, "Smagorinsky": Smagorinsky}

@@ -95,6 +95,7 @@ class VOF(Model):
         for fi, fj in ps._pinned:
             flags[fi, fj] |= 16
         self._vflags = _lib.to_dev(flags)
+        self.volume0 = 0.0
         ps.ensure_workspace()
         sim.variable_density = True
         sim.variable_viscosity = True
@@ -102,6 +103,7 @@ class VOF(Model):
         sim._set_vof(self)
         sim._vof_properties()
         self.volume0 = self.volume()
+        sim._invalidate()  # the volume error monitor refers to volume0
 
     def fill_struct(self, V) -> None:
         sim = self.sim
@@ -150,6 +152,14 @@ class VOF(Model):
         out["hoehe_links"] = float(g.yc[col.max()] + 0.5 * g.dy) if col.size else 0.0
         return out
 
+    def device_monitors(self, sim):
+        a = self._alpha.data_ptr()
+        M = _lib.Monitor
+        return [("volumen_phase1", M(_lib.MON_SUM_FLUID, 0, 0, 0, a, 0.0)),
+                ("volumenfehler_rel", M(_lib.MON_VOLUME_ERROR, 0, 0, 0, a, float(self.volume0))),
+                ("front_x", M(_lib.MON_FRONT_X, 0, 0, 0, a, 0.0)),
+                ("hoehe_links", M(_lib.MON_HEIGHT_LEFT, 0, 0, 0, a, 0.0))]
+
     def state(self) -> dict:
         return {"alpha": self.alpha, "volume0": np.array(self.volume0)}
 
@@ -162,6 +172,7 @@ class VOF(Model):
             m.snap[...] = state["alpha"]
         if "volume0" in state:
             self.volume0 = float(state["volume0"])
+            sim._invalidate()
         sim._vof_properties()
 
     def fields(self, sim) -> dict:

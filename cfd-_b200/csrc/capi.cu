@@ -249,8 +249,9 @@ int step_finish(const cfd2d_sim* sim, cudaStream_t s) {
     // 7. model post-step hooks: scalar transport (k then omega for SST), VOF transport
     for (int k = 0; k < S.nscalars; ++k) CFD_TRY(stage_scalar(S, k, s));
     if (S.vof_on) CFD_TRY(stage_vof_transport(S, s));
-    // 8. residual, counters, history record
+    // 8. residual, counters, history record, model monitors
     CFD_TRY(stage_end(S, s));
+    CFD_TRY(stage_monitors(S, s));
     return CFD2D_OK;
 }
 

@@ -29,6 +29,7 @@ cudaError_t stage_apply_bc(const cfd2d_sim& S, int begin, cudaStream_t s);
 cudaError_t stage_sst_pre(const cfd2d_sim& S, cudaStream_t s);
 cudaError_t stage_smag_pre(const cfd2d_sim& S, cudaStream_t s);
 cudaError_t stage_vof_curvature(const cfd2d_sim& S, cudaStream_t s);
+cudaError_t stage_monitors(const cfd2d_sim& S, cudaStream_t s);
 cudaError_t stage_vof_operator(const cfd2d_sim& S, cudaStream_t s);
 cudaError_t stage_vof_transport(const cfd2d_sim& S, cudaStream_t s);
 cudaError_t stage_vof_properties(const cfd2d_sim& S, cudaStream_t s);

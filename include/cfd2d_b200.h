@@ -173,6 +173,29 @@ typedef struct cfd2d_vof {
                                  CFD2D_S_VOF_SUBSTEPS */
 } cfd2d_vof;
 
+/* Per-step model monitors (the model part of cfd2d/solver.py:441-443 _record): one
+ * value per monitor and step, written into sim->mon_ring after the step. */
+#define CFD2D_MAX_MONITORS 12
+#define CFD2D_MON_SUM_FLUID 0     /* (sum of data over fluid cells) dx dy: ScalarField.total,
+                                     VOF volume (cfd2d/models.py:221-224, vof.py:229-231) */
+#define CFD2D_MON_MEAN_FLUID 1    /* mean of data over fluid cells (np.nanmean of cell()) */
+#define CFD2D_MON_MAX_ALL 2       /* max of data over all (nx+2)(ny+2) cells (nu_t_max) */
+#define CFD2D_MON_NUSSELT 3       /* |mean wall flux of scalar `slot` at side `side`| / param
+                                     (cfd2d/models.py:226-250, 407-412) */
+#define CFD2D_MON_VOLUME_ERROR 4  /* (sum of data over fluid cells) dx dy / max(param, 1e-300) - 1 */
+#define CFD2D_MON_FRONT_X 5       /* right face of the last cell of the first row with data > 0.5,
+                                     0 if none (cfd2d/vof.py:292-294) */
+#define CFD2D_MON_HEIGHT_LEFT 6   /* top face of the last cell of the first column with data > 0.5 */
+
+typedef struct cfd2d_monitor {
+    int kind;                 /* CFD2D_MON_* */
+    int slot;                 /* NUSSELT: scalar slot */
+    int side;                 /* NUSSELT: CFD2D_LEFT .. CFD2D_TOP */
+    int pad;
+    const double* data;       /* padded (nx+2)(ny+2) cell array */
+    double param;
+} cfd2d_monitor;
+
 /* A whole simulation: geometry, boundary data, device fields and parameters.
  * Filled by the host once; every pointer is a device pointer. */
 typedef struct cfd2d_sim {
@@ -211,6 +234,9 @@ typedef struct cfd2d_sim {
     cfd2d_smagorinsky smag;
     int vof_on;               /* two-phase VOF with variable density */
     cfd2d_vof vof;
+    int nmon;                 /* model monitors recorded after every step */
+    cfd2d_monitor mon[CFD2D_MAX_MONITORS];
+    double* mon_ring;         /* hist_cap records of CFD2D_MAX_MONITORS doubles */
     cfd2d_state* state;
     double* red;              /* reduction scratch, cfd2d_sim_scratch_doubles() */
     double* hist;             /* history ring: hist_cap records of CFD2D_HIST_FIELDS doubles:

@@ -183,6 +183,10 @@ def _run(sim, nsteps, keep_at, fields, out, prefix):
             out[prefix + "_hist_" + k] = np.array(val)
     if sim.flow_rate is not None:
         out[prefix + "_hist_flow_force"] = np.array(sim.history.extra["antriebskraft"])
+    # the models' monitors, recorded after every step (cfd2d/solver.py:441-443)
+    for k, vals in sim.history.extra.items():
+        if k != "antriebskraft":
+            out[prefix + "_extra_" + k] = np.array(vals, dtype=float)
     print(f"{prefix}: {nsteps} steps in {time.time() - t0:.1f}s, mean CG it {np.mean(its):.1f}",
           flush=True)
 
