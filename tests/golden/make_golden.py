@@ -417,6 +417,12 @@ def gen_vof():
     f["alpha"] = lambda s: vof.alpha
     _run(case.sim, 20, {1, 20}, f, out, "dam")
     out["dam_volume"] = np.array(vof.volume())
+    # the reference's default size, 100 steps
+    case = cases.dam_break(n=96)
+    vof = case.sim.model("multiphase")
+    f = dict(UVP)
+    f["alpha"] = lambda s: vof.alpha
+    _run(case.sim, 100, {100}, f, out, "d96")
     _save("golden_vof", out)
 
 

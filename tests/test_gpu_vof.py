@@ -151,3 +151,20 @@ def test_checkpoint_restart_vof(cuda_lib, tmp_path):
     va = b.sim.model("multiphase").alpha
     vr = ref.sim.model("multiphase").alpha
     assert np.allclose(va, vr, atol=1e-10)
+
+
+def test_dam_break_96_100_steps(cuda_lib):
+    """The reference's default dam break (96 x 96), 100 steps: the direct solve of the
+    reference against the device PCG at rtol 1e-13 over a longer trajectory."""
+    from cfd2d_b200 import cases
+
+    g = golden("golden_vof")
+    case = cases.dam_break(n=96)
+    sim = case.sim
+    vof = sim.model("multiphase")
+    sim.advance(100)
+    errs = {f: rel(getattr(sim, f), g[f"d96_{f}_100"]) for f in "uvp"}
+    errs["alpha"] = rel(vof.alpha, g["d96_alpha_100"])
+    errs["dt"] = rel(sim.history.dt, g["d96_dt"])
+    assert max(errs.values()) < 1e-7, errs
+    assert sim.history.extra["front_x"] == list(g["d96_extra_front_x"])
