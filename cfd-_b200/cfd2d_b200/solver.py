@@ -29,6 +29,20 @@ from .grid import Grid
 from .pressure import PressureSolver
 
 HIST_CAP = 4096
+
+
+def _ring_rows(ring, first: int, n: int) -> np.ndarray:
+    """Rows first..n-1 (step numbers, n - first <= capacity) of a device ring buffer,
+    copied to the host as at most two contiguous slices."""
+    cap = ring.shape[0]
+    a, b = first % cap, n % cap
+    if n - first == cap and a == b:
+        parts = [ring[a:], ring[:a]]
+    elif a < b:
+        parts = [ring[a:b]]
+    else:
+        parts = [ring[a:], ring[:b]]
+    return np.concatenate([t.cpu().numpy() for t in parts if t.shape[0] > 0], axis=0)
 GRAPH_SIZES = (64, 8, 1)
 
 
@@ -639,11 +653,10 @@ class Simulation:
         if n <= first:
             self._hist_seen = n
             return
-        idx = np.arange(first, n) % HIST_CAP
-        recs = self._hist.view(HIST_CAP, _lib.HIST_FIELDS).cpu().numpy()[idx]
+        recs = _ring_rows(self._hist.view(HIST_CAP, _lib.HIST_FIELDS), first, n)
         nm = len(self._mon_keys)
-        mrecs = self._mon_ring.view(HIST_CAP, _lib.MAX_MONITORS)[:, :nm].cpu().numpy()[idx] if nm else \
-            np.zeros((len(idx), 0))
+        mrecs = (_ring_rows(self._mon_ring.view(HIST_CAP, _lib.MAX_MONITORS), first, n)[:, :nm] if nm
+                 else np.zeros((n - first, 0)))
         h = self.history
         for k, r, rm in zip(range(first + 1, n + 1), recs, mrecs):
             h.step.append(k)
