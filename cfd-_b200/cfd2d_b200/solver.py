@@ -185,9 +185,11 @@ class Simulation:
     def _push(self):
         buf = bytes(self._st)
         self._d_state.copy_(self._t.frombuffer(bytearray(buf), dtype=self._t.uint8), non_blocking=False)
+        self._st_fresh = True
 
     def _pull(self):
         self._st = _lib.State.from_buffer_copy(bytes(self._d_state.cpu().numpy()))
+        self._st_fresh = True
         return self._st
 
     def _invalidate(self):
@@ -262,6 +264,7 @@ class Simulation:
         S.p_tmp = self._p_tmp.data_ptr()
 
     def _call(self, fn, *args):
+        self._st_fresh = False
         rc = getattr(_lib.lib(), fn)(C.byref(self._S), *args, _lib.stream_ptr(self._stream))
         _lib.check(rc, fn)
 
@@ -494,6 +497,7 @@ class Simulation:
         return g
 
     def _launch_steps(self, nsteps: int) -> None:
+        self._st_fresh = False
         if self.function_objects:
             self._steps_with_functions(int(nsteps))
             return
@@ -569,7 +573,8 @@ class Simulation:
         self._call("cfd2d_sim_step_finish")
 
     def _set_run_limits(self, t_end=math.inf, max_steps=-1, steady_tol=0.0):
-        st = self._pull()
+        # the host copy of the state is current unless device work ran since it was read
+        st = self._st if getattr(self, "_st_fresh", False) else self._pull()
         changed = (st.t_end != t_end or st.max_steps != max_steps or st.steady_tol != steady_tol
                    or st.stop_reason != 0 or (st.status & _lib.S_NONFINITE))
         if changed:
