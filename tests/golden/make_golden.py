@@ -6,7 +6,7 @@ Run in a container that holds the reference checkout (default
     python tests/golden/make_golden.py [group ...]
 
 Groups: kernels geometry pressure cavity cylinder sst misc checkpoint smagorinsky
-functions vof (default: all).
+functions vof validation (default: all).
 The reference imports matplotlib at module load; ``mplstub/`` stands in for it
 (no fixture case needs plotting or polygon masks). Every pressure solve uses the
 reference's own ``PressureSolver`` (scipy CG or SuperLU) with
@@ -426,6 +426,53 @@ def gen_vof():
     _save("golden_vof", out)
 
 
+def gen_validation():
+    """The reference's validation tests (tests/test_cfd2d.py:57-95, tests/test_models.py:
+    69-84, 102-113) run by the reference itself: the physical figures each test checks,
+    so the GPU runs can be compared with the reference's results rather than with the
+    literature tables (which stay in the reference)."""
+    from cfd2d import validation
+
+    out = {}
+    ys = np.linspace(0.0, 1.0, 33)
+    case = cases.lid_driven_cavity(re=100, n=32)
+    case.sim.run(40, steady_tol=1e-5, verbose=False)
+    err = validation.cavity_centerline_errors(case.sim, 100)
+    out["ghia_u_line"] = case.sim.sample_u(np.full_like(ys, 0.5), ys)
+    out["ghia_v_line"] = case.sim.sample_v(ys, np.full_like(ys, 0.5))
+    out["ghia_errors"] = np.array([err["u_max_fehler"], err["v_max_fehler"]])
+    out["ghia_n"] = np.array(case.sim.n)
+    case = cases.cylinder_flow(re=20, nx=220, ny=41, t_end=3.0)
+    case.sim.run(case.t_end, verbose=False)
+    fx, fy = case.sim.obstacle_forces()
+    out["cyl20_cd_cl"] = np.array(validation.force_coefficients(fx, fy, 1.0, 0.1))
+    out["cyl20_n"] = np.array(case.sim.n)
+    case = cases.backward_facing_step(re=200, length=8, ny=16, t_end=30)
+    case.sim.run(case.t_end, steady_tol=1e-4, verbose=False)
+    out["step_xr"] = np.array(validation.reattachment_length(case.sim, case.info["x_stufe"]))
+    out["step_n"] = np.array(case.sim.n)
+    case = cases.heated_cavity(ra=1e4, n=32)
+    case.sim.run(case.t_end, steady_tol=case.steady_tol, verbose=False)
+    th = case.sim.model("thermal")
+    out["dvd_nusselt"] = np.array([th.nusselt("left"), th.nusselt("right")])
+    out["dvd_n"] = np.array(case.sim.n)
+    for ra in (1200.0, 5000.0):
+        case = cases.rayleigh_benard(ra=ra, ny=12, t_end=250)
+        case.sim.run(case.t_end, steady_tol=1e-6, verbose=False)
+        out[f"rb{int(ra)}_nusselt"] = np.array(case.sim.model("thermal").nusselt("bottom"))
+        out[f"rb{int(ra)}_n"] = np.array(case.sim.n)
+    case = cases.turbulent_channel(re_tau=120, y_plus_1=2.0, t_end=250)
+    case.sim.run(case.t_end, steady_tol=1e-5, verbose=False)
+    sim, g = case.sim, case.sim.grid
+    u = sim.u[2, 1:-1]
+    tau_w = sim.nu * 0.5 * (u[0] + u[-1]) / (0.5 * g.dy)  # as cfd2d/report.py:455-461
+    utau = np.sqrt(max(tau_w, 1e-300))
+    out["chan_cf_uplus"] = np.array([2 * tau_w / case.U_ref ** 2, u[g.ny // 2 - 1] / utau])
+    out["chan_u"] = sim.u.copy()
+    out["chan_n"] = np.array(sim.n)
+    _save("golden_validation", out)
+
+
 def gen_checkpoint():
     """A checkpoint written by the reference itself (cfd2d/functions.py:326) after 40
     steps of the 88 x 17 cylinder with a passive scalar, and the reference's state
@@ -462,7 +509,7 @@ def gen_checkpoint():
 GROUPS = {"kernels": gen_kernels, "geometry": gen_geometry, "pressure": gen_pressure,
           "cavity": gen_cavity, "cylinder": gen_cylinder, "sst": gen_sst, "misc": gen_misc,
           "checkpoint": gen_checkpoint, "smagorinsky": gen_smagorinsky, "functions": gen_functions,
-          "vof": gen_vof}
+          "vof": gen_vof, "validation": gen_validation}
 
 if __name__ == "__main__":
     import warnings
