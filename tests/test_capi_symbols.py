@@ -6,6 +6,8 @@ import ctypes
 import re
 from pathlib import Path
 
+import pytest
+
 from conftest import ROOT
 
 HEADER = ROOT / "include" / "cfd2d_b200.h"
@@ -46,3 +48,38 @@ def test_struct_sizes_match_the_header():
 
     assert ctypes.sizeof(_lib.State) % 8 == 0
     assert _lib.Sim.state.offset > _lib.Sim.sst.offset
+
+
+STRUCTS = {"State": "cfd2d_state", "Poisson": "cfd2d_poisson", "Scalar": "cfd2d_scalar", "SST": "cfd2d_sst",
+           "Smagorinsky": "cfd2d_smagorinsky", "Vof": "cfd2d_vof", "Monitor": "cfd2d_monitor", "Sim": "cfd2d_sim",
+           "FcgScalars": "cfd2d_fcg_scalars", "FcgControl": "cfd2d_fcg_control", "Field": "cfd2d_field",
+           "ProbeSeries": "cfd2d_probe_series", "FieldAverage": "cfd2d_field_average"}
+
+
+def test_ctypes_layout_equals_the_c_header(tmp_path):
+    """Every ctypes mirror has the C struct's size and every field its offset: a C
+    program compiled against include/cfd2d_b200.h prints them."""
+    import shutil
+    import subprocess
+
+    from cfd2d_b200 import _lib
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    lines = ["#include <stddef.h>", "#include <stdio.h>", f'#include "{HEADER}"', "int main(void) {"]
+    expect = []
+    for py, cname in STRUCTS.items():
+        cls = getattr(_lib, py)
+        lines.append(f'printf("%zu\\n", sizeof({cname}));')
+        expect.append(ctypes.sizeof(cls))
+        for name, _ in cls._fields_:
+            lines.append(f'printf("%zu\\n", offsetof({cname}, {name}));')
+            expect.append(getattr(cls, name).offset)
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-std=c11", str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    assert got == expect
