@@ -72,6 +72,18 @@ def wall_adjacent_cells(sim):
     return adj, dist
 
 
+def strain_rate_squared(sim) -> np.ndarray:
+    """S^2 = 2 S_ij S_ij at the cell centres, (nx, ny) (cfd2d/turbulence.py:89-100), from
+    the host view of the velocities (the model kernels evaluate it on the device)."""
+    g = sim.grid
+    u, v = sim.u, sim.v
+    dudx = (u[1:, 1:-1] - u[:-1, 1:-1]) / g.dx
+    dvdy = (v[1:-1, 1:] - v[1:-1, :-1]) / g.dy
+    shear = (u[:, 1:] - u[:, :-1]) / g.dy + (v[1:, :] - v[:-1, :]) / g.dx
+    sh2 = 0.25 * (shear[:-1, :-1] ** 2 + shear[1:, :-1] ** 2 + shear[:-1, 1:] ** 2 + shear[1:, 1:] ** 2)
+    return 2.0 * (dudx ** 2 + dvdy ** 2) + sh2
+
+
 class KOmegaSST(Model):
     """Menter SST k-omega, low-Re form (cfd2d/turbulence.py:166-325)."""
 
