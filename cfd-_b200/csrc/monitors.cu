@@ -88,7 +88,7 @@ __device__ double monitor_value(const cfd2d_sim& S, const cfd2d_monitor& M, doub
 
 __global__ void __launch_bounds__(kMonThreads) k_monitors(cfd2d_sim S) {
     const cfd2d_state* st = S.state;
-    if (st && !st->active) return;
+    if (!st || !st->active) return;
     __shared__ double sred[64];
     double* rec = S.mon_ring + (size_t)((st->n - 1) % S.hist_cap) * CFD2D_MAX_MONITORS;
     for (int k = 0; k < S.nmon; ++k) {
@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(kMonThreads) k_monitors(cfd2d_sim S) {
 }  // namespace
 
 cudaError_t stage_monitors(const cfd2d_sim& S, cudaStream_t s) {
-    if (S.nmon <= 0 || !S.mon_ring || S.hist_cap <= 0) return cudaSuccess;
+    if (S.nmon <= 0 || !S.mon_ring || S.hist_cap <= 0 || !S.state) return cudaSuccess;
     k_monitors<<<1, kMonThreads, 0, s>>>(S);
     return cudaGetLastError();
 }
