@@ -34,9 +34,10 @@ int project(const cfd2d_sim* sim, double* p_out, bool unit_dt, bool main_solve, 
         L.op.by = V.by;
         L.op.diag = V.vdiag;
         L.op.dinv = V.vdinv;
-        L.op.cluster = 0;
         L.op.mixed = 0;
-        if ((long long)sim->nx * sim->ny <= 262144) L.op.grid_ctas = 16;
+        // the on-chip solver of the plan when the four coefficient arrays fit beside it
+        if (L.op.cluster > 0 && !pcg_var_cluster_fits(sim->nx, sim->ny, L.op.cluster)) L.op.cluster = 0;
+        if (L.op.cluster == 0 && (long long)sim->nx * sim->ny <= 262144) L.op.grid_ctas = 16;
     }
     L.rhs_mode = 1;
     L.F = sim->F;

@@ -110,7 +110,18 @@ __device__ __forceinline__ void cluster_sum(cg::cluster_group& cluster, double (
 
 }  // namespace
 
-template <int CPT, bool PAIR>
+// Off-diagonal entries -(b dx2), -(b dy2) of row (i, j) of the variable-coefficient
+// operator (cfd2d/pressure.py:199-216); the west face of column 0 is the periodic face nx
+__device__ __forceinline__ void var_coef(const cfd2d_poisson& op, int i, int j, double& w, double& e, double& s,
+                                         double& n) {
+    const int nx = op.nx, ny = op.ny;
+    w = -(op.bx[(size_t)((i == 0) ? nx : i) * (ny + 2) + j + 1] * op.dx2);
+    e = -(op.bx[(size_t)(i + 1) * (ny + 2) + j + 1] * op.dx2);
+    s = -(op.by[(size_t)(i + 1) * (ny + 1) + j] * op.dy2);
+    n = -(op.by[(size_t)(i + 1) * (ny + 1) + j + 1] * op.dy2);
+}
+
+template <int CPT, bool PAIR, bool VAR>
 __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cluster(PcgLaunch L) {
     cg::cluster_group cluster = cg::this_cluster();
     const int C = (int)cluster.num_blocks();
@@ -136,7 +147,12 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cluster(PcgLaunch L) {
     double* DI = P1 + cap;
     double* DG = DI + cap;
     double* Z = DG + cap;
-    uint8_t* NB = reinterpret_cast<uint8_t*>(Z + cap);
+    // variable coefficients (VAR): the four off-diagonal entries of every row
+    double* KW = Z + cap;
+    double* KE = KW + cap;
+    double* KS = KE + cap;
+    double* KN = KS + cap;
+    uint8_t* NB = reinterpret_cast<uint8_t*>(Z + cap + (VAR ? 4 * cap : 0));
     __shared__ double red_smem[32 * kMaxK];
     __shared__ double slotsA[16 * kMaxK];
     __shared__ double slotsB[16 * kMaxK];
@@ -179,6 +195,10 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cluster(PcgLaunch L) {
         X[c] = x0;
         DI[c] = op.dinv[gidx];
         DG[c] = op.diag[gidx];
+        if constexpr (VAR) {
+            const int li = (int)__umulhi((unsigned)c, magic);
+            var_coef(op, r0 + li, c - li * ny, KW[c], KE[c], KS[c], KN[c]);
+        }
         double braw = 0.0;
         if (nb & 0x80) {
             if (L.rhs_mode == 0) {
@@ -232,10 +252,12 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cluster(PcgLaunch L) {
             const int li = (int)__umulhi((unsigned)c, magic);
             const int j = c - li * ny;
             double tW = 0.0, tS = 0.0, tN = 0.0, tE = 0.0;
-            if (nb & 2) tS = mdy2 * X[c - 1];
-            if (nb & 4) tN = mdy2 * X[c + 1];
-            if (nb & 1) tW = mdx2 * ((li > 0) ? X[c - ny] : baseW[j]);
-            if (nb & 8) tE = mdx2 * ((li < rows - 1) ? X[c + ny] : baseE[j]);
+            const double kS = VAR ? KS[c] : mdy2, kN = VAR ? KN[c] : mdy2;
+            const double kW = VAR ? KW[c] : mdx2, kE = VAR ? KE[c] : mdx2;
+            if (nb & 2) tS = kS * X[c - 1];
+            if (nb & 4) tN = kN * X[c + 1];
+            if (nb & 1) tW = kW * ((li > 0) ? X[c - ny] : baseW[j]);
+            if (nb & 8) tE = kE * ((li < rows - 1) ? X[c + ny] : baseE[j]);
             r = b - row_sum(periodic, r0 + li, nx, tW, tS, DG[c] * X[c], tN, tE);
         }
         // R and Z are read by other CTAs only inside the loop, after the barrier of
@@ -292,11 +314,21 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cluster(PcgLaunch L) {
                         pC1 = o2.y * beta + z2.y;
                     }
                     // solid cells carry p = z = 0 and no coupling bits, so their terms vanish
+                    double kS0 = mdy2, kS1 = mdy2, kN0 = mdy2, kN1 = mdy2;
+                    double kW0 = mdx2, kW1 = mdx2, kE0 = mdx2, kE1 = mdx2;
+                    if constexpr (VAR) {
+                        const double2 ks = *reinterpret_cast<const double2*>(KS + c);
+                        const double2 kn = *reinterpret_cast<const double2*>(KN + c);
+                        const double2 kw = *reinterpret_cast<const double2*>(KW + c);
+                        const double2 ke = *reinterpret_cast<const double2*>(KE + c);
+                        kS0 = ks.x; kS1 = ks.y; kN0 = kn.x; kN1 = kn.y;
+                        kW0 = kw.x; kW1 = kw.y; kE0 = ke.x; kE1 = ke.y;
+                    }
                     double tW0 = 0.0, tW1 = 0.0, tE0 = 0.0, tE1 = 0.0;
-                    const double tS0 = (nb0 & 2) ? mdy2 * (first ? Z[c - 1] : Po[c - 1] * beta + Z[c - 1]) : 0.0;
-                    const double tN0 = (nb0 & 4) ? mdy2 * pC1 : 0.0;
-                    const double tS1 = (nb1 & 2) ? mdy2 * pC0 : 0.0;
-                    const double tN1 = (nb1 & 4) ? mdy2 * (first ? Z[c + 2] : Po[c + 2] * beta + Z[c + 2]) : 0.0;
+                    const double tS0 = (nb0 & 2) ? kS0 * (first ? Z[c - 1] : Po[c - 1] * beta + Z[c - 1]) : 0.0;
+                    const double tN0 = (nb0 & 4) ? kN0 * pC1 : 0.0;
+                    const double tS1 = (nb1 & 2) ? kS1 * pC0 : 0.0;
+                    const double tN1 = (nb1 & 4) ? kN1 * (first ? Z[c + 2] : Po[c + 2] * beta + Z[c + 2]) : 0.0;
                     if ((nb0 | nb1) & 1) {
                         const double* g = (li > 0) ? (X + c - ny) : (baseW + j);
                         const double2 gz = *reinterpret_cast<const double2*>(g + 6 * cap);
@@ -306,8 +338,8 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cluster(PcgLaunch L) {
                             w0 = go.x * beta + gz.x;
                             w1 = go.y * beta + gz.y;
                         }
-                        if (nb0 & 1) tW0 = mdx2 * w0;
-                        if (nb1 & 1) tW1 = mdx2 * w1;
+                        if (nb0 & 1) tW0 = kW0 * w0;
+                        if (nb1 & 1) tW1 = kW1 * w1;
                     }
                     if ((nb0 | nb1) & 8) {
                         const double* g = (li < rows - 1) ? (X + c + ny) : (baseE + j);
@@ -318,8 +350,8 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cluster(PcgLaunch L) {
                             e0 = go.x * beta + gz.x;
                             e1 = go.y * beta + gz.y;
                         }
-                        if (nb0 & 8) tE0 = mdx2 * e0;
-                        if (nb1 & 8) tE1 = mdx2 * e1;
+                        if (nb0 & 8) tE0 = kE0 * e0;
+                        if (nb1 & 8) tE1 = kE1 * e1;
                     }
                     const double2 dg = *reinterpret_cast<const double2*>(DG + c);
                     const int i = r0 + li;
@@ -344,16 +376,18 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cluster(PcgLaunch L) {
                 // p_new = beta * p_old + z, recomputed for the neighbours from their
                 // previous p and z instead of waiting for their owners
                 const double pC = first ? Z[c] : Po[c] * beta + Z[c];
+                const double kS = VAR ? KS[c] : mdy2, kN = VAR ? KN[c] : mdy2;
+                const double kW = VAR ? KW[c] : mdx2, kE = VAR ? KE[c] : mdx2;
                 double tW = 0.0, tS = 0.0, tN = 0.0, tE = 0.0;
-                if (nb & 2) tS = mdy2 * (first ? Z[c - 1] : Po[c - 1] * beta + Z[c - 1]);
-                if (nb & 4) tN = mdy2 * (first ? Z[c + 1] : Po[c + 1] * beta + Z[c + 1]);
+                if (nb & 2) tS = kS * (first ? Z[c - 1] : Po[c - 1] * beta + Z[c - 1]);
+                if (nb & 4) tN = kN * (first ? Z[c + 1] : Po[c + 1] * beta + Z[c + 1]);
                 if (nb & 1) {
                     const double* g = (li > 0) ? (X + c - ny) : (baseW + j);
-                    tW = mdx2 * (first ? g[6 * cap] : g[po] * beta + g[6 * cap]);
+                    tW = kW * (first ? g[6 * cap] : g[po] * beta + g[6 * cap]);
                 }
                 if (nb & 8) {
                     const double* g = (li < rows - 1) ? (X + c + ny) : (baseE + j);
-                    tE = mdx2 * (first ? g[6 * cap] : g[po] * beta + g[6 * cap]);
+                    tE = kE * (first ? g[6 * cap] : g[po] * beta + g[6 * cap]);
                 }
                 const double qq = row_sum(periodic, r0 + li, nx, tW, tS, DG[c] * pC, tN, tE);
                 Pn[c] = pC;
@@ -1274,12 +1308,14 @@ cudaError_t pcg_grid_launch(const PcgLaunch& L, cudaStream_t s) {
 // ---------------------------------------------------------------- launch
 namespace {
 
-size_t smem_bytes(int cap) { return (size_t)cap * (kArrays * sizeof(double) + 1) + 16; }
+size_t smem_bytes(int cap, bool var = false) {
+    return (size_t)cap * ((kArrays + (var ? 4 : 0)) * sizeof(double) + 1) + 16;
+}
 
 // Kernel attributes are set once per instantiation, outside any stream capture
 // (cfd2d_pcg_plan runs before the first launch): the maximum dynamic shared
 // memory the hardware allows and permission for 16-CTA clusters.
-template <int CPT, bool PAIR>
+template <int CPT, bool PAIR, bool VAR = false>
 cudaError_t configure_cpt() {
     static bool done = false;
     if (done) return cudaSuccess;
@@ -1289,19 +1325,19 @@ cudaError_t configure_cpt() {
     e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     if (e != cudaSuccess) return e;
     const int dyn = optin - (int)((32 * kMaxK + 2 * 16 * kMaxK + CFD2D_MAX_COMPONENTS) * sizeof(double)) - 1024;
-    e = cudaFuncSetAttribute(k_pcg_cluster<CPT, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+    e = cudaFuncSetAttribute(k_pcg_cluster<CPT, PAIR, VAR>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_pcg_cluster<CPT, PAIR>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    e = cudaFuncSetAttribute(k_pcg_cluster<CPT, PAIR, VAR>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     if (e != cudaSuccess) return e;
     done = true;
     return cudaSuccess;
 }
 
-template <int CPT, bool PAIR>
+template <int CPT, bool PAIR, bool VAR = false>
 cudaError_t launch_cpt(const PcgLaunch& L, int C, cudaStream_t s) {
-    auto kern = k_pcg_cluster<CPT, PAIR>;
-    const size_t bytes = smem_bytes(L.cap_cells);
-    cudaError_t e = configure_cpt<CPT, PAIR>();
+    auto kern = k_pcg_cluster<CPT, PAIR, VAR>;
+    const size_t bytes = smem_bytes(L.cap_cells, VAR);
+    cudaError_t e = configure_cpt<CPT, PAIR, VAR>();
     if (e != cudaSuccess) return e;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(C, 1, 1);
@@ -1363,6 +1399,18 @@ int cpt_for(int cap) {
 
 }  // namespace
 
+// Whether the on-chip solver holds the variable-coefficient operator of an nx x ny
+// grid on C CTAs (ny even: the paired-cell form; at most 4 cell pairs per thread).
+bool pcg_var_cluster_fits(int nx, int ny, int C) {
+    if (C < 1 || C > 16 || ny % 2 != 0) return false;
+    int dev = 0, optin = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return false;
+    if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return false;
+    const size_t dyn = (size_t)optin - (32 * kMaxK + 2 * 16 * kMaxK + CFD2D_MAX_COMPONENTS) * sizeof(double) - 1024;
+    const int cap = ((nx + C - 1) / C) * ny;
+    return smem_bytes(cap, true) <= dyn && cpt_for((cap + 1) / 2) != 0 && cpt_for((cap + 1) / 2) <= 4;
+}
+
 // Max cells one CTA can hold for a given dynamic shared-memory budget.
 int pcg_cluster_capacity(size_t smem_limit) {
     return (int)((smem_limit - 16) / (kArrays * sizeof(double) + 1));
@@ -1407,10 +1455,10 @@ int pcg_cluster_plan(int nx, int ny) {
         cudaError_t e = cudaSuccess;
         const void* f = nullptr;
         switch (cpt) {
-            case 1: e = configure_cpt<1, false>(); f = (const void*)k_pcg_cluster<1, false>; break;
-            case 2: e = configure_cpt<2, false>(); f = (const void*)k_pcg_cluster<2, false>; break;
-            case 4: e = configure_cpt<4, false>(); f = (const void*)k_pcg_cluster<4, false>; break;
-            default: e = configure_cpt<8, false>(); f = (const void*)k_pcg_cluster<8, false>; break;
+            case 1: e = configure_cpt<1, false>(); f = (const void*)k_pcg_cluster<1, false, false>; break;
+            case 2: e = configure_cpt<2, false>(); f = (const void*)k_pcg_cluster<2, false, false>; break;
+            case 4: e = configure_cpt<4, false>(); f = (const void*)k_pcg_cluster<4, false, false>; break;
+            default: e = configure_cpt<8, false>(); f = (const void*)k_pcg_cluster<8, false, false>; break;
         }
         // the paired variant (even ny) has the same block size and shared memory
         if (e == cudaSuccess) {
@@ -1434,10 +1482,19 @@ cudaError_t pcg_launch(const PcgLaunch& L0, cudaStream_t s) {
     PcgLaunch L = L0;
     const int C = L.op.cluster;
     if (C == 0) return pcg_grid_launch(L, s);
-    if (L.op.bx) return cudaErrorInvalidValue;  // variable coefficients: grid solver only
     if (C < 1 || C > 16) return cudaErrorInvalidValue;
     const int rows = (L.op.nx + C - 1) / C;
     L.cap_cells = rows * L.op.ny;
+    if (L.op.bx) {
+        // variable coefficients: four more arrays per cell (pcg_var_cluster_fits)
+        if (!L.op.by || L.op.mixed || L.op.ny % 2 != 0) return cudaErrorInvalidValue;
+        switch (cpt_for((L.cap_cells + 1) / 2)) {
+            case 1: return launch_cpt<1, true, true>(L, C, s);
+            case 2: return launch_cpt<2, true, true>(L, C, s);
+            case 4: return launch_cpt<4, true, true>(L, C, s);
+            default: return cudaErrorInvalidValue;
+        }
+    }
     if (L.op.mixed) {
         // the cluster planned for the FP64 solver holds the 45-byte cells as well
         switch (cpt_for(L.cap_cells)) {
