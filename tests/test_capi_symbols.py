@@ -83,3 +83,31 @@ def test_ctypes_layout_equals_the_c_header(tmp_path):
     subprocess.run([cc, "-std=c11", str(src), "-o", str(exe)], check=True)
     got = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
     assert got == expect
+
+
+def test_entry_points_reject_invalid_arguments_before_any_device_work():
+    """The C ABI checks its arguments first and answers CFD2D_E_ARG (-1) without
+    touching the device (runs without a GPU)."""
+    from cfd2d_b200 import _lib
+
+    lib = _lib.lib()
+    E_ARG = _lib.E_ARG
+    null = None
+    sim = _lib.Sim()  # nx = ny = 0, no state
+    assert lib.cfd2d_sim_step(null, null) == E_ARG
+    assert lib.cfd2d_sim_step(ctypes.byref(sim), null) == E_ARG
+    assert lib.cfd2d_sim_smagorinsky_pre_momentum(ctypes.byref(sim), null) == E_ARG
+    assert lib.cfd2d_sim_sst_pre_momentum(ctypes.byref(sim), null) == E_ARG
+    assert lib.cfd2d_sim_vof_properties(ctypes.byref(sim), null) == E_ARG
+    assert lib.cfd2d_sim_wall_distance(ctypes.byref(sim), null, null, 0, null) == E_ARG
+    assert lib.cfd2d_sample(ctypes.byref(sim), null, 0, null, null, 0, null, null) == E_ARG
+    assert lib.cfd2d_probe_record(ctypes.byref(sim), null, 0, null, null, 0, null, null) == E_ARG
+    assert lib.cfd2d_field_average_accumulate(ctypes.byref(sim), null, null) == E_ARG
+    assert lib.cfd2d_streamfunction(ctypes.byref(sim), null, null) == E_ARG
+    assert lib.cfd2d_vtk_pack(ctypes.byref(sim), null, 0, null, null) == E_ARG
+    assert lib.cfd2d_cell_values(ctypes.byref(sim), null, null, null) == E_ARG
+    assert lib.cfd2d_vof_advect(null, null, null, null, 4, 4, 0.1, 0.1, 0.01, 1.0, 0, 0.0, null, null) == E_ARG
+    assert lib.cfd2d_pressure_solve(null, null, null, 1e-8, 10, null, null, null) == E_ARG
+    op = _lib.Poisson()
+    assert lib.cfd2d_pressure_solve_static(ctypes.byref(op), null, null, 1e-8, 10, null, null, null) == E_ARG
+    assert lib.cfd2d_wall_distance_workspace_bytes(0, 4) == 0
