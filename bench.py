@@ -152,6 +152,14 @@ class _Clocks:
                 "reasons": sorted(reasons)}
 
 
+def _clocks_path(name: str) -> str:
+    """Where the nvidia-smi clock samples of the timed region go: CFD2D_CLOCKS_DIR if
+    set (to keep them), else the temporary directory."""
+    import tempfile
+
+    return str(Path(os.environ.get("CFD2D_CLOCKS_DIR") or tempfile.gettempdir()) / name)
+
+
 def _ncu_traffic():
     """DRAM bytes per launch of the solver kernel from the committed ncu summary, if any."""
     f = ROOT / "profiles" / "pcg_cluster_cylinder440x82.txt"
@@ -481,8 +489,7 @@ def run_b200(args, dist, rank, world):
         _barrier(dist)
         torch.cuda.synchronize()
         step_ms, solve_ms = [], []
-        with _Clocks(str(ROOT / "gpurun_out" / f"clocks_rank{rank}.csv")
-                     if (ROOT / "gpurun_out").exists() else "/tmp/cfd2d_clocks.csv") as clk:
+        with _Clocks(_clocks_path(f"clocks_rank{rank}.csv")) as clk:
             t0 = time.perf_counter()
             for _ in range(args.steps):
                 a, b = one_step()
@@ -621,8 +628,7 @@ def run_batch(args, dist, rank, world):
     b.advance(args.warmup)
     _barrier(dist)
     torch.cuda.synchronize()
-    with _Clocks(str(ROOT / "gpurun_out" / f"clocks_batch_rank{rank}.csv")
-                 if (ROOT / "gpurun_out").exists() else "/tmp/cfd2d_clocks_batch.csv") as clk:
+    with _Clocks(_clocks_path(f"clocks_batch_rank{rank}.csv")) as clk:
         ms = b.timed_advance(args.steps, concurrent=True)
     ms_max = _max_over_ranks(dist, ms)
     # per-case loop: each case alone, one after another, timed per case on the device,

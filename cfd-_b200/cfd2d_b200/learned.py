@@ -275,7 +275,7 @@ def net_backward(net: LPCNet, ws: Workspace, x_in, dout):
 
 def torch_reference_forward(net: LPCNet, x_in, masks):
     """The same network in PyTorch (CPU, FP32 on BF16-rounded weights and activations):
-    the checker of the CUDA kernels and their gradients."""
+    the reference computation for the CUDA kernels and their gradients."""
     t = _t()
     F = t.nn.functional
 

@@ -4,7 +4,7 @@ TEST INFRASTRUCTURE ONLY. This package restates, in NumPy, the arithmetic of the
 reference solver (kaeptnzursee1910/CFD-, package ``cfd2d``) so that the CUDA
 implementation in ``cfd-_b200/`` can be checked against it. Only ``tests/``,
 ``__graft_entry__.smoke()`` and the ``cpu_baseline`` / ``--impl reference`` legs of
-``bench.py`` may import it, and only as the checker or the timed CPU baseline;
+``bench.py`` may import it, and only to check results or as the timed CPU baseline;
 the product never calls into it.
 
 Parity is pinned: ``tests/golden/make_golden.py`` runs the reference itself (in

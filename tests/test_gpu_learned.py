@@ -3,7 +3,7 @@
 The CPU checker is PyTorch on the same BF16-rounded weights and activations: the
 forward pass must agree to BF16 resolution and every weight gradient of the
 hand-written backward kernels to a few percent (the kernels keep activations in
-BF16 and accumulate in FP32, the checker in FP32 throughout).
+BF16 and accumulate in FP32, the PyTorch computation in FP32 throughout).
 """
 
 from __future__ import annotations
