@@ -1781,7 +1781,8 @@ def available_fields(sim):
     out = dict(BASE_FIELDS)
     for k, (label, _) in _model_fields(sim).items():
         out[k] = label
-    if getattr(sim, "variable_viscosity", False) and "nu_t" not in out:
+    if (getattr(sim, "variable_viscosity", False) and not getattr(sim, "variable_density", False)
+            and "nu_t" not in out):
         out["nu_t"] = "Turbulente Viskosität ν_t"
     return out
 
@@ -2106,6 +2107,12 @@ class OVOF(OModel):
             self.alpha[:] = self._tmp
             self.fill_ghosts()
         self.update_properties()
+
+    def fields(self, sim):
+        # cfd2d/vof.py:302-306
+        solid = ~sim.grid.fluid[1:-1, 1:-1]
+        return {"alpha": ("Volumenanteil α (Phase 1)", np.where(solid, np.nan, self.alpha[1:-1, 1:-1])),
+                "rho": ("Dichte ρ", np.where(solid, np.nan, sim.rho[1:-1, 1:-1]))}
 
     def dt_limit(self, sim):
         # cfd2d/vof.py:273-284

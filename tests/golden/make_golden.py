@@ -375,8 +375,11 @@ def gen_vof():
     """The VOF path of the reference (cfd2d/vof.py, PressureSolver.solve_variable):
     vof_advect on seeded inputs, solve_variable (sparse direct) on three geometries
     with a 1000:1 density interface, and a 32 x 32 dam break over 20 steps."""
+    import tempfile
+
     from inputs import rho_field, vof_cases
 
+    from cfd2d import functions
     from cfd2d.vof import vof_advect
 
     out = {}
@@ -417,6 +420,10 @@ def gen_vof():
     f["alpha"] = lambda s: vof.alpha
     _run(case.sim, 20, {1, 20}, f, out, "dam")
     out["dam_volume"] = np.array(vof.volume())
+    out["dam_t"] = np.array(case.sim.t)
+    with tempfile.TemporaryDirectory() as td:
+        raw = functions.write_vtk(case.sim, Path(td) / "dam.vtk").read_bytes()
+    out["dam_vtk"] = np.frombuffer(raw, dtype=np.uint8)
     # the reference's default size, 100 steps
     case = cases.dam_break(n=96)
     vof = case.sim.model("multiphase")

@@ -234,3 +234,21 @@ def test_case_json_roundtrip_with_function_objects(cuda_lib, tmp_path):
     series = json.loads((out / "vtk/feld.vtk.series").read_text())
     assert len(series["files"]) >= 2
     assert len(case.sim.function_objects[0].t) == case.sim.n
+
+
+def test_vof_fields_in_probes_and_vtk(cuda_lib, tmp_path):
+    """alpha and rho of the VOF model through the device function objects."""
+    import oracle as O
+    from cfd2d_b200 import cases, functions
+
+    sim = cases.dam_break(n=32).sim
+    pts = [(0.1, 0.1), (0.3, 0.05), (0.2, 0.29), (0.29, 0.03)]
+    pr = functions.Probes(pts, fields=("alpha", "rho", "pressure"))
+    sim.function_objects.append(pr)
+    sim.advance(10)
+    xs, ys = [p[0] for p in pts], [p[1] for p in pts]
+    for f in ("alpha", "rho", "pressure"):
+        assert _eq(pr.data[f][-1], O.sample_field(sim, f, xs, ys)), f
+    raw = functions.write_vtk(sim, tmp_path / "dam.vtk").read_bytes()
+    assert raw == O.write_vtk_bytes(sim)
+    assert b"SCALARS alpha float 1" in raw and b"SCALARS rho float 1" in raw

@@ -363,3 +363,16 @@ def test_dam_break_20_steps():
             assert rel(vof.alpha, g[f"dam_alpha_{n}"]) < 1e-10, n
     assert rel(sim.hist["dt"], g["dam_dt"]) < 1e-12
     assert vof.volume() == pytest.approx(float(g["dam_volume"]), rel=1e-12)
+
+
+def test_vof_vtk_bytes_on_the_reference_state():
+    """The VTK file of the reference's dam break after 20 steps (alpha, rho, no nu_t:
+    cfd2d/visualization.py:86-88) from the oracle, byte for byte."""
+    g = golden("golden_vof")
+    sim = O.dam_break(n=32)
+    vof = sim.model("multiphase")
+    sim.u, sim.v, sim.p = g["dam_u_20"].copy(), g["dam_v_20"].copy(), g["dam_p_20"].copy()
+    vof.alpha[:] = g["dam_alpha_20"]
+    vof.update_properties()
+    sim.t = float(g["dam_t"])
+    assert O.write_vtk_bytes(sim) == g["dam_vtk"].tobytes()
