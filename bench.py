@@ -289,6 +289,20 @@ def stencil_roofline(peak: float, reps: int = 10) -> dict:
         med = float(np.median(ms))
         gbs = STENCIL_BYTES[name] * nx * ny / (med * 1e-3) / 1e9
         res[name] = {"ms": med, "bytes_per_cell": STENCIL_BYTES[name], "achieved_gbs": gbs, "frac": gbs / peak}
+    # the tile autotuner on the momentum drop-in at this size (cfd2d_b200.autotune); the
+    # shape changes no result, and the default shape is restored afterwards
+    from cfd2d_b200 import autotune
+
+    default = autotune.get_tile(autotune.MOMENTUM)
+    try:
+        best, timings = autotune.tune_momentum(nx, ny, reps=reps, store=False)
+        ms_best = float(timings[best])
+        gbs = STENCIL_BYTES["momentum_tendencies"] * nx * ny / (ms_best * 1e-3) / 1e9
+        res["momentum_tendencies_tuned"] = {"tile": list(best), "ms": ms_best, "achieved_gbs": gbs,
+                                            "frac": gbs / peak,
+                                            "ms_by_tile": {f"{a}x{b}": t for (a, b), t in timings.items()}}
+    finally:
+        autotune.set_tile(autotune.MOMENTUM, *default)
     del u, v, fluid, phi, diff, out, hu, hv, flush
     torch.cuda.empty_cache()
     return {"grid": [nx, ny], "l2": "flushed before each launch", **res}

@@ -339,6 +339,10 @@ int cfd2d_sim_vof_properties(const cfd2d_sim* sim, void* stream) {
     return status_of(stage_vof_properties(*sim, as_stream(stream)));
 }
 
+int cfd2d_set_tile(int which, int tx, int ty) { return set_tile(which, tx, ty) == 0 ? CFD2D_OK : CFD2D_E_ARG; }
+
+int cfd2d_get_tile(int which, int* tx, int* ty) { return get_tile(which, tx, ty) == 0 ? CFD2D_OK : CFD2D_E_ARG; }
+
 int cfd2d_graph_capture_steps_ex(const cfd2d_sim* sim, int nsteps, void* stream, void* const* events,
                                  void** graph_out, int* kernel_nodes) {
     if (!sim || nsteps < 1 || !graph_out) return CFD2D_E_ARG;

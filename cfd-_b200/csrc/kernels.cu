@@ -996,7 +996,32 @@ inline dim3 grid_rows(int width, int rows) {
     return dim3((width + kTileX - 1) / kTileX, (rows + kTileY - 1) / kTileY, 1);
 }
 inline cudaError_t last() { return cudaGetLastError(); }
+
+// Thread-block shapes of the row kernels that index by blockDim (every thread its own
+// cells, so the shape changes only the speed): [0] the momentum_tendencies drop-in,
+// [1] the step's row kernels. The transport kernels keep kTile (shared-memory tile).
+int g_tile[2][2] = {{kTileX, kTileY}, {kTileX, kTileY}};
+inline dim3 tile(int which) { return dim3(g_tile[which][0], g_tile[which][1], 1); }
+inline dim3 grid_tile(int which, int width, int rows) {
+    const int tx = g_tile[which][0], ty = g_tile[which][1];
+    return dim3((width + tx - 1) / tx, (rows + ty - 1) / ty, 1);
+}
+constexpr int kMom = 0, kStep = 1;
 }  // namespace
+
+int set_tile(int which, int tx, int ty) {
+    if (which < 0 || which > 1 || tx < 16 || tx % 16 != 0 || ty < 1 || tx * ty > 256) return -1;
+    g_tile[which][0] = tx;
+    g_tile[which][1] = ty;
+    return 0;
+}
+
+int get_tile(int which, int* tx, int* ty) {
+    if (which < 0 || which > 1 || !tx || !ty) return -1;
+    *tx = g_tile[which][0];
+    *ty = g_tile[which][1];
+    return 0;
+}
 
 int reduction_blocks(int ncell) {
     int b = (ncell + kBlock - 1) / kBlock;
@@ -1010,15 +1035,16 @@ cudaError_t launch_momentum(const double* u, const double* v, const uint8_t* fl,
                             int periodic, double* hu, double* hv, const double* rho, int var_density,
                             cudaStream_t s) {
     const InvSpacing inv = inv_spacing(dx, dy);
-    const dim3 grd = grid_rows(ny + 2, nx + 2);
+    const dim3 grd = grid_tile(kMom, ny + 2, nx + 2);
+    const dim3 blk = tile(kMom);
     if (variable && var_density)
-        k_momentum<true, true><<<grd, kTile, 0, s>>>(u, v, fl, nx, ny, inv, nu, gamma, periodic, hu, hv, rho);
+        k_momentum<true, true><<<grd, blk, 0, s>>>(u, v, fl, nx, ny, inv, nu, gamma, periodic, hu, hv, rho);
     else if (variable)
-        k_momentum<true, false><<<grd, kTile, 0, s>>>(u, v, fl, nx, ny, inv, nu, gamma, periodic, hu, hv, rho);
+        k_momentum<true, false><<<grd, blk, 0, s>>>(u, v, fl, nx, ny, inv, nu, gamma, periodic, hu, hv, rho);
     else if (var_density)
-        k_momentum<false, true><<<grd, kTile, 0, s>>>(u, v, fl, nx, ny, inv, nu, gamma, periodic, hu, hv, rho);
+        k_momentum<false, true><<<grd, blk, 0, s>>>(u, v, fl, nx, ny, inv, nu, gamma, periodic, hu, hv, rho);
     else
-        k_momentum<false, false><<<grd, kTile, 0, s>>>(u, v, fl, nx, ny, inv, nu, gamma, periodic, hu, hv, rho);
+        k_momentum<false, false><<<grd, blk, 0, s>>>(u, v, fl, nx, ny, inv, nu, gamma, periodic, hu, hv, rho);
     return last();
 }
 
@@ -1060,14 +1086,14 @@ cudaError_t stage_apply_bc(const cfd2d_sim& S, int begin, cudaStream_t s) {
 }
 
 cudaError_t stage_sst_pre(const cfd2d_sim& S, cudaStream_t s) {
-    k_sst_pre<<<grid_rows(S.ny, S.nx), kTile, 0, s>>>(S);
-    k_nut_ghosts<true><<<grid_rows(S.ny + 2, S.nx + 2), kTile, 0, s>>>(S);
+    k_sst_pre<<<grid_tile(kStep, S.ny, S.nx), tile(kStep), 0, s>>>(S);
+    k_nut_ghosts<true><<<grid_tile(kStep, S.ny + 2, S.nx + 2), tile(kStep), 0, s>>>(S);
     return last();
 }
 
 cudaError_t stage_smag_pre(const cfd2d_sim& S, cudaStream_t s) {
-    k_smag_pre<<<grid_rows(S.ny, S.nx), kTile, 0, s>>>(S);
-    k_nut_ghosts<false><<<grid_rows(S.ny + 2, S.nx + 2), kTile, 0, s>>>(S);
+    k_smag_pre<<<grid_tile(kStep, S.ny, S.nx), tile(kStep), 0, s>>>(S);
+    k_nut_ghosts<false><<<grid_tile(kStep, S.ny + 2, S.nx + 2), tile(kStep), 0, s>>>(S);
     return last();
 }
 
@@ -1077,18 +1103,18 @@ cudaError_t stage_dt(const cfd2d_sim& S, cudaStream_t s) {
 }
 
 cudaError_t stage_predictor(const cfd2d_sim& S, int copy_only, cudaStream_t s) {
-    k_predictor<<<grid_rows(S.ny + 2, S.nx + 2), kTile, 0, s>>>(S, copy_only, inv_spacing(S.dx, S.dy));
+    k_predictor<<<grid_tile(kStep, S.ny + 2, S.nx + 2), tile(kStep), 0, s>>>(S, copy_only, inv_spacing(S.dx, S.dy));
     return last();
 }
 
 cudaError_t stage_correct(const cfd2d_sim& S, const double* p, int unit_dt, cudaStream_t s) {
-    k_correct<<<grid_rows(S.ny + 2, S.nx + 2), kTile, 0, s>>>(S, p, unit_dt);
+    k_correct<<<grid_tile(kStep, S.ny + 2, S.nx + 2), tile(kStep), 0, s>>>(S, p, unit_dt);
     return last();
 }
 
 cudaError_t stage_flow_shift(const cfd2d_sim& S, cudaStream_t s) {
     k_bulk<<<reduction_blocks(S.nx * S.ny), kBlock, 0, s>>>(S, S.red);
-    k_shift_u<<<grid_rows(S.ny + 2, S.nx + 1), kTile, 0, s>>>(S);
+    k_shift_u<<<grid_tile(kStep, S.ny + 2, S.nx + 1), tile(kStep), 0, s>>>(S);
     return last();
 }
 
@@ -1097,10 +1123,10 @@ cudaError_t stage_scalar(const cfd2d_sim& S, int slot, cudaStream_t s) {
     if (sc.turb_div > 0.0 && S.variable_viscosity)
         k_scalar_turb_diff<<<reduction_blocks((S.nx + 2) * (S.ny + 2)), kBlock, 0, s>>>(S, slot);
     k_scalar_rhs<<<grid_rows(S.ny + 2, S.nx + 2), kTile, 0, s>>>(S, slot);
-    k_scalar_update<<<grid_rows(S.ny, S.nx), kTile, 0, s>>>(S, slot);
+    k_scalar_update<<<grid_tile(kStep, S.ny, S.nx), tile(kStep), 0, s>>>(S, slot);
     cudaError_t e = stage_scalar_ghosts(S, slot, s);
     if (e != cudaSuccess || sc.source != 2) return e;
-    k_sst_wall_omega<<<grid_rows(S.ny, S.nx), kTile, 0, s>>>(S);
+    k_sst_wall_omega<<<grid_tile(kStep, S.ny, S.nx), tile(kStep), 0, s>>>(S);
     return stage_scalar_ghosts(S, slot, s);
 }
 
@@ -1109,7 +1135,7 @@ cudaError_t stage_scalar_ghosts(const cfd2d_sim& S, int slot, cudaStream_t s) {
     const int n = S.nx + S.ny;
     k_scalar_ghost_domain<<<(n + kBlock - 1) / kBlock, kBlock, 0, s>>>(S, slot);
     if (S.has_solid)
-        k_scalar_ghost_solid<<<grid_rows(S.ny, S.nx), kTile, 0, s>>>(S, slot, sc.obs_t == 1 ? 1 : 0, sc.obs_v);
+        k_scalar_ghost_solid<<<grid_tile(kStep, S.ny, S.nx), tile(kStep), 0, s>>>(S, slot, sc.obs_t == 1 ? 1 : 0, sc.obs_v);
     return last();
 }
 

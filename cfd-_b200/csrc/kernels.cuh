@@ -30,6 +30,8 @@ cudaError_t stage_sst_pre(const cfd2d_sim& S, cudaStream_t s);
 cudaError_t stage_smag_pre(const cfd2d_sim& S, cudaStream_t s);
 cudaError_t stage_vof_curvature(const cfd2d_sim& S, cudaStream_t s);
 cudaError_t stage_monitors(const cfd2d_sim& S, cudaStream_t s);
+int set_tile(int which, int tx, int ty);
+int get_tile(int which, int* tx, int* ty);
 cudaError_t stage_vof_operator(const cfd2d_sim& S, cudaStream_t s);
 cudaError_t stage_vof_transport(const cfd2d_sim& S, cudaStream_t s);
 cudaError_t stage_vof_properties(const cfd2d_sim& S, cudaStream_t s);

@@ -611,6 +611,15 @@ int cfd2d_streamfunction(const cfd2d_sim* sim, double* psi, void* stream);
  * field. The host writes the text header lines around these blocks. */
 int cfd2d_vtk_pack(const cfd2d_sim* sim, const cfd2d_field* fields, int nfields, uint8_t* out, void* stream);
 
+/* Thread-block shape (tx along j, ty along i) of the row kernels: which = 0 the
+ * momentum_tendencies drop-in, 1 the step's row kernels (predictor, correction,
+ * turbulence, scalar update and ghosts). tx a multiple of 16, tx * ty <= 256. Every
+ * thread computes its own cells, so results do not depend on the shape; captured
+ * step graphs keep the shape they were captured with. Default 32 x 8. No reference
+ * counterpart: the knob of the tile autotuner (cfd2d_b200.autotune). */
+int cfd2d_set_tile(int which, int tx, int ty);
+int cfd2d_get_tile(int which, int* tx, int* ty);
+
 /* Library version string (host memory, static). */
 const char* cfd2d_version(void);
 
