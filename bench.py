@@ -555,9 +555,9 @@ def run_b200(args, dist, rank, world):
             out["p"].copy_(sim._p, non_blocking=True)
             out["c"].copy_(phi_dev, non_blocking=True)
             stream.synchronize()
-            host["u"].copy_(out["u"])
-            host["v"].copy_(out["v"])
-            host["c"].copy_(out["c"])
+            # this step's results are the next step's inputs: swap the pinned buffers
+            for nm in ("u", "v", "c"):
+                host[nm], out[nm] = out[nm], host[nm]
         e2e_s = time.perf_counter() - t0
     e2e_s = _max_over_ranks(dist, e2e_s)
     e2e = world * cells * e2e_steps / e2e_s
