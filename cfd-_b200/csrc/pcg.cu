@@ -917,19 +917,13 @@ __device__ __forceinline__ bool grid_sum(double (&v)[K], double* red_smem, doubl
     return true;
 }
 
-// Off-diagonal entries of row (i, j): -dx2 and -dy2, or with variable coefficients
-// -(b dx2) of the face (the matrix values of cfd2d/pressure.py:199-216; the west
-// face of column 0 is the periodic face nx)
+// Off-diagonal entries of row (i, j): -dx2 and -dy2, or var_coef's
 template <bool VAR>
 struct Coef {
     double w, s, n, e;
     __device__ __forceinline__ Coef(const cfd2d_poisson& op, int i, int j) {
         if constexpr (VAR) {
-            const int nx = op.nx, ny = op.ny;
-            w = -(op.bx[(size_t)((i == 0) ? nx : i) * (ny + 2) + j + 1] * op.dx2);
-            e = -(op.bx[(size_t)(i + 1) * (ny + 2) + j + 1] * op.dx2);
-            s = -(op.by[(size_t)(i + 1) * (ny + 1) + j] * op.dy2);
-            n = -(op.by[(size_t)(i + 1) * (ny + 1) + j + 1] * op.dy2);
+            var_coef(op, i, j, w, e, s, n);
         } else {
             w = e = -op.dx2;
             s = n = -op.dy2;
