@@ -463,6 +463,60 @@ def vof_section(steps: int = 50, n: int = 96) -> dict:
                                 "per call as scipy runs it), mean of 3 calls"}
 
 
+def configs_section(cavity_steps: int = 2000, sst_steps: int = 500) -> dict:
+    """The other two single-case workloads of the reference's benchmark list, timed by
+    events around advance(): the lid-driven cavity 64 x 64 (AB2, gamma 0.1, tau 0.5,
+    CG rtol 1e-8, 2000 steps from rest) and the periodic k-omega SST channel 128 x 192
+    (bulk velocity 1, Re_b 1e4, laminar profile with 5 % seeded noise, CG rtol 1e-8)."""
+    import numpy as np
+    import torch
+
+    from cfd2d_b200 import cases
+    from cfd2d_b200.boundary import BoundaryCondition as BC
+    from cfd2d_b200.grid import Grid
+    from cfd2d_b200.solver import Simulation
+    from cfd2d_b200.turbulence import KOmegaSST
+
+    def timed(sim, n):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        sim.advance(3)
+        torch.cuda.synchronize()
+        with torch.cuda.stream(sim.stream):
+            ev[0].record()
+            sim.launch_steps(n)
+            ev[1].record()
+        sim.finish_steps()
+        torch.cuda.synchronize()
+        ms = ev[0].elapsed_time(ev[1])
+        its = np.array(sim.history.extra["cg_iterationen"][-n:], dtype=float)
+        g = sim.grid
+        return {"ms_per_step": ms / n, "cell_updates_per_s": g.nx * g.ny * n / (ms / 1e3),
+                "poisson_iters_per_step": float(its.mean())}
+
+    case = cases.lid_driven_cavity(re=100, n=64, scheme="ab2", gamma=0.1, tau=0.5, pressure_solver="cg")
+    case.sim.pressure.tol = CG_RTOL
+    cav = timed(case.sim, cavity_steps)
+    nx, ny = 128, 192
+    grid = Grid(nx, ny, 2 * np.pi, 2.0)
+    bcs = dict(left=BC("periodic"), right=BC("periodic"), bottom=BC("noslip"), top=BC("noslip"))
+    nu = 2.0 / 1e4
+    sst = KOmegaSST(intensity=np.sqrt(1e-3 / 1.5), viscosity_ratio=1e-3 / (nu * 10.0), U_ref=1.0)
+    sim = Simulation(grid, bcs, nu=nu, flow_rate=1.0, models=[sst], pressure_solver="cg")
+    sim.pressure.tol = CG_RTOL
+    rng = np.random.default_rng(0)
+    y = (np.arange(ny) + 0.5) * grid.dy
+    u = sim.u
+    u[1:nx + 1, 1:ny + 1] = (1.5 * y * (2.0 - y))[None, :] * (1.0 + 0.05 * rng.uniform(-1.0, 1.0, (nx, ny)))
+    v = sim.v
+    v[1:nx + 1, 1:ny] = 0.05 * rng.uniform(-1.0, 1.0, (nx, ny - 1))
+    u[~sim.u_fluid] = 0.0
+    v[~sim.v_fluid] = 0.0
+    sim._apply_bc()
+    sim._project_initial()
+    return {"cavity_64x64": {"steps": cavity_steps, **cav},
+            "sst_channel_128x192": {"steps": sst_steps, **timed(sim, sst_steps)}}
+
+
 # ------------------------------------------------------------------ GPU arm
 def run_b200(args, dist, rank, world):
     import numpy as np
@@ -574,6 +628,12 @@ def run_b200(args, dist, rank, world):
             mixed = mixed_section()
         except Exception as exc:  # an optional section never costs the bench line
             mixed = {"error": f"{type(exc).__name__}: {exc}"}
+    other = None
+    if not args.no_configs:
+        try:
+            other = configs_section()
+        except Exception as exc:  # an optional section never costs the bench line
+            other = {"error": f"{type(exc).__name__}: {exc}"}
     vof = None
     if not args.no_vof:
         try:
@@ -615,6 +675,7 @@ def run_b200(args, dist, rank, world):
         "learned_pc": learned_pc,
         "mixed_precision": mixed,
         "vof_dam_break": vof,
+        "other_workloads": other,
     }
     print(json.dumps(line), flush=True)
 
@@ -697,6 +758,7 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner section")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision section")
     ap.add_argument("--no-vof", action="store_true", help="skip the two-phase dam-break section")
+    ap.add_argument("--no-configs", action="store_true", help="skip the cavity and SST channel section")
     ap.add_argument("--workload", choices=["cylinder", "batch"], default="cylinder",
                     help="cylinder: the headline; batch: 256 uneven cavities stepped together")
     ap.add_argument("--batch-cases", type=int, default=256)

@@ -106,6 +106,7 @@ class Vof(C.Structure):
 
 
 MAX_MONITORS = 12
+MONITOR_SCRATCH = 2 * MAX_MONITORS * 296
 MON_SUM_FLUID, MON_MEAN_FLUID, MON_MAX_ALL, MON_NUSSELT, MON_VOLUME_ERROR, MON_FRONT_X, MON_HEIGHT_LEFT = range(7)
 
 
@@ -132,7 +133,7 @@ class Sim(C.Structure):
         ("gx", C.c_double), ("gy", C.c_double), ("T_ref", C.c_double), ("sst_on", C.c_int),
         ("sst", SST), ("smag_on", C.c_int), ("smag", Smagorinsky),
         ("vof_on", C.c_int), ("vof", Vof), ("nmon", C.c_int), ("mon", Monitor * MAX_MONITORS),
-        ("mon_ring", _vp), ("state", _vp), ("red", _vp), ("hist", _vp), ("hist_cap", C.c_int),
+        ("mon_ring", _vp), ("mon_part", _vp), ("state", _vp), ("red", _vp), ("hist", _vp), ("hist_cap", C.c_int),
         ("p_tmp", _vp),
     ]
 

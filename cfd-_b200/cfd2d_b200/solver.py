@@ -152,6 +152,7 @@ class Simulation:
             self._red = z(int(_lib.lib().cfd2d_sim_scratch_doubles(nx, ny)))
             self._hist = z(HIST_CAP * _lib.HIST_FIELDS)
             self._mon_ring = z(HIST_CAP * _lib.MAX_MONITORS)
+            self._mon_part = z(_lib.MONITOR_SCRATCH)
             self._mon_keys: list = []
             st = _lib.State()
             st.t_end = math.inf
@@ -257,6 +258,7 @@ class Simulation:
         for k, (_, mon) in enumerate(mons):
             S.mon[k] = mon
         S.mon_ring = self._mon_ring.data_ptr()
+        S.mon_part = self._mon_part.data_ptr()
         S.state = self._d_state.data_ptr()
         S.red = self._red.data_ptr()
         S.hist = self._hist.data_ptr()

@@ -176,6 +176,7 @@ typedef struct cfd2d_vof {
 /* Per-step model monitors (the model part of cfd2d/solver.py:441-443 _record): one
  * value per monitor and step, written into sim->mon_ring after the step. */
 #define CFD2D_MAX_MONITORS 12
+#define CFD2D_MONITOR_SCRATCH (2 * CFD2D_MAX_MONITORS * 296)
 #define CFD2D_MON_SUM_FLUID 0     /* (sum of data over fluid cells) dx dy: ScalarField.total,
                                      VOF volume (cfd2d/models.py:221-224, vof.py:229-231) */
 #define CFD2D_MON_MEAN_FLUID 1    /* mean of data over fluid cells (np.nanmean of cell()) */
@@ -237,6 +238,7 @@ typedef struct cfd2d_sim {
     int nmon;                 /* model monitors recorded after every step */
     cfd2d_monitor mon[CFD2D_MAX_MONITORS];
     double* mon_ring;         /* hist_cap records of CFD2D_MAX_MONITORS doubles */
+    double* mon_part;         /* scratch, CFD2D_MONITOR_SCRATCH doubles */
     cfd2d_state* state;
     double* red;              /* reduction scratch, cfd2d_sim_scratch_doubles() */
     double* hist;             /* history ring: hist_cap records of CFD2D_HIST_FIELDS doubles:
