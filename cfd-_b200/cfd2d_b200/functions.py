@@ -6,7 +6,7 @@ on the device, so the steps keep running without a host synchronisation);
 ``LineSample``, ``sample_field`` and ``write_vtk`` evaluate or pack the fields on the
 device and copy only the samples or the finished VTK payload to the host. Files
 have the reference's names and formats; the PNG plots the reference draws beside
-them need matplotlib, which this image does not have, and are not written.
+them need matplotlib, which this package does not depend on, and are not written.
 ``VTKWriter``, ``Checkpoint`` and user-defined function objects run on the host
 after every step, which synchronises each step as in the reference.
 

@@ -3,7 +3,7 @@
 ``available_fields`` and ``field_data`` keep the reference's names, labels and
 order; the function objects (cfd2d_b200.functions) use ``device_field`` to read
 the same fields on the device. Live plots and animations are not part of this
-package (no matplotlib in the B200 image).
+package (it does not depend on matplotlib).
 """
 
 from __future__ import annotations
