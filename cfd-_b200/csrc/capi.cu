@@ -339,6 +339,11 @@ int cfd2d_sim_vof_properties(const cfd2d_sim* sim, void* stream) {
     return status_of(stage_vof_properties(*sim, as_stream(stream)));
 }
 
+int cfd2d_barrier_selftest(unsigned int* bar, int* status, int* ok_out, void* stream) {
+    if (!bar || !status || !ok_out) return CFD2D_E_ARG;
+    return status_of(barrier_selftest(bar, status, ok_out, as_stream(stream)));
+}
+
 int cfd2d_set_tile(int which, int tx, int ty) { return set_tile(which, tx, ty) == 0 ? CFD2D_OK : CFD2D_E_ARG; }
 
 int cfd2d_get_tile(int which, int* tx, int* ty) { return get_tile(which, tx, ty) == 0 ? CFD2D_OK : CFD2D_E_ARG; }

@@ -1227,6 +1227,18 @@ int grid_blocks_for(int n) {
 
 }  // namespace
 
+// The bounded grid barrier of the persistent solvers on a grid of one block, with the
+// barrier words as the caller set them (cfd2d_barrier_selftest).
+__global__ void k_barrier_probe(unsigned int* bar, int* status, int* ok_out) {
+    const bool ok = grid_barrier(bar, status);
+    if (threadIdx.x == 0) *ok_out = ok ? 1 : 0;
+}
+
+cudaError_t barrier_selftest(unsigned int* bar, int* status, int* ok_out, cudaStream_t s) {
+    k_barrier_probe<<<1, 32, 0, s>>>(bar, status, ok_out);
+    return cudaGetLastError();
+}
+
 __global__ void k_matvec(cfd2d_poisson op, const double* x, double* y) {
     const int n = op.nx * op.ny;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {

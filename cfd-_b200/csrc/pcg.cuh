@@ -32,6 +32,7 @@ struct PcgLaunch {
 
 int pcg_cluster_plan(int nx, int ny);
 bool pcg_var_cluster_fits(int nx, int ny, int C);
+cudaError_t barrier_selftest(unsigned int* bar, int* status, int* ok_out, cudaStream_t s);
 size_t pcg_grid_workspace_doubles(int nx, int ny);
 cudaError_t pcg_launch(const PcgLaunch& L, cudaStream_t s);
 cudaError_t pcg_matvec(const cfd2d_poisson& op, const double* x, double* y, cudaStream_t s);
