@@ -515,6 +515,45 @@ class Simulation:
                 _lib.check(rc, "cfd2d_graph_launch")
                 left -= size
 
+    def stage_times(self, nsteps: int = 10) -> dict:
+        """Device time of the three parts of a step, in ms averaged over ``nsteps``
+        steps that advance the simulation: before the pressure solve (boundary
+        conditions, model hooks, dt, tendencies, predictor), the solve, and after it
+        (correction, boundary conditions, flow-rate control, model post-steps,
+        history and monitors). CUDA events recorded inside one captured step graph.
+        The reference only accumulates wall time (cfd2d/solver.py:328, 393)."""
+        if self.function_objects or self._learned is not None:
+            raise ValueError("stage_times runs the plain step graph: detach function objects and the "
+                             "learned preconditioner first")
+        L = _lib.lib()
+        ev = (C.c_void_p * 4)()
+        _lib.check(L.cfd2d_events_create(4, ev), "cfd2d_events_create")
+        graph, knodes = C.c_void_p(0), C.c_int(0)
+        tot = [0.0, 0.0, 0.0]
+        try:
+            with self._on_stream():
+                self._flush_mirrors()
+                self._set_run_limits()
+                s = _lib.stream_ptr(self._stream)
+                _lib.check(L.cfd2d_graph_capture_steps_ex(C.byref(self._S), 1, s, ev, C.byref(graph),
+                                                          C.byref(knodes)), "cfd2d_graph_capture_steps_ex")
+                for _ in range(int(nsteps)):
+                    self._st_fresh = False
+                    _lib.check(L.cfd2d_graph_launch(graph, s), "cfd2d_graph_launch")
+                    for k in range(3):
+                        ms = C.c_float()
+                        _lib.check(L.cfd2d_event_elapsed_ms(ev[k], ev[k + 1], C.byref(ms)), "elapsed")
+                        tot[k] += ms.value
+                self._sync()
+                self._after_steps()
+        finally:
+            if graph.value:
+                L.cfd2d_graph_destroy(graph)
+            L.cfd2d_events_destroy(4, ev)
+        n = max(int(nsteps), 1)
+        return {"pre_solve_ms": tot[0] / n, "solve_ms": tot[1] / n, "post_solve_ms": tot[2] / n,
+                "kernels_per_step": int(knodes.value)}
+
     def _steps_with_functions(self, nsteps: int) -> None:
         """Steps one at a time with the function objects after each (cfd2d/solver.py:401-403).
         Device function objects only queue kernels behind the step; host ones (and

@@ -89,3 +89,17 @@ def test_bounded_grid_barrier_gives_up_and_the_context_stays_usable(cuda_lib):
     case = cases.lid_driven_cavity(re=100, n=16)
     case.sim.advance(5)
     assert case.sim.max_divergence() < 1e-10
+
+
+def test_stage_times(cuda_lib):
+    """Simulation.stage_times: event-timed parts of the step (the solve dominates)."""
+    from cfd2d_b200 import cases
+
+    case = cases.lid_driven_cavity(re=100, n=64, pressure_solver="cg")
+    sim = case.sim
+    sim.pressure.tol = 1e-8
+    sim.advance(3)
+    st = sim.stage_times(5)
+    assert sim.n == 8 and len(sim.history.t) == 8
+    assert st["solve_ms"] > 0 and st["pre_solve_ms"] > 0 and st["post_solve_ms"] > 0
+    assert st["solve_ms"] > st["pre_solve_ms"] and st["kernels_per_step"] >= 8
