@@ -194,6 +194,8 @@ def lib():
         "cfd2d_sim_wall_distance": ([vp, vp, vp, sz, vp], i),
         "cfd2d_sample": ([vp, vp, i, vp, vp, i, vp, vp], i),
         "cfd2d_set_tile": ([i, i, i], i),
+        "cfd2d_mask_polygon": ([i, i, d, d, vp, vp, i, vp, vp], i),
+        "cfd2d_mask_image": ([i, i, d, d, vp, i, i, d, d, d, d, vp, vp], i),
         "cfd2d_barrier_selftest": ([vp, vp, vp, vp], i),
         "cfd2d_get_tile": ([i, C.POINTER(C.c_int), C.POINTER(C.c_int)], i),
         "cfd2d_vof_advect": ([vp, vp, vp, vp, i, i, d, d, d, d, i, d, vp, vp], i),
@@ -261,7 +263,7 @@ def exported_symbols():
         "cfd2d_sim_scratch_doubles", "cfd2d_sim_apply_bc", "cfd2d_sim_project_initial",
         "cfd2d_sim_step", "cfd2d_sim_scalar_fill_ghosts", "cfd2d_sim_sst_pre_momentum",
         "cfd2d_sim_smagorinsky_pre_momentum", "cfd2d_wall_distance_workspace_bytes",
-        "cfd2d_sim_wall_distance", "cfd2d_sample", "cfd2d_barrier_selftest", "cfd2d_set_tile", "cfd2d_get_tile", "cfd2d_cell_values", "cfd2d_vof_advect", "cfd2d_sim_vof_properties", "cfd2d_probe_record", "cfd2d_field_average_accumulate",
+        "cfd2d_sim_wall_distance", "cfd2d_sample", "cfd2d_mask_polygon", "cfd2d_mask_image", "cfd2d_barrier_selftest", "cfd2d_set_tile", "cfd2d_get_tile", "cfd2d_cell_values", "cfd2d_vof_advect", "cfd2d_sim_vof_properties", "cfd2d_probe_record", "cfd2d_field_average_accumulate",
         "cfd2d_streamfunction", "cfd2d_vtk_pack", "cfd2d_graph_capture_steps", "cfd2d_graph_launch", "cfd2d_graph_destroy",
         "cfd2d_graph_capture_steps_ex", "cfd2d_events_create", "cfd2d_events_destroy",
         "cfd2d_event_elapsed_ms", "cfd2d_sim_step_begin", "cfd2d_sim_step_finish", "cfd2d_poisson_matvec",

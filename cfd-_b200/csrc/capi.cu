@@ -125,6 +125,18 @@ int cfd2d_mask_rectangle(int nx, int ny, double dx, double dy, double xa, double
     return status_of(launch_mask(2, nx, ny, dx, dy, q, mask, as_stream(stream)));
 }
 
+int cfd2d_mask_polygon(int nx, int ny, double dx, double dy, const double* px, const double* py, int npts,
+                       uint8_t* mask, void* stream) {
+    if (!mask || !px || !py || npts < 3 || nx < 1 || ny < 1) return CFD2D_E_ARG;
+    return status_of(launch_mask_polygon(nx, ny, dx, dy, px, py, npts, mask, as_stream(stream)));
+}
+
+int cfd2d_mask_image(int nx, int ny, double dx, double dy, const uint8_t* solid, int h, int w, double x0, double y0,
+                     double width, double height, uint8_t* mask, void* stream) {
+    if (!mask || !solid || h < 1 || w < 1 || nx < 1 || ny < 1 || !(width > 0) || !(height > 0)) return CFD2D_E_ARG;
+    return status_of(launch_mask_image(nx, ny, dx, dy, solid, h, w, x0, y0, width, height, mask, as_stream(stream)));
+}
+
 size_t cfd2d_pcg_workspace_bytes(int nx, int ny) {
     return pcg_grid_workspace_doubles(nx, ny) * sizeof(double);
 }

@@ -199,6 +199,50 @@ __global__ void k_mask_rect(int nx, int ny, double dx, double dy, double xa, dou
     mask[i * ny + j] = (X >= xa && X <= xb && Y >= ya && Y <= yb) ? 1 : 0;
 }
 
+// Closed polygon (cfd2d/geometry.py:43-51, matplotlib Path.contains_points): crossing
+// test of a ray from the cell centre towards +x against every edge, the edge counted
+// when its end points lie on opposite sides of the centre's y (one side inclusive).
+__global__ void k_mask_polygon(int nx, int ny, double dx, double dy, const double* px, const double* py, int np,
+                               uint8_t* mask) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y * blockDim.y + threadIdx.y;
+    if (j >= ny || i >= nx) return;
+    const double X = ((double)i + 0.5) * dx, Y = ((double)j + 0.5) * dy;
+    bool inside = false;
+    double x0 = px[np - 1], y0 = py[np - 1];
+    bool above0 = y0 >= Y;
+    for (int k = 0; k < np; ++k) {
+        const double x1 = px[k], y1 = py[k];
+        const bool above1 = y1 >= Y;
+        if (above0 != above1) {
+            // the edge crosses the centre's row: is the crossing right of the centre?
+            if (((y1 - Y) * (x0 - x1) >= (x1 - X) * (y0 - y1)) == above1) inside = !inside;
+        }
+        x0 = x1;
+        y0 = y1;
+        above0 = above1;
+    }
+    mask[i * ny + j] = inside ? 1 : 0;
+}
+
+// Image obstacle (cfd2d/geometry.py:119-163): the cell centre's pixel of a solid
+// bitmap (h rows from the top, w columns) placed on [x0, x0 + width] x [y0, y0 + height]
+__global__ void k_mask_image(int nx, int ny, double dx, double dy, const uint8_t* solid, int h, int w, double x0,
+                             double y0, double width, double height, uint8_t* mask) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y * blockDim.y + threadIdx.y;
+    if (j >= ny || i >= nx) return;
+    const double X = ((double)i + 0.5) * dx, Y = ((double)j + 0.5) * dy;
+    const double sx = (X - x0) / width, sy = (Y - y0) / height;
+    const bool in = sx >= 0 && sx < 1 && sy >= 0 && sy < 1;
+    uint8_t m = 0;
+    if (in) {
+        long long col = (long long)(sx * (double)w), row = (long long)((1.0 - sy) * (double)h);
+        col = col < 0 ? 0 : (col > w - 1 ? w - 1 : col);
+        row = row < 0 ? 0 : (row > h - 1 ? h - 1 : row);
+        m = solid[row * w + col];
+    }
+    mask[i * ny + j] = m;
+}
+
 // ================================================================ domain boundary
 // cfd2d/boundary.py:143-223 in one block: the statement groups of the reference
 // (periodic copies; left/right; bottom/top; closing of blocked faces) depend on
@@ -1071,6 +1115,18 @@ cudaError_t launch_mask(int kind, int nx, int ny, double dx, double dy, const do
     if (kind == 0) k_mask_circle<<<grd, kTile, 0, s>>>(nx, ny, dx, dy, q[0], q[1], q[2], mask);
     else if (kind == 1) k_mask_ellipse<<<grd, kTile, 0, s>>>(nx, ny, dx, dy, q[0], q[1], q[2], q[3], q[4], q[5], mask);
     else k_mask_rect<<<grd, kTile, 0, s>>>(nx, ny, dx, dy, q[0], q[1], q[2], q[3], mask);
+    return last();
+}
+
+cudaError_t launch_mask_polygon(int nx, int ny, double dx, double dy, const double* px, const double* py, int np,
+                                uint8_t* mask, cudaStream_t s) {
+    k_mask_polygon<<<grid_rows(ny, nx), kTile, 0, s>>>(nx, ny, dx, dy, px, py, np, mask);
+    return last();
+}
+
+cudaError_t launch_mask_image(int nx, int ny, double dx, double dy, const uint8_t* solid, int h, int w, double x0,
+                              double y0, double width, double height, uint8_t* mask, cudaStream_t s) {
+    k_mask_image<<<grid_rows(ny, nx), kTile, 0, s>>>(nx, ny, dx, dy, solid, h, w, x0, y0, width, height, mask);
     return last();
 }
 

@@ -22,6 +22,10 @@ cudaError_t launch_scalar_transport(const double* phi, const double* u, const do
                                     cudaStream_t s);
 cudaError_t launch_mask(int kind, int nx, int ny, double dx, double dy, const double* prm,
                         uint8_t* mask, cudaStream_t s);
+cudaError_t launch_mask_polygon(int nx, int ny, double dx, double dy, const double* px, const double* py, int np,
+                                uint8_t* mask, cudaStream_t s);
+cudaError_t launch_mask_image(int nx, int ny, double dx, double dy, const uint8_t* solid, int h, int w, double x0,
+                              double y0, double width, double height, uint8_t* mask, cudaStream_t s);
 
 // step stages (all read step-varying scalars from S.state)
 cudaError_t stage_domain_bc(const cfd2d_sim& S, double* u, double* v, int begin, cudaStream_t s);

@@ -293,6 +293,20 @@ int cfd2d_mask_ellipse(int nx, int ny, double dx, double dy, double xc, double y
 int cfd2d_mask_rectangle(int nx, int ny, double dx, double dy, double xa, double ya, double xb,
                          double yb, uint8_t* mask, void* stream);
 
+/* Closed polygon with npts vertices (device arrays px, py; the last vertex joins the
+ * first): cell centres inside by the crossing test. Replaces cfd2d/geometry.py:43
+ * polygon(grid, points) (matplotlib Path.contains_points); NACA profiles
+ * (geometry.py:105 naca4) are polygons of their outline. */
+int cfd2d_mask_polygon(int nx, int ny, double dx, double dy, const double* px, const double* py, int npts,
+                       uint8_t* mask, void* stream);
+
+/* Image obstacle: `solid` is the h x w solid-pixel bitmap (row 0 at the top, device),
+ * placed on [x0, x0 + width] x [y0, y0 + height]; each cell centre takes its pixel.
+ * Replaces the pixel lookup of cfd2d/geometry.py:119 from_image (the image is decoded
+ * and thresholded on the host). */
+int cfd2d_mask_image(int nx, int ny, double dx, double dy, const uint8_t* solid, int h, int w, double x0, double y0,
+                     double width, double height, uint8_t* mask, void* stream);
+
 /* ---- pressure Poisson (drop-in for cfd2d/pressure.py) -------------------- */
 
 /* Bytes of scratch the solver needs for an nx x ny grid (cfd2d_poisson.work). */

@@ -29,7 +29,8 @@ __all__ = [
     "wall_adjacent_cells", "strain_rate_squared", "KAPPA", "cell_velocity", "cell_pressure",
     "cell_vorticity", "streamfunction", "available_fields", "field_data", "sample_u", "sample_v",
     "sample_field", "line_points", "OFieldAverage", "write_vtk_bytes",
-    "vof_advect", "OVOF", "dam_break", "rectangle_mask",
+    "vof_advect", "OVOF", "dam_break", "polygon_mask", "naca4_coordinates", "naca4_mask",
+    "image_solid_pixels", "image_mask",
 ]
 
 SIDES = ("left", "right", "bottom", "top")
@@ -144,8 +145,117 @@ def rectangle_mask(g, x0, y0, x1, y1):
     return (X >= xa) & (X <= xb) & (Y >= ya) & (Y <= yb)
 
 
+def polygon_mask(g, points):
+    """cfd2d/geometry.py:43-51: cell centres inside a closed polygon.
+
+    The reference asks matplotlib (>= 3.7, not installed here) for
+    ``Path(points).contains_points(centres)`` with radius 0. That is the crossings
+    test of E. Haines, "Point in Polygon Strategies" (Graphics Gems IV, 1994): a ray
+    from the point towards +x, an edge counted when its end points lie on opposite
+    sides (y >= Y against y < Y) and the sign test
+    ``(y1 - Y) (x0 - x1) >= (x1 - X) (y0 - y1)`` equals the side of the second end
+    point; the polygon is closed from the last point back to the first. Restated
+    here edge by edge over all centres at once."""
+    pts = np.asarray(points, dtype=float)
+    if pts.ndim != 2 or pts.shape[1] != 2 or len(pts) < 3:
+        raise ValueError("a polygon needs at least 3 points (x, y)")
+    X, Y = g.centres()
+    inside = np.zeros(X.shape, dtype=bool)
+    x0, y0 = pts[-1]
+    for x1, y1 in pts:
+        f0, f1 = y0 >= Y, y1 >= Y
+        hit = (f0 != f1) & (((y1 - Y) * (x0 - x1) >= (x1 - X) * (y0 - y1)) == f1)
+        inside ^= hit
+        x0, y0 = x1, y1
+    return inside
+
+
+def naca4_coordinates(code, chord=1.0, n=200, closed_te=True):
+    """cfd2d/geometry.py:54-102: outline of a NACA 4-digit section from the published
+    formulas (Abbott and von Doenhoff, Theory of Wing Sections, 1959): thickness
+    5 t (0.2969 sqrt(x) - 0.1260 x - 0.3516 x^2 + 0.2843 x^3 + a4 x^4), a4 = -0.1036
+    for a closed trailing edge, else -0.1015; camber line m/p^2 (2 p x - x^2) ahead of
+    p, m/(1-p)^2 ((1 - 2p) + 2 p x - x^2) behind it; the thickness is laid off normal
+    to the camber line. n cosine-spaced stations per side; the outline runs from the
+    trailing edge over the upper side to the nose and back along the lower side."""
+    code = str(code).strip()
+    if len(code) != 4 or not code.isdigit():
+        raise ValueError("a NACA code has exactly 4 digits")
+    m, p, t = int(code[0]) / 100.0, int(code[1]) / 10.0, int(code[2:]) / 100.0
+    if t <= 0:
+        raise ValueError("the thickness must be positive")
+    beta = np.linspace(0.0, np.pi, n)
+    x = 0.5 * (1.0 - np.cos(beta))
+    a4 = -0.1036 if closed_te else -0.1015
+    yt = 5 * t * (0.2969 * np.sqrt(x) - 0.1260 * x - 0.3516 * x**2 + 0.2843 * x**3 + a4 * x**4)
+    yc, dyc = np.zeros_like(x), np.zeros_like(x)
+    if m > 0 and p > 0:
+        f = x < p
+        b = ~f
+        yc[f] = m / p**2 * (2 * p * x[f] - x[f] ** 2)
+        dyc[f] = 2 * m / p**2 * (p - x[f])
+        yc[b] = m / (1 - p) ** 2 * ((1 - 2 * p) + 2 * p * x[b] - x[b] ** 2)
+        dyc[b] = 2 * m / (1 - p) ** 2 * (p - x[b])
+    th = np.arctan(dyc)
+    xu, yu = x - yt * np.sin(th), yc + yt * np.cos(th)
+    xl, yl = x + yt * np.sin(th), yc - yt * np.cos(th)
+    return np.column_stack([np.concatenate([xu[::-1], xl[1:]]) * chord,
+                            np.concatenate([yu[::-1], yl[1:]]) * chord])
+
+
+def naca4_mask(g, code, x_le, y_le, chord, angle_of_attack_deg=0.0):
+    # cfd2d/geometry.py:105-116: outline turned clockwise about the leading edge
+    pts = naca4_coordinates(code, chord)
+    a = np.deg2rad(angle_of_attack_deg)
+    xr = pts[:, 0] * np.cos(a) + pts[:, 1] * np.sin(a)
+    yr = -pts[:, 0] * np.sin(a) + pts[:, 1] * np.cos(a)
+    return polygon_mask(g, np.column_stack([xr + x_le, yr + y_le]))
+
+
+def image_solid_pixels(path, threshold=0.5, invert=False):
+    """cfd2d/geometry.py:136-149: solid pixels of an image file (PIL). Dark pixels
+    (mean grey < threshold) are solid; with an alpha channel opaque pixels are, and
+    where every pixel is opaque the dark opaque ones."""
+    from PIL import Image
+
+    img = Image.open(path)
+    if img.mode in ("RGBA", "LA") or (img.mode == "P" and "transparency" in img.info):
+        rgba = np.asarray(img.convert("RGBA"), dtype=float) / 255.0
+        grey = rgba[..., :3].mean(axis=2)
+        a = rgba[..., 3]
+        solid = (a > 0.5) & (grey < threshold) if a.min() > 0.5 else a > 0.5
+    else:
+        solid = np.asarray(img.convert("L"), dtype=float) / 255.0 < threshold
+    return ~solid if invert else solid
+
+
+def image_mask(g, path, x0=0.0, y0=0.0, width=None, height=None, threshold=0.5, invert=False):
+    """cfd2d/geometry.py:119-163: the bitmap laid on [x0, x0 + width] x
+    [y0, y0 + height] (the whole domain without width; the aspect ratio kept without
+    height); a centre inside takes the pixel at column floor(sx w), row
+    floor((1 - sy) h), clamped (row 0 is the top of the image)."""
+    from pathlib import Path as _P
+
+    if not _P(path).exists():
+        raise FileNotFoundError(path)
+    solid = image_solid_pixels(path, threshold, invert)
+    h, w = solid.shape
+    if width is None:
+        x0, y0, width, height = 0.0, 0.0, g.lx, g.ly
+    if height is None:
+        height = width * h / w
+    X, Y = g.centres()
+    sx, sy = (X - x0) / width, (Y - y0) / height
+    inside = (sx >= 0) & (sx < 1) & (sy >= 0) & (sy < 1)
+    col = np.clip((sx * w).astype(int), 0, w - 1)
+    row = np.clip(((1.0 - sy) * h).astype(int), 0, h - 1)
+    out = np.zeros(X.shape, dtype=bool)
+    out[inside] = solid[row[inside], col[inside]]
+    return out
+
+
 def obstacle_mask(g, spec):
-    # cfd2d/geometry.py:166-195 (the three analytic shapes)
+    # cfd2d/geometry.py:166-195
     typ = spec.get("typ", "").lower()
     if typ == "kreis":
         return circle_mask(g, spec["x"], spec["y"], spec["r"])
@@ -153,7 +263,15 @@ def obstacle_mask(g, spec):
         return ellipse_mask(g, spec["x"], spec["y"], spec["a"], spec["b"], spec.get("winkel", 0.0))
     if typ == "rechteck":
         return rectangle_mask(g, spec["x0"], spec["y0"], spec["x1"], spec["y1"])
-    raise ValueError(f"obstacle type {typ!r} not restated by the oracle")
+    if typ == "naca":
+        return naca4_mask(g, spec.get("code", "0012"), spec["x"], spec["y"], spec["sehne"],
+                          spec.get("winkel", 0.0))
+    if typ == "polygon":
+        return polygon_mask(g, spec["punkte"])
+    if typ == "bild":
+        return image_mask(g, spec["pfad"], spec.get("x", 0.0), spec.get("y", 0.0), spec.get("breite"),
+                          spec.get("hoehe"), spec.get("schwelle", 0.5), spec.get("invertieren", False))
+    raise ValueError(f"unknown obstacle type {typ!r}")
 
 
 # --------------------------------------------------------------------------- #

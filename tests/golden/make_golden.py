@@ -6,9 +6,10 @@ Run in a container that holds the reference checkout (default
     python tests/golden/make_golden.py [group ...]
 
 Groups: kernels geometry pressure cavity cylinder sst misc checkpoint smagorinsky
-functions vof validation (default: all).
+functions vof validation shapes (default: all).
 The reference imports matplotlib at module load; ``mplstub/`` stands in for it
-(no fixture case needs plotting or polygon masks). Every pressure solve uses the
+(no fixture case needs plotting or polygon masks; NACA outlines and image
+obstacles do not use it). Every pressure solve uses the
 reference's own ``PressureSolver`` (scipy CG or SuperLU) with
 ``sim.pressure.tol`` set after construction, exactly as a user of the reference
 would. Nothing at test time imports this script or the reference.
@@ -513,10 +514,57 @@ def gen_checkpoint():
     _save("golden_checkpoint", out)
 
 
+def _images():
+    """Synthetic obstacle images: grey, RGBA with transparency, RGBA fully opaque."""
+    rng = np.random.default_rng(91)
+    grey = np.full((50, 100), 255, dtype=np.uint8)
+    grey[10:40, 20:40] = 0
+    grey[5:12, 60:90] = 90
+    rgba = np.zeros((37, 53, 4), dtype=np.uint8)
+    rgba[..., :3] = rng.integers(0, 256, (37, 53, 3))
+    rgba[8:30, 10:45, 3] = 255
+    opaque = rng.integers(0, 256, (64, 48, 4)).astype(np.uint8)
+    opaque[..., 3] = 255
+    return {"grey": grey, "rgba": rgba, "opaque": opaque}
+
+
+def gen_shapes():
+    """NACA outlines and image obstacles from the reference (matplotlib is not
+    needed by either; polygon masks themselves need it and are not here)."""
+    import tempfile
+
+    from PIL import Image
+
+    out = {}
+    for k, (code, chord, n, closed) in enumerate((("0012", 1.0, 200, True), ("2412", 0.6, 200, True),
+                                                   ("4415", 1.3, 57, False), ("6409", 0.25, 200, True))):
+        out[f"naca{k}_spec"] = np.array([code, str(chord), str(n), str(int(closed))])
+        out[f"naca{k}_pts"] = geometry.naca4_coordinates(code, chord, n, closed)
+    imgs = _images()
+    cases_ = (("grey", (100, 50, 2.0, 1.0), {}),
+              ("grey", (80, 40, 2.0, 1.0), {"x0": 0.3, "y0": 0.1, "width": 1.1, "threshold": 0.4}),
+              ("grey", (61, 33, 1.0, 0.5), {"invert": True}),
+              ("rgba", (90, 70, 1.5, 1.0), {"x0": 0.2, "y0": 0.15, "width": 1.0, "height": 0.7}),
+              ("opaque", (64, 96, 1.0, 1.5), {"threshold": 0.6}))
+    with tempfile.TemporaryDirectory() as td:
+        for k, (name, (nx, ny, lx, ly), kw) in enumerate(cases_):
+            path = Path(td) / f"{name}.png"
+            Image.fromarray(imgs[name]).save(path)
+            g = Grid(nx, ny, lx, ly)
+            out[f"img{k}_name"] = np.array(name)
+            out[f"img{k}_grid"] = np.array([nx, ny, lx, ly])
+            out[f"img{k}_kw"] = np.array([f"{a}={b}" for a, b in kw.items()])
+            out[f"img{k}_mask"] = geometry.from_image(g, path, **kw)
+    out["n_naca"], out["n_img"] = np.array(4), np.array(len(cases_))
+    for name, arr in imgs.items():
+        out[f"pixels_{name}"] = arr
+    _save("golden_shapes", out)
+
+
 GROUPS = {"kernels": gen_kernels, "geometry": gen_geometry, "pressure": gen_pressure,
           "cavity": gen_cavity, "cylinder": gen_cylinder, "sst": gen_sst, "misc": gen_misc,
           "checkpoint": gen_checkpoint, "smagorinsky": gen_smagorinsky, "functions": gen_functions,
-          "vof": gen_vof, "validation": gen_validation}
+          "vof": gen_vof, "validation": gen_validation, "shapes": gen_shapes}
 
 if __name__ == "__main__":
     import warnings

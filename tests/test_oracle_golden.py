@@ -376,3 +376,100 @@ def test_vof_vtk_bytes_on_the_reference_state():
     vof.update_properties()
     sim.t = float(g["dam_t"])
     assert O.write_vtk_bytes(sim) == g["dam_vtk"].tobytes()
+
+
+# ---------------------------------------------------------------- polygon, NACA, image obstacles
+def _shape_image(g, k, tmp_path):
+    from PIL import Image
+
+    name = str(g[f"img{k}_name"])
+    path = tmp_path / f"{name}_{k}.png"
+    Image.fromarray(g[f"pixels_{name}"]).save(path)
+    kw = {}
+    for item in g[f"img{k}_kw"]:
+        a, b = str(item).split("=")
+        kw[a] = b == "True" if b in ("True", "False") else float(b)
+    return path, kw
+
+
+def test_naca_outline_and_image_masks_bitwise(tmp_path):
+    g = golden("golden_shapes")
+    for k in range(int(g["n_naca"])):
+        code, chord, n, closed = g[f"naca{k}_spec"]
+        pts = O.naca4_coordinates(str(code), float(chord), int(n), bool(int(closed)))
+        assert np.array_equal(pts, g[f"naca{k}_pts"]), k
+    for k in range(int(g["n_img"])):
+        nx, ny, lx, ly = g[f"img{k}_grid"]
+        path, kw = _shape_image(g, k, tmp_path)
+        og = O.OGrid(int(nx), int(ny), lx, ly)
+        m = O.image_mask(og, path, **kw)
+        assert np.array_equal(m, g[f"img{k}_mask"]), k
+
+
+def _exact_inside(points, X, Y):
+    """Crossing count in exact rational arithmetic for a point on no edge."""
+    from fractions import Fraction as F
+
+    pts = [(F(float(a)), F(float(b))) for a, b in points]
+    X, Y = F(float(X)), F(float(Y))
+    inside, on_edge = False, False
+    for (x0, y0), (x1, y1) in zip(pts[-1:] + pts[:-1], pts):
+        cross = (x1 - x0) * (Y - y0) - (y1 - y0) * (X - x0)
+        if cross == 0 and min(x0, x1) <= X <= max(x0, x1) and min(y0, y1) <= Y <= max(y0, y1):
+            on_edge = True
+        if (y0 > Y) != (y1 > Y):
+            xs = x0 + (Y - y0) * (x1 - x0) / (y1 - y0)
+            if xs > X:
+                inside = not inside
+    return inside, on_edge
+
+
+def test_polygon_crossing_test_against_exact_arithmetic():
+    """The restated crossings test (matplotlib's Path.contains_points, which the
+    reference calls, is not installed here) against an exact rational crossing count at
+    every cell centre that lies on no edge, for star-shaped and self-intersecting
+    polygons and NACA outlines."""
+    rng = np.random.default_rng(5)
+    og = O.OGrid(37, 29, 1.0, 0.8)
+    X, Y = og.centres()
+    polys = []
+    for n in (3, 5, 9, 17):
+        ang = np.sort(rng.uniform(0, 2 * np.pi, n))
+        r = rng.uniform(0.1, 0.38, n)
+        polys.append(np.column_stack([0.5 + r * np.cos(ang), 0.4 + r * np.sin(ang)]))
+    polys.append(rng.uniform(0.05, 0.95, (7, 2)) * [1.0, 0.8])  # self-intersecting
+    pts = O.naca4_coordinates("2412", 0.7)
+    a = np.deg2rad(12.0)
+    polys.append(np.column_stack([pts[:, 0] * np.cos(a) + pts[:, 1] * np.sin(a) + 0.15,
+                                  -pts[:, 0] * np.sin(a) + pts[:, 1] * np.cos(a) + 0.45]))
+    checked = 0
+    for P in polys:
+        m = O.polygon_mask(og, P)
+        for i in range(og.nx):
+            for j in range(og.ny):
+                inside, on_edge = _exact_inside(P, X[i, j], Y[i, j])
+                if not on_edge:
+                    assert m[i, j] == inside, (i, j)
+                    checked += 1
+    assert checked > 5000
+
+
+def test_reference_shape_tests_on_the_oracle(tmp_path):
+    """tests/test_cfd2d.py:121-145 of the reference on the restated shapes."""
+    from PIL import Image
+
+    pts = O.naca4_coordinates("0012", chord=1.0)
+    assert pts[:, 1].max() - pts[:, 1].min() == pytest.approx(0.12, rel=0.02)
+    og = O.OGrid(200, 100, 2.0, 1.0)
+    m = O.naca4_mask(og, "0012", 0.5, 0.5, 1.0, 0.0)
+    assert m.sum() * og.dx * og.dy == pytest.approx(0.0822, rel=0.05)
+    img = np.full((50, 100), 255, dtype=np.uint8)
+    img[10:40, 20:40] = 0
+    path = tmp_path / "hindernis.png"
+    Image.fromarray(img).save(path)
+    og = O.OGrid(100, 50, 2.0, 1.0)
+    m = O.image_mask(og, path)
+    assert m.sum() == pytest.approx(30 * 20, rel=0.05)
+    yc = (np.arange(og.ny) + 0.5) * og.dy
+    ys = yc[np.where(m.any(axis=0))[0]]
+    assert ys.min() == pytest.approx(0.2, abs=0.03) and ys.max() == pytest.approx(0.8, abs=0.03)
