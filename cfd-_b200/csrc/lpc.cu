@@ -4,13 +4,14 @@
 // Activations are BF16 in NHWC layout (pixel = MAC cell (i, j) flattened as
 // i*W + j with j contiguous, 32 channels innermost); every product is accumulated
 // in FP32. The 32 -> 32 channel 3x3 convolutions (the FLOP-heavy layers) are
-// implicit GEMMs on the 5th-generation tensor cores: per CTA a tile of 128
-// consecutive pixels of one grid row (M = 128), N = 32 output channels,
-// K = 9 taps x 32 input channels = 288, issued as 18 tcgen05.mma (kind::f16, BF16
-// inputs, FP32 accumulator in tensor memory) by one thread; operands are staged in
-// shared memory in the K-major no-swizzle core-matrix layout (8 rows x 16 bytes
-// per core matrix) described by UMMA shared-memory descriptors; the epilogue reads
-// the accumulator with tcgen05.ld and fuses bias, skip addition, ReLU and the
+// implicit GEMMs on the 5th-generation tensor cores: per CTA four grid rows of 128
+// consecutive pixels (M = 128 per row), N = 32 output channels, K = 9 taps x 32
+// input channels = 288, issued as 18 tcgen05.mma per row (kind::f16, BF16 inputs,
+// FP32 accumulator in tensor memory) by one thread; the input rows are staged once
+// in shared memory in a layout where every tap is a K-major no-swizzle operand
+// (8 rows x 16 bytes per core matrix) at its own descriptor offset, so no im2col
+// copy is made; the epilogue reads the accumulators with tcgen05.ld and fuses bias,
+// skip addition, ReLU and the
 // fluid mask. The 1-channel layers, pooling, upsampling and the backward pass run
 // on CUDA cores with FP32 accumulation.
 //
@@ -32,7 +33,6 @@ constexpr int KDIM = 9 * CH;            // 288
 constexpr int TM = 128;                 // pixels per tile
 constexpr int CORE_BYTES = 128;         // one core matrix: 8 rows x 16 bytes
 constexpr int SBO = (KDIM / 8) * CORE_BYTES;  // 4608 bytes between 8-row groups
-constexpr int A_BYTES = (TM / 8) * SBO;       // 73728
 constexpr int B_BYTES = (CH / 8) * SBO;       // 18432
 constexpr uint32_t kWaitLimit = 1u << 24;
 
@@ -65,6 +65,30 @@ __device__ __forceinline__ float bf2f(__nv_bfloat16 x) { return __bfloat162float
 // ---------------------------------------------------------------- 32 -> 32 conv (tensor cores)
 // y[p][n] = act(bias[n] + sum_{tap, c} w[n][c][tap] * x[p + tap][c] (+ skip[p][n])), masked.
 // wpack is the B operand image (N = 32 rows, K = 288) in the shared-memory layout.
+//
+// One CTA computes ROWS output rows i0 .. i0+ROWS-1 of one 128-pixel segment
+// j0 .. j0+127. The ROWS + 2 input rows it needs, pixels j0-1 .. j0+128 (XP = 130,
+// zero outside the grid), are copied once into shared memory, channel-chunk major:
+// chunk c (channels 8c .. 8c+7, 16 bytes) of pixel q of staged row r sits at
+// r*XROW + c*XCHUNK + q*16. In that layout the A operand of tap (di, dj) for output
+// row r is already a K-major no-swizzle matrix: pixel m of the tile is 16 bytes after
+// pixel m-1 (8-row groups 128 bytes apart: SBO = 128) and the two 8-channel core
+// matrices of one 16-channel MMA step are XCHUNK apart (LBO = XCHUNK), starting at
+// (r + di + 1)*XROW + 2h*XCHUNK + (dj + 1)*16. So the nine taps are nine descriptor
+// offsets into the same staged rows, with no im2col copy; each output row takes 18
+// MMAs into its own 32 TMEM columns, and one commit covers all ROWS*18.
+constexpr int ROWS = 4;
+constexpr int XP = TM + 2;
+constexpr int XCHUNK = XP * 16;            // 2080
+constexpr int XROW = 4 * XCHUNK;           // 8320
+constexpr int X_BYTES = (ROWS + 2) * XROW; // 49920
+constexpr int XQ = (ROWS + 2) * XP * 4;    // 16-byte chunks staged per CTA (3120)
+constexpr int XPER = (XQ + TM - 1) / TM;   // per thread (25)
+constexpr int XB = 13;                     // loads in flight per thread and batch
+constexpr uint32_t kTmemCols = 32 * ROWS;  // 128 (a power of two >= 32)
+static_assert(B_BYTES / 16 % TM == 0, "the B image splits evenly over the threads");
+static_assert((kTmemCols & (kTmemCols - 1)) == 0 && kTmemCols >= 32 && kTmemCols <= 512, "TMEM columns");
+
 __global__ void __launch_bounds__(TM) k_conv32_tc(const __nv_bfloat16* __restrict__ x,
                                                   const uint4* __restrict__ wpack,
                                                   const float* __restrict__ bias,
@@ -73,18 +97,18 @@ __global__ void __launch_bounds__(TM) k_conv32_tc(const __nv_bfloat16* __restric
                                                   __nv_bfloat16* __restrict__ y, int H, int W,
                                                   int relu, int* __restrict__ err) {
     extern __shared__ __align__(1024) uint8_t smem[];
-    uint8_t* As = smem;
-    uint8_t* Bs = smem + A_BYTES;
+    uint8_t* Bs = smem;            // 18432 bytes, offset 0
+    uint8_t* Xs = smem + B_BYTES;  // 49920 bytes, 16-byte aligned
     __shared__ __align__(8) uint64_t mbar;
     __shared__ uint32_t tmem_slot;
     __shared__ int ok;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int i = blockIdx.y;
+    const int i0 = blockIdx.y * ROWS;
     const int j0 = blockIdx.x * TM;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
-                     "r"(32));
+                     "r"(kTmemCols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0) {
@@ -92,23 +116,37 @@ __global__ void __launch_bounds__(TM) k_conv32_tc(const __nv_bfloat16* __restric
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         ok = 1;
     }
-    // B operand: a straight copy of the prepacked image
-    for (int q = tid; q < B_BYTES / 16; q += TM) reinterpret_cast<uint4*>(Bs)[q] = wpack[q];
-    // A operand: row m = pixel (i, j0 + m); K index k = tap * 32 + c, tap = (di+1)*3 + (dj+1)
+    // B operand: a straight copy of the prepacked image, all loads of a thread in flight
     {
-        const int m = tid;
-        const int j = j0 + m;
-        uint8_t* rowbase = As + (m >> 3) * SBO + (m & 7) * 16;
+        uint4 v[B_BYTES / 16 / TM];
 #pragma unroll
-        for (int tap = 0; tap < 9; ++tap) {
-            const int ii = i + tap / 3 - 1, jj = j + tap % 3 - 1;
-            const bool in = (j < W) && ii >= 0 && ii < H && jj >= 0 && jj < W;
-            const uint4* src = reinterpret_cast<const uint4*>(x + ((size_t)ii * W + jj) * CH);
+        for (int k = 0; k < B_BYTES / 16 / TM; ++k) v[k] = wpack[tid + k * TM];
 #pragma unroll
-            for (int c8 = 0; c8 < 4; ++c8) {
-                uint4 v = make_uint4(0u, 0u, 0u, 0u);
-                if (in) v = src[c8];
-                *reinterpret_cast<uint4*>(rowbase + (tap * 4 + c8) * CORE_BYTES) = v;
+        for (int k = 0; k < B_BYTES / 16 / TM; ++k) reinterpret_cast<uint4*>(Bs)[tid + k * TM] = v[k];
+    }
+    // staged input rows: consecutive threads take consecutive 16-byte chunks in global
+    // order (chunk fastest, then pixel), so each warp reads 512 contiguous bytes; the
+    // loads go out in batches of XB per thread before their shared-memory stores
+#pragma unroll
+    for (int k0 = 0; k0 < XPER; k0 += XB) {
+        uint4 v[XB];
+#pragma unroll
+        for (int k = 0; k < XB; ++k) {
+            const int q = tid + (k0 + k) * TM;
+            const int c = q & 3, t = q >> 2;
+            const int r = t / XP, px = t - r * XP;
+            const int ii = i0 - 1 + r, jj = j0 - 1 + px;
+            v[k] = make_uint4(0u, 0u, 0u, 0u);
+            if (k0 + k < XPER && q < XQ && ii >= 0 && ii < H && jj >= 0 && jj < W)
+                v[k] = reinterpret_cast<const uint4*>(x + ((size_t)ii * W + jj) * CH)[c];
+        }
+#pragma unroll
+        for (int k = 0; k < XB; ++k) {
+            const int q = tid + (k0 + k) * TM;
+            if (k0 + k < XPER && q < XQ) {
+                const int c = q & 3, t = q >> 2;
+                const int r = t / XP, px = t - r * XP;
+                *reinterpret_cast<uint4*>(Xs + r * XROW + c * XCHUNK + px * 16) = v[k];
             }
         }
     }
@@ -119,22 +157,27 @@ __global__ void __launch_bounds__(TM) k_conv32_tc(const __nv_bfloat16* __restric
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_slot;
     if (tid == 0) {
-        const uint32_t a0 = smem_u32(As), b0 = smem_u32(Bs);
+        const uint32_t x0 = smem_u32(Xs), b0 = smem_u32(Bs);
+        for (int r = 0; r < ROWS; ++r) {
 #pragma unroll
-        for (int s = 0; s < KDIM / 16; ++s) {
-            const uint64_t ad = umma_desc(a0 + s * 2 * CORE_BYTES, CORE_BYTES, SBO);
-            const uint64_t bd = umma_desc(b0 + s * 2 * CORE_BYTES, CORE_BYTES, SBO);
-            const uint32_t acc = s > 0 ? 1u : 0u;
-            asm volatile(
-                "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
-                "l"(ad), "l"(bd), "r"(kIdesc), "r"(acc));
+            for (int s = 0; s < KDIM / 16; ++s) {
+                const int tap = s >> 1, h = s & 1;
+                const int di = tap / 3, dj = tap % 3;  // di, dj in 0..2 stand for -1..1
+                const uint32_t aaddr = x0 + (uint32_t)((r + di) * XROW + 2 * h * XCHUNK + dj * 16);
+                const uint64_t ad = umma_desc(aaddr, XCHUNK, CORE_BYTES);
+                const uint64_t bd = umma_desc(b0 + s * 2 * CORE_BYTES, CORE_BYTES, SBO);
+                const uint32_t acc = s > 0 ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem + (uint32_t)(32 * r)),
+                    "l"(ad), "l"(bd), "r"(kIdesc), "r"(acc));
+            }
         }
         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                          smem_u32(&mbar))
                      : "memory");
     }
-    // bounded wait for the accumulator
+    // bounded wait for the accumulators
     {
         uint32_t done = 0;
         for (uint32_t spin = 0; spin < kWaitLimit && !done; ++spin) {
@@ -152,41 +195,50 @@ __global__ void __launch_bounds__(TM) k_conv32_tc(const __nv_bfloat16* __restric
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (ok) {
-        float acc[CH];
-#pragma unroll
-        for (int c0 = 0; c0 < CH; c0 += 8) {
-            uint32_t r[8];
-            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
-            asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-                         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
-                           "=r"(r[6]), "=r"(r[7])
-                         : "r"(taddr));
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-            for (int q = 0; q < 8; ++q) acc[c0 + q] = __uint_as_float(r[q]);
-        }
         const int m = warp * 32 + lane;
         const int j = j0 + m;
-        if (j < W) {
-            const size_t p = (size_t)i * W + j;
-            const bool fl = mask ? (mask[p] != 0) : true;
-            __align__(16) __nv_bfloat16 out[CH];
+        for (int r = 0; r < ROWS; ++r) {
+            float acc[CH];
 #pragma unroll
-            for (int n = 0; n < CH; ++n) {
-                float v = acc[n] + bias[n];
-                if (skip) v += bf2f(skip[p * CH + n]);
-                if (relu) v = fmaxf(v, 0.0f);
-                out[n] = __float2bfloat16(fl ? v : 0.0f);
+            for (int c0 = 0; c0 < CH; c0 += 8) {
+                uint32_t v[8];
+                const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(32 * r + c0);
+                asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                             : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+                               "=r"(v[6]), "=r"(v[7])
+                             : "r"(taddr));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                for (int q = 0; q < 8; ++q) acc[c0 + q] = __uint_as_float(v[q]);
             }
-            uint4* dst = reinterpret_cast<uint4*>(y + p * CH);
+            const int i = i0 + r;
+            if (j < W && i < H) {
+                const size_t p = (size_t)i * W + j;
+                const bool fl = mask ? (mask[p] != 0) : true;
+                __align__(16) __nv_bfloat16 sk[CH];
+                if (skip) {
 #pragma unroll
-            for (int q = 0; q < 4; ++q) dst[q] = reinterpret_cast<const uint4*>(out)[q];
+                    for (int q = 0; q < 4; ++q)
+                        reinterpret_cast<uint4*>(sk)[q] = reinterpret_cast<const uint4*>(skip + p * CH)[q];
+                }
+                __align__(16) __nv_bfloat16 out[CH];
+#pragma unroll
+                for (int n = 0; n < CH; ++n) {
+                    float val = acc[n] + bias[n];
+                    if (skip) val += bf2f(sk[n]);
+                    if (relu) val = fmaxf(val, 0.0f);
+                    out[n] = __float2bfloat16(fl ? val : 0.0f);
+                }
+                uint4* dst = reinterpret_cast<uint4*>(y + p * CH);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) dst[q] = reinterpret_cast<const uint4*>(out)[q];
+            }
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0) {
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(32));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
     }
 }
 
@@ -246,34 +298,114 @@ __global__ void k_conv_generic(const void* __restrict__ x, int xbf, const float*
     }
 }
 
+// Forward 1 -> 32 layer (FP32 input, BF16 output) and 32 -> 1 layer (BF16 input,
+// FP32 output): one thread per pixel, 16-byte channel vectors, the 288 weights
+// broadcast from shared memory. Taps and channels are summed in the same order as
+// k_conv_generic, so both give the same bits.
+__global__ void k_conv_1to32(const float* __restrict__ x, const float* __restrict__ w,
+                             const float* __restrict__ bias, const uint8_t* __restrict__ mask,
+                             __nv_bfloat16* __restrict__ y, int H, int W, int relu) {
+    __shared__ float ws[CH * 9];
+    for (int e = threadIdx.x; e < CH * 9; e += blockDim.x) ws[e] = w[e];
+    __syncthreads();
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= H * W) return;
+    const int i = p / W, j = p - (p / W) * W;
+    float acc[CH];
+#pragma unroll
+    for (int o = 0; o < CH; ++o) acc[o] = bias ? bias[o] : 0.0f;
+#pragma unroll
+    for (int tap = 0; tap < 9; ++tap) {
+        const int ii = i + tap / 3 - 1, jj = j + tap % 3 - 1;
+        if (ii < 0 || ii >= H || jj < 0 || jj >= W) continue;
+        const float xv = x[(size_t)ii * W + jj];
+#pragma unroll
+        for (int o = 0; o < CH; ++o) acc[o] += ws[o * 9 + tap] * xv;
+    }
+    const bool fl = mask ? (mask[p] != 0) : true;
+    __align__(16) __nv_bfloat16 out[CH];
+#pragma unroll
+    for (int o = 0; o < CH; ++o) {
+        float v = acc[o];
+        if (relu) v = fmaxf(v, 0.0f);
+        out[o] = __float2bfloat16(fl ? v : 0.0f);
+    }
+    uint4* dst = reinterpret_cast<uint4*>(y + (size_t)p * CH);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) dst[q] = reinterpret_cast<const uint4*>(out)[q];
+}
+
+__global__ void k_conv_32to1(const __nv_bfloat16* __restrict__ x, const float* __restrict__ w,
+                             const float* __restrict__ bias, const uint8_t* __restrict__ mask,
+                             float* __restrict__ y, int H, int W, int relu) {
+    __shared__ float ws[CH * 9];
+    for (int e = threadIdx.x; e < CH * 9; e += blockDim.x) ws[e] = w[e];
+    __syncthreads();
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= H * W) return;
+    const int i = p / W, j = p - (p / W) * W;
+    float acc = bias ? bias[0] : 0.0f;
+#pragma unroll
+    for (int tap = 0; tap < 9; ++tap) {
+        const int ii = i + tap / 3 - 1, jj = j + tap % 3 - 1;
+        if (ii < 0 || ii >= H || jj < 0 || jj >= W) continue;
+        const uint4* src = reinterpret_cast<const uint4*>(x + ((size_t)ii * W + jj) * CH);
+        uint4 v[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) v[q] = src[q];
+        const __nv_bfloat16* xv = reinterpret_cast<const __nv_bfloat16*>(v);
+#pragma unroll
+        for (int c = 0; c < CH; ++c) acc += ws[c * 9 + tap] * bf2f(xv[c]);
+    }
+    if (relu) acc = fmaxf(acc, 0.0f);
+    const bool fl = mask ? (mask[p] != 0) : true;
+    y[p] = fl ? acc : 0.0f;
+}
+
 // ---------------------------------------------------------------- pooling, upsampling
-// coarse (Hc, Wc) = (ceil(H/2), ceil(W/2)): mean of the in-range children
+// coarse (Hc, Wc) = (ceil(H/2), ceil(W/2)): mean of the in-range children; one thread
+// per 8 channels of a coarse pixel (one 16-byte vector)
 __global__ void k_pool2(const __nv_bfloat16* __restrict__ x, __nv_bfloat16* __restrict__ y, int H, int W) {
     const int Hc = (H + 1) / 2, Wc = (W + 1) / 2;
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= Hc * Wc * CH) return;
-    const int c = e % CH, q = e / CH;
-    const int ic = q / Wc, jc = q % Wc;
-    float s = 0.0f;
+    if (e >= Hc * Wc * (CH / 8)) return;
+    const int c8 = e & 3, q = e >> 2;
+    const int ic = q / Wc, jc = q - (q / Wc) * Wc;
+    float s[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     int n = 0;
     for (int a = 0; a < 2; ++a)
         for (int b = 0; b < 2; ++b) {
             const int i = 2 * ic + a, j = 2 * jc + b;
-            if (i < H && j < W) { s += bf2f(x[((size_t)i * W + j) * CH + c]); ++n; }
+            if (i < H && j < W) {
+                const uint4 v = reinterpret_cast<const uint4*>(x + ((size_t)i * W + j) * CH)[c8];
+                const __nv_bfloat16* h = reinterpret_cast<const __nv_bfloat16*>(&v);
+#pragma unroll
+                for (int k = 0; k < 8; ++k) s[k] += bf2f(h[k]);
+                ++n;
+            }
         }
-    y[e] = __float2bfloat16(s / (float)n);
+    __align__(16) __nv_bfloat16 out[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) out[k] = __float2bfloat16(s[k] / (float)n);
+    reinterpret_cast<uint4*>(y)[e] = *reinterpret_cast<const uint4*>(out);
 }
 
-// y[p] = coarse[parent(p)] + skip[p]
+// y[p] = coarse[parent(p)] + skip[p]; one thread per 8 channels of a pixel
 __global__ void k_upadd(const __nv_bfloat16* __restrict__ coarse, const __nv_bfloat16* __restrict__ skip,
                         __nv_bfloat16* __restrict__ y, int H, int W) {
     const int Wc = (W + 1) / 2;
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= H * W * CH) return;
-    const int c = e % CH, p = e / CH;
-    const int i = p / W, j = p % W;
-    const float v = bf2f(coarse[((size_t)(i / 2) * Wc + j / 2) * CH + c]) + bf2f(skip[e]);
-    y[e] = __float2bfloat16(v);
+    if (e >= H * W * (CH / 8)) return;
+    const int c8 = e & 3, p = e >> 2;
+    const int i = p / W, j = p - (p / W) * W;
+    const uint4 cv = reinterpret_cast<const uint4*>(coarse + ((size_t)(i / 2) * Wc + j / 2) * CH)[c8];
+    const uint4 sv = reinterpret_cast<const uint4*>(skip)[e];
+    const __nv_bfloat16* ch = reinterpret_cast<const __nv_bfloat16*>(&cv);
+    const __nv_bfloat16* sh = reinterpret_cast<const __nv_bfloat16*>(&sv);
+    __align__(16) __nv_bfloat16 out[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) out[k] = __float2bfloat16(bf2f(ch[k]) + bf2f(sh[k]));
+    reinterpret_cast<uint4*>(y)[e] = *reinterpret_cast<const uint4*>(out);
 }
 
 // coarse mask: any child fluid
@@ -377,7 +509,7 @@ namespace {
 inline int cdiv(long long a, int b) { return (int)((a + b - 1) / b); }
 }  // namespace
 
-size_t conv32_smem_bytes() { return (size_t)A_BYTES + B_BYTES; }
+size_t conv32_smem_bytes() { return (size_t)B_BYTES + X_BYTES; }
 
 cudaError_t conv32_tc(const __nv_bfloat16* x, const __nv_bfloat16* wpack, const float* bias,
                       const __nv_bfloat16* skip, const uint8_t* mask, __nv_bfloat16* y, int H, int W, int relu,
@@ -389,7 +521,7 @@ cudaError_t conv32_tc(const __nv_bfloat16* x, const __nv_bfloat16* wpack, const 
         if (e != cudaSuccess) return e;
         configured = true;
     }
-    dim3 grid(cdiv(W, TM), H);
+    dim3 grid(cdiv(W, TM), cdiv(H, ROWS));
     k_conv32_tc<<<grid, TM, conv32_smem_bytes(), s>>>(x, reinterpret_cast<const uint4*>(wpack), bias, skip,
                                                       mask, y, H, W, relu, err);
     return cudaGetLastError();
@@ -405,6 +537,16 @@ cudaError_t conv_generic(int cin, int cout, const void* x, int xbf, const float*
                          cudaStream_t s) {
     const int n = H * W;
     const int blk = 128;
+    if (!transposed && cin == 1 && cout == 32 && !xbf && ybf) {
+        k_conv_1to32<<<cdiv(n, blk), blk, 0, s>>>(static_cast<const float*>(x), w, bias, mask,
+                                                   static_cast<__nv_bfloat16*>(y), H, W, relu);
+        return cudaGetLastError();
+    }
+    if (!transposed && cin == 32 && cout == 1 && xbf && !ybf) {
+        k_conv_32to1<<<cdiv(n, blk), blk, 0, s>>>(static_cast<const __nv_bfloat16*>(x), w, bias, mask,
+                                                   static_cast<float*>(y), H, W, relu);
+        return cudaGetLastError();
+    }
     if (cin == 1 && cout == 32)
         k_conv_generic<1, 32><<<cdiv(n, blk), blk, 0, s>>>(x, xbf, w, bias, mask, y, ybf, H, W, relu, transposed);
     else if (cin == 32 && cout == 1)
@@ -417,7 +559,7 @@ cudaError_t conv_generic(int cin, int cout, const void* x, int xbf, const float*
 }
 
 cudaError_t pool2(const __nv_bfloat16* x, __nv_bfloat16* y, int H, int W, cudaStream_t s) {
-    const int n = ((H + 1) / 2) * ((W + 1) / 2) * CH;
+    const int n = ((H + 1) / 2) * ((W + 1) / 2) * (CH / 8);
     k_pool2<<<cdiv(n, 256), 256, 0, s>>>(x, y, H, W);
     return cudaGetLastError();
 }
@@ -430,7 +572,7 @@ cudaError_t pool_mask(const uint8_t* m, uint8_t* mc, int H, int W, cudaStream_t 
 
 cudaError_t upadd(const __nv_bfloat16* coarse, const __nv_bfloat16* skip, __nv_bfloat16* y, int H, int W,
                   cudaStream_t s) {
-    k_upadd<<<cdiv((long long)H * W * CH, 256), 256, 0, s>>>(coarse, skip, y, H, W);
+    k_upadd<<<cdiv((long long)H * W * (CH / 8), 256), 256, 0, s>>>(coarse, skip, y, H, W);
     return cudaGetLastError();
 }
 

@@ -84,6 +84,47 @@ def test_cuda_core_conv_and_adjoint(L, cin, cout):
     assert abs(lhs - rhs) <= 1e-4 * max(abs(lhs), 1.0)
 
 
+def test_forward_fast_paths_match_the_generic_kernel(L):
+    """The forward 1 -> 32 (FP32 in, BF16 out) and 32 -> 1 (BF16 in, FP32 out) layers
+    take their own vectorised kernels; they give the generic kernel's bits and agree
+    with torch."""
+    torch, _lib, learned = L
+    F = torch.nn.functional
+    H, W = 37, 141
+    g = torch.Generator().manual_seed(7)
+    dev = _lib.device()
+    lib = _lib.lib()
+    m = torch.from_numpy(_random_mask(H, W, 3)).to(dev)
+    # 1 -> 32, ReLU, mask
+    x = torch.randn((H, W, 1), generator=g).to(dev)
+    w = (torch.randn((32, 1, 3, 3), generator=g) * 0.3).to(dev).contiguous()
+    b = (torch.randn(32, generator=g) * 0.1).to(dev)
+    fast = torch.zeros((H, W, 32), dtype=torch.bfloat16, device=dev)
+    gen = torch.zeros((H, W, 32), device=dev)
+    P = _lib.ptr
+    _lib.check(lib.cfd2d_lpc_conv(1, 32, P(x), 0, P(w), P(b), P(m), P(fast), 1, H, W, 1, 0, _lib.stream_ptr()), "1to32")
+    _lib.check(lib.cfd2d_lpc_conv(1, 32, P(x), 0, P(w), P(b), P(m), P(gen), 0, H, W, 1, 0, _lib.stream_ptr()), "gen")
+    assert torch.equal(fast, gen.to(torch.bfloat16))
+    ref = torch.relu(F.conv2d(x.cpu().permute(2, 0, 1)[None], w.cpu(), b.cpu(), padding=1)[0].permute(1, 2, 0))
+    ref = ref * m.cpu()[..., None]
+    assert relerr(fast.float().cpu(), ref) < 1e-2
+    # 32 -> 1, no ReLU, mask
+    xb = torch.randn((H, W, 32), generator=g).to(torch.bfloat16).to(dev)
+    w1 = (torch.randn((1, 32, 3, 3), generator=g) * 0.1).to(dev).contiguous()
+    b1 = (torch.randn(1, generator=g) * 0.1).to(dev)
+    fast1 = torch.zeros((H, W, 1), device=dev)
+    gen1 = torch.zeros((H, W, 1), device=dev)
+    xf = xb.float().contiguous()
+    _lib.check(lib.cfd2d_lpc_conv(32, 1, P(xb), 1, P(w1), P(b1), P(m), P(fast1), 0, H, W, 0, 0, _lib.stream_ptr()),
+               "32to1")
+    _lib.check(lib.cfd2d_lpc_conv(32, 1, P(xf), 0, P(w1), P(b1), P(m), P(gen1), 0, H, W, 0, 0, _lib.stream_ptr()),
+               "gen")
+    assert torch.equal(fast1, gen1)
+    ref1 = F.conv2d(xf.cpu().permute(2, 0, 1)[None], w1.cpu(), b1.cpu(), padding=1)[0].permute(1, 2, 0)
+    ref1 = ref1 * m.cpu()[..., None]
+    assert relerr(fast1.cpu(), ref1) < 1e-5
+
+
 def _random_mask(H, W, seed):
     rng = np.random.default_rng(seed)
     m = np.ones((H, W), dtype=np.uint8)
