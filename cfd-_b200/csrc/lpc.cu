@@ -66,7 +66,7 @@ __device__ __forceinline__ float bf2f(__nv_bfloat16 x) { return __bfloat162float
 // y[p][n] = act(bias[n] + sum_{tap, c} w[n][c][tap] * x[p + tap][c] (+ skip[p][n])), masked.
 // wpack is the B operand image (N = 32 rows, K = 288) in the shared-memory layout.
 //
-// One CTA computes ROWS output rows i0 .. i0+ROWS-1 of one 128-pixel segment
+// One CTA computes ROWS (1, 2 or 4) output rows i0 .. i0+ROWS-1 of one 128-pixel segment
 // j0 .. j0+127. The ROWS + 2 input rows it needs, pixels j0-1 .. j0+128 (XP = 130,
 // zero outside the grid), are copied once into shared memory, channel-chunk major:
 // chunk c (channels 8c .. 8c+7, 16 bytes) of pixel q of staged row r sits at
@@ -77,18 +77,14 @@ __device__ __forceinline__ float bf2f(__nv_bfloat16 x) { return __bfloat162float
 // (r + di + 1)*XROW + 2h*XCHUNK + (dj + 1)*16. So the nine taps are nine descriptor
 // offsets into the same staged rows, with no im2col copy; each output row takes 18
 // MMAs into its own 32 TMEM columns, and one commit covers all ROWS*18.
-constexpr int ROWS = 4;
 constexpr int XP = TM + 2;
 constexpr int XCHUNK = XP * 16;            // 2080
 constexpr int XROW = 4 * XCHUNK;           // 8320
-constexpr int X_BYTES = (ROWS + 2) * XROW; // 49920
-constexpr int XQ = (ROWS + 2) * XP * 4;    // 16-byte chunks staged per CTA (3120)
-constexpr int XPER = (XQ + TM - 1) / TM;   // per thread (25)
 constexpr int XB = 13;                     // loads in flight per thread and batch
-constexpr uint32_t kTmemCols = 32 * ROWS;  // 128 (a power of two >= 32)
 static_assert(B_BYTES / 16 % TM == 0, "the B image splits evenly over the threads");
-static_assert((kTmemCols & (kTmemCols - 1)) == 0 && kTmemCols >= 32 && kTmemCols <= 512, "TMEM columns");
+constexpr int x_bytes(int rows) { return (rows + 2) * XROW; }
 
+template <int ROWS>
 __global__ void __launch_bounds__(TM) k_conv32_tc(const __nv_bfloat16* __restrict__ x,
                                                   const uint4* __restrict__ wpack,
                                                   const float* __restrict__ bias,
@@ -96,9 +92,13 @@ __global__ void __launch_bounds__(TM) k_conv32_tc(const __nv_bfloat16* __restric
                                                   const uint8_t* __restrict__ mask,
                                                   __nv_bfloat16* __restrict__ y, int H, int W,
                                                   int relu, int* __restrict__ err) {
+    constexpr int XQ = (ROWS + 2) * XP * 4;    // 16-byte chunks staged per CTA
+    constexpr int XPER = (XQ + TM - 1) / TM;   // per thread
+    constexpr uint32_t kTmemCols = 32u * ROWS;
+    static_assert((kTmemCols & (kTmemCols - 1)) == 0 && kTmemCols >= 32 && kTmemCols <= 512, "TMEM columns");
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t* Bs = smem;            // 18432 bytes, offset 0
-    uint8_t* Xs = smem + B_BYTES;  // 49920 bytes, 16-byte aligned
+    uint8_t* Xs = smem + B_BYTES;  // x_bytes(ROWS) bytes, 16-byte aligned
     __shared__ __align__(8) uint64_t mbar;
     __shared__ uint32_t tmem_slot;
     __shared__ int ok;
@@ -195,9 +195,27 @@ __global__ void __launch_bounds__(TM) k_conv32_tc(const __nv_bfloat16* __restric
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (ok) {
+        // The MMAs have finished reading the staged rows, so their buffer stages the
+        // epilogue: 128 pixels x 80 bytes per output row (skip input in, result out),
+        // read and written in global memory as contiguous 16-byte chunks.
         const int m = warp * 32 + lane;
         const int j = j0 + m;
+        const int npx = min(TM, W - j0);
+        uint4* st = reinterpret_cast<uint4*>(Xs);
+        const uint4* skip4 = reinterpret_cast<const uint4*>(skip);
+        uint4* y4 = reinterpret_cast<uint4*>(y);
         for (int r = 0; r < ROWS; ++r) {
+            const int i = i0 + r;
+            if (i >= H) break;
+            const size_t rowp = (size_t)i * W + j0;
+            if (skip) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int q = tid + k * TM, px = q >> 2;
+                    if (px < npx) st[px * 5 + (q & 3)] = skip4[(rowp + px) * 4 + (q & 3)];
+                }
+            }
+            __syncthreads();
             float acc[CH];
 #pragma unroll
             for (int c0 = 0; c0 < CH; c0 += 8) {
@@ -211,15 +229,13 @@ __global__ void __launch_bounds__(TM) k_conv32_tc(const __nv_bfloat16* __restric
 #pragma unroll
                 for (int q = 0; q < 8; ++q) acc[c0 + q] = __uint_as_float(v[q]);
             }
-            const int i = i0 + r;
-            if (j < W && i < H) {
-                const size_t p = (size_t)i * W + j;
+            if (j < W) {
+                const size_t p = rowp + m;
                 const bool fl = mask ? (mask[p] != 0) : true;
                 __align__(16) __nv_bfloat16 sk[CH];
                 if (skip) {
 #pragma unroll
-                    for (int q = 0; q < 4; ++q)
-                        reinterpret_cast<uint4*>(sk)[q] = reinterpret_cast<const uint4*>(skip + p * CH)[q];
+                    for (int q = 0; q < 4; ++q) reinterpret_cast<uint4*>(sk)[q] = st[m * 5 + q];
                 }
                 __align__(16) __nv_bfloat16 out[CH];
 #pragma unroll
@@ -229,10 +245,16 @@ __global__ void __launch_bounds__(TM) k_conv32_tc(const __nv_bfloat16* __restric
                     if (relu) val = fmaxf(val, 0.0f);
                     out[n] = __float2bfloat16(fl ? val : 0.0f);
                 }
-                uint4* dst = reinterpret_cast<uint4*>(y + p * CH);
 #pragma unroll
-                for (int q = 0; q < 4; ++q) dst[q] = reinterpret_cast<const uint4*>(out)[q];
+                for (int q = 0; q < 4; ++q) st[m * 5 + q] = reinterpret_cast<const uint4*>(out)[q];
             }
+            __syncthreads();
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int q = tid + k * TM, px = q >> 2;
+                if (px < npx) y4[(rowp + px) * 4 + (q & 3)] = st[px * 5 + (q & 3)];
+            }
+            __syncthreads();
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -299,63 +321,110 @@ __global__ void k_conv_generic(const void* __restrict__ x, int xbf, const float*
 }
 
 // Forward 1 -> 32 layer (FP32 input, BF16 output) and 32 -> 1 layer (BF16 input,
-// FP32 output): one thread per pixel, 16-byte channel vectors, the 288 weights
-// broadcast from shared memory. Taps and channels are summed in the same order as
-// k_conv_generic, so both give the same bits.
-__global__ void k_conv_1to32(const float* __restrict__ x, const float* __restrict__ w,
-                             const float* __restrict__ bias, const uint8_t* __restrict__ mask,
-                             __nv_bfloat16* __restrict__ y, int H, int W, int relu) {
-    __shared__ float ws[CH * 9];
-    for (int e = threadIdx.x; e < CH * 9; e += blockDim.x) ws[e] = w[e];
+// FP32 output): one thread per pixel (128 consecutive pixels per block), the 288
+// weights tap-major in shared memory (16-byte vectors over the channels). The
+// 32-channel side goes through shared memory with an 80-byte pixel stride (no bank
+// conflicts for 16-byte accesses), so that global memory is read and written in
+// contiguous 16-byte chunks by consecutive threads. Taps and channels are summed in
+// the same order as k_conv_generic, so both give the same bits.
+constexpr int FP = 128;      // pixels per block
+constexpr int PSTRIDE = 5;   // uint4 per staged pixel (4 used)
+
+__global__ void __launch_bounds__(FP) k_conv_1to32(const float* __restrict__ x, const float* __restrict__ w,
+                                                   const float* __restrict__ bias,
+                                                   const uint8_t* __restrict__ mask,
+                                                   __nv_bfloat16* __restrict__ y, int H, int W, int relu) {
+    __shared__ __align__(16) float ws[9 * CH];
+    __shared__ uint4 os[FP * PSTRIDE];
+    for (int e = threadIdx.x; e < CH * 9; e += blockDim.x) ws[(e % 9) * CH + e / 9] = w[e];
     __syncthreads();
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= H * W) return;
-    const int i = p / W, j = p - (p / W) * W;
-    float acc[CH];
+    const long long n = (long long)H * W;
+    const long long p0 = (long long)blockIdx.x * FP;
+    const long long p = p0 + threadIdx.x;
+    if (p < n) {
+        const int i = (int)(p / W), j = (int)(p - (long long)i * W);
+        float acc[CH];
 #pragma unroll
-    for (int o = 0; o < CH; ++o) acc[o] = bias ? bias[o] : 0.0f;
+        for (int o = 0; o < CH; ++o) acc[o] = bias ? bias[o] : 0.0f;
 #pragma unroll
-    for (int tap = 0; tap < 9; ++tap) {
-        const int ii = i + tap / 3 - 1, jj = j + tap % 3 - 1;
-        if (ii < 0 || ii >= H || jj < 0 || jj >= W) continue;
-        const float xv = x[(size_t)ii * W + jj];
+        for (int tap = 0; tap < 9; ++tap) {
+            const int ii = i + tap / 3 - 1, jj = j + tap % 3 - 1;
+            if (ii < 0 || ii >= H || jj < 0 || jj >= W) continue;
+            const float xv = x[(size_t)ii * W + jj];
 #pragma unroll
-        for (int o = 0; o < CH; ++o) acc[o] += ws[o * 9 + tap] * xv;
+            for (int o = 0; o < CH; ++o) acc[o] += ws[tap * CH + o] * xv;
+        }
+        const bool fl = mask ? (mask[p] != 0) : true;
+        __align__(16) __nv_bfloat16 out[CH];
+#pragma unroll
+        for (int o = 0; o < CH; ++o) {
+            float v = acc[o];
+            if (relu) v = fmaxf(v, 0.0f);
+            out[o] = __float2bfloat16(fl ? v : 0.0f);
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) os[threadIdx.x * PSTRIDE + q] = reinterpret_cast<const uint4*>(out)[q];
     }
-    const bool fl = mask ? (mask[p] != 0) : true;
-    __align__(16) __nv_bfloat16 out[CH];
+    __syncthreads();
+    uint4* y4 = reinterpret_cast<uint4*>(y);
 #pragma unroll
-    for (int o = 0; o < CH; ++o) {
-        float v = acc[o];
-        if (relu) v = fmaxf(v, 0.0f);
-        out[o] = __float2bfloat16(fl ? v : 0.0f);
+    for (int k = 0; k < 4; ++k) {
+        const int q = threadIdx.x + k * FP;
+        const int px = q >> 2, c = q & 3;
+        if (p0 + px < n) y4[(p0 + px) * 4 + c] = os[px * PSTRIDE + c];
     }
-    uint4* dst = reinterpret_cast<uint4*>(y + (size_t)p * CH);
-#pragma unroll
-    for (int q = 0; q < 4; ++q) dst[q] = reinterpret_cast<const uint4*>(out)[q];
 }
 
-__global__ void k_conv_32to1(const __nv_bfloat16* __restrict__ x, const float* __restrict__ w,
-                             const float* __restrict__ bias, const uint8_t* __restrict__ mask,
-                             float* __restrict__ y, int H, int W, int relu) {
-    __shared__ float ws[CH * 9];
-    for (int e = threadIdx.x; e < CH * 9; e += blockDim.x) ws[e] = w[e];
+__global__ void __launch_bounds__(FP) k_conv_32to1(const __nv_bfloat16* __restrict__ x,
+                                                   const float* __restrict__ w, const float* __restrict__ bias,
+                                                   const uint8_t* __restrict__ mask, float* __restrict__ y, int H,
+                                                   int W, int relu) {
+    constexpr int SP = FP + 2;             // staged pixels per tap row
+    constexpr int SQ = 3 * SP * 4;         // staged 16-byte chunks (1560)
+    constexpr int SPER = (SQ + FP - 1) / FP;
+    __shared__ __align__(16) float ws[9 * CH];
+    __shared__ uint4 xs[3 * SP * PSTRIDE];
+    for (int e = threadIdx.x; e < CH * 9; e += blockDim.x) ws[(e % 9) * CH + e / 9] = w[e];
+    const long long n = (long long)H * W;
+    const long long p0 = (long long)blockIdx.x * FP;
+    // tap row d (di = d - 1) holds pixels p0 + di*W - 1 .. p0 + di*W + FP; taps that
+    // leave the grid are skipped below, so the clamp to [0, n) only avoids reading
+    // outside the array
+    const uint4* x4 = reinterpret_cast<const uint4*>(x);
+    {
+        uint4 v[SPER];
+#pragma unroll
+        for (int k = 0; k < SPER; ++k) {
+            const int q = threadIdx.x + k * FP;
+            const int d = q / (SP * 4), rem = q - d * (SP * 4);
+            const long long g = p0 + (long long)(d - 1) * W - 1 + (rem >> 2);
+            v[k] = make_uint4(0u, 0u, 0u, 0u);
+            if (q < SQ && g >= 0 && g < n) v[k] = x4[g * 4 + (rem & 3)];
+        }
+#pragma unroll
+        for (int k = 0; k < SPER; ++k) {
+            const int q = threadIdx.x + k * FP;
+            const int d = q / (SP * 4), rem = q - d * (SP * 4);
+            if (q < SQ) xs[(d * SP + (rem >> 2)) * PSTRIDE + (rem & 3)] = v[k];
+        }
+    }
     __syncthreads();
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= H * W) return;
-    const int i = p / W, j = p - (p / W) * W;
+    const long long p = p0 + threadIdx.x;
+    if (p >= n) return;
+    const int i = (int)(p / W), j = (int)(p - (long long)i * W);
     float acc = bias ? bias[0] : 0.0f;
 #pragma unroll
     for (int tap = 0; tap < 9; ++tap) {
-        const int ii = i + tap / 3 - 1, jj = j + tap % 3 - 1;
+        const int di = tap / 3 - 1, dj = tap % 3 - 1;
+        const int ii = i + di, jj = j + dj;
         if (ii < 0 || ii >= H || jj < 0 || jj >= W) continue;
-        const uint4* src = reinterpret_cast<const uint4*>(x + ((size_t)ii * W + jj) * CH);
+        const uint4* src = xs + ((di + 1) * SP + threadIdx.x + dj + 1) * PSTRIDE;
         uint4 v[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) v[q] = src[q];
         const __nv_bfloat16* xv = reinterpret_cast<const __nv_bfloat16*>(v);
 #pragma unroll
-        for (int c = 0; c < CH; ++c) acc += ws[c * 9 + tap] * bf2f(xv[c]);
+        for (int c = 0; c < CH; ++c) acc += ws[tap * CH + c] * bf2f(xv[c]);
     }
     if (relu) acc = fmaxf(acc, 0.0f);
     const bool fl = mask ? (mask[p] != 0) : true;
@@ -509,22 +578,34 @@ namespace {
 inline int cdiv(long long a, int b) { return (int)((a + b - 1) / b); }
 }  // namespace
 
-size_t conv32_smem_bytes() { return (size_t)B_BYTES + X_BYTES; }
+size_t conv32_smem_bytes(int rows) { return (size_t)B_BYTES + x_bytes(rows); }
 
-cudaError_t conv32_tc(const __nv_bfloat16* x, const __nv_bfloat16* wpack, const float* bias,
-                      const __nv_bfloat16* skip, const uint8_t* mask, __nv_bfloat16* y, int H, int W, int relu,
-                      int* err, cudaStream_t s) {
+template <int ROWS>
+static cudaError_t conv32_launch(const __nv_bfloat16* x, const __nv_bfloat16* wpack, const float* bias,
+                                 const __nv_bfloat16* skip, const uint8_t* mask, __nv_bfloat16* y, int H, int W,
+                                 int relu, int* err, cudaStream_t s) {
     static bool configured = false;
     if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(k_conv32_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)conv32_smem_bytes());
+        cudaError_t e = cudaFuncSetAttribute(k_conv32_tc<ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)conv32_smem_bytes(ROWS));
         if (e != cudaSuccess) return e;
         configured = true;
     }
     dim3 grid(cdiv(W, TM), cdiv(H, ROWS));
-    k_conv32_tc<<<grid, TM, conv32_smem_bytes(), s>>>(x, reinterpret_cast<const uint4*>(wpack), bias, skip,
-                                                      mask, y, H, W, relu, err);
+    k_conv32_tc<ROWS><<<grid, TM, conv32_smem_bytes(ROWS), s>>>(x, reinterpret_cast<const uint4*>(wpack), bias,
+                                                                 skip, mask, y, H, W, relu, err);
     return cudaGetLastError();
+}
+
+// Rows per CTA: four where that still leaves about six CTAs per SM (three resident,
+// two waves), else fewer, so that the small levels of the network spread over the SMs.
+cudaError_t conv32_tc(const __nv_bfloat16* x, const __nv_bfloat16* wpack, const float* bias,
+                      const __nv_bfloat16* skip, const uint8_t* mask, __nv_bfloat16* y, int H, int W, int relu,
+                      int* err, cudaStream_t s) {
+    const long long segs = cdiv(W, TM);
+    if (segs * cdiv(H, 4) >= 6 * 148) return conv32_launch<4>(x, wpack, bias, skip, mask, y, H, W, relu, err, s);
+    if (segs * cdiv(H, 2) >= 6 * 148) return conv32_launch<2>(x, wpack, bias, skip, mask, y, H, W, relu, err, s);
+    return conv32_launch<1>(x, wpack, bias, skip, mask, y, H, W, relu, err, s);
 }
 
 cudaError_t pack_w32(const float* w, __nv_bfloat16* img, cudaStream_t s) {
@@ -538,12 +619,12 @@ cudaError_t conv_generic(int cin, int cout, const void* x, int xbf, const float*
     const int n = H * W;
     const int blk = 128;
     if (!transposed && cin == 1 && cout == 32 && !xbf && ybf) {
-        k_conv_1to32<<<cdiv(n, blk), blk, 0, s>>>(static_cast<const float*>(x), w, bias, mask,
+        k_conv_1to32<<<cdiv(n, FP), FP, 0, s>>>(static_cast<const float*>(x), w, bias, mask,
                                                    static_cast<__nv_bfloat16*>(y), H, W, relu);
         return cudaGetLastError();
     }
     if (!transposed && cin == 32 && cout == 1 && xbf && !ybf) {
-        k_conv_32to1<<<cdiv(n, blk), blk, 0, s>>>(static_cast<const __nv_bfloat16*>(x), w, bias, mask,
+        k_conv_32to1<<<cdiv(n, FP), FP, 0, s>>>(static_cast<const __nv_bfloat16*>(x), w, bias, mask,
                                                    static_cast<float*>(y), H, W, relu);
         return cudaGetLastError();
     }

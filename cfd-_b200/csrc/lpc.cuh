@@ -10,7 +10,7 @@
 namespace cfd {
 namespace lpc {
 
-size_t conv32_smem_bytes();
+size_t conv32_smem_bytes(int rows);
 cudaError_t conv32_tc(const __nv_bfloat16* x, const __nv_bfloat16* wpack, const float* bias,
                       const __nv_bfloat16* skip, const uint8_t* mask, __nv_bfloat16* y, int H, int W, int relu,
                       int* err, cudaStream_t s);

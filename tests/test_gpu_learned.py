@@ -30,10 +30,12 @@ def relerr(a, b):
     return np.abs(a - b).max() / max(np.abs(b).max(), 1e-30)
 
 
-def test_conv32_tensor_cores_match_torch(L):
+# one full and one partial 128-pixel segment per row; the sizes select 1, 2 and 4 rows
+# per CTA, with a partial block of rows in each
+@pytest.mark.parametrize("H,W", [(7, 200), (601, 300), (1201, 300)])
+def test_conv32_tensor_cores_match_torch(L, H, W):
     torch, _lib, learned = L
     F = torch.nn.functional
-    H, W = 7, 200  # one full and one partial 128-pixel tile per row
     g = torch.Generator().manual_seed(1)
     x = torch.randn((H, W, 32), generator=g).to(torch.bfloat16)
     w = torch.randn((32, 32, 3, 3), generator=g) * 0.1
