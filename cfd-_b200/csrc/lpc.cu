@@ -81,11 +81,15 @@ constexpr int XP = TM + 2;
 constexpr int XCHUNK = XP * 16;            // 2080
 constexpr int XROW = 4 * XCHUNK;           // 8320
 constexpr int XB = 13;                     // loads in flight per thread and batch
-static_assert(B_BYTES / 16 % TM == 0, "the B image splits evenly over the threads");
-constexpr int x_bytes(int rows) { return (rows + 2) * XROW; }
+// Two warpgroups per CTA: both stage operands (twice the loads in flight of one), one
+// thread issues the MMAs, and in the epilogue warpgroup g takes rows g, g + 2, ...
+// (warp w reads TMEM lanes 32 (w % 4) .. 32 (w % 4) + 31, its 32 pixels).
+constexpr int NT = 256;
+constexpr int ST_BYTES = TM * 5 * 16;      // epilogue staging of one row: 128 pixels x 80 bytes
+__host__ __device__ constexpr int x_bytes(int rows) { return (rows + 2) * XROW; }
 
 template <int ROWS>
-__global__ void __launch_bounds__(TM) k_conv32_tc(const __nv_bfloat16* __restrict__ x,
+__global__ void __launch_bounds__(NT) k_conv32_tc(const __nv_bfloat16* __restrict__ x,
                                                   const uint4* __restrict__ wpack,
                                                   const float* __restrict__ bias,
                                                   const __nv_bfloat16* __restrict__ skip,
@@ -93,7 +97,9 @@ __global__ void __launch_bounds__(TM) k_conv32_tc(const __nv_bfloat16* __restric
                                                   __nv_bfloat16* __restrict__ y, int H, int W,
                                                   int relu, int* __restrict__ err) {
     constexpr int XQ = (ROWS + 2) * XP * 4;    // 16-byte chunks staged per CTA
-    constexpr int XPER = (XQ + TM - 1) / TM;   // per thread
+    constexpr int XPER = (XQ + NT - 1) / NT;   // per thread
+    constexpr int BQ = B_BYTES / 16, BPER = (BQ + NT - 1) / NT;
+    static_assert(2 * ST_BYTES <= x_bytes(ROWS), "epilogue staging fits in the operand buffer");
     constexpr uint32_t kTmemCols = 32u * ROWS;
     static_assert((kTmemCols & (kTmemCols - 1)) == 0 && kTmemCols >= 32 && kTmemCols <= 512, "TMEM columns");
     extern __shared__ __align__(1024) uint8_t smem[];
@@ -118,11 +124,13 @@ __global__ void __launch_bounds__(TM) k_conv32_tc(const __nv_bfloat16* __restric
     }
     // B operand: a straight copy of the prepacked image, all loads of a thread in flight
     {
-        uint4 v[B_BYTES / 16 / TM];
+        uint4 v[BPER];
 #pragma unroll
-        for (int k = 0; k < B_BYTES / 16 / TM; ++k) v[k] = wpack[tid + k * TM];
+        for (int k = 0; k < BPER; ++k)
+            if (tid + k * NT < BQ) v[k] = wpack[tid + k * NT];
 #pragma unroll
-        for (int k = 0; k < B_BYTES / 16 / TM; ++k) reinterpret_cast<uint4*>(Bs)[tid + k * TM] = v[k];
+        for (int k = 0; k < BPER; ++k)
+            if (tid + k * NT < BQ) reinterpret_cast<uint4*>(Bs)[tid + k * NT] = v[k];
     }
     // staged input rows: consecutive threads take consecutive 16-byte chunks in global
     // order (chunk fastest, then pixel), so each warp reads 512 contiguous bytes; the
@@ -132,7 +140,7 @@ __global__ void __launch_bounds__(TM) k_conv32_tc(const __nv_bfloat16* __restric
         uint4 v[XB];
 #pragma unroll
         for (int k = 0; k < XB; ++k) {
-            const int q = tid + (k0 + k) * TM;
+            const int q = tid + (k0 + k) * NT;
             const int c = q & 3, t = q >> 2;
             const int r = t / XP, px = t - r * XP;
             const int ii = i0 - 1 + r, jj = j0 - 1 + px;
@@ -142,7 +150,7 @@ __global__ void __launch_bounds__(TM) k_conv32_tc(const __nv_bfloat16* __restric
         }
 #pragma unroll
         for (int k = 0; k < XB; ++k) {
-            const int q = tid + (k0 + k) * TM;
+            const int q = tid + (k0 + k) * NT;
             if (k0 + k < XPER && q < XQ) {
                 const int c = q & 3, t = q >> 2;
                 const int r = t / XP, px = t - r * XP;
@@ -196,31 +204,33 @@ __global__ void __launch_bounds__(TM) k_conv32_tc(const __nv_bfloat16* __restric
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (ok) {
         // The MMAs have finished reading the staged rows, so their buffer stages the
-        // epilogue: 128 pixels x 80 bytes per output row (skip input in, result out),
-        // read and written in global memory as contiguous 16-byte chunks.
-        const int m = warp * 32 + lane;
+        // epilogue: 128 pixels x 80 bytes per output row and warpgroup (skip input in,
+        // result out), read and written in global memory as contiguous 16-byte chunks.
+        // Each warpgroup synchronises on its own named barrier (1 or 2).
+        const int g = warp >> 2, wq = warp & 3, lt = tid & (TM - 1);
+        const int m = wq * 32 + lane;
         const int j = j0 + m;
         const int npx = min(TM, W - j0);
-        uint4* st = reinterpret_cast<uint4*>(Xs);
+        uint4* st = reinterpret_cast<uint4*>(Xs + g * ST_BYTES);
         const uint4* skip4 = reinterpret_cast<const uint4*>(skip);
         uint4* y4 = reinterpret_cast<uint4*>(y);
-        for (int r = 0; r < ROWS; ++r) {
+        for (int r = g; r < ROWS; r += 2) {
             const int i = i0 + r;
             if (i >= H) break;
             const size_t rowp = (size_t)i * W + j0;
             if (skip) {
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
-                    const int q = tid + k * TM, px = q >> 2;
+                    const int q = lt + k * TM, px = q >> 2;
                     if (px < npx) st[px * 5 + (q & 3)] = skip4[(rowp + px) * 4 + (q & 3)];
                 }
             }
-            __syncthreads();
+            asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(TM) : "memory");
             float acc[CH];
 #pragma unroll
             for (int c0 = 0; c0 < CH; c0 += 8) {
                 uint32_t v[8];
-                const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(32 * r + c0);
+                const uint32_t taddr = tmem + ((uint32_t)(wq * 32) << 16) + (uint32_t)(32 * r + c0);
                 asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
                              : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
                                "=r"(v[6]), "=r"(v[7])
@@ -248,13 +258,13 @@ __global__ void __launch_bounds__(TM) k_conv32_tc(const __nv_bfloat16* __restric
 #pragma unroll
                 for (int q = 0; q < 4; ++q) st[m * 5 + q] = reinterpret_cast<const uint4*>(out)[q];
             }
-            __syncthreads();
+            asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(TM) : "memory");
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
-                const int q = tid + k * TM, px = q >> 2;
+                const int q = lt + k * TM, px = q >> 2;
                 if (px < npx) y4[(rowp + px) * 4 + (q & 3)] = st[px * 5 + (q & 3)];
             }
-            __syncthreads();
+            asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(TM) : "memory");
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -592,7 +602,7 @@ static cudaError_t conv32_launch(const __nv_bfloat16* x, const __nv_bfloat16* wp
         configured = true;
     }
     dim3 grid(cdiv(W, TM), cdiv(H, ROWS));
-    k_conv32_tc<ROWS><<<grid, TM, conv32_smem_bytes(ROWS), s>>>(x, reinterpret_cast<const uint4*>(wpack), bias,
+    k_conv32_tc<ROWS><<<grid, NT, conv32_smem_bytes(ROWS), s>>>(x, reinterpret_cast<const uint4*>(wpack), bias,
                                                                  skip, mask, y, H, W, relu, err);
     return cudaGetLastError();
 }
