@@ -4,7 +4,7 @@
 // Activations are BF16 in NHWC layout (pixel = MAC cell (i, j) flattened as
 // i*W + j with j contiguous, 32 channels innermost); every product is accumulated
 // in FP32. The 32 -> 32 channel 3x3 convolutions (the FLOP-heavy layers) are
-// implicit GEMMs on the 5th-generation tensor cores: per CTA four grid rows of 128
+// implicit GEMMs on the 5th-generation tensor cores: per CTA one or two grid rows of 128
 // consecutive pixels (M = 128 per row), N = 32 output channels, K = 9 taps x 32
 // input channels = 288, issued as 18 tcgen05.mma per row (kind::f16, BF16 inputs,
 // FP32 accumulator in tensor memory) by one thread; the input rows are staged once
@@ -66,7 +66,7 @@ __device__ __forceinline__ float bf2f(__nv_bfloat16 x) { return __bfloat162float
 // y[p][n] = act(bias[n] + sum_{tap, c} w[n][c][tap] * x[p + tap][c] (+ skip[p][n])), masked.
 // wpack is the B operand image (N = 32 rows, K = 288) in the shared-memory layout.
 //
-// One CTA computes ROWS (1, 2 or 4) output rows i0 .. i0+ROWS-1 of one 128-pixel segment
+// One CTA computes ROWS (1 or 2) output rows i0 .. i0+ROWS-1 of one 128-pixel segment
 // j0 .. j0+127. The ROWS + 2 input rows it needs, pixels j0-1 .. j0+128 (XP = 130,
 // zero outside the grid), are copied once into shared memory, channel-chunk major:
 // chunk c (channels 8c .. 8c+7, 16 bytes) of pixel q of staged row r sits at
@@ -607,13 +607,14 @@ static cudaError_t conv32_launch(const __nv_bfloat16* x, const __nv_bfloat16* wp
     return cudaGetLastError();
 }
 
-// Rows per CTA: four where that still leaves about six CTAs per SM (three resident,
-// two waves), else fewer, so that the small levels of the network spread over the SMs.
+// Rows per CTA: two where that still leaves about six CTAs per SM (two waves at the
+// four CTAs of 52 KB that fit), else one, so that the small levels of the network
+// spread over the SMs. (Four rows per CTA halve the halo reads but fit only three CTAs
+// per SM and measured slower: 36.4 against 32.5 us at 1024 x 512.)
 cudaError_t conv32_tc(const __nv_bfloat16* x, const __nv_bfloat16* wpack, const float* bias,
                       const __nv_bfloat16* skip, const uint8_t* mask, __nv_bfloat16* y, int H, int W, int relu,
                       int* err, cudaStream_t s) {
     const long long segs = cdiv(W, TM);
-    if (segs * cdiv(H, 4) >= 6 * 148) return conv32_launch<4>(x, wpack, bias, skip, mask, y, H, W, relu, err, s);
     if (segs * cdiv(H, 2) >= 6 * 148) return conv32_launch<2>(x, wpack, bias, skip, mask, y, H, W, relu, err, s);
     return conv32_launch<1>(x, wpack, bias, skip, mask, y, H, W, relu, err, s);
 }

@@ -30,8 +30,8 @@ def relerr(a, b):
     return np.abs(a - b).max() / max(np.abs(b).max(), 1e-30)
 
 
-# one full and one partial 128-pixel segment per row; the sizes select 1, 2 and 4 rows
-# per CTA, with a partial block of rows in each
+# one full and one partial 128-pixel segment per row; the sizes select 1, 2 and 2 rows
+# per CTA (the last two with a partial block of rows)
 @pytest.mark.parametrize("H,W", [(7, 200), (601, 300), (1201, 300)])
 def test_conv32_tensor_cores_match_torch(L, H, W):
     torch, _lib, learned = L
