@@ -1,29 +1,34 @@
 """Benchmark of the projection step on B200 (one JSON line on rank 0).
 
-Workload: the cylinder channel with a passive scalar -- 440 x 82 MAC grid, domain
-2.2 x 0.41, circle D = 0.1 at (0.2, 0.2), parabolic inflow U = 1, Re = 100,
-van Leer scalar entering on 0.15 < y < 0.25 (D = 1e-3), AB2 with automatic upwind
-fraction, tau 0.5, pressure by Jacobi-PCG to a relative residual of 1e-8 in FP64.
-Synthetic: the flow starts from rest, as the reference case does.
+Workload (headline): the seeded obstacle flow -- 1024 x 512 MAC grid on a 2 x 1
+channel, 2-12 circles, ellipses or rectangles from the obstacle-flow generator
+(``cases.obstacle_flow(seed=13)``: 11 obstacles, Re 1465), block inflow U = 1,
+outflow p = 0, slip walls, AB2 with automatic upwind fraction, tau 0.5; pressure
+by Jacobi-PCG to a relative residual of 1e-8 in FP64. Synthetic: the flow starts
+from rest, as the reference's cases do.
 
 A step is one full projection step (all stages, one captured CUDA graph).
 value     = cell-updates/s (nx*ny cells per step, summed over ranks) from CUDA
             events around every timed step on the solver's stream; L2 is flushed
             (256 MiB write) between timed steps.
-e2e       = the same metric through the public API (``sim.step()``) with the state
-            copied in from pinned host memory and u, v, p, c copied back out every step.
+poisson_ms = event time of the pressure solve inside the step graph.
+e2e       = the same metric through the public API (``sim.step()``) with u, v copied
+            in from pinned host memory and u, v, p copied back out every step.
 roofline  = the pressure solver kernel: algorithmic bytes 88 B per cell per CG
             iteration (FP64 x, r, p, q, z traffic of a streaming implementation)
             over its event-timed duration.
+learned   = the same workload with the pressure solved by flexible CG with the
+            shipped learned preconditioner (to the same 1e-8): per-step time and
+            cell-updates/s inside sim.step(), and Poisson ms and iterations of
+            both solvers on the same system from the same warm start.
+grid_2048x1024 = the same generator and seed at 2048 x 1024: plain steps and the
+            Poisson comparison (the CG cap is raised so that both reach 1e-8).
+cylinder_440x82 = the cylinder channel with a van Leer scalar (plain FP64 path).
 stencils  = the kernel-level stencil drop-ins on a 4096 x 2048 grid against the
             measured HBM peak (compulsory bytes per cell over event time).
-mixed_precision = the workload with FP32 solver iterations and FP64 refinement against
-            the FP64 solver: ms per step and the per-field error of the end state.
-learned_pc = Poisson ms and iterations at 1e-8 on a seeded 1024 x 512 obstacle flow:
-            plain Jacobi-PCG against flexible CG with the shipped learned
-            preconditioner.
 --impl reference times the CPU restatement of the reference (the oracle: NumPy
-stencils and scipy's CG iteration) on the same workload.
+stencils, scipy's CG called as the reference calls it) on the same workload, a
+bounded sample per step (see run_reference).
 """
 
 from __future__ import annotations
@@ -44,14 +49,20 @@ for p in (str(ROOT / "cfd-_b200"), str(ROOT)):
         sys.path.insert(0, p)
 
 METRIC = "cell-updates/s and Poisson ms at 1e-8 residual: learned-PC vs plain CG on B200"
-NX, NY = 440, 82
+NX, NY, SEED = 1024, 512, 13
 CG_RTOL = 1e-8
 BYTES_PER_CELL_ITER = 88.0
 BYTES_PER_CELL_SOLVE = 32.0
-SPEC = {"fall": "cylinder", "parameter": {"re": 100, "nx": NX, "ny": NY},
-        "numerik": {"pressure_solver": "cg"},
-        "skalar": {"name": "c", "diffusivity": 1e-3, "inflow_band": [0.15, 0.25], "limiter": "vanleer"}}
-WORKLOAD = "cylinder 440x82 Re100 + van Leer scalar, FP64 Jacobi-PCG rtol 1e-8"
+WORKLOAD = (f"obstacle flow {NX}x{NY} (generator seed {SEED}: 2-12 circles/ellipses/rectangles, sizes "
+            f"0.02-0.08 of the height, block inflow U=1, outflow p=0, slip walls, Re log-uniform 200-2000), "
+            f"FP64 Jacobi-PCG rtol 1e-8")
+CYL_NX, CYL_NY = 440, 82
+CYL_SPEC = {"fall": "cylinder", "parameter": {"re": 100, "nx": CYL_NX, "ny": CYL_NY},
+            "numerik": {"pressure_solver": "cg"},
+            "skalar": {"name": "c", "diffusivity": 1e-3, "inflow_band": [0.15, 0.25], "limiter": "vanleer"}}
+CYL_WORKLOAD = "cylinder 440x82 Re100 + van Leer scalar, FP64 Jacobi-PCG rtol 1e-8"
+# the CPU arms time this many CG iterations per step and scale to the full solve
+CPU_CG_SAMPLE = 150
 
 
 def _peaks():
@@ -160,9 +171,9 @@ def _clocks_path(name: str) -> str:
     return str(Path(os.environ.get("CFD2D_CLOCKS_DIR") or tempfile.gettempdir()) / name)
 
 
-def _ncu_traffic():
-    """DRAM bytes per launch of the solver kernel from the committed ncu summary, if any."""
-    f = ROOT / "profiles" / "pcg_cluster_cylinder440x82.txt"
+def _ncu_traffic(profile: str):
+    """DRAM bytes per launch of a kernel from its committed ncu summary, if any."""
+    f = ROOT / "profiles" / profile
     if not f.exists():
         return None
     for line in f.read_text().splitlines():
@@ -174,54 +185,103 @@ def _ncu_traffic():
     return None
 
 
+def _obstacle_spec(seed: int = SEED):
+    from cfd2d_b200.cases import random_obstacle_spec
+    import numpy as np
+
+    return random_obstacle_spec(np.random.default_rng(seed))
+
+
 # ------------------------------------------------------------------ CPU timings
-def cpu_oracle_rate(steps: int, warmup: int, threads: int | None) -> dict:
-    """Time the oracle (CPU restatement) on the bench workload in a child process."""
+def cpu_oracle_sample(full_steps: int, warm_steps: int, steps: int, threads: int | None,
+                      iters_per_step: float | None = None) -> dict:
+    """Bounded CPU sample of the headline workload, timed in a child process: the
+    oracle's projection step (NumPy stencils; the pressure system solved by scipy's
+    cg with the Jacobi preconditioner, the call cfd2d/pressure.py:171 makes).
+    ``full_steps`` untimed steps from rest solve to 1e-8 (the last one's iteration
+    count is the full solve's length unless ``iters_per_step`` is given); the
+    ``warm_steps`` + ``steps`` steps after them run at most CPU_CG_SAMPLE CG
+    iterations, and each timed step's time is scaled to the full solve: time
+    outside the solve + solve time x (full iterations / sampled iterations). With
+    ``iters_per_step`` given, the initial projection the case makes while it is
+    built is capped as well (it only prepares a state to time)."""
     env = dict(os.environ)
     if threads is not None:
         for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
             env[k] = str(threads)
+    obst, re = _obstacle_spec()
     code = f"""
 import sys, time, json, warnings
 sys.path.insert(0, {str(ROOT)!r})
 warnings.simplefilter("ignore")
 import oracle as O
-sim = O.cylinder(re=100, nx={NX}, ny={NY}, tol={CG_RTOL})
-O.add_scalar(sim, "c", 1e-3, inflow_band=(0.15, 0.25), limiter="vanleer")
-for _ in range({warmup}):
+O.OPressure.engine = "scipy"
+if {iters_per_step!r}:
+    O.OPressure.maxiter = {CPU_CG_SAMPLE}
+sim = O.custom_obstacles({obst!r}, lx=2.0, ly=1.0, nx={NX}, ny={NY}, re={re!r}, tol={CG_RTOL})
+O.OPressure.maxiter = 5000
+ps = sim.pressure
+spent = [0.0]
+solve = ps.solve
+def timed_solve(rhs):
+    t0 = time.perf_counter()
+    out = solve(rhs)
+    spent[0] += time.perf_counter() - t0
+    return out
+ps.solve = timed_solve
+n_full = None
+for _ in range({full_steps}):
     sim.step()
-t0 = time.perf_counter()
+    n_full = ps.last_iterations
+n_target = {iters_per_step!r} or n_full
+ps.maxiter = {CPU_CG_SAMPLE}
+for _ in range({warm_steps}):
+    sim.step()
+est, raw, its = [], [], []
 for _ in range({steps}):
+    spent[0] = 0.0
+    t0 = time.perf_counter()
     sim.step()
-el = time.perf_counter() - t0
-print(json.dumps({{"seconds": el, "steps": {steps}, "its": sim.iterations[-{steps}:]}}))
+    el = time.perf_counter() - t0
+    k = max(1, ps.last_iterations)
+    its.append(k)
+    raw.append(el)
+    est.append(el - spent[0] + spent[0] * n_target / k)
+print(json.dumps({{"est_s": est, "raw_s": raw, "sampled_iters": its, "full_iters": n_target}}))
 """
     out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, check=True)
     d = json.loads(out.stdout.strip().splitlines()[-1])
-    d["rate"] = NX * NY * d["steps"] / d["seconds"]
+    d["seconds_per_step"] = sum(d["est_s"]) / len(d["est_s"])
+    d["rate"] = NX * NY / d["seconds_per_step"]
     return d
 
 
 def run_reference(args, dist, rank, world):
-    # the reference arm runs on rank 0 only; the other ranks exit without work
+    """The CPU arm: the oracle (the reference's algorithm restated; its CG is scipy's
+    cg as the reference calls it) on the headline workload with every host thread
+    it can use. Each step is a bounded sample (cpu_oracle_sample): the first two
+    warm-up steps solve in full (their iteration count sets the full-solve length),
+    the other warm-up steps and the timed steps run CPU_CG_SAMPLE CG iterations and
+    are scaled to the full solve. Rank 0 only; the other ranks exit without work."""
     if rank != 0:
         return
-    steps = max(1, min(args.steps, 8))
-    warm = max(0, min(args.warmup, 2))
-    d = cpu_oracle_rate(steps, warm, None)
+    full = min(2, args.warmup)
+    d = cpu_oracle_sample(full, args.warmup - full, args.steps, None)
     value = d["rate"]
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "cell-updates/s",
-        "n_gpus": world, "steps": steps, "warmup": warm, "ms_per_step": 1e3 * d["seconds"] / steps,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * d["seconds_per_step"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (flow from rest, as the reference case)",
+        "data": "synthetic (seeded obstacle flow from rest, as the reference's cases start)",
         "config": {"workload": WORKLOAD, "grid": [NX, NY], "cells": NX * NY, "parallelism": "replicas"},
-        "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": os.cpu_count(),
-                         "kind": "port",
-                         "sample": f"{steps} steps after {warm} warm-up steps of the oracle "
-                                   f"(NumPy + scipy-form CG) on the same workload"},
+        "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": os.cpu_count(), "kind": "port",
+                         "sample": f"oracle step (NumPy stencils, scipy cg + Jacobi as cfd2d/pressure.py:171); "
+                                   f"{full} full warm-up steps from rest set the solve length "
+                                   f"({d['full_iters']} CG iterations), then each step runs {CPU_CG_SAMPLE} CG "
+                                   f"iterations and its solve time is scaled to the full length"},
         "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "poisson_iters_per_step": float(sum(d["its"]) / len(d["its"])),
+        "poisson_iters_per_step": float(d["full_iters"]),
+        "raw_sample_ms_per_step": 1e3 * sum(d["raw_s"]) / len(d["raw_s"]),
     }
     print(json.dumps(line), flush=True)
 
@@ -309,33 +369,34 @@ def stencil_roofline(peak: float, reps: int = 10) -> dict:
 
 
 # ------------------------------------------------------------------ learned preconditioner
-def learned_section() -> dict:
-    """Pressure solve of a seeded 1024 x 512 obstacle flow (2-12 obstacles, uniform
-    inflow, outflow p = 0) to 1e-8: plain Jacobi-PCG against flexible CG with the
-    shipped learned preconditioner, from the same warm start (the previous step's
-    pressure), event-timed on the device after one untimed warm-up solve each."""
-    import numpy as np
+def _rhs_of(sim):
+    """The pressure right-hand side div(F, G) / dt of the simulation's last predictor."""
+    import torch
+
+    g = sim.grid
+    F, G = sim.F, sim.G
+    return torch.from_numpy(((F[1:, 1:-1] - F[:-1, 1:-1]) / g.dx + (G[1:-1, 1:] - G[1:-1, :-1]) / g.dy)
+                            / sim.dt).cuda()
+
+
+def poisson_compare(sim, net, maxiter: int) -> dict:
+    """One pressure system of ``sim`` (its last predictor) solved to 1e-8 by the plain
+    Jacobi-PCG and by flexible CG with the learned preconditioner, each from the same
+    warm start (the step's previous pressure), event-timed on the device after one
+    untimed solve of the same system."""
     import torch
 
     from cfd2d_b200 import learned
 
-    rng = np.random.default_rng(13)
-    case = learned.obstacle_case(rng, 1024, 512)
-    sim = case.sim
-    sim.pressure.tol = CG_RTOL
-    sim.advance(1)
     ps = sim.pressure
     xprev = ps._d_x0.clone()
     sim.advance(1)
-    g = sim.grid
-    F, G = sim.F, sim.G
-    rhs = torch.from_numpy(((F[1:, 1:-1] - F[:-1, 1:-1]) / g.dx + (G[1:-1, 1:] - G[1:-1, :-1]) / g.dy)
-                           / sim.dt).cuda()
-    fcg = learned.LearnedPCG(ps, learned.pretrained(), maxiter=6000)
+    rhs = _rhs_of(sim)
+    fcg = learned.LearnedPCG(ps, net, maxiter=maxiter)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-    out = {"workload": "obstacles 1024x512 (seed 13), warm start, FP64, rtol 1e-8"}
+    out = {}
     for name, solve in (("plain", lambda: ps.solve(rhs)), ("learned", lambda: fcg.solve(rhs))):
-        for timed in (False, True):
+        for _timed in (False, True):
             ps._d_x0.copy_(xprev)
             torch.cuda.synchronize()
             ev[0].record()
@@ -347,6 +408,7 @@ def learned_section() -> dict:
         if name == "learned":
             out[name]["fcg_iterations"] = int(fcg.last_iterations)
             out[name]["fell_back"] = bool(fcg.last_reason != 1)
+    out["speedup_learned_vs_plain"] = out["plain"]["poisson_ms"] / out["learned"]["poisson_ms"]
     # one application of the network alone, launched directly (outside the solve's
     # graph, whose conditional node keeps profilers from seeing its kernels)
     fcg.precondition()
@@ -357,17 +419,165 @@ def learned_section() -> dict:
         fcg.precondition()
     ev[1].record()
     torch.cuda.synchronize()
-    net_ms = ev[0].elapsed_time(ev[1]) / reps
-    # 2 * pixels * 9 * 32 * 32 for the seven 32 -> 32 layers on the tensor cores
-    # (two per level on levels 0-2, one on level 3; pixels per level H*W / 4^level)
-    px = [1024 * 512 // (4 ** lvl) for lvl in range(4)]
-    tc_flops = 2 * 9 * 32 * 32 * (px[0] * 2 + px[1] * 2 + px[2] * 2 + px[3])
-    out["network"] = {"ms_per_application": net_ms, "tensor_core_flops": tc_flops,
-                      "tensor_core_tflops_over_whole_application": tc_flops / (net_ms * 1e-3) / 1e12}
+    out["network_ms_per_application"] = ev[0].elapsed_time(ev[1]) / reps
     fcg.close()
+    ps._d_x0.copy_(xprev)
+    return out
+
+
+def learned_steps(nx: int, ny: int, steps: int, warmup: int, flush, maxiter: int = 5000) -> dict:
+    """The obstacle flow with every step's pressure solved by flexible CG with the
+    learned preconditioner (Simulation.set_pressure_preconditioner): device time of
+    each sim.step() from events on the simulation's stream (L2 flushed before each),
+    end-to-end wall time of the same calls, FCG iterations and fallbacks per step."""
+    import numpy as np
+    import torch
+
+    from cfd2d_b200 import cases, learned
+
+    case = cases.obstacle_flow(SEED, nx, ny, pressure_solver="cg")
+    sim = case.sim
+    sim.pressure.tol = CG_RTOL
+    sim.pressure.maxiter = maxiter
+    sim.set_pressure_preconditioner(learned.pretrained(), maxiter=maxiter)
+    sim.advance(warmup)
+    stream = sim.stream
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ms, fallbacks = [], 0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    wall = 0.0
+    for _ in range(steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        ev[0].record(stream)
+        sim.step()
+        ev[1].record(stream)
+        ev[1].synchronize()
+        wall += time.perf_counter() - t1
+        ms.append(ev[0].elapsed_time(ev[1]))
+        fallbacks += int(sim._learned.last_reason != 1)
+    del t0
+    its = np.array(sim.history.extra["cg_iterationen"][-steps:], dtype=float)
+    dev_s = sum(ms) / 1e3
+    out = {"steps": steps, "warmup": warmup, "ms_per_step": 1e3 * dev_s / steps,
+           "cell_updates_per_s": nx * ny * steps / dev_s, "wall_cell_updates_per_s": nx * ny * steps / wall,
+           "fcg_iters_per_step": float(its.mean()), "fallback_steps": fallbacks}
+    sim.set_pressure_preconditioner(None)
+    return out
+
+
+def grid2048_section(steps: int, flush) -> dict:
+    """The obstacle-flow generator's seed at 2048 x 1024: plain FP64 steps (event-timed
+    over ``steps`` steps after 2, CG cap raised to 20000 so every solve reaches 1e-8)
+    and the Poisson comparison with the learned preconditioner."""
+    import numpy as np
+    import torch
+
+    from cfd2d_b200 import cases, learned
+
+    nx, ny = 2 * NX, 2 * NY
+    case = cases.obstacle_flow(SEED, nx, ny, pressure_solver="cg")
+    sim = case.sim
+    sim.pressure.tol = CG_RTOL
+    sim.pressure.maxiter = 20000
+    sim.advance(2)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    flush.fill_(1.0)
+    torch.cuda.synchronize()
+    with torch.cuda.stream(sim.stream):
+        ev[0].record()
+        sim.launch_steps(steps)
+        ev[1].record()
+    sim.finish_steps()
+    torch.cuda.synchronize()
+    ms = ev[0].elapsed_time(ev[1]) / steps
+    its = np.array(sim.history.extra["cg_iterationen"][-steps:], dtype=float)
+    out = {"workload": f"obstacle flow {nx}x{ny} (generator seed {SEED}), FP64 Jacobi-PCG rtol 1e-8",
+           "plain": {"steps": steps, "ms_per_step": ms, "cell_updates_per_s": nx * ny / (ms / 1e3),
+                     "poisson_iters_per_step": float(its.mean())}}
+    out["poisson"] = poisson_compare(sim, learned.pretrained(), maxiter=20000)
     del sim, case
     torch.cuda.empty_cache()
     return out
+
+
+def _graph_steps(sim, steps: int, warmup: int, flush, clock_name: str | None = None):
+    """Replay a one-step graph with events at its start, around its pressure solve and
+    at its end: ``warmup`` untimed steps, then ``steps`` timed ones with L2 flushed
+    before each. Returns (step ms list, solve ms list, kernels per step, clocks)."""
+    import torch
+
+    from cfd2d_b200 import _lib
+
+    L = _lib.lib()
+    stream = sim._stream
+    sptr = _lib.stream_ptr(stream)
+    ev = (C.c_void_p * 4)()
+    _lib.check(L.cfd2d_events_create(4, ev), "events")
+    graph = C.c_void_p(0)
+    knodes = C.c_int(0)
+    clk = None
+    try:
+        with torch.cuda.stream(stream):
+            sim._flush_mirrors()
+            sim._set_run_limits()
+            _lib.check(L.cfd2d_graph_capture_steps_ex(C.byref(sim._S), 1, sptr, ev, C.byref(graph),
+                                                      C.byref(knodes)), "capture")
+
+            def one_step():
+                flush.fill_(1.0)  # L2 flush (256 MiB write) outside the timed events
+                _lib.check(L.cfd2d_graph_launch(graph, sptr), "launch")
+                ms_step, ms_solve = C.c_float(), C.c_float()
+                _lib.check(L.cfd2d_event_elapsed_ms(ev[0], ev[3], C.byref(ms_step)), "elapsed")
+                _lib.check(L.cfd2d_event_elapsed_ms(ev[1], ev[2], C.byref(ms_solve)), "elapsed")
+                return ms_step.value, ms_solve.value
+
+            for _ in range(warmup):
+                one_step()
+            torch.cuda.synchronize()
+            step_ms, solve_ms = [], []
+            if clock_name:
+                clk = _Clocks(_clocks_path(clock_name)).__enter__()
+            try:
+                for _ in range(steps):
+                    a, b = one_step()
+                    step_ms.append(a)
+                    solve_ms.append(b)
+                torch.cuda.synchronize()
+            finally:
+                if clk is not None:
+                    clk.__exit__(None, None, None)
+            sim._st_fresh = False
+            sim._after_steps()
+    finally:
+        if graph.value:
+            L.cfd2d_graph_destroy(graph)
+        L.cfd2d_events_destroy(4, ev)
+    return step_ms, solve_ms, int(knodes.value), clk
+
+
+def cylinder_section(steps: int, warmup: int, flush) -> dict:
+    """The cylinder channel with a passive scalar (plain FP64 path), graph-timed."""
+    import numpy as np
+
+    from cfd2d_b200 import cases
+
+    case = cases.build_case(CYL_SPEC)
+    sim = case.sim
+    sim.pressure.tol = CG_RTOL
+    step_ms, solve_ms, knodes, _ = _graph_steps(sim, steps, warmup, flush)
+    its = np.array(sim.history.extra["cg_iterationen"][-steps:], dtype=float)
+    dev_s = sum(step_ms) / 1e3
+    solve_s = sum(solve_ms) / 1e3
+    cells = CYL_NX * CYL_NY
+    achieved = (BYTES_PER_CELL_ITER * cells * its.sum() + BYTES_PER_CELL_SOLVE * cells * len(its)) / solve_s / 1e9
+    peak, _ = _peaks()
+    return {"workload": CYL_WORKLOAD, "steps": steps, "ms_per_step": 1e3 * dev_s / steps,
+            "cell_updates_per_s": cells * steps / dev_s, "poisson_ms": 1e3 * solve_s / steps,
+            "poisson_iters_per_step": float(its.mean()), "kernels_per_step": knodes,
+            "solver": "k_pcg_cluster (on-chip)", "solver_equiv_gbs": achieved, "solver_equiv_frac": achieved / peak}
 
 
 # ------------------------------------------------------------------ mixed precision
@@ -385,7 +595,7 @@ def mixed_section(steps: int = 300) -> dict:
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     res = {}
     for prec in ("fp64", "mixed"):
-        case = cases.build_case(SPEC)
+        case = cases.build_case(CYL_SPEC)
         sim = case.sim
         sim.pressure.tol = CG_RTOL
         sim.pressure.precision = prec
@@ -402,7 +612,7 @@ def mixed_section(steps: int = 300) -> dict:
     e = lambda a, b: float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))  # noqa: E731
     f64, mx = res["fp64"], res["mixed"]
     return {
-        "workload": f"{WORKLOAD}, {steps} steps after 5 from rest",
+        "workload": f"{CYL_WORKLOAD}, {steps} steps after 5 from rest",
         "fp64": {"ms_per_step": f64["ms_per_step"], "poisson_iters_per_step": f64["iters"]},
         "mixed": {"ms_per_step": mx["ms_per_step"], "poisson_iters_per_step": mx["iters"]},
         "rel_err_vs_fp64": {"u": e(mx["fields"][0], f64["fields"][0]), "v": e(mx["fields"][1], f64["fields"][1]),
@@ -518,6 +728,17 @@ def configs_section(cavity_steps: int = 2000, sst_steps: int = 500) -> dict:
 
 
 # ------------------------------------------------------------------ GPU arm
+def _optional(flag: bool, fn):
+    """An optional section: None when skipped, an error record if it fails (an
+    optional section never costs the bench line)."""
+    if flag:
+        return None
+    try:
+        return fn()
+    except Exception as exc:
+        return {"error": f"{type(exc).__name__}: {exc}"}
+
+
 def run_b200(args, dist, rank, world):
     import numpy as np
     import torch
@@ -526,52 +747,19 @@ def run_b200(args, dist, rank, world):
     torch.cuda.set_device(local)
     from cfd2d_b200 import _lib, cases
 
-    L = _lib.lib()
-    case = cases.build_case(SPEC)
+    case = cases.obstacle_flow(SEED, NX, NY, pressure_solver="cg")
     sim = case.sim
     sim.pressure.tol = CG_RTOL
     stream = sim._stream
-    sptr = _lib.stream_ptr(stream)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    ev = (C.c_void_p * 4)()
-    _lib.check(L.cfd2d_events_create(4, ev), "events")
-    graph = C.c_void_p(0)
-    knodes = C.c_int(0)
-    with torch.cuda.stream(stream):
-        sim._flush_mirrors()
-        sim._set_run_limits()
-        _lib.check(L.cfd2d_graph_capture_steps_ex(C.byref(sim._S), 1, sptr, ev, C.byref(graph),
-                                                  C.byref(knodes)), "capture")
-
-        def one_step():
-            flush.fill_(1.0)  # L2 flush (256 MiB write) outside the timed events
-            _lib.check(L.cfd2d_graph_launch(graph, sptr), "launch")
-            ms_step, ms_solve = C.c_float(), C.c_float()
-            _lib.check(L.cfd2d_event_elapsed_ms(ev[0], ev[3], C.byref(ms_step)), "elapsed")
-            _lib.check(L.cfd2d_event_elapsed_ms(ev[1], ev[2], C.byref(ms_solve)), "elapsed")
-            return ms_step.value, ms_solve.value
-
-        for _ in range(args.warmup):
-            one_step()
-        n0 = sim._pull().n
-        _barrier(dist)
-        torch.cuda.synchronize()
-        step_ms, solve_ms = [], []
-        with _Clocks(_clocks_path(f"clocks_rank{rank}.csv")) as clk:
-            t0 = time.perf_counter()
-            for _ in range(args.steps):
-                a, b = one_step()
-                step_ms.append(a)
-                solve_ms.append(b)
-            torch.cuda.synchronize()
-            wall = time.perf_counter() - t0
-        _barrier(dist)
-        st = sim._pull()
-        if st.status & (_lib.S_NONFINITE | _lib.S_BARRIER_TIMEOUT):
-            raise RuntimeError(f"device status {st.status} during the bench")
-        sim._pull_history()
-        its = np.array(sim.history.extra["cg_iterationen"][-args.steps:], dtype=float)
-    assert st.n - n0 == args.steps
+    n0 = sim._pull().n
+    _barrier(dist)
+    step_ms, solve_ms, knodes, clk = _graph_steps(sim, args.steps, args.warmup, flush,
+                                                  f"clocks_rank{rank}.csv")
+    _barrier(dist)
+    st = sim._pull()
+    assert st.n - n0 == args.steps + args.warmup
+    its = np.array(sim.history.extra["cg_iterationen"][-args.steps:], dtype=float)
     dev_s = sum(step_ms) / 1e3
     dev_s_max = _max_over_ranks(dist, dev_s)
     cells = NX * NY
@@ -582,18 +770,14 @@ def run_b200(args, dist, rank, world):
     peak, peak_kind = _peaks()
 
     # ---- end to end through the public API with host buffers
-    e2e_steps = max(1, min(args.steps, 100))
-    host = {}
-    names = ("u", "v")
-    phi_dev = sim.scalars["c"].phi_gpu
+    e2e_steps = args.steps
     with torch.cuda.stream(stream):
-        for nm in names:
-            host[nm] = torch.empty(getattr(sim, "_" + nm).shape, dtype=torch.float64).pin_memory()
+        host = {nm: torch.empty(getattr(sim, "_" + nm).shape, dtype=torch.float64).pin_memory()
+                for nm in ("u", "v")}
+        for nm in host:
             host[nm].copy_(getattr(sim, "_" + nm))
-        host["c"] = torch.empty(phi_dev.shape, dtype=torch.float64).pin_memory()
-        host["c"].copy_(phi_dev)
-        out = {nm: torch.empty(t.shape, dtype=torch.float64).pin_memory()
-               for nm, t in (("u", sim._u), ("v", sim._v), ("p", sim._p), ("c", phi_dev))}
+        out = {nm: torch.empty(getattr(sim, "_" + nm).shape, dtype=torch.float64).pin_memory()
+               for nm in ("u", "v", "p")}
         h2d = sum(t.numel() * 8 for t in host.values())
         d2h = sum(t.numel() * 8 for t in out.values())
         _barrier(dist)
@@ -602,77 +786,74 @@ def run_b200(args, dist, rank, world):
         for _ in range(e2e_steps):
             sim._u.copy_(host["u"], non_blocking=True)
             sim._v.copy_(host["v"], non_blocking=True)
-            phi_dev.copy_(host["c"], non_blocking=True)
             sim.step()
-            out["u"].copy_(sim._u, non_blocking=True)
-            out["v"].copy_(sim._v, non_blocking=True)
-            out["p"].copy_(sim._p, non_blocking=True)
-            out["c"].copy_(phi_dev, non_blocking=True)
+            for nm in out:
+                out[nm].copy_(getattr(sim, "_" + nm), non_blocking=True)
             stream.synchronize()
             # this step's results are the next step's inputs: swap the pinned buffers
-            for nm in ("u", "v", "c"):
+            for nm in ("u", "v"):
                 host[nm], out[nm] = out[nm], host[nm]
         e2e_s = time.perf_counter() - t0
     e2e_s = _max_over_ranks(dist, e2e_s)
     e2e = world * cells * e2e_steps / e2e_s
-    L.cfd2d_graph_destroy(graph)
-    L.cfd2d_events_destroy(4, ev)
-    clocks = clk.summary(local)
+    clocks = clk.summary(local) if clk is not None else None
 
     if rank != 0:
         return
-    stencils = stencil_roofline(peak) if not args.no_stencils else None
-    mixed = None
-    if not args.no_mixed:
-        try:
-            mixed = mixed_section()
-        except Exception as exc:  # an optional section never costs the bench line
-            mixed = {"error": f"{type(exc).__name__}: {exc}"}
-    other = None
-    if not args.no_configs:
-        try:
-            other = configs_section()
-        except Exception as exc:  # an optional section never costs the bench line
-            other = {"error": f"{type(exc).__name__}: {exc}"}
-    vof = None
-    if not args.no_vof:
-        try:
-            vof = vof_section()
-        except Exception as exc:  # an optional section never costs the bench line
-            vof = {"error": f"{type(exc).__name__}: {exc}"}
-    learned_pc = None
-    if not args.no_learned:
-        try:
-            learned_pc = learned_section()
-        except Exception as exc:  # an optional section never costs the bench line
-            learned_pc = {"error": f"{type(exc).__name__}: {exc}"}
+    fluid_cells = int(sim.pressure.n)
+    del sim, case
+    torch.cuda.empty_cache()
+
+    def learned_all():
+        from cfd2d_b200 import learned
+
+        steps_rec = learned_steps(NX, NY, args.steps, args.warmup, flush)
+        c2 = cases.obstacle_flow(SEED, NX, NY, pressure_solver="cg")
+        c2.sim.pressure.tol = CG_RTOL
+        c2.sim.advance(args.warmup)
+        cmp = poisson_compare(c2.sim, learned.pretrained(), maxiter=5000)
+        return {"workload": f"{WORKLOAD}; pressure by flexible CG with the learned preconditioner to the same "
+                            f"rtol (plain Jacobi-PCG continues if it stalls)",
+                "value": steps_rec["cell_updates_per_s"], "unit": "cell-updates/s", "step": steps_rec,
+                "poisson": cmp}
+
+    learned_rec = _optional(args.no_learned, learned_all)
+    big = _optional(args.no_large, lambda: grid2048_section(3, flush))
+    cyl = _optional(args.no_cylinder, lambda: cylinder_section(100, 10, flush))
+    stencils = _optional(args.no_stencils, lambda: stencil_roofline(peak))
+    mixed = _optional(args.no_mixed, mixed_section)
+    other = _optional(args.no_configs, configs_section)
+    vof = _optional(args.no_vof, vof_section)
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
-        d = cpu_oracle_rate(3, 1, 1)
+        d = cpu_oracle_sample(0, 1, 2, 1, iters_per_step=iters)
         cpu = {"value": d["rate"], "unit": "cell-updates/s", "cores": 1, "kind": "port",
-               "sample": "3 steps after 1 warm-up step of the oracle (NumPy + scipy-form CG, "
-                         "1 thread) on the same workload from rest"}
+               "sample": f"oracle step on 1 thread (NumPy stencils, scipy cg + Jacobi as cfd2d/pressure.py:171): "
+                         f"1 warm-up and 2 timed steps from rest, each running {CPU_CG_SAMPLE} CG iterations, "
+                         f"its solve time scaled to the {iters:.0f} iterations per step of this run"}
     line = {
         "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dev_s_max / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (flow from rest, as the reference case)",
-        "config": {"workload": WORKLOAD, "grid": [NX, NY], "cells": cells, "fluid_cells": int(sim.pressure.n),
+        "data": "synthetic (seeded obstacle flow from rest, as the reference's cases start)",
+        "config": {"workload": WORKLOAD, "grid": [NX, NY], "cells": cells, "fluid_cells": fluid_cells,
                    "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"replicas x{world}",
-                   "pcg_cluster_ctas": int(sim.pressure.cluster)},
+                   "solver": "plain FP64 Jacobi-PCG (k_pcg_grid)"},
         "poisson_ms": 1e3 * solve_s / args.steps,
         "poisson_iters_per_step": iters,
-        "wall_ms_per_step": 1e3 * wall / args.steps,
         "e2e": {"value": e2e, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "steps": e2e_steps},
-        "gpu_launches": int(knodes.value) * args.steps,
+        "gpu_launches": knodes * args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": _ncu_traffic(),
-                     "kernel": "k_pcg_cluster (on-chip FP64 Jacobi-PCG)", "peak_kind": peak_kind},
+                     "frac": achieved / peak, "traffic": _ncu_traffic("pcg_grid_obstacles1024x512.txt"),
+                     "kernel": "k_pcg_grid (FP64 Jacobi-PCG, one persistent launch per solve)",
+                     "peak_kind": peak_kind},
         "cpu_baseline": cpu,
         "clocks": clocks,
+        "learned": learned_rec,
+        "grid_2048x1024": big,
+        "cylinder_440x82": cyl,
         "stencils": stencils,
-        "learned_pc": learned_pc,
         "mixed_precision": mixed,
         "vof_dam_break": vof,
         "other_workloads": other,
@@ -759,8 +940,10 @@ def main():
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision section")
     ap.add_argument("--no-vof", action="store_true", help="skip the two-phase dam-break section")
     ap.add_argument("--no-configs", action="store_true", help="skip the cavity and SST channel section")
-    ap.add_argument("--workload", choices=["cylinder", "batch"], default="cylinder",
-                    help="cylinder: the headline; batch: 256 uneven cavities stepped together")
+    ap.add_argument("--no-large", action="store_true", help="skip the 2048 x 1024 section")
+    ap.add_argument("--no-cylinder", action="store_true", help="skip the cylinder 440 x 82 section")
+    ap.add_argument("--workload", choices=["obstacles", "batch"], default="obstacles",
+                    help="obstacles: the headline; batch: 256 uneven cavities stepped together")
     ap.add_argument("--batch-cases", type=int, default=256)
     args = ap.parse_args()
     if args.warmup < 3:

@@ -144,6 +144,49 @@ def custom_obstacles(obstacles: list, lx: float = 4.0, ly: float = 1.0, nx: int 
     return Case("custom", "Eigene Hindernisse", sim, t_end, steady_tol, U, L_ref, re, info)
 
 
+def random_obstacles(rng, lx: float = 2.0, ly: float = 1.0, nmin: int = 2, nmax: int = 12) -> list:
+    """Seeded obstacle list of the obstacle-flow workload: 2-12 circles, ellipses or
+    rectangles (``custom_obstacles`` specs), centres uniform in the middle 70 % of
+    each side, sizes (radius, semi-axis, half-width) uniform in 0.02-0.08 of the
+    domain height. Draws from ``rng`` in a fixed order, so a seed names the list."""
+    specs = []
+    for _ in range(int(rng.integers(nmin, nmax + 1))):
+        kind = rng.integers(0, 3)
+        x = float(rng.uniform(0.15 * lx, 0.85 * lx))
+        y = float(rng.uniform(0.15 * ly, 0.85 * ly))
+        size = float(rng.uniform(0.02, 0.08) * ly)
+        if kind == 0:
+            specs.append({"typ": "kreis", "x": x, "y": y, "r": size})
+        elif kind == 1:
+            specs.append({"typ": "ellipse", "x": x, "y": y, "a": size, "b": size * float(rng.uniform(0.4, 1.0)),
+                          "winkel": float(rng.uniform(0, 180))})
+        else:
+            specs.append({"typ": "rechteck", "x0": x - size, "y0": y - 0.6 * size, "x1": x + size,
+                          "y1": y + 0.6 * size})
+    return specs
+
+
+def random_obstacle_spec(rng, lx: float = 2.0, ly: float = 1.0) -> tuple[list, float]:
+    """(obstacles, Re) of one seeded obstacle flow: Re log-uniform in 200-2000 (drawn
+    first), then ``random_obstacles``."""
+    re = float(np.exp(rng.uniform(np.log(200.0), np.log(2000.0))))
+    return random_obstacles(rng, lx, ly), re
+
+
+def random_obstacle_flow(rng, nx: int, ny: int, lx: float = 2.0, ly: float = 1.0, **num) -> Case:
+    """One seeded obstacle flow: ``custom_obstacles`` with a block inflow U = 1,
+    outflow p = 0, slip walls and the obstacles and Re of ``random_obstacle_spec``."""
+    obstacles, re = random_obstacle_spec(rng, lx, ly)
+    return custom_obstacles(obstacles, lx=lx, ly=ly, nx=nx, ny=ny, re=re, inflow_profile="uniform",
+                            walls="slip", **num)
+
+
+def obstacle_flow(seed: int = 13, nx: int = 1024, ny: int = 512, **num) -> Case:
+    """The obstacle-flow benchmark case: ``random_obstacle_flow`` on a 2 x 1 domain
+    drawn from ``np.random.default_rng(seed)``."""
+    return random_obstacle_flow(np.random.default_rng(seed), nx, ny, **num)
+
+
 def heated_cavity(ra: float = 1e4, pr: float = 0.71, n: int = 48, t_end: float = 500.0,
                   steady_tol: float | None = 1e-6, limiter: str = "vanleer", **num) -> Case:
     """Differentially heated square cavity (cfd2d/cases.py:207-223)."""

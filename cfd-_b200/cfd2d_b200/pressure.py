@@ -29,6 +29,7 @@ from .grid import Grid
 
 DIRECT_RTOL = 1e-13
 DIRECT_MAXITER = 50000
+CG_MAXITER = 5000  # scipy cg's maxiter in cfd2d/pressure.py:171
 
 
 class PressureSolver:
@@ -41,6 +42,7 @@ class PressureSolver:
         self.grid = grid
         self.method = "direct" if method == "lu" else method
         self._tol = float(tol)
+        self._cg_maxiter = CG_MAXITER
         self.on_change = None
         nx, ny = grid.nx, grid.ny
         self.dx2 = dx2 = 1.0 / grid.dx ** 2
@@ -221,7 +223,17 @@ class PressureSolver:
 
     @property
     def maxiter(self) -> int:
-        return DIRECT_MAXITER if self.method == "direct" else 5000
+        """Iteration cap of the CG: 5000 for 'cg' as the reference (settable, e.g. for
+        grids whose solve needs more), 50000 for 'direct'."""
+        return DIRECT_MAXITER if self.method == "direct" else self._cg_maxiter
+
+    @maxiter.setter
+    def maxiter(self, value: int) -> None:
+        if int(value) < 1:
+            raise ValueError("maxiter must be positive")
+        self._cg_maxiter = int(value)
+        if self.on_change is not None:
+            self.on_change()
 
     @property
     def _x0(self) -> np.ndarray:
@@ -271,13 +283,11 @@ class PressureSolver:
             warnings.warn(f"CG-Drucklöser nicht konvergiert ({self.maxiter} Iterationen)")
         return p.cpu().numpy() if host else p
 
-    def solve_variable(self, rhs, bx, by):
-        """Solve div(b grad p) = rhs with face coefficients b = 1/rho (cfd2d/pressure.py:187-244):
-        bx (nx+1, ny) on the x faces (face nx couples columns nx-1 and 0 when periodic),
-        by (nx, ny+1). The reference rebuilds the matrix and solves it directly on every
-        call; here the diagonal is assembled in its order on the host and the system is
-        solved by the variable-coefficient PCG on the device to a relative residual of
-        1e-13. The time step itself builds the operator on the device."""
+    def variable_operator(self, bx, by):
+        """The C-ABI operator of div(b grad p) with face coefficients bx (nx+1, ny) and
+        by (nx, ny+1), the diagonal assembled on the host in the reference's order
+        (cfd2d/pressure.py:187-236), with a zero warm start. Returns (op, tensors): the
+        device tensors the operator points to, which must outlive its use."""
         t = _lib.torch()
         g = self.grid
         nx, ny = g.nx, g.ny
@@ -320,6 +330,17 @@ class PressureSolver:
         op.x0 = x0.data_ptr()
         op.cluster, op.mixed = 0, 0
         op.grid_ctas = 16 if nx * ny <= 262144 else 0
+        return op, dev + [x0]
+
+    def solve_variable(self, rhs, bx, by):
+        """Solve div(b grad p) = rhs with face coefficients b = 1/rho (cfd2d/pressure.py:187-244):
+        bx (nx+1, ny) on the x faces (face nx couples columns nx-1 and 0 when periodic),
+        by (nx, ny+1). The reference rebuilds the matrix and solves it directly on every
+        call; here the diagonal is assembled in its order on the host and the system is
+        solved by the variable-coefficient PCG on the device to a relative residual of
+        1e-13. The time step itself builds the operator on the device."""
+        t = _lib.torch()
+        op, _keep = self.variable_operator(bx, by)
         r = _lib.to_dev(np.asarray(rhs, dtype=np.float64), t.float64)
         p = t.empty_like(r)
         st = t.zeros(1, dtype=t.int32, device=_lib.device())

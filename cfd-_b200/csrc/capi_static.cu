@@ -67,7 +67,8 @@ extern "C" int cfd2d_pressure_solve_static(const cfd2d_poisson* op, const double
     }
     PcgLaunch L = {};
     L.op = *op;
-    L.op.cluster = 0;  // the grid-persistent solver, the variant that uses scratch
+    L.op.cluster = 0;    // the grid-persistent solver, the variant that uses scratch,
+    L.op.grid_ctas = 0;  // as a cooperative launch over every SM (never the 16-CTA form)
     L.op.work = scratch;
     L.op.work_bytes = kScratchDoubles * sizeof(double);
     L.rhs_mode = 0;

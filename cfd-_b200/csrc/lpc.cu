@@ -266,6 +266,29 @@ __global__ void __launch_bounds__(NT) k_conv32_tc(const __nv_bfloat16* __restric
             }
             asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(TM) : "memory");
         }
+    } else {
+        // The accumulators never arrived: this CTA's output rows are written as zeros
+        // (a defined output; the host reads *err and abandons the result), and the
+        // MMAs get a second bounded wait before their TMEM columns are freed. TMEM
+        // contents are undefined after a timeout.
+        const int npx = min(TM, W - j0);
+        uint4* y4 = reinterpret_cast<uint4*>(y);
+        for (int r = 0; r < ROWS; ++r) {
+            const int i = i0 + r;
+            if (i >= H) break;
+            const size_t rowp = (size_t)i * W + j0;
+            for (int q = tid; q < npx * 4; q += NT) y4[rowp * 4 + q] = make_uint4(0u, 0u, 0u, 0u);
+        }
+        if (tid == 0) {
+            uint32_t done = 0;
+            for (uint32_t spin = 0; spin < kWaitLimit && !done; ++spin) {
+                asm volatile(
+                    "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+                    "selp.b32 %0, 1, 0, P1;\n\t}\n"
+                    : "=r"(done)
+                    : "r"(smem_u32(&mbar)), "r"(0));
+            }
+        }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();

@@ -431,13 +431,19 @@ int cfd2d_pressure_solve_snapshots(const cfd2d_poisson* op, const double* rhs, d
  * For callers that cannot provide cfd2d_poisson.work: a C or ctypes host that owns
  * no device allocator, or a time loop that must not call cudaMalloc/cudaFree
  * between steps (both can synchronise the device). Same arguments, results and
- * error codes as cfd2d_pressure_solve, always on the grid-persistent solver
- * (op->cluster and op->work are ignored); its scratch is a static device array of
- * the library (8.2 MiB per device), so nothing is allocated.
+ * error codes as cfd2d_pressure_solve, always on the grid-persistent solver as a
+ * cooperative launch over every SM: op->cluster, op->grid_ctas, op->work and
+ * op->work_bytes are ignored; every other field of *op is used as by
+ * cfd2d_pressure_solve (constant or variable coefficients, Neumann components).
+ * Its scratch is a static device array of the library (8.2 MiB per device), so
+ * nothing is allocated.
  *  - Grids above CFD2D_STATIC_MAX_CELLS cells return CFD2D_E_CAPACITY.
  *  - The first call on each device looks the array up (cudaGetSymbolAddress, which
  *    can load the library's module on that device): make it outside any stream
- *    capture, with that device current.
+ *    capture, with that device current. The address is kept for the life of the
+ *    process: a cudaDeviceReset (or anything else that destroys the device's
+ *    primary context) invalidates it, and the entry point must not be called on
+ *    that device afterwards.
  *  - Nothing has to start at zero: each call clears the solver's barrier words on
  *    `stream` before its launch, and the solver writes the rest before reading it.
  *  - All calls on one device share the array: two calls whose kernels can overlap

@@ -724,6 +724,15 @@ def pcg_scipy_trajectory(matvec, b, x0, rtol, maxiter, dinv, callback=None):
 class OPressure:
     """5-point operator A = -Lap over the fluid cells (cfd2d/pressure.py:32-140)."""
 
+    # scipy cg's maxiter in cfd2d/pressure.py:171; the CPU timing arm lowers it to
+    # time a bounded sample of a solve
+    maxiter = 5000
+    # "numpy": pcg_scipy_trajectory on the stencil matvec (the parity form);
+    # "scipy": scipy.sparse.linalg.cg on the assembled matrix with the Jacobi
+    # preconditioner, the call cfd2d/pressure.py:171 makes (the timing form).
+    # Set on the class to reach the solve a simulation makes while it is built.
+    engine = "numpy"
+
     def __init__(self, g, boundary, method="cg", tol=1e-10):
         if method == "lu":
             method = "direct"
@@ -791,6 +800,7 @@ class OPressure:
         self.x0 = np.zeros(n)
         self.last_iterations = 0
         self.last_info = 0
+        self._A = None
         if method == "direct":
             from scipy.sparse import csc_matrix
             from scipy.sparse.linalg import splu
@@ -807,6 +817,22 @@ class OPressure:
                [np.full(bp.sum(), -self.dx2)] * 2 + [self.diag[f]]
         return csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
                           shape=(self.n, self.n))
+
+    def _scipy_cg(self, b):
+        """scipy's cg with the Jacobi preconditioner, as cfd2d/pressure.py:165-172."""
+        from scipy.sparse.linalg import LinearOperator, cg
+
+        if self._A is None:
+            self._A = self._assemble().tocsc()
+            dinv = self.dinv
+            self._M = LinearOperator((self.n, self.n), matvec=lambda r: dinv * r)
+        it = [0]
+
+        def cb(_):
+            it[0] += 1
+
+        x, info = cg(self._A, b, x0=self.x0, rtol=self.tol, maxiter=self.maxiter, M=self._M, callback=cb)
+        return x, info, it[0]
 
     def matvec(self, xc):
         """y = A x summed per row in increasing column order, as scipy's csc_matvec.
@@ -851,7 +877,10 @@ class OPressure:
             x = self._lu.solve(b)
             self.last_iterations = 1
         else:
-            x, info, it = pcg_scipy_trajectory(self.matvec, b, self.x0, self.tol, 5000, self.dinv)
+            if self.engine == "scipy":
+                x, info, it = self._scipy_cg(b)
+            else:
+                x, info, it = pcg_scipy_trajectory(self.matvec, b, self.x0, self.tol, self.maxiter, self.dinv)
             self.last_iterations = it
             self.last_info = info
             if info > 0:

@@ -6,7 +6,7 @@ Run in a container that holds the reference checkout (default
     python tests/golden/make_golden.py [group ...]
 
 Groups: kernels geometry pressure cavity cylinder sst misc checkpoint smagorinsky
-functions vof validation shapes (default: all).
+functions vof validation shapes obstacles (default: all).
 The reference imports matplotlib at module load; ``mplstub/`` stands in for it
 (no fixture case needs plotting or polygon masks; NACA outlines and image
 obstacles do not use it). Every pressure solve uses the
@@ -561,10 +561,58 @@ def gen_shapes():
     _save("golden_shapes", out)
 
 
+def _obstacle_spec(seed):
+    """Obstacles and Re of the seeded obstacle flow (the package's generator, pure NumPy)."""
+    sys.path.insert(0, str(HERE.parent.parent / "cfd-_b200"))
+    from cfd2d_b200.cases import random_obstacle_spec
+
+    return random_obstacle_spec(np.random.default_rng(seed))
+
+
+def _digest(prefix, name, a, out, stride=8):
+    """Size-bounded record of a large field: every stride-th entry in both directions,
+    the sums of every row and every column, and the max-norm."""
+    out[f"{prefix}_{name}_sub"] = np.ascontiguousarray(a[::stride, ::stride])
+    out[f"{prefix}_{name}_rows"] = a.sum(axis=1)
+    out[f"{prefix}_{name}_cols"] = a.sum(axis=0)
+    out[f"{prefix}_{name}_max"] = np.array(np.abs(a).max())
+
+
+def gen_obstacles():
+    """The obstacle-flow benchmark case (seed 13, 1024 x 512, 2-12 obstacles, block
+    inflow, outflow p = 0, slip walls; scipy CG at 1e-8) run for 3 steps from rest;
+    fields stored as digests (_digest) at steps 1 and 3, the packed fluid flags
+    in full."""
+    out = {}
+    obst, re = _obstacle_spec(13)
+    out["obs1024_spec"] = np.array(repr((obst, re)))
+    case = cases.custom_obstacles(obst, lx=2.0, ly=1.0, nx=1024, ny=512, re=re, inflow_profile="uniform",
+                                  walls="slip", pressure_solver="cg")
+    sim = case.sim
+    sim.pressure.tol = TOL
+    out["obs1024_fluid_bits"] = np.packbits(sim.grid.fluid.astype(np.uint8), axis=None)
+    its, dts = [], []
+    t0 = time.time()
+    for n in range(1, 4):
+        sim.step()
+        its.append(sim.pressure.last_iterations)
+        dts.append(sim.dt)
+        if n in (1, 3):
+            for name in ("u", "v", "p"):
+                _digest(f"obs1024_{n}", name, getattr(sim, name), out)
+        print(f"obs1024 step {n}: {time.time() - t0:.0f}s, CG it {its[-1]}", flush=True)
+    out["obs1024_its"] = np.array(its)
+    out["obs1024_dt"] = np.array(dts)
+    out["obs1024_hist_fx"] = np.array(sim.history.fx)
+    out["obs1024_hist_fy"] = np.array(sim.history.fy)
+    _save("golden_obstacles1024", out)
+
+
 GROUPS = {"kernels": gen_kernels, "geometry": gen_geometry, "pressure": gen_pressure,
           "cavity": gen_cavity, "cylinder": gen_cylinder, "sst": gen_sst, "misc": gen_misc,
           "checkpoint": gen_checkpoint, "smagorinsky": gen_smagorinsky, "functions": gen_functions,
-          "vof": gen_vof, "validation": gen_validation, "shapes": gen_shapes}
+          "vof": gen_vof, "validation": gen_validation, "shapes": gen_shapes,
+          "obstacles": gen_obstacles}
 
 if __name__ == "__main__":
     import warnings

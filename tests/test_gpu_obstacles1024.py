@@ -1,0 +1,70 @@
+"""Step parity on the benchmark workload: the seeded 1024 x 512 obstacle flow.
+
+The fixture (tests/golden/golden_obstacles1024.npz, written by make_golden.py's
+``obstacles`` group) holds the reference's own run of this case (scipy CG at
+1e-8, 3 steps from rest): the fluid flags in full and, at steps 1 and 3, every
+8th value of u, v and p in both directions, the sums of every row and column and
+the max-norm. The device run must give the same flags bit for bit, the same CG
+iteration counts within 3, the same dt series and fields within 1e-10 relative
+(max-norm of the difference over the max-norm of the reference field); the row
+and column sums, which see every cell, within 1e-10 of the sums' scale.
+"""
+
+from __future__ import annotations
+
+import ast
+
+import numpy as np
+import pytest
+
+from conftest import golden
+
+TOL = 1e-10
+
+
+def _fixture():
+    return golden("golden_obstacles1024")
+
+
+def test_fixture_spec_is_the_generator_seed():
+    """The fixture's obstacles and Re are what the package's generator draws for seed 13."""
+    from cfd2d_b200.cases import random_obstacle_spec
+
+    g = _fixture()
+    obst, re = ast.literal_eval(str(g["obs1024_spec"]))
+    obst2, re2 = random_obstacle_spec(np.random.default_rng(13))
+    assert re == re2
+    assert obst == obst2
+
+
+@pytest.mark.gpu
+def test_obstacle_flow_1024x512_three_steps(cuda_lib):
+    from cfd2d_b200 import cases
+
+    g = _fixture()
+    case = cases.obstacle_flow(13, 1024, 512, pressure_solver="cg")
+    sim = case.sim
+    sim.pressure.tol = 1e-8
+    flags = np.packbits(sim.grid.fluid.astype(np.uint8), axis=None)
+    assert np.array_equal(flags, g["obs1024_fluid_bits"])
+    for n in (1, 2, 3):
+        sim.step()
+        if n not in (1, 3):
+            continue
+        for name in ("u", "v", "p"):
+            a = getattr(sim, name)
+            ref_max = float(g[f"obs1024_{n}_{name}_max"])
+            sub = a[::8, ::8]
+            d_sub = np.abs(sub - g[f"obs1024_{n}_{name}_sub"]).max() / ref_max
+            assert d_sub < TOL, (n, name, d_sub)
+            for ax, key in ((1, "rows"), (0, "cols")):
+                s = a.sum(axis=ax)
+                ref = g[f"obs1024_{n}_{name}_{key}"]
+                scale = ref_max * a.shape[ax]
+                d = np.abs(s - ref).max() / scale
+                assert d < TOL, (n, name, key, d)
+    its = np.array(sim.history.extra["cg_iterationen"][-3:])
+    assert np.abs(its - g["obs1024_its"]).max() <= 3, (its, g["obs1024_its"])
+    np.testing.assert_allclose(sim.history.dt[-3:], g["obs1024_dt"], rtol=1e-12)
+    fx = np.array(sim.history.fx[-3:])
+    assert np.abs(fx - g["obs1024_hist_fx"]).max() / np.abs(g["obs1024_hist_fx"]).max() < 1e-9

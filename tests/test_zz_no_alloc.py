@@ -100,3 +100,59 @@ def test_static_scratch_rejects_grids_above_capacity(cuda_lib):
     rc = lib.cfd2d_pressure_solve_static(C.byref(op), _lib.ptr(buf), _lib.ptr(buf), 1e-8, 10, None, None,
                                          _lib.stream_ptr())
     assert rc == _lib.E_CAPACITY
+
+
+@pytest.mark.parametrize("kind", ["variable_coefficients", "neumann_components"])
+def test_static_scratch_other_operators(cuda_lib, kind):
+    """The other operators the entry point accepts: variable face coefficients (the
+    two-phase projection's, here random positive 1/rho on a cavity) and a domain with
+    two Neumann-only components (walls all round, split by a solid column), each
+    against cfd2d_pressure_solve's grid-persistent form on a caller workspace, two
+    calls in a row."""
+    import torch
+
+    from cfd2d_b200 import _lib, geometry
+    from cfd2d_b200.boundary import BoundaryCondition as BC
+    from cfd2d_b200.grid import Grid
+    from cfd2d_b200.solver import Simulation
+
+    nx, ny = 96, 80
+    grid = Grid(nx, ny, 1.2, 1.0)
+    if kind == "neumann_components":
+        grid.add_obstacle(geometry.rectangle(grid, 0.58, -1.0, 0.62, 2.0))
+    bcs = {s: BC("noslip") for s in ("left", "right", "bottom", "top")}
+    sim = Simulation(grid, bcs, nu=0.01, pressure_solver="cg")
+    ps = sim.pressure
+    ps.tol = 1e-10
+    ps.ensure_workspace()
+    rng = np.random.default_rng(5)
+    keep = []
+    if kind == "variable_coefficients":
+        bx = rng.uniform(0.001, 1.0, (nx + 1, ny))
+        by = rng.uniform(0.001, 1.0, (nx, ny + 1))
+        op, keep = ps.variable_operator(bx, by)
+        x0_d = keep[-1].view(-1)
+    else:
+        assert len(ps.neumann_components) == 2
+        op = _lib.Poisson.from_buffer_copy(ps.op)
+        x0_d = ps._d_x0.view(-1)
+    lib = _lib.lib()
+    work = torch.zeros(int(lib.cfd2d_pcg_workspace_bytes(nx, ny)) // 8, dtype=torch.float64, device=_lib.device())
+    op_grid = _lib.Poisson.from_buffer_copy(op)
+    op_grid.cluster, op_grid.grid_ctas = 0, 0
+    op_grid.work, op_grid.work_bytes = work.data_ptr(), work.numel() * 8
+    op_static = _lib.Poisson.from_buffer_copy(op)
+    op_static.work, op_static.work_bytes = 0, 0
+    start = torch.zeros_like(x0_d)
+    for call in range(2):
+        rhs = rng.standard_normal((nx, ny)) * grid.fluid_interior
+        rhs_d = _lib.to_dev(rhs, torch.float64)
+        p_s, x_s, it_s = _solve(lib.cfd2d_pressure_solve_static, op_static, rhs_d, x0_d, start.clone(), 1e-10,
+                                20000, torch, _lib)
+        p_g, x_g, it_g = _solve(lib.cfd2d_pressure_solve, op_grid, rhs_d, x0_d, start.clone(), 1e-10, 20000,
+                                torch, _lib)
+        assert it_s > 0 and it_s == it_g, (kind, call, it_s, it_g)
+        assert _relerr(p_s, p_g) < SAME_VARIANT_RTOL, (kind, call)
+        assert _relerr(x_s, x_g) < SAME_VARIANT_RTOL, (kind, call)
+        start = torch.from_numpy(x_s).to(x0_d.device).view_as(x0_d)
+    del keep
