@@ -31,6 +31,9 @@ namespace {
 
 constexpr int kPcgThreads = 512;
 constexpr int kSlot = 4 + CFD2D_MAX_COMPONENTS;  // doubles per CTA partial (grid kernel)
+// Upper bound on the CTAs of the workspace solver (its partial arrays are sized for
+// it; the launch checks the device's actual count against it): 148 SMs x 32.
+constexpr int kMaxGridCtas = 148 * 32;
 constexpr int kArrays = 7;                       // X, R, P0, P1, DI, DG, Z per cell
 constexpr int kMaxK = 4;                         // values per cluster reduction
 
@@ -1205,24 +1208,537 @@ __global__ void __launch_bounds__(CL ? kClusterL2Threads : kGridThreads, 1) k_pc
 #undef SSUM
 }
 
+// ---------------------------------------------------------------- slab solver
+// The grid-persistent solver for grids beyond one cluster whose state still fits in
+// the shared memory of one CTA per SM (k_pcg_slab): CTA b owns a slab of whole rows
+// and keeps x, r, z, p (two buffers), 1/diag, diag and the coupling bits of its cells
+// on chip for the whole solve, as the cluster solver does; only the first and last
+// row of each slab cross to its two neighbours, through global memory (L2), and the
+// dot products are reduced over the grid without atomics (flag_sum). Per iteration:
+// phase A (p = z + beta p, q = A p, p.q partial; the slab's boundary rows of p are
+// published), reduction 1, the neighbours' boundary rows of p are read; phase B (x, r,
+// z update, r.r and r.z partials; boundary rows of z published), reduction 2, the
+// neighbours' boundary rows of z are read. Same iteration form and operation order as
+// the other forms (scipy's, csc_matvec row order).
 namespace {
 
+constexpr int kSlabThreads = 512;
+constexpr int kFlagStride = 24;  // doubles per reduction slot: kSlot values, then the sequence word
+constexpr long long kFlagSpinLimit = 1LL << 24;
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Grid-wide sum of K values without atomics or a separate barrier. Thread 0 of each
+// CTA stores its block partial and then, with release semantics, the reduction's
+// sequence number `seq` in the CTA's own slot (two slot sets, used by the parity of
+// seq). Warp 0 of every CTA polls all G slots until each carries `seq` (bounded: a
+// wait that gives up sets CFD2D_S_BARRIER_TIMEOUT and the call returns false), then
+// adds the partials lane-strided and by a butterfly, the same order in every CTA, so
+// every CTA gets the same bits. A CTA rewrites a slot set two reductions later, which
+// it reaches only after every CTA has written the reduction in between, i.e. after
+// every CTA has finished reading this one. Global stores a CTA made before the call
+// are visible to every CTA after it (read them with __ldcg: L1 is not coherent).
+template <int K>
+__device__ __forceinline__ bool flag_sum(double (&v)[K], double* red_smem, double* slots, unsigned long long seq,
+                                         int* status) {
+    static_assert(K <= kSlot, "slot capacity");
+    __shared__ double fsum[kSlot];
+    __shared__ int fok;
+    block_sum<K>(v, red_smem);
+    const int G = gridDim.x;
+    double* set = slots + (size_t)(seq & 1ull) * G * kFlagStride;
+    if (threadIdx.x == 0) {
+        double* my = set + (size_t)blockIdx.x * kFlagStride;
+#pragma unroll
+        for (int k = 0; k < K; ++k) my[k] = v[k];
+        __threadfence();
+        st_release_u64(reinterpret_cast<unsigned long long*>(my + kSlot), seq);
+    }
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        bool ok = true;
+        double x[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) x[k] = 0.0;
+        for (int b = lane; b < G && ok; b += 32) {
+            const double* sl = set + (size_t)b * kFlagStride;
+            const unsigned long long* gw = reinterpret_cast<const unsigned long long*>(sl + kSlot);
+            long long spins = 0;
+            while (ld_acquire_u64(gw) != seq) {
+                if (++spins > kFlagSpinLimit) {
+                    ok = false;
+                    break;
+                }
+            }
+            if (ok) {
+#pragma unroll
+                for (int k = 0; k < K; ++k) x[k] += __ldcg(sl + k);
+            }
+        }
+        ok = __all_sync(0xffffffffu, ok);
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) x[k] += __shfl_xor_sync(0xffffffffu, x[k], o);
+        }
+        if (lane == 0) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) fsum[k] = x[k];
+            fok = ok ? 1 : 0;
+            if (!ok && status) atomicOr(status, CFD2D_S_BARRIER_TIMEOUT);
+        }
+        __threadfence();
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = fsum[k];
+    // fsum is rewritten by the next call only after its block_sum barrier
+    return fok != 0;
+}
+
+}  // namespace
+
+// Shared memory of one slab: seven doubles and one byte per own cell, two halo rows
+// of z and two of p (the latter hold x0 in the prologue).
+size_t pcg_slab_smem_bytes(int cap, int ny) { return (size_t)cap * (kArrays * sizeof(double) + 1) + 4 * (size_t)ny * sizeof(double) + 16; }
+
+template <int CPT>
+__global__ void __launch_bounds__(kSlabThreads, 1) k_pcg_slab(PcgLaunch L) {
+    if (L.active && *L.active == 0) return;  // uniform over the grid
+    const cfd2d_poisson& op = L.op;
+    const int nx = op.nx, ny = op.ny;
+    const bool periodic = op.periodic != 0;
+    const int G = gridDim.x, me = blockIdx.x;
+    const int r0 = row0_of(me, nx, G), r1 = row0_of(me + 1, nx, G);
+    const int rows = r1 - r0;
+    const int nloc = rows * ny;
+    const int cap = L.cap_cells;
+    const int tid = threadIdx.x;
+    const double mdx2 = -op.dx2, mdy2 = -op.dy2;
+    const int goff = r0 * ny;
+    const int n = nx * ny;
+
+    extern __shared__ __align__(16) double sm[];
+    double* X = sm;
+    double* R = X + cap;
+    double* P0 = R + cap;
+    double* P1 = P0 + cap;
+    double* DI = P1 + cap;
+    double* DG = DI + cap;
+    double* Z = DG + cap;
+    double* HZ = Z + cap;        // z of the west halo row at [0, ny), of the east one at [ny, 2 ny)
+    double* HP = HZ + 2 * ny;    // p of the halo rows (x0 in the prologue), same layout
+    uint8_t* NB = reinterpret_cast<uint8_t*>(HP + 2 * ny);
+    __shared__ double red_smem[32 * kSlot];
+    __shared__ double cmean[CFD2D_MAX_COMPONENTS];
+    // global exchange rows and reduction slots in the workspace
+    double* GZ = op.work;
+    double* GP = op.work + n;
+    double* slots = op.work + 3 * (size_t)n;
+    unsigned long long seq = 0;
+    int* status = L.status_out;
+    const int iw = (r0 == 0) ? (periodic ? nx - 1 : -1) : r0 - 1;
+    const int ie = (r1 == nx) ? (periodic ? 0 : -1) : r1;
+    const unsigned magic = (unsigned)(((1ull << 32) + (unsigned)ny - 1) / (unsigned)ny);
+
+    // ------------------------------------------------------------ prologue
+    double dt = 1.0;
+    if (L.rhs_mode == 1) dt = L.dt_ptr ? *L.dt_ptr : L.dt_const;
+    double csum[CFD2D_MAX_COMPONENTS + 1];
+#pragma unroll
+    for (int k = 0; k <= CFD2D_MAX_COMPONENTS; ++k) csum[k] = 0.0;
+    for (int c = tid; c < nloc; c += kSlabThreads) {
+        const int gidx = goff + c;
+        const uint8_t nb = op.nbr[gidx];
+        NB[c] = nb;
+        const double x0 = op.x0[gidx];
+        X[c] = x0;
+        DI[c] = op.dinv[gidx];
+        DG[c] = op.diag[gidx];
+        double braw = 0.0;
+        if (nb & 0x80) {
+            if (L.rhs_mode == 0) {
+                braw = L.rhs[gidx];
+            } else {
+                // div(F, G) / dt at interior cell (i+1, j+1) (cfd2d/solver.py:264-266)
+                const int li = (int)__umulhi((unsigned)c, magic);
+                const int j = c - li * ny;
+                const int pu = ny + 2, pv = ny + 1;
+                const int ig = r0 + li + 1, jg = j + 1;
+                const double div = (L.F[ig * pu + jg] - L.F[(ig - 1) * pu + jg]) / L.dx +
+                                   (L.G[ig * pv + jg] - L.G[ig * pv + jg - 1]) / L.dy;
+                braw = div / dt;
+            }
+            const int lab = op.ncomp > 0 ? op.label[gidx] : -1;
+#pragma unroll
+            for (int k = 0; k < CFD2D_MAX_COMPONENTS; ++k)
+                if (k == lab) csum[k] += braw;
+            if (x0 != 0.0) csum[CFD2D_MAX_COMPONENTS] += 1.0;
+        }
+        R[c] = braw;
+    }
+    // x0 of the halo rows: written by the caller before the launch, rewritten by this
+    // kernel only in its epilogue, which no CTA reaches before every CTA is past here
+    for (int t = tid; t < 2 * ny; t += kSlabThreads) {
+        const int row = t < ny ? iw : ie;
+        HP[t] = row >= 0 ? op.x0[(size_t)row * ny + (t < ny ? t : t - ny)] : 0.0;
+    }
+    // scipy computes A x0 only if x0 has a nonzero; Neumann-component sums of b
+    if (!flag_sum<CFD2D_MAX_COMPONENTS + 1>(csum, red_smem, slots, ++seq, status)) return;
+    const bool x_any = csum[CFD2D_MAX_COMPONENTS] > 0.0;
+    const int ncomp = op.ncomp;
+    if (tid < ncomp) cmean[tid] = csum[tid] / op.comp_count[tid];
+    __syncthreads();
+
+    double part[3] = {0.0, 0.0, 0.0};
+    for (int c = tid; c < nloc; c += kSlabThreads) {
+        const uint8_t nb = NB[c];
+        if (!(nb & 0x80)) { P1[c] = 0.0; P0[c] = 0.0; R[c] = 0.0; Z[c] = 0.0; continue; }
+        double b = R[c];
+        if (ncomp > 0) {
+            const int lab = op.label[goff + c];
+            if (lab >= 0) b = b - cmean[lab];
+        }
+        b = -b;
+        P1[c] = b;  // kept for the ||b|| == 0 return
+        double r = b;
+        if (x_any) {
+            const int li = (int)__umulhi((unsigned)c, magic);
+            const int j = c - li * ny;
+            double tW = 0.0, tS = 0.0, tN = 0.0, tE = 0.0;
+            if (nb & 2) tS = mdy2 * X[c - 1];
+            if (nb & 4) tN = mdy2 * X[c + 1];
+            if (nb & 1) tW = mdx2 * ((li > 0) ? X[c - ny] : HP[j]);
+            if (nb & 8) tE = mdx2 * ((li < rows - 1) ? X[c + ny] : HP[ny + j]);
+            r = b - row_sum(periodic, r0 + li, nx, tW, tS, DG[c] * X[c], tN, tE);
+        }
+        R[c] = r;
+        P0[c] = 0.0;
+        const double z = DI[c] * r;
+        Z[c] = z;
+        part[0] += b * b;
+        part[1] += r * r;
+        part[2] += r * z;
+    }
+    __syncthreads();
+    // boundary rows of z for the neighbours (iteration 0 reads z of the halo rows)
+    for (int t = tid; t < 2 * ny; t += kSlabThreads) {
+        const int lr = t < ny ? 0 : rows - 1;
+        const int j = t < ny ? t : t - ny;
+        GZ[(size_t)(r0 + lr) * ny + j] = Z[lr * ny + j];
+    }
+    if (!flag_sum<3>(part, red_smem, slots, ++seq, status)) return;
+    for (int t = tid; t < 2 * ny; t += kSlabThreads) {
+        const int row = t < ny ? iw : ie;
+        HZ[t] = row >= 0 ? __ldcg(GZ + (size_t)row * ny + (t < ny ? t : t - ny)) : 0.0;
+    }
+    __syncthreads();
+    const double bnrm2 = sqrt(part[0]);
+    double rr = part[1];
+    double rho = part[2];
+    const double atol = L.rtol * bnrm2;
+    int it = 0;
+    bool converged = false;
+    if (bnrm2 == 0.0) {
+        for (int c = tid; c < nloc; c += kSlabThreads) X[c] = P1[c];
+        converged = true;
+    } else {
+        double beta = 0.0;
+        int cur = 0;
+        double q[2 * CPT];
+        for (it = 0; it < L.maxiter; ++it) {
+            if (sqrt(rr) < atol) { converged = true; break; }
+            double* Pn = cur ? P1 : P0;
+            const double* Po = cur ? P0 : P1;
+            const bool first = (it == 0);
+            double pq = 0.0;
+            // two cells (c, c+1) of one row per slot; ny is even, so c is even and
+            // every 16-byte pair load is aligned
+#pragma unroll
+            for (int k = 0; k < CPT; ++k) {
+                q[2 * k] = 0.0;
+                q[2 * k + 1] = 0.0;
+                const int c = 2 * (tid + k * kSlabThreads);
+                if (c >= nloc) continue;
+                const unsigned nb2 = *reinterpret_cast<const uint16_t*>(NB + c);
+                const unsigned nb0 = nb2 & 0xFFu, nb1 = nb2 >> 8;
+                if (!((nb0 | nb1) & 0x80u)) continue;
+                const int li = (int)__umulhi((unsigned)c, magic);
+                const int j = c - li * ny;
+                const double2 z2 = *reinterpret_cast<const double2*>(Z + c);
+                double pC0 = z2.x, pC1 = z2.y;
+                if (!first) {
+                    const double2 o2 = *reinterpret_cast<const double2*>(Po + c);
+                    pC0 = o2.x * beta + z2.x;
+                    pC1 = o2.y * beta + z2.y;
+                }
+                // solid cells carry p = z = 0 and no coupling bits, so their terms vanish
+                double tW0 = 0.0, tW1 = 0.0, tE0 = 0.0, tE1 = 0.0;
+                const double tS0 = (nb0 & 2) ? mdy2 * (first ? Z[c - 1] : Po[c - 1] * beta + Z[c - 1]) : 0.0;
+                const double tN0 = (nb0 & 4) ? mdy2 * pC1 : 0.0;
+                const double tS1 = (nb1 & 2) ? mdy2 * pC0 : 0.0;
+                const double tN1 = (nb1 & 4) ? mdy2 * (first ? Z[c + 2] : Po[c + 2] * beta + Z[c + 2]) : 0.0;
+                if ((nb0 | nb1) & 1) {
+                    const bool own = li > 0;
+                    const double2 gz = *reinterpret_cast<const double2*>(own ? (Z + c - ny) : (HZ + j));
+                    double w0 = gz.x, w1 = gz.y;
+                    if (!first) {
+                        const double2 go = *reinterpret_cast<const double2*>(own ? (Po + c - ny) : (HP + j));
+                        w0 = go.x * beta + gz.x;
+                        w1 = go.y * beta + gz.y;
+                    }
+                    if (nb0 & 1) tW0 = mdx2 * w0;
+                    if (nb1 & 1) tW1 = mdx2 * w1;
+                }
+                if ((nb0 | nb1) & 8) {
+                    const bool own = li < rows - 1;
+                    const double2 gz = *reinterpret_cast<const double2*>(own ? (Z + c + ny) : (HZ + ny + j));
+                    double e0 = gz.x, e1 = gz.y;
+                    if (!first) {
+                        const double2 go = *reinterpret_cast<const double2*>(own ? (Po + c + ny) : (HP + ny + j));
+                        e0 = go.x * beta + gz.x;
+                        e1 = go.y * beta + gz.y;
+                    }
+                    if (nb0 & 8) tE0 = mdx2 * e0;
+                    if (nb1 & 8) tE1 = mdx2 * e1;
+                }
+                const double2 dg = *reinterpret_cast<const double2*>(DG + c);
+                const int i = r0 + li;
+                const double q0 = row_sum(periodic, i, nx, tW0, tS0, dg.x * pC0, tN0, tE0);
+                const double q1 = row_sum(periodic, i, nx, tW1, tS1, dg.y * pC1, tN1, tE1);
+                *reinterpret_cast<double2*>(Pn + c) = make_double2(pC0, pC1);
+                q[2 * k] = q0;
+                q[2 * k + 1] = q1;
+                pq += pC0 * q0;
+                pq += pC1 * q1;
+            }
+            __syncthreads();
+            // boundary rows of the new p: the neighbours' p_old of the next iteration
+            for (int t = tid; t < 2 * ny; t += kSlabThreads) {
+                const int lr = t < ny ? 0 : rows - 1;
+                const int j = t < ny ? t : t - ny;
+                GP[(size_t)(r0 + lr) * ny + j] = Pn[lr * ny + j];
+            }
+            {
+                double v[1] = {pq};
+                if (!flag_sum<1>(v, red_smem, slots, ++seq, status)) return;
+                pq = v[0];
+            }
+            // the halo rows' new p; phase B does not read HP, the next phase A does
+            // (after the reduction below, whose barrier orders these stores)
+            for (int t = tid; t < 2 * ny; t += kSlabThreads) {
+                const int row = t < ny ? iw : ie;
+                HP[t] = row >= 0 ? __ldcg(GP + (size_t)row * ny + (t < ny ? t : t - ny)) : 0.0;
+            }
+            const double alpha = rho / pq;
+            double v2[2] = {0.0, 0.0};
+#pragma unroll
+            for (int k = 0; k < CPT; ++k) {
+                const int c = 2 * (tid + k * kSlabThreads);
+                if (c >= nloc) continue;
+                const unsigned nb2 = *reinterpret_cast<const uint16_t*>(NB + c);
+                const bool f0 = nb2 & 0x80u, f1 = (nb2 >> 8) & 0x80u;
+                if (!(f0 || f1)) continue;
+                double2 x2 = *reinterpret_cast<const double2*>(X + c);
+                double2 r2 = *reinterpret_cast<const double2*>(R + c);
+                double2 z2 = *reinterpret_cast<const double2*>(Z + c);
+                const double2 p2 = *reinterpret_cast<const double2*>(Pn + c);
+                const double2 d2 = *reinterpret_cast<const double2*>(DI + c);
+                if (f0) {
+                    x2.x = x2.x + alpha * p2.x;
+                    r2.x = r2.x - alpha * q[2 * k];
+                    z2.x = d2.x * r2.x;
+                    v2[0] += r2.x * r2.x;
+                    v2[1] += r2.x * z2.x;
+                }
+                if (f1) {
+                    x2.y = x2.y + alpha * p2.y;
+                    r2.y = r2.y - alpha * q[2 * k + 1];
+                    z2.y = d2.y * r2.y;
+                    v2[0] += r2.y * r2.y;
+                    v2[1] += r2.y * z2.y;
+                }
+                *reinterpret_cast<double2*>(X + c) = x2;
+                *reinterpret_cast<double2*>(R + c) = r2;
+                *reinterpret_cast<double2*>(Z + c) = z2;
+            }
+            __syncthreads();
+            for (int t = tid; t < 2 * ny; t += kSlabThreads) {
+                const int lr = t < ny ? 0 : rows - 1;
+                const int j = t < ny ? t : t - ny;
+                GZ[(size_t)(r0 + lr) * ny + j] = Z[lr * ny + j];
+            }
+            if (!flag_sum<2>(v2, red_smem, slots, ++seq, status)) return;
+            for (int t = tid; t < 2 * ny; t += kSlabThreads) {
+                const int row = t < ny ? iw : ie;
+                HZ[t] = row >= 0 ? __ldcg(GZ + (size_t)row * ny + (t < ny ? t : t - ny)) : 0.0;
+            }
+            __syncthreads();
+            rr = v2[0];
+            beta = v2[1] / rho;
+            rho = v2[1];
+            cur ^= 1;
+        }
+    }
+    // ------------------------------------------------------------ epilogue
+    __syncthreads();
+    double xs[CFD2D_MAX_COMPONENTS];
+#pragma unroll
+    for (int k = 0; k < CFD2D_MAX_COMPONENTS; ++k) xs[k] = 0.0;
+    for (int c = tid; c < nloc; c += kSlabThreads) {
+        op.x0[goff + c] = X[c];
+        if (op.ncomp > 0 && (NB[c] & 0x80)) {
+            const int lab = op.label[goff + c];
+#pragma unroll
+            for (int k = 0; k < CFD2D_MAX_COMPONENTS; ++k)
+                if (k == lab) xs[k] += X[c];
+        }
+    }
+    if (ncomp > 0) {
+        if (!flag_sum<CFD2D_MAX_COMPONENTS>(xs, red_smem, slots, ++seq, status)) return;
+        if (tid < ncomp) cmean[tid] = xs[tid] / op.comp_count[tid];
+    }
+    __syncthreads();
+    const int pp = ny + 2;
+    for (int c = tid; c < nloc; c += kSlabThreads) {
+        const int li = (int)__umulhi((unsigned)c, magic);
+        const int j = c - li * ny;
+        const int i = r0 + li;
+        double pv = 0.0;
+        if (NB[c] & 0x80) {
+            pv = X[c];
+            if (ncomp > 0) {
+                const int lab = op.label[goff + c];
+                if (lab >= 0) pv = pv - cmean[lab];
+            }
+        }
+        if (!L.p_padded) {
+            L.p_out[goff + c] = pv;
+        } else {
+            L.p_out[(i + 1) * pp + j + 1] = pv;
+            // periodic ghost rows: p[0,:] = p[nx,:], p[nx+1,:] = p[1,:]
+            if (periodic && i == nx - 1) L.p_out[j + 1] = pv;
+            if (periodic && i == 0) L.p_out[(nx + 1) * pp + j + 1] = pv;
+        }
+    }
+    if (L.p_padded) {
+        for (int i = r0 + tid; i < r1; i += kSlabThreads) {
+            L.p_out[(i + 1) * pp] = 0.0;
+            L.p_out[(i + 1) * pp + ny + 1] = 0.0;
+        }
+        if (me == 0) {
+            for (int j = tid; j < pp; j += kSlabThreads)
+                if (!periodic || j == 0 || j == ny + 1) L.p_out[j] = 0.0;
+        }
+        if (me == G - 1) {
+            for (int j = tid; j < pp; j += kSlabThreads)
+                if (!periodic || j == 0 || j == ny + 1) L.p_out[(nx + 1) * pp + j] = 0.0;
+        }
+    }
+    if (me == 0 && tid == 0) {
+        if (L.iters_out) *L.iters_out = it;
+        if (L.iters_out2) *L.iters_out2 = it;
+        if (L.status_out && !converged) atomicOr(L.status_out, CFD2D_S_CG_MAXITER);
+    }
+}
+
+namespace {
+
+constexpr int kMaxDevices = 64;
+
+// SM count and opt-in shared memory per block of the current device, looked up once
+// per device (0 SMs: the lookup failed).
+struct DevLimits {
+    int sms = 0, smem_optin = 0, dev = -1;
+};
+DevLimits dev_limits() {
+    static DevLimits cache[kMaxDevices];
+    DevLimits d;
+    if (cudaGetDevice(&d.dev) != cudaSuccess || d.dev < 0) return DevLimits{};
+    if (d.dev < kMaxDevices && cache[d.dev].sms > 0) return cache[d.dev];
+    if (cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, d.dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&d.smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, d.dev) != cudaSuccess)
+        return DevLimits{};
+    if (d.dev < kMaxDevices) cache[d.dev] = d;
+    return d;
+}
+
+// CTAs of the workspace solver: every SM times the CTAs that fit on one, at most
+// one per 256 cells; per device.
 template <bool VAR>
 int grid_blocks_for(int n) {
-    static int per_sm = -1, sms = 0;
-    if (per_sm < 0) {
-        int dev = 0;
-        if (cudaGetDevice(&dev) != cudaSuccess) return 0;
-        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+    static int per_sm_cache[kMaxDevices];
+    const DevLimits d = dev_limits();
+    if (d.sms <= 0) return 0;
+    int per_sm = d.dev < kMaxDevices ? per_sm_cache[d.dev] : 0;
+    if (per_sm <= 0) {
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_grid<false, VAR>, kGridThreads, 0) !=
             cudaSuccess)
             return 0;
+        if (d.dev < kMaxDevices) per_sm_cache[d.dev] = per_sm;
     }
-    long long g = (long long)per_sm * sms;
+    long long g = (long long)per_sm * d.sms;
     const long long need = (n + kGridThreads - 1) / kGridThreads;
     if (g > need) g = need;
     if (g < 1) g = 1;
     return (int)g;
+}
+
+// Cell pairs per thread of the slab solver for `cap` cells per CTA (0: too many).
+int slab_cpt_for(int cap) {
+    const int need = ((cap + 1) / 2 + kSlabThreads - 1) / kSlabThreads;
+    if (need <= 1) return 1;
+    if (need <= 2) return 2;
+    if (need <= 4) return 4;
+    if (need <= 8) return 8;
+    return 0;
+}
+
+// The slab solver's launch for an nx x ny constant-coefficient grid: one CTA per SM
+// (at most one per row) when ny is even and a slab of ceil(nx / G) rows fits in the
+// opt-in shared memory beside the kernel's static arrays. False: use the workspace form.
+bool slab_plan(int nx, int ny, int* G_out, int* cap_out) {
+    if (ny % 2 != 0) return false;
+    const DevLimits d = dev_limits();
+    if (d.sms <= 0) return false;
+    const int G = nx < d.sms ? nx : d.sms;
+    if (G < 2) return false;
+    const int cap = ((nx + G - 1) / G) * ny;
+    const size_t static_bytes = (32 * kSlot + kSlot + CFD2D_MAX_COMPONENTS) * sizeof(double) + 1024;
+    if (pcg_slab_smem_bytes(cap, ny) + static_bytes > (size_t)d.smem_optin) return false;
+    if (slab_cpt_for(cap) == 0) return false;
+    *G_out = G;
+    *cap_out = cap;
+    return true;
+}
+
+template <int CPT>
+cudaError_t launch_slab(const PcgLaunch& L0, int G, int cap, cudaStream_t s) {
+    static bool configured[kMaxDevices];
+    const DevLimits d = dev_limits();
+    if (d.sms <= 0 || d.dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    const size_t bytes = pcg_slab_smem_bytes(cap, L0.op.ny);
+    if (!configured[d.dev]) {
+        const int dyn = d.smem_optin - (int)((32 * kSlot + kSlot + CFD2D_MAX_COMPONENTS) * sizeof(double)) - 1024;
+        cudaError_t e = cudaFuncSetAttribute(k_pcg_slab<CPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+        if (e != cudaSuccess) return e;
+        configured[d.dev] = true;
+    }
+    PcgLaunch L = L0;
+    L.cap_cells = cap;
+    const size_t n = (size_t)L.op.nx * L.op.ny;
+    // reduction slots start from sequence 0 on every launch
+    cudaError_t e = cudaMemsetAsync(L.op.work + 3 * n, 0, (size_t)2 * G * kFlagStride * sizeof(double), s);
+    if (e != cudaSuccess) return e;
+    void* args[] = {&L};
+    return cudaLaunchCooperativeKernel((const void*)k_pcg_slab<CPT>, dim3(G), dim3(kSlabThreads), args, bytes, s);
 }
 
 }  // namespace
@@ -1256,19 +1772,33 @@ cudaError_t pcg_matvec(const cfd2d_poisson& op, const double* x, double* y, cuda
 }
 
 size_t pcg_grid_workspace_doubles(int nx, int ny) {
-    // R, P0, P1 + three partial arrays for up to 148 * 32 CTAs + barrier words
-    return (size_t)3 * nx * ny + (size_t)3 * 148 * 32 * kSlot + 8;
+    // R, P0, P1 (the slab form: boundary rows of z and p) + three partial arrays
+    // (the slab form: two sets of reduction slots) for up to kMaxGridCtas CTAs +
+    // barrier words
+    static_assert(2 * kFlagStride <= 3 * kSlot, "slab reduction slots fit in the partial arrays");
+    return (size_t)3 * nx * ny + (size_t)3 * kMaxGridCtas * kSlot + 8;
 }
 
 template <bool VAR>
 cudaError_t pcg_grid_launch_t(const PcgLaunch& L, cudaStream_t s) {
     const int n = L.op.nx * L.op.ny;
     const bool cl = L.op.grid_ctas == 16;
-    const int G = cl ? 16 : grid_blocks_for<VAR>(n);
-    if (G < 1 || G > 148 * 32) return cudaErrorInvalidConfiguration;
-    if (L.op.grid_ctas != 0 && !cl) return cudaErrorInvalidValue;
+    if (L.op.grid_ctas != 0 && L.op.grid_ctas != -1 && !cl) return cudaErrorInvalidValue;
     if (L.op.work == nullptr || L.op.work_bytes < pcg_grid_workspace_doubles(L.op.nx, L.op.ny) * sizeof(double))
         return cudaErrorInvalidValue;
+    if constexpr (!VAR) {
+        int Gs = 0, cap = 0;
+        if (L.op.grid_ctas == 0 && !L.snap && slab_plan(L.op.nx, L.op.ny, &Gs, &cap)) {
+            switch (slab_cpt_for(cap)) {
+                case 1: return launch_slab<1>(L, Gs, cap, s);
+                case 2: return launch_slab<2>(L, Gs, cap, s);
+                case 4: return launch_slab<4>(L, Gs, cap, s);
+                default: return launch_slab<8>(L, Gs, cap, s);
+            }
+        }
+    }
+    const int G = cl ? 16 : grid_blocks_for<VAR>(n);
+    if (G < 1 || G > kMaxGridCtas) return cudaErrorInvalidConfiguration;
     PcgLaunch Lc = L;
     // the barrier words start from zero on every launch, whatever an earlier
     // launch that gave up on a wait left behind
@@ -1278,11 +1808,13 @@ cudaError_t pcg_grid_launch_t(const PcgLaunch& L, cudaStream_t s) {
     if (cl) {
         // one 16-CTA cluster: its reductions use cluster barriers, so several such
         // solves (of different cases) can run side by side on the other SMs
-        static bool configured = false;
-        if (!configured) {
+        static bool configured[kMaxDevices];
+        const DevLimits d = dev_limits();
+        if (d.sms <= 0 || d.dev >= kMaxDevices) return cudaErrorInvalidDevice;
+        if (!configured[d.dev]) {
             e = cudaFuncSetAttribute(k_pcg_grid<true, VAR>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
             if (e != cudaSuccess) return e;
-            configured = true;
+            configured[d.dev] = true;
         }
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(16, 1, 1);
