@@ -1225,6 +1225,7 @@ namespace {
 constexpr int kSlabThreads = 512;
 constexpr int kFlagStride = 24;  // doubles per reduction slot: kSlot values, then the sequence word
 constexpr long long kFlagSpinLimit = 1LL << 24;
+constexpr int kHaloRegs = 4;  // halo values per thread: two rows of ny <= 2 * kSlabThreads
 
 __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
     unsigned long long v;
@@ -1238,69 +1239,80 @@ __device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned l
 // Grid-wide sum of K values without atomics or a separate barrier. Thread 0 of each
 // CTA stores its block partial and then, with release semantics, the reduction's
 // sequence number `seq` in the CTA's own slot (two slot sets, used by the parity of
-// seq). Warp 0 of every CTA polls all G slots until each carries `seq` (bounded: a
-// wait that gives up sets CFD2D_S_BARRIER_TIMEOUT and the call returns false), then
-// adds the partials lane-strided and by a butterfly, the same order in every CTA, so
-// every CTA gets the same bits. A CTA rewrites a slot set two reductions later, which
-// it reaches only after every CTA has written the reduction in between, i.e. after
-// every CTA has finished reading this one. Global stores a CTA made before the call
-// are visible to every CTA after it (read them with __ldcg: L1 is not coherent).
+// seq). Thread b of every CTA (b < G) polls slot b until it carries `seq` (bounded:
+// a wait that gives up sets CFD2D_S_BARRIER_TIMEOUT and the call returns false) and
+// loads that partial, so the G polls run in parallel; the partials are then added by
+// warp butterflies and a butterfly over the warp sums, the same order in every CTA,
+// so every CTA gets the same bits. A CTA rewrites a slot set two reductions later,
+// which it reaches only after every CTA has written the reduction in between, i.e.
+// after every CTA has finished reading this one. Global stores a CTA made before the
+// call are visible to every CTA after it (read them with __ldcg: L1 is not coherent).
 template <int K>
 __device__ __forceinline__ bool flag_sum(double (&v)[K], double* red_smem, double* slots, unsigned long long seq,
                                          int* status) {
     static_assert(K <= kSlot, "slot capacity");
     __shared__ double fsum[kSlot];
-    __shared__ int fok;
     block_sum<K>(v, red_smem);
     const int G = gridDim.x;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     double* set = slots + (size_t)(seq & 1ull) * G * kFlagStride;
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
         double* my = set + (size_t)blockIdx.x * kFlagStride;
 #pragma unroll
         for (int k = 0; k < K; ++k) my[k] = v[k];
         __threadfence();
         st_release_u64(reinterpret_cast<unsigned long long*>(my + kSlot), seq);
     }
-    if (threadIdx.x < 32) {
-        const int lane = threadIdx.x;
-        bool ok = true;
-        double x[K];
+    double x[K];
 #pragma unroll
-        for (int k = 0; k < K; ++k) x[k] = 0.0;
-        for (int b = lane; b < G && ok; b += 32) {
-            const double* sl = set + (size_t)b * kFlagStride;
-            const unsigned long long* gw = reinterpret_cast<const unsigned long long*>(sl + kSlot);
-            long long spins = 0;
-            while (ld_acquire_u64(gw) != seq) {
-                if (++spins > kFlagSpinLimit) {
-                    ok = false;
-                    break;
-                }
-            }
-            if (ok) {
-#pragma unroll
-                for (int k = 0; k < K; ++k) x[k] += __ldcg(sl + k);
+    for (int k = 0; k < K; ++k) x[k] = 0.0;
+    int ok = 1;
+    if (tid < G) {
+        const double* sl = set + (size_t)tid * kFlagStride;
+        const unsigned long long* gw = reinterpret_cast<const unsigned long long*>(sl + kSlot);
+        long long spins = 0;
+        while (ld_acquire_u64(gw) != seq) {
+            if (++spins > kFlagSpinLimit) {
+                ok = 0;
+                break;
             }
         }
-        ok = __all_sync(0xffffffffu, ok);
+        if (ok) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) x[k] = __ldcg(sl + k);
+        }
+    }
+    // every lane of a warp ends with the same bits (each butterfly stage adds the
+    // same two values in both partner lanes)
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x[k] += __shfl_xor_sync(0xffffffffu, x[k], o);
+    }
+    const int nwg = (G + 31) >> 5;  // warps that hold slots
+    if (lane == 0 && w < nwg) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) red_smem[k * 32 + w] = x[k];
+    }
+    ok = __syncthreads_and(ok);
+    if (w == 0) {
 #pragma unroll
         for (int k = 0; k < K; ++k) {
+            double y = lane < nwg ? red_smem[k * 32 + lane] : 0.0;
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) x[k] += __shfl_xor_sync(0xffffffffu, x[k], o);
+            for (int o = 16; o > 0; o >>= 1) y += __shfl_xor_sync(0xffffffffu, y, o);
+            if (lane == 0) fsum[k] = y;
         }
-        if (lane == 0) {
-#pragma unroll
-            for (int k = 0; k < K; ++k) fsum[k] = x[k];
-            fok = ok ? 1 : 0;
-            if (!ok && status) atomicOr(status, CFD2D_S_BARRIER_TIMEOUT);
-        }
-        __threadfence();
+    }
+    if (!ok) {
+        if (tid == 0 && status) atomicOr(status, CFD2D_S_BARRIER_TIMEOUT);
+        return false;
     }
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < K; ++k) v[k] = fsum[k];
-    // fsum is rewritten by the next call only after its block_sum barrier
-    return fok != 0;
+    // fsum and red_smem are rewritten by the next call only after its block_sum barrier
+    return true;
 }
 
 }  // namespace
@@ -1435,11 +1447,26 @@ __global__ void __launch_bounds__(kSlabThreads, 1) k_pcg_slab(PcgLaunch L) {
         GZ[(size_t)(r0 + lr) * ny + j] = Z[lr * ny + j];
     }
     if (!flag_sum<3>(part, red_smem, slots, ++seq, status)) return;
-    for (int t = tid; t < 2 * ny; t += kSlabThreads) {
-        const int row = t < ny ? iw : ie;
-        HZ[t] = row >= 0 ? __ldcg(GZ + (size_t)row * ny + (t < ny ? t : t - ny)) : 0.0;
-    }
-    __syncthreads();
+    // halo rows of z and p go through registers: the loads are issued right after a
+    // reduction and stored to shared memory only where they are needed, so their
+    // latency overlaps the cells that do not need them
+    double hz[kHaloRegs], hp[kHaloRegs];
+    auto load_halo = [&](double (&h)[kHaloRegs], const double* src) {
+#pragma unroll
+        for (int u = 0; u < kHaloRegs; ++u) {
+            const int t = tid + u * kSlabThreads;
+            const int row = t < ny ? iw : ie;
+            h[u] = (t < 2 * ny && row >= 0) ? __ldcg(src + (size_t)row * ny + (t < ny ? t : t - ny)) : 0.0;
+        }
+    };
+    auto store_halo = [&](const double (&h)[kHaloRegs], double* dst) {
+#pragma unroll
+        for (int u = 0; u < kHaloRegs; ++u) {
+            const int t = tid + u * kSlabThreads;
+            if (t < 2 * ny) dst[t] = h[u];
+        }
+    };
+    load_halo(hz, GZ);
     const double bnrm2 = sqrt(part[0]);
     double rr = part[1];
     double rho = part[2];
@@ -1460,17 +1487,20 @@ __global__ void __launch_bounds__(kSlabThreads, 1) k_pcg_slab(PcgLaunch L) {
             const bool first = (it == 0);
             double pq = 0.0;
             // two cells (c, c+1) of one row per slot; ny is even, so c is even and
-            // every 16-byte pair load is aligned
-#pragma unroll
-            for (int k = 0; k < CPT; ++k) {
+            // every 16-byte pair load is aligned. Pass 0 takes the pairs of the slab's
+            // inner rows, pass 1 (after the halo z reaches shared memory) the pairs of
+            // its first and last rows.
+            auto pair_a = [&](int k, int pass) {
+                const int c = 2 * (tid + k * kSlabThreads);
+                if (c >= nloc) return;
+                const int li = (int)__umulhi((unsigned)c, magic);
+                const bool edge = (li == 0) || (li == rows - 1);
+                if (edge != (pass == 1)) return;
                 q[2 * k] = 0.0;
                 q[2 * k + 1] = 0.0;
-                const int c = 2 * (tid + k * kSlabThreads);
-                if (c >= nloc) continue;
                 const unsigned nb2 = *reinterpret_cast<const uint16_t*>(NB + c);
                 const unsigned nb0 = nb2 & 0xFFu, nb1 = nb2 >> 8;
-                if (!((nb0 | nb1) & 0x80u)) continue;
-                const int li = (int)__umulhi((unsigned)c, magic);
+                if (!((nb0 | nb1) & 0x80u)) return;
                 const int j = c - li * ny;
                 const double2 z2 = *reinterpret_cast<const double2*>(Z + c);
                 double pC0 = z2.x, pC1 = z2.y;
@@ -1518,7 +1548,13 @@ __global__ void __launch_bounds__(kSlabThreads, 1) k_pcg_slab(PcgLaunch L) {
                 q[2 * k + 1] = q1;
                 pq += pC0 * q0;
                 pq += pC1 * q1;
-            }
+            };
+#pragma unroll
+            for (int k = 0; k < CPT; ++k) pair_a(k, 0);
+            store_halo(hz, HZ);
+            __syncthreads();
+#pragma unroll
+            for (int k = 0; k < CPT; ++k) pair_a(k, 1);
             __syncthreads();
             // boundary rows of the new p: the neighbours' p_old of the next iteration
             for (int t = tid; t < 2 * ny; t += kSlabThreads) {
@@ -1531,12 +1567,8 @@ __global__ void __launch_bounds__(kSlabThreads, 1) k_pcg_slab(PcgLaunch L) {
                 if (!flag_sum<1>(v, red_smem, slots, ++seq, status)) return;
                 pq = v[0];
             }
-            // the halo rows' new p; phase B does not read HP, the next phase A does
-            // (after the reduction below, whose barrier orders these stores)
-            for (int t = tid; t < 2 * ny; t += kSlabThreads) {
-                const int row = t < ny ? iw : ie;
-                HP[t] = row >= 0 ? __ldcg(GP + (size_t)row * ny + (t < ny ? t : t - ny)) : 0.0;
-            }
+            // the halo rows' new p: phase B does not read HP, the next phase A does
+            load_halo(hp, GP);
             const double alpha = rho / pq;
             double v2[2] = {0.0, 0.0};
 #pragma unroll
@@ -1569,6 +1601,9 @@ __global__ void __launch_bounds__(kSlabThreads, 1) k_pcg_slab(PcgLaunch L) {
                 *reinterpret_cast<double2*>(R + c) = r2;
                 *reinterpret_cast<double2*>(Z + c) = z2;
             }
+            // phase A of this iteration is done with HP (the barrier of the p.q
+            // reduction); the next one reads it after the barriers below
+            store_halo(hp, HP);
             __syncthreads();
             for (int t = tid; t < 2 * ny; t += kSlabThreads) {
                 const int lr = t < ny ? 0 : rows - 1;
@@ -1576,11 +1611,8 @@ __global__ void __launch_bounds__(kSlabThreads, 1) k_pcg_slab(PcgLaunch L) {
                 GZ[(size_t)(r0 + lr) * ny + j] = Z[lr * ny + j];
             }
             if (!flag_sum<2>(v2, red_smem, slots, ++seq, status)) return;
-            for (int t = tid; t < 2 * ny; t += kSlabThreads) {
-                const int row = t < ny ? iw : ie;
-                HZ[t] = row >= 0 ? __ldcg(GZ + (size_t)row * ny + (t < ny ? t : t - ny)) : 0.0;
-            }
-            __syncthreads();
+            // phase A of this iteration is done with HZ; the next stores the new rows
+            load_halo(hz, GZ);
             rr = v2[0];
             beta = v2[1] / rho;
             rho = v2[1];
@@ -1705,7 +1737,7 @@ int slab_cpt_for(int cap) {
 // (at most one per row) when ny is even and a slab of ceil(nx / G) rows fits in the
 // opt-in shared memory beside the kernel's static arrays. False: use the workspace form.
 bool slab_plan(int nx, int ny, int* G_out, int* cap_out) {
-    if (ny % 2 != 0) return false;
+    if (ny % 2 != 0 || 2 * ny > kHaloRegs * kSlabThreads) return false;
     const DevLimits d = dev_limits();
     if (d.sms <= 0) return false;
     const int G = nx < d.sms ? nx : d.sms;

@@ -47,6 +47,7 @@ def test_obstacle_flow_1024x512_three_steps(cuda_lib):
     sim.pressure.tol = 1e-8
     flags = np.packbits(sim.grid.fluid.astype(np.uint8), axis=None)
     assert np.array_equal(flags, g["obs1024_fluid_bits"])
+    errs = {}
     for n in (1, 2, 3):
         sim.step()
         if n not in (1, 3):
@@ -54,16 +55,15 @@ def test_obstacle_flow_1024x512_three_steps(cuda_lib):
         for name in ("u", "v", "p"):
             a = getattr(sim, name)
             ref_max = float(g[f"obs1024_{n}_{name}_max"])
-            sub = a[::8, ::8]
-            d_sub = np.abs(sub - g[f"obs1024_{n}_{name}_sub"]).max() / ref_max
-            assert d_sub < TOL, (n, name, d_sub)
+            errs[(n, name, "sub")] = np.abs(a[::8, ::8] - g[f"obs1024_{n}_{name}_sub"]).max() / ref_max
             for ax, key in ((1, "rows"), (0, "cols")):
-                s = a.sum(axis=ax)
                 ref = g[f"obs1024_{n}_{name}_{key}"]
-                scale = ref_max * a.shape[ax]
-                d = np.abs(s - ref).max() / scale
-                assert d < TOL, (n, name, key, d)
+                errs[(n, name, key)] = np.abs(a.sum(axis=ax) - ref).max() / (ref_max * a.shape[ax])
     its = np.array(sim.history.extra["cg_iterationen"][-3:])
+    print("iterations", its, "reference", g["obs1024_its"])
+    print({k: f"{v:.2e}" for k, v in errs.items()})
+    bad = {k: v for k, v in errs.items() if not v < TOL}
+    assert not bad, bad
     assert np.abs(its - g["obs1024_its"]).max() <= 3, (its, g["obs1024_its"])
     np.testing.assert_allclose(sim.history.dt[-3:], g["obs1024_dt"], rtol=1e-12)
     fx = np.array(sim.history.fx[-3:])
