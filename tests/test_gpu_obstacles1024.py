@@ -5,9 +5,17 @@ The fixture (tests/golden/golden_obstacles1024.npz, written by make_golden.py's
 1e-8, 3 steps from rest): the fluid flags in full and, at steps 1 and 3, every
 8th value of u, v and p in both directions, the sums of every row and column and
 the max-norm. The device run must give the same flags bit for bit, the same CG
-iteration counts within 3, the same dt series and fields within 1e-10 relative
-(max-norm of the difference over the max-norm of the reference field); the row
-and column sums, which see every cell, within 1e-10 of the sums' scale.
+iteration counts within 3, the same dt series and u, v within 1e-10 relative
+(max-norm of the difference over the max-norm of the reference field; the row
+and column sums, which see every cell, within 1e-10 of the sums' scale).
+
+p is held to 2e-9. At this size a solve takes ~3800 CG iterations to 1e-8, and
+the pressure left unconverged at that tolerance is a smooth field that moves with
+the rounding of the dot products: the same scipy-form CG with its dot products
+summed pairwise instead of by BLAS (tests/golden/sensitivity_obstacles1024.py)
+stops at the same iteration with u, v within 9e-13 of the reference's and p
+within 5.4e-10. The velocity correction sees only differences of p, which is why
+u and v agree to 1e-10 where p cannot.
 """
 
 from __future__ import annotations
@@ -20,6 +28,7 @@ import pytest
 from conftest import golden
 
 TOL = 1e-10
+TOL_P = 2e-9
 
 
 def _fixture():
@@ -62,7 +71,7 @@ def test_obstacle_flow_1024x512_three_steps(cuda_lib):
     its = np.array(sim.history.extra["cg_iterationen"][-3:])
     print("iterations", its, "reference", g["obs1024_its"])
     print({k: f"{v:.2e}" for k, v in errs.items()})
-    bad = {k: v for k, v in errs.items() if not v < TOL}
+    bad = {k: v for k, v in errs.items() if not v < (TOL_P if k[1] == "p" else TOL)}
     assert not bad, bad
     assert np.abs(its - g["obs1024_its"]).max() <= 3, (its, g["obs1024_its"])
     np.testing.assert_allclose(sim.history.dt[-3:], g["obs1024_dt"], rtol=1e-12)
