@@ -838,15 +838,16 @@ def run_b200(args, dist, rank, world):
         "data": "synthetic (seeded obstacle flow from rest, as the reference's cases start)",
         "config": {"workload": WORKLOAD, "grid": [NX, NY], "cells": cells, "fluid_cells": fluid_cells,
                    "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"replicas x{world}",
-                   "solver": "plain FP64 Jacobi-PCG (k_pcg_grid)"},
+                   "solver": "plain FP64 Jacobi-PCG (k_pcg_slab)"},
         "poisson_ms": 1e3 * solve_s / args.steps,
         "poisson_iters_per_step": iters,
         "e2e": {"value": e2e, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "steps": e2e_steps},
         "gpu_launches": knodes * args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": _ncu_traffic("pcg_grid_obstacles1024x512.txt"),
-                     "kernel": "k_pcg_grid (FP64 Jacobi-PCG, one persistent launch per solve)",
+                     "frac": achieved / peak, "traffic": _ncu_traffic("pcg_slab_obstacles1024x512.txt"),
+                     "kernel": "k_pcg_slab (FP64 Jacobi-PCG, one persistent launch per solve, vectors in "
+                               "shared memory)",
                      "peak_kind": peak_kind},
         "cpu_baseline": cpu,
         "clocks": clocks,
