@@ -855,28 +855,29 @@ __device__ __forceinline__ unsigned int ld_acquire_gpu(const unsigned int* p) {
     return v;
 }
 
-__device__ bool grid_barrier(unsigned int* bar, int* status) {
+// Bounded grid barrier with one atomic per CTA (a sense-reversing counter): thread 0
+// of each CTA adds 1 to the 32-bit counter, except CTA 0, which adds 2^31 - (G - 1);
+// the G additions of one barrier total exactly 2^31, so the counter's top bit flips
+// once, at the last arrival, and never before. Each CTA remembers the top bit it saw
+// when it arrived and polls the one word until the bit differs. The counter starts
+// at zero (cleared before every launch) and returns to a multiple of 2^31 after
+// every barrier. A wait that gives up after about a second sets
+// CFD2D_S_BARRIER_TIMEOUT and returns false (uniform over the CTA). `nblocks` is the
+// number of CTAs that take part (gridDim.x, except in the self-test).
+__device__ bool grid_barrier(unsigned int* bar, int* status, unsigned int nblocks) {
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) {
         ok = 1;
-        unsigned int* gen = bar + 1;
-        const unsigned int g0 = ld_acquire_gpu(gen);
+        const unsigned int add = (blockIdx.x == 0) ? (0x80000000u - (nblocks - 1u)) : 1u;
         __threadfence();
-        const unsigned int arrived = atomicAdd(bar, 1u) + 1u;
-        if (arrived == gridDim.x) {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(gen, 1u);
-        } else {
-            long long spins = 0;
-            while (ld_acquire_gpu(gen) == g0) {
-                if (++spins > (1LL << 25)) {
-                    if (status) atomicOr(status, CFD2D_S_BARRIER_TIMEOUT);
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(16);
+        const unsigned int seen = atomicAdd(bar, add);
+        long long spins = 0;
+        while (((seen ^ ld_acquire_gpu(bar)) & 0x80000000u) == 0u) {
+            if (++spins > (1LL << 24)) {
+                if (status) atomicOr(status, CFD2D_S_BARRIER_TIMEOUT);
+                ok = 0;
+                break;
             }
         }
         __threadfence();
@@ -885,38 +886,60 @@ __device__ bool grid_barrier(unsigned int* bar, int* status) {
     return ok != 0;
 }
 
-// grid-wide sum of K values: block tree, partials to part[b*kSlot + k], barrier,
-// then warp 0 of every block adds the G partials in one fixed order (lane-strided,
-// then a butterfly, so every block gets the same bits) and shares the sums through
-// shared memory. (Having every warp read all G partials cost a third of an
-// iteration at 1024 x 512.)
+// Grid-wide sum of K values: block tree, thread 0 stores the CTA partial in set
+// (parity & 1) of the partial arrays (two sets, so a CTA that runs ahead into the
+// next reduction never overwrites partials another CTA is still reading: it reaches
+// this set again only after the barrier of the reduction in between), barrier, then
+// thread t of every CTA loads partials t, t + blockDim, ... in parallel and the
+// values are added by warp butterflies and a butterfly over the warp sums: one fixed
+// order, so every CTA gets the same bits. Global stores a CTA made before the call
+// are visible to every CTA after it (read them with __ldcg: L1 is not coherent).
 template <int K>
-__device__ __forceinline__ bool grid_sum(double (&v)[K], double* red_smem, double* part,
-                                         unsigned int* bar, int* status) {
-    static_assert(K <= CFD2D_MAX_COMPONENTS + 1, "gsum holds at most MAX_COMPONENTS + 1 values");
+__device__ __forceinline__ bool grid_sum(double (&v)[K], double* red_smem, double* parts, unsigned int* bar,
+                                         int* status, unsigned int parity) {
+    static_assert(K <= kSlot, "partial slot capacity");
+    __shared__ double gsum[kSlot];
+    const int G = gridDim.x, tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     block_sum<K>(v, red_smem);
-    if (threadIdx.x == 0) {
+    double* set = parts + (size_t)(parity & 1u) * G * kSlot;
+    if (tid == 0) {
 #pragma unroll
-        for (int k = 0; k < K; ++k) part[(size_t)blockIdx.x * kSlot + k] = v[k];
+        for (int k = 0; k < K; ++k) set[(size_t)blockIdx.x * kSlot + k] = v[k];
     }
-    if (!grid_barrier(bar, status)) return false;
-    __shared__ double gsum[CFD2D_MAX_COMPONENTS + 1];
-    if (threadIdx.x < 32) {
-        const int lane = threadIdx.x;
-        const int G = gridDim.x;
+    if (!grid_barrier(bar, status, (unsigned int)G)) return false;
+    double x[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) x[k] = 0.0;
+    for (int b = tid; b < G; b += blockDim.x) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) x[k] += __ldcg(set + (size_t)b * kSlot + k);
+    }
+    // every lane of a warp ends with the same bits (each butterfly stage adds the
+    // same two values in both partner lanes)
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x[k] += __shfl_xor_sync(0xffffffffu, x[k], o);
+    }
+    const int nwg = min((int)(blockDim.x >> 5), (G + 31) >> 5);  // warps that loaded partials
+    if (lane == 0 && w < nwg) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) red_smem[k * 32 + w] = x[k];
+    }
+    __syncthreads();
+    if (w == 0) {
 #pragma unroll
         for (int k = 0; k < K; ++k) {
-            double x = 0.0;
-            for (int b = lane; b < G; b += 32) x += __ldcg(&part[(size_t)b * kSlot + k]);
+            double y = lane < nwg ? red_smem[k * 32 + lane] : 0.0;
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-            if (lane == 0) gsum[k] = x;
+            for (int o = 16; o > 0; o >>= 1) y += __shfl_xor_sync(0xffffffffu, y, o);
+            if (lane == 0) gsum[k] = y;
         }
     }
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < K; ++k) v[k] = gsum[k];
-    // gsum is rewritten by the next reduction only after its block tree and barrier
+    // gsum and red_smem are rewritten by the next call only after its block_sum barrier
     return true;
 }
 
@@ -998,13 +1021,13 @@ __device__ __forceinline__ void cluster_sum_any(double (&v)[K], double* red_smem
 // The reduction of the grid-persistent solver: over the whole cooperative grid (CL =
 // false, counting barrier, may give up) or over one cluster (CL = true).
 template <bool CL, int K>
-__device__ __forceinline__ bool sync_sum(double (&v)[K], double* red_smem, double* part, unsigned int* bar,
+__device__ __forceinline__ bool sync_sum(double (&v)[K], double* red_smem, double* parts, unsigned int* bar,
                                          int* status, double* slotA, double* slotB, int& nred) {
     if constexpr (CL) {
         cluster_sum_any<K>(v, red_smem, (nred++ & 1) ? slotB : slotA);
         return true;
     } else {
-        return grid_sum<K>(v, red_smem, part, bar, status);
+        return grid_sum<K>(v, red_smem, parts, bar, status, (unsigned int)(nred++));
     }
 }
 
@@ -1083,7 +1106,7 @@ __global__ void __launch_bounds__(CL ? kClusterL2Threads : kGridThreads, 1) k_pc
         part[1] += r * r;
         part[2] += r * (op.dinv[c] * r);
     }
-    if (!SSUM(3, part, W.partB)) return;
+    if (!SSUM(3, part, W.partA)) return;
     const double bnrm2 = sqrt(part[0]);
     double rr = part[1];
     double rho = part[2];
@@ -1146,7 +1169,7 @@ __global__ void __launch_bounds__(CL ? kClusterL2Threads : kGridThreads, 1) k_pc
                 if ((it + 1) % L.snap_every == 0 && k <= L.snap_max)
                     for (int c = c0 + tid; c < c1; c += TPB) L.snap[(size_t)(k - 1) * n + c] = X[c];
             }
-            if (!SSUM(2, v2, W.partB)) return;
+            if (!SSUM(2, v2, W.partA)) return;
             rr = v2[0];
             beta = v2[1] / rho;
             rho = v2[1];
@@ -1164,7 +1187,7 @@ __global__ void __launch_bounds__(CL ? kClusterL2Threads : kGridThreads, 1) k_pc
             for (int k = 0; k < CFD2D_MAX_COMPONENTS; ++k)
                 if (k == lab) xs[k] += X[c];
         }
-        if (!SSUM(CFD2D_MAX_COMPONENTS, xs, W.partC)) return;
+        if (!SSUM(CFD2D_MAX_COMPONENTS, xs, W.partA)) return;
     }
     const int pp = ny + 2;
     for (int c = c0 + tid; c < c1; c += TPB) {
@@ -1214,7 +1237,7 @@ __global__ void __launch_bounds__(CL ? kClusterL2Threads : kGridThreads, 1) k_pc
 // and keeps x, r, z, p (two buffers), 1/diag, diag and the coupling bits of its cells
 // on chip for the whole solve, as the cluster solver does; only the first and last
 // row of each slab cross to its two neighbours, through global memory (L2), and the
-// dot products are reduced over the grid without atomics (flag_sum). Per iteration:
+// dot products are reduced over the grid by grid_sum (one atomic per CTA). Per iteration:
 // phase A (p = z + beta p, q = A p, p.q partial; the slab's boundary rows of p are
 // published), reduction 1, the neighbours' boundary rows of p are read; phase B (x, r,
 // z update, r.r and r.z partials; boundary rows of z published), reduction 2, the
@@ -1223,97 +1246,7 @@ __global__ void __launch_bounds__(CL ? kClusterL2Threads : kGridThreads, 1) k_pc
 namespace {
 
 constexpr int kSlabThreads = 512;
-constexpr int kFlagStride = 24;  // doubles per reduction slot: kSlot values, then the sequence word
-constexpr long long kFlagSpinLimit = 1LL << 24;
 constexpr int kHaloRegs = 4;  // halo values per thread: two rows of ny <= 2 * kSlabThreads
-
-__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
-    unsigned long long v;
-    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
-    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-
-// Grid-wide sum of K values without atomics or a separate barrier. Thread 0 of each
-// CTA stores its block partial and then, with release semantics, the reduction's
-// sequence number `seq` in the CTA's own slot (two slot sets, used by the parity of
-// seq). Thread b of every CTA (b < G) polls slot b until it carries `seq` (bounded:
-// a wait that gives up sets CFD2D_S_BARRIER_TIMEOUT and the call returns false) and
-// loads that partial, so the G polls run in parallel; the partials are then added by
-// warp butterflies and a butterfly over the warp sums, the same order in every CTA,
-// so every CTA gets the same bits. A CTA rewrites a slot set two reductions later,
-// which it reaches only after every CTA has written the reduction in between, i.e.
-// after every CTA has finished reading this one. Global stores a CTA made before the
-// call are visible to every CTA after it (read them with __ldcg: L1 is not coherent).
-template <int K>
-__device__ __forceinline__ bool flag_sum(double (&v)[K], double* red_smem, double* slots, unsigned long long seq,
-                                         int* status) {
-    static_assert(K <= kSlot, "slot capacity");
-    __shared__ double fsum[kSlot];
-    block_sum<K>(v, red_smem);
-    const int G = gridDim.x;
-    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    double* set = slots + (size_t)(seq & 1ull) * G * kFlagStride;
-    if (tid == 0) {
-        double* my = set + (size_t)blockIdx.x * kFlagStride;
-#pragma unroll
-        for (int k = 0; k < K; ++k) my[k] = v[k];
-        __threadfence();
-        st_release_u64(reinterpret_cast<unsigned long long*>(my + kSlot), seq);
-    }
-    double x[K];
-#pragma unroll
-    for (int k = 0; k < K; ++k) x[k] = 0.0;
-    int ok = 1;
-    if (tid < G) {
-        const double* sl = set + (size_t)tid * kFlagStride;
-        const unsigned long long* gw = reinterpret_cast<const unsigned long long*>(sl + kSlot);
-        long long spins = 0;
-        while (ld_acquire_u64(gw) != seq) {
-            if (++spins > kFlagSpinLimit) {
-                ok = 0;
-                break;
-            }
-        }
-        if (ok) {
-#pragma unroll
-            for (int k = 0; k < K; ++k) x[k] = __ldcg(sl + k);
-        }
-    }
-    // every lane of a warp ends with the same bits (each butterfly stage adds the
-    // same two values in both partner lanes)
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) x[k] += __shfl_xor_sync(0xffffffffu, x[k], o);
-    }
-    const int nwg = (G + 31) >> 5;  // warps that hold slots
-    if (lane == 0 && w < nwg) {
-#pragma unroll
-        for (int k = 0; k < K; ++k) red_smem[k * 32 + w] = x[k];
-    }
-    ok = __syncthreads_and(ok);
-    if (w == 0) {
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-            double y = lane < nwg ? red_smem[k * 32 + lane] : 0.0;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) y += __shfl_xor_sync(0xffffffffu, y, o);
-            if (lane == 0) fsum[k] = y;
-        }
-    }
-    if (!ok) {
-        if (tid == 0 && status) atomicOr(status, CFD2D_S_BARRIER_TIMEOUT);
-        return false;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < K; ++k) v[k] = fsum[k];
-    // fsum and red_smem are rewritten by the next call only after its block_sum barrier
-    return true;
-}
 
 }  // namespace
 
@@ -1353,8 +1286,9 @@ __global__ void __launch_bounds__(kSlabThreads, 1) k_pcg_slab(PcgLaunch L) {
     // global exchange rows and reduction slots in the workspace
     double* GZ = op.work;
     double* GP = op.work + n;
-    double* slots = op.work + 3 * (size_t)n;
-    unsigned long long seq = 0;
+    double* parts = op.work + 3 * (size_t)n;
+    unsigned int* bar = reinterpret_cast<unsigned int*>(parts + (size_t)2 * G * kSlot);
+    unsigned int seq = 0;
     int* status = L.status_out;
     const int iw = (r0 == 0) ? (periodic ? nx - 1 : -1) : r0 - 1;
     const int ie = (r1 == nx) ? (periodic ? 0 : -1) : r1;
@@ -1403,7 +1337,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) k_pcg_slab(PcgLaunch L) {
         HP[t] = row >= 0 ? op.x0[(size_t)row * ny + (t < ny ? t : t - ny)] : 0.0;
     }
     // scipy computes A x0 only if x0 has a nonzero; Neumann-component sums of b
-    if (!flag_sum<CFD2D_MAX_COMPONENTS + 1>(csum, red_smem, slots, ++seq, status)) return;
+    if (!grid_sum<CFD2D_MAX_COMPONENTS + 1>(csum, red_smem, parts, bar, status, ++seq)) return;
     const bool x_any = csum[CFD2D_MAX_COMPONENTS] > 0.0;
     const int ncomp = op.ncomp;
     if (tid < ncomp) cmean[tid] = csum[tid] / op.comp_count[tid];
@@ -1446,7 +1380,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) k_pcg_slab(PcgLaunch L) {
         const int j = t < ny ? t : t - ny;
         GZ[(size_t)(r0 + lr) * ny + j] = Z[lr * ny + j];
     }
-    if (!flag_sum<3>(part, red_smem, slots, ++seq, status)) return;
+    if (!grid_sum<3>(part, red_smem, parts, bar, status, ++seq)) return;
     // halo rows of z and p go through registers: the loads are issued right after a
     // reduction and stored to shared memory only where they are needed, so their
     // latency overlaps the cells that do not need them
@@ -1564,7 +1498,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) k_pcg_slab(PcgLaunch L) {
             }
             {
                 double v[1] = {pq};
-                if (!flag_sum<1>(v, red_smem, slots, ++seq, status)) return;
+                if (!grid_sum<1>(v, red_smem, parts, bar, status, ++seq)) return;
                 pq = v[0];
             }
             // the halo rows' new p: phase B does not read HP, the next phase A does
@@ -1610,7 +1544,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) k_pcg_slab(PcgLaunch L) {
                 const int j = t < ny ? t : t - ny;
                 GZ[(size_t)(r0 + lr) * ny + j] = Z[lr * ny + j];
             }
-            if (!flag_sum<2>(v2, red_smem, slots, ++seq, status)) return;
+            if (!grid_sum<2>(v2, red_smem, parts, bar, status, ++seq)) return;
             // phase A of this iteration is done with HZ; the next stores the new rows
             load_halo(hz, GZ);
             rr = v2[0];
@@ -1634,7 +1568,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) k_pcg_slab(PcgLaunch L) {
         }
     }
     if (ncomp > 0) {
-        if (!flag_sum<CFD2D_MAX_COMPONENTS>(xs, red_smem, slots, ++seq, status)) return;
+        if (!grid_sum<CFD2D_MAX_COMPONENTS>(xs, red_smem, parts, bar, status, ++seq)) return;
         if (tid < ncomp) cmean[tid] = xs[tid] / op.comp_count[tid];
     }
     __syncthreads();
@@ -1766,8 +1700,9 @@ cudaError_t launch_slab(const PcgLaunch& L0, int G, int cap, cudaStream_t s) {
     PcgLaunch L = L0;
     L.cap_cells = cap;
     const size_t n = (size_t)L.op.nx * L.op.ny;
-    // reduction slots start from sequence 0 on every launch
-    cudaError_t e = cudaMemsetAsync(L.op.work + 3 * n, 0, (size_t)2 * G * kFlagStride * sizeof(double), s);
+    // the barrier counter starts from zero on every launch, whatever an earlier launch
+    // that gave up on a wait left behind
+    cudaError_t e = cudaMemsetAsync(L.op.work + 3 * n + (size_t)2 * G * kSlot, 0, sizeof(double), s);
     if (e != cudaSuccess) return e;
     void* args[] = {&L};
     return cudaLaunchCooperativeKernel((const void*)k_pcg_slab<CPT>, dim3(G), dim3(kSlabThreads), args, bytes, s);
@@ -1778,7 +1713,8 @@ cudaError_t launch_slab(const PcgLaunch& L0, int G, int cap, cudaStream_t s) {
 // The bounded grid barrier of the persistent solvers on a grid of one block, with the
 // barrier words as the caller set them (cfd2d_barrier_selftest).
 __global__ void k_barrier_probe(unsigned int* bar, int* status, int* ok_out) {
-    const bool ok = grid_barrier(bar, status);
+    const unsigned int expected = bar[1] > 0u ? bar[1] : 1u;
+    const bool ok = grid_barrier(bar, status, expected);
     if (threadIdx.x == 0) *ok_out = ok ? 1 : 0;
 }
 
@@ -1804,10 +1740,9 @@ cudaError_t pcg_matvec(const cfd2d_poisson& op, const double* x, double* y, cuda
 }
 
 size_t pcg_grid_workspace_doubles(int nx, int ny) {
-    // R, P0, P1 (the slab form: boundary rows of z and p) + three partial arrays
-    // (the slab form: two sets of reduction slots) for up to kMaxGridCtas CTAs +
-    // barrier words
-    static_assert(2 * kFlagStride <= 3 * kSlot, "slab reduction slots fit in the partial arrays");
+    // R, P0, P1 (the slab form: boundary rows of z and p) + three partial arrays for
+    // up to kMaxGridCtas CTAs (two used, as the parity sets of grid_sum) + barrier words
+
     return (size_t)3 * nx * ny + (size_t)3 * kMaxGridCtas * kSlot + 8;
 }
 

@@ -637,11 +637,12 @@ int cfd2d_streamfunction(const cfd2d_sim* sim, double* psi, void* stream);
 int cfd2d_vtk_pack(const cfd2d_sim* sim, const cfd2d_field* fields, int nfields, uint8_t* out, void* stream);
 
 /* Self-test of the bounded grid barrier the persistent solvers use (no reference
- * counterpart): one block runs it with the barrier words bar[0] (arrivals so far) and
- * bar[1] (generation) as given, writes 1 to *ok_out when it passed and 0 when it gave
- * up. With bar[0] = 0 the single block is the last to arrive and passes at once; with
- * bar[0] > 0 no one releases it, and after its spin limit (about a second) it sets
- * CFD2D_S_BARRIER_TIMEOUT in *status and returns, leaving the context usable. */
+ * counterpart): one block runs it on the counter bar[0] as given, as if bar[1] CTAs
+ * (at least 1) took part, and writes 1 to *ok_out when it passed and 0 when it gave
+ * up. With bar[0] = 0 and bar[1] = 1 the single block is the last to arrive and passes
+ * at once; with bar[1] > 1 the others never arrive, and after its spin limit (about a
+ * second) it sets CFD2D_S_BARRIER_TIMEOUT in *status and returns, leaving the context
+ * usable. */
 int cfd2d_barrier_selftest(unsigned int* bar, int* status, int* ok_out, void* stream);
 
 /* Thread-block shape (tx along j, ty along i) of the row kernels: which = 0 the

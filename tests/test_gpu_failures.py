@@ -77,8 +77,10 @@ def test_bounded_grid_barrier_gives_up_and_the_context_stays_usable(cuda_lib):
 
     lib = _lib.lib()
     dev = _lib.device()
-    for arrivals, passes in ((0, True), (7, False)):
-        bar = torch.tensor([arrivals, 0], dtype=torch.int32, device=dev)
+    # bar = [counter, CTAs taking part]: alone it passes at once; told that 8 CTAs take
+    # part, it waits for 7 that never come, gives up and reports the timeout
+    for ctas, passes in ((1, True), (8, False)):
+        bar = torch.tensor([0, ctas], dtype=torch.int32, device=dev)
         status = torch.zeros(1, dtype=torch.int32, device=dev)
         ok = torch.full((1,), -1, dtype=torch.int32, device=dev)
         rc = lib.cfd2d_barrier_selftest(_lib.ptr(bar), _lib.ptr(status), _lib.ptr(ok), _lib.stream_ptr())
