@@ -6,7 +6,7 @@ Run in a container that holds the reference checkout (default
     python tests/golden/make_golden.py [group ...]
 
 Groups: kernels geometry pressure cavity cylinder sst misc checkpoint smagorinsky
-functions vof validation shapes obstacles (default: all).
+functions vof validation shapes obstacles cylinder_long (default: all).
 The reference imports matplotlib at module load; ``mplstub/`` stands in for it
 (no fixture case needs plotting or polygon masks; NACA outlines and image
 obstacles do not use it). Every pressure solve uses the
@@ -608,11 +608,40 @@ def gen_obstacles():
     _save("golden_obstacles1024", out)
 
 
+def gen_cylinder_long():
+    """The cylinder channel with the van Leer scalar (the side workload of the
+    benchmark) over 2000 steps from rest with the reference's direct (SuperLU)
+    pressure solver: field digests (_digest, every 2nd value) at steps 1000 and 2000,
+    the force history and the drag/lift coefficients by the reference's
+    validation.force_coefficients (U = 1, L = D = 0.1)."""
+    from cfd2d import validation
+
+    out = {}
+    case = cases.build_case({"fall": "cylinder", "parameter": {"re": 100, "nx": 440, "ny": 82},
+                             "numerik": {"pressure_solver": "direct"},
+                             "skalar": {"name": "c", "diffusivity": 1e-3, "inflow_band": [0.15, 0.25],
+                                        "limiter": "vanleer"}})
+    sim = case.sim
+    t0 = time.time()
+    for n in range(1, 2001):
+        sim.step()
+        if n in (1000, 2000):
+            for name, a in (("u", sim.u), ("v", sim.v), ("p", sim.p), ("c", sim.scalars["c"].phi)):
+                _digest(f"cyl2k_{n}", name, a, out, stride=2)
+            print(f"cyl2k step {n}: {time.time() - t0:.0f}s", flush=True)
+    out["cyl2k_t"] = np.array(sim.history.t)
+    out["cyl2k_fx"] = np.array(sim.history.fx)
+    out["cyl2k_fy"] = np.array(sim.history.fy)
+    cd, cl = validation.force_coefficients(sim.history.fx, sim.history.fy, U=1.0, L=0.1)
+    out["cyl2k_cd"], out["cyl2k_cl"] = np.asarray(cd), np.asarray(cl)
+    _save("golden_cylinder2000", out)
+
+
 GROUPS = {"kernels": gen_kernels, "geometry": gen_geometry, "pressure": gen_pressure,
           "cavity": gen_cavity, "cylinder": gen_cylinder, "sst": gen_sst, "misc": gen_misc,
           "checkpoint": gen_checkpoint, "smagorinsky": gen_smagorinsky, "functions": gen_functions,
           "vof": gen_vof, "validation": gen_validation, "shapes": gen_shapes,
-          "obstacles": gen_obstacles}
+          "obstacles": gen_obstacles, "cylinder_long": gen_cylinder_long}
 
 if __name__ == "__main__":
     import warnings
