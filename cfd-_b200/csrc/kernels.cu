@@ -109,6 +109,7 @@ __device__ __forceinline__ double transport_tile(const double* __restrict__ phi,
 
 // Inputs and outputs never alias (the C ABI requires it): __restrict__ lets the
 // compiler issue every stencil load of a thread before its stores.
+constexpr int kMomRows = 4;
 // The viscosity and density forms are template parameters, so each instance carries
 // only the arithmetic it needs.
 template <bool VARIABLE, bool VAR_DENSITY>
@@ -119,17 +120,29 @@ __global__ void __launch_bounds__(256) k_momentum(const double* __restrict__ u, 
                                                   const double* __restrict__ rho) {
     const Grid2 g{nx, ny};
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = (blockIdx.y * blockDim.y + threadIdx.y);
-    if (j >= ny + 2 || i >= nx + 2) return;
+    // kMomRows consecutive rows per thread: a thread issues the loads of all its faces
+    // before any arithmetic needs them (more bytes in flight per thread), and the rows
+    // it shares with its own neighbours come from L1
+    const int i0 = (blockIdx.y * blockDim.y + threadIdx.y) * kMomRows;
+    if (j >= ny + 2 || i0 >= nx + 2) return;
     const MomCoef m = mom_coef_inv(inv, gamma, __ldg(&nu[g.c(1, 1)]));
     const int imax = periodic ? nx : nx - 1;
-    // both tendencies first, then both stores: every load of the thread can be in
-    // flight together
-    double hU = 0.0, hV = 0.0;
-    if (i >= 1 && i <= imax && j >= 1 && j <= ny) hU = mom_u(u, v, fl, nu, rho, g, m, VARIABLE, VAR_DENSITY, i, j);
-    if (i >= 1 && i <= nx && j >= 1 && j <= ny - 1) hV = mom_v(u, v, fl, nu, rho, g, m, VARIABLE, VAR_DENSITY, i, j);
-    if (i <= nx) hu[g.u(i, j)] = hU;
-    if (j <= ny) hv[g.v(i, j)] = hV;
+    // all tendencies first, then all stores
+    double hU[kMomRows], hV[kMomRows];
+#pragma unroll
+    for (int r = 0; r < kMomRows; ++r) {
+        const int i = i0 + r;
+        hU[r] = 0.0;
+        hV[r] = 0.0;
+        if (i >= 1 && i <= imax && j >= 1 && j <= ny) hU[r] = mom_u(u, v, fl, nu, rho, g, m, VARIABLE, VAR_DENSITY, i, j);
+        if (i >= 1 && i <= nx && j >= 1 && j <= ny - 1) hV[r] = mom_v(u, v, fl, nu, rho, g, m, VARIABLE, VAR_DENSITY, i, j);
+    }
+#pragma unroll
+    for (int r = 0; r < kMomRows; ++r) {
+        const int i = i0 + r;
+        if (i <= nx) hu[g.u(i, j)] = hU[r];
+        if (j <= ny && i <= nx + 1) hv[g.v(i, j)] = hV[r];
+    }
 }
 
 __global__ void k_obstacle_bc(double* u, double* v, const uint8_t* fl, int nx, int ny,
@@ -1079,7 +1092,7 @@ cudaError_t launch_momentum(const double* u, const double* v, const uint8_t* fl,
                             int periodic, double* hu, double* hv, const double* rho, int var_density,
                             cudaStream_t s) {
     const InvSpacing inv = inv_spacing(dx, dy);
-    const dim3 grd = grid_tile(kMom, ny + 2, nx + 2);
+    const dim3 grd = grid_tile(kMom, ny + 2, (nx + 2 + kMomRows - 1) / kMomRows);
     const dim3 blk = tile(kMom);
     if (variable && var_density)
         k_momentum<true, true><<<grd, blk, 0, s>>>(u, v, fl, nx, ny, inv, nu, gamma, periodic, hu, hv, rho);
