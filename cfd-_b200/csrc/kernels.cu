@@ -30,25 +30,31 @@ __device__ __forceinline__ bool v_fluid(const cfd2d_sim& S, Grid2 g, int i, int 
 // that the stencil rows a block reads are shared through L1 by its warps
 constexpr int kTileX = 32, kTileY = 8;
 
-// TVD transport (cfd2d/kernels.py:271-391) of the kTileY x kTileX cells of one block,
-// every interior face flux computed once and shared by its two cells. FX[r][c] holds
-// xflux/dx of the west face of cell (i0 + r, j0 + c) (row kTileY: the east face of
-// the tile's last row, which is also the periodic face nx -> 1); FY[r][c] holds
-// yflux/dy of the south face of cell (i0 + r, j0 + c). The cell then assembles
-// ((west + east) + south) + north exactly as transport_cell does, with -FX / -FY for
-// its east and north faces, so the result is bit-identical. Every thread of the
-// block must call it (it synchronises the block).
-__device__ __forceinline__ double transport_tile(const double* __restrict__ phi, const double* __restrict__ u,
-                                                 const double* __restrict__ v, const uint8_t* __restrict__ fl,
-                                                 const double* __restrict__ diff, Grid2 g, double dx, double dy,
-                                                 int lim, bool periodic, const ScalarBCView& bc, int obs_t,
-                                                 double obs_v) {
-    __shared__ double FX[kTileY + 1][kTileX];
-    __shared__ double FY[kTileY][kTileX + 1];
+// TVD transport (cfd2d/kernels.py:271-391) of the (kTileY * ROWS) x kTileX cells of
+// one block, every interior face flux computed once and shared by its two cells.
+// Thread (tx, ty) takes cells (i0 + ty + kTileY r, j0 + tx), r < ROWS, so each warp
+// stays on one row and its loads stay coalesced; all ROWS face fluxes of a thread are
+// computed before the block synchronises, which puts ROWS independent chains of
+// (data-dependent) loads in flight per thread. FX[q][c] holds xflux/dx of the west
+// face of cell (i0 + q, j0 + c) (row kTileY ROWS: the east face of the tile's last
+// row, which is also the periodic face nx -> 1); FY[q][c] holds yflux/dy of the south
+// face of cell (i0 + q, j0 + c). Each cell then assembles ((west + east) + south) +
+// north exactly as transport_cell does, with -FX / -FY for its east and north faces,
+// so the result is bit-identical. Every thread of the block must call it (it
+// synchronises the block); out[r] receives the value of its row r.
+template <int ROWS>
+__device__ __forceinline__ void transport_tile(const double* __restrict__ phi, const double* __restrict__ u,
+                                               const double* __restrict__ v, const uint8_t* __restrict__ fl,
+                                               const double* __restrict__ diff, Grid2 g, double dx, double dy,
+                                               int lim, bool periodic, const ScalarBCView& bc, int obs_t,
+                                               double obs_v, double (&res)[ROWS]) {
+    constexpr int TY = kTileY * ROWS;
+    __shared__ double FX[TY + 1][kTileX];
+    __shared__ double FY[TY][kTileX + 1];
     const int nx = g.nx, ny = g.ny;
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int j = blockIdx.x * kTileX + tx;
-    const int i = blockIdx.y * kTileY + ty;
+    const int ib = blockIdx.y * TY;
     const bool jin = (j >= 1 && j <= ny);
     // west face of cell ii (1 <= ii <= nx + 1); the domain faces are not shared
     auto west = [&](int ii) -> double {
@@ -62,50 +68,64 @@ __device__ __forceinline__ double transport_tile(const double* __restrict__ phi,
         if (!(fl[g.c(L, j)] && fl[g.c(R, j)])) return 0.0;
         return xflux(phi, u, fl, diff, g, dx, lim, periodic, fi, L, R, j) / dx;
     };
-    // south face of cell jj (2 <= jj <= ny)
-    auto south = [&](int jj) -> double {
-        if (!(fl[g.c(i, jj - 1)] && fl[g.c(i, jj)])) return 0.0;
-        return yflux(phi, v, fl, diff, g, dy, lim, i, jj - 1) / dy;
+    // south face of cell (ii, jj) (2 <= jj <= ny)
+    auto south = [&](int ii, int jj) -> double {
+        if (!(fl[g.c(ii, jj - 1)] && fl[g.c(ii, jj)])) return 0.0;
+        return yflux(phi, v, fl, diff, g, dy, lim, ii, jj - 1) / dy;
     };
-    if (jin && i >= 1 && i <= nx + 1) {
-        FX[ty][tx] = west(i);
-        if (ty == kTileY - 1 && i + 1 <= nx + 1) FX[kTileY][tx] = west(i + 1);
+#pragma unroll
+    for (int r = 0; r < ROWS; ++r) {
+        const int q = ty + kTileY * r;
+        const int i = ib + q;
+        if (jin && i >= 1 && i <= nx + 1) {
+            FX[q][tx] = west(i);
+            if (q == TY - 1 && i + 1 <= nx + 1) FX[TY][tx] = west(i + 1);
+        }
+        if (i >= 1 && i <= nx && j >= 2 && j <= ny) FY[q][tx] = south(i, j);
+        if (tx == kTileX - 1 && i >= 1 && i <= nx && j + 1 >= 2 && j + 1 <= ny) FY[q][kTileX] = south(i, j + 1);
     }
-    if (i >= 1 && i <= nx && j >= 2 && j <= ny) FY[ty][tx] = south(j);
-    if (tx == kTileX - 1 && i >= 1 && i <= nx && j + 1 >= 2 && j + 1 <= ny) FY[ty][kTileX] = south(j + 1);
     __syncthreads();
-    if (!(jin && i >= 1 && i <= nx) || !fl[g.c(i, j)]) return 0.0;
-    const double phP = phi[g.c(i, j)];
-    const double DP = diff[g.c(i, j)];
-    double xw = 0.0, xe = 0.0, ys = 0.0, yn = 0.0;
-    if (i == 1 && !periodic) {
-        xw = boundary_term(u[g.u(0, j)], phP, DP, bc.bt[0][j - 1], bc.bv[0][j - 1], dx);
-    } else {
-        const int L = (i == 1) ? nx : i - 1;
-        if (fl[g.c(L, j)]) xw = FX[ty][tx];
-        else if (obs_t == 1) xw = ((DP * (obs_v - phP)) / (0.5 * dx)) / dx;
+#pragma unroll
+    for (int r = 0; r < ROWS; ++r) {
+        const int q = ty + kTileY * r;
+        const int i = ib + q;
+        res[r] = 0.0;
+        if (!(jin && i >= 1 && i <= nx) || !fl[g.c(i, j)]) continue;
+        const double phP = phi[g.c(i, j)];
+        const double DP = diff[g.c(i, j)];
+        double xw = 0.0, xe = 0.0, ys = 0.0, yn = 0.0;
+        if (i == 1 && !periodic) {
+            xw = boundary_term(u[g.u(0, j)], phP, DP, bc.bt[0][j - 1], bc.bv[0][j - 1], dx);
+        } else {
+            const int L = (i == 1) ? nx : i - 1;
+            if (fl[g.c(L, j)]) xw = FX[q][tx];
+            else if (obs_t == 1) xw = ((DP * (obs_v - phP)) / (0.5 * dx)) / dx;
+        }
+        if (i == nx && !periodic) {
+            xe = boundary_term(-u[g.u(nx, j)], phP, DP, bc.bt[1][j - 1], bc.bv[1][j - 1], dx);
+        } else {
+            const int R = (i == nx) ? 1 : i + 1;
+            if (fl[g.c(R, j)]) xe = -FX[q + 1][tx];
+            else if (obs_t == 1) xe = ((DP * (obs_v - phP)) / (0.5 * dx)) / dx;
+        }
+        if (j == 1) {
+            ys = boundary_term(v[g.v(i, 0)], phP, DP, bc.bt[2][i - 1], bc.bv[2][i - 1], dy);
+        } else {
+            if (fl[g.c(i, j - 1)]) ys = FY[q][tx];
+            else if (obs_t == 1) ys = ((DP * (obs_v - phP)) / (0.5 * dy)) / dy;
+        }
+        if (j == ny) {
+            yn = boundary_term(-v[g.v(i, ny)], phP, DP, bc.bt[3][i - 1], bc.bv[3][i - 1], dy);
+        } else {
+            if (fl[g.c(i, j + 1)]) yn = -FY[q][tx + 1];
+            else if (obs_t == 1) yn = ((DP * (obs_v - phP)) / (0.5 * dy)) / dy;
+        }
+        res[r] = ((xw + xe) + ys) + yn;
     }
-    if (i == nx && !periodic) {
-        xe = boundary_term(-u[g.u(nx, j)], phP, DP, bc.bt[1][j - 1], bc.bv[1][j - 1], dx);
-    } else {
-        const int R = (i == nx) ? 1 : i + 1;
-        if (fl[g.c(R, j)]) xe = -FX[ty + 1][tx];
-        else if (obs_t == 1) xe = ((DP * (obs_v - phP)) / (0.5 * dx)) / dx;
-    }
-    if (j == 1) {
-        ys = boundary_term(v[g.v(i, 0)], phP, DP, bc.bt[2][i - 1], bc.bv[2][i - 1], dy);
-    } else {
-        if (fl[g.c(i, j - 1)]) ys = FY[ty][tx];
-        else if (obs_t == 1) ys = ((DP * (obs_v - phP)) / (0.5 * dy)) / dy;
-    }
-    if (j == ny) {
-        yn = boundary_term(-v[g.v(i, ny)], phP, DP, bc.bt[3][i - 1], bc.bv[3][i - 1], dy);
-    } else {
-        if (fl[g.c(i, j + 1)]) yn = -FY[ty][tx + 1];
-        else if (obs_t == 1) yn = ((DP * (obs_v - phP)) / (0.5 * dy)) / dy;
-    }
-    return ((xw + xe) + ys) + yn;
 }
+
+// rows per thread of the transport tile
+constexpr int kTransportRows = 4;
 
 // Inputs and outputs never alias (the C ABI requires it): __restrict__ lets the
 // compiler issue every stencil load of a thread before its stores.
@@ -176,9 +196,13 @@ __global__ void __launch_bounds__(256) k_scalar_transport(const double* __restri
     if (!is_active(st)) return;  // uniform over the grid
     const Grid2 g{nx, ny};
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = (blockIdx.y * blockDim.y + threadIdx.y);
-    const double r = transport_tile(phi, u, v, fl, diff, g, dx, dy, limiter, periodic != 0, bc, obs_t, obs_v);
-    if (j < ny + 2 && i < nx + 2) out[g.c(i, j)] = r;
+    double r[kTransportRows];
+    transport_tile<kTransportRows>(phi, u, v, fl, diff, g, dx, dy, limiter, periodic != 0, bc, obs_t, obs_v, r);
+#pragma unroll
+    for (int k = 0; k < kTransportRows; ++k) {
+        const int i = blockIdx.y * kTileY * kTransportRows + threadIdx.y + kTileY * k;
+        if (j < ny + 2 && i < nx + 2) out[g.c(i, j)] = r[k];
+    }
 }
 
 // cfd2d/geometry.py:17-22: (X - xc)**2 + (Y - yc)**2 <= r**2, X = (i + 0.5) * dx
@@ -787,14 +811,18 @@ __global__ void k_scalar_rhs(cfd2d_sim S, int s) {
     const int nx = S.nx, ny = S.ny;
     const Grid2 g{nx, ny};
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = (blockIdx.y * blockDim.y + threadIdx.y);
     const cfd2d_scalar& sc = S.scalars[s];
     ScalarBCView bc;
     for (int k = 0; k < 4; ++k) { bc.bt[k] = sc.bt[k]; bc.bv[k] = sc.bv[k]; }
     // rhs does not overlap phi, u, v, diff or the flags
-    const double r = transport_tile(sc.phi, S.u, S.v, S.fluid, sc.diff, g, S.dx, S.dy, sc.limiter,
-                                    S.periodic != 0, bc, sc.obs_t, sc.obs_v);
-    if (j < ny + 2 && i < nx + 2) sc.rhs[g.c(i, j)] = r;
+    double r[kTransportRows];
+    transport_tile<kTransportRows>(sc.phi, S.u, S.v, S.fluid, sc.diff, g, S.dx, S.dy, sc.limiter,
+                                   S.periodic != 0, bc, sc.obs_t, sc.obs_v, r);
+#pragma unroll
+    for (int k = 0; k < kTransportRows; ++k) {
+        const int i = blockIdx.y * kTileY * kTransportRows + threadIdx.y + kTileY * k;
+        if (j < ny + 2 && i < nx + 2) sc.rhs[g.c(i, j)] = r[k];
+    }
 }
 
 // Euler update with point-implicit source and clipping (cfd2d/models.py:196-207);
@@ -1116,7 +1144,7 @@ cudaError_t launch_scalar_transport(const double* phi, const double* u, const do
                                     const double* diff, int limiter, int periodic,
                                     const ScalarBCView& bc, int obs_t, double obs_v, double* out,
                                     cudaStream_t s) {
-    k_scalar_transport<<<grid_rows(ny + 2, nx + 2), kTile, 0, s>>>(phi, u, v, fl, nx, ny, dx, dy, diff,
+    k_scalar_transport<<<grid_rows(ny + 2, (nx + 2 + kTransportRows - 1) / kTransportRows), kTile, 0, s>>>(phi, u, v, fl, nx, ny, dx, dy, diff,
                                                                    limiter, periodic, bc, obs_t, obs_v,
                                                                    out, nullptr);
     return last();
@@ -1191,7 +1219,7 @@ cudaError_t stage_scalar(const cfd2d_sim& S, int slot, cudaStream_t s) {
     const cfd2d_scalar& sc = S.scalars[slot];
     if (sc.turb_div > 0.0 && S.variable_viscosity)
         k_scalar_turb_diff<<<reduction_blocks((S.nx + 2) * (S.ny + 2)), kBlock, 0, s>>>(S, slot);
-    k_scalar_rhs<<<grid_rows(S.ny + 2, S.nx + 2), kTile, 0, s>>>(S, slot);
+    k_scalar_rhs<<<grid_rows(S.ny + 2, (S.nx + 2 + kTransportRows - 1) / kTransportRows), kTile, 0, s>>>(S, slot);
     k_scalar_update<<<grid_tile(kStep, S.ny, S.nx), tile(kStep), 0, s>>>(S, slot);
     cudaError_t e = stage_scalar_ghosts(S, slot, s);
     if (e != cudaSuccess || sc.source != 2) return e;
