@@ -1615,6 +1615,402 @@ __global__ void __launch_bounds__(kSlabThreads, 1) k_pcg_slab(PcgLaunch L) {
     }
 }
 
+// Single-reduction form of the slab solver (k_pcg_slab1): the same layout, with the
+// Jacobi-PCG recurrence of Chronopoulos and Gear (1989), which needs one grid-wide
+// reduction per iteration instead of two. Each iteration updates p = z + beta p,
+// q = w + beta q (= A p), x, r and z = D^-1 r of the slab's own cells, publishes the
+// slab's boundary rows of z with a per-CTA sequence word (release store), computes
+// w = A z on the inner rows while those rows travel, waits (bounded) for the two
+// neighbours' words, finishes w on its first and last row and reduces r.z, z.w and
+// r.r together; p.q = z.w - beta r.z / alpha_prev. In exact arithmetic the iterates
+// are scipy's; in floating point they round differently (measured on the CPU with
+// the oracle: the 2000-step 64 x 64 cavity stays within 1e-11 of the reference with
+// CG iteration counts within 2).
+template <int CPT>
+__global__ void __launch_bounds__(kSlabThreads, 1) k_pcg_slab1(PcgLaunch L) {
+    if (L.active && *L.active == 0) return;  // uniform over the grid
+    const cfd2d_poisson& op = L.op;
+    const int nx = op.nx, ny = op.ny;
+    const bool periodic = op.periodic != 0;
+    const int G = gridDim.x, me = blockIdx.x;
+    const int r0 = row0_of(me, nx, G), r1 = row0_of(me + 1, nx, G);
+    const int rows = r1 - r0;
+    const int nloc = rows * ny;
+    const int cap = L.cap_cells;
+    const int tid = threadIdx.x;
+    const double mdx2 = -op.dx2, mdy2 = -op.dy2;
+    const int goff = r0 * ny;
+    const int n = nx * ny;
+
+    extern __shared__ __align__(16) double sm[];
+    double* X = sm;
+    double* R = X + cap;
+    double* P0 = R + cap;   // p (P1 holds b until the first iteration)
+    double* P1 = P0 + cap;  // q = A p, by its recurrence
+    double* DI = P1 + cap;
+    double* DG = DI + cap;
+    double* Z = DG + cap;
+    double* HZ = Z + cap;        // z of the west halo row at [0, ny), of the east one at [ny, 2 ny)
+    double* HP = HZ + 2 * ny;    // x0 of the halo rows (prologue only), same layout
+    uint8_t* NB = reinterpret_cast<uint8_t*>(HP + 2 * ny);
+    __shared__ double red_smem[32 * kSlot];
+    __shared__ double cmean[CFD2D_MAX_COMPONENTS];
+    // global exchange rows and reduction slots in the workspace
+    double* GZ = op.work;
+    // one sequence word per CTA (boundary rows of z published), after the barrier word
+    double* parts = op.work + 3 * (size_t)n;
+    unsigned int* bar = reinterpret_cast<unsigned int*>(parts + (size_t)2 * G * kSlot);
+    unsigned int* zflag = bar + 2;
+    unsigned int seq = 0;
+    int* status = L.status_out;
+    const int iw = (r0 == 0) ? (periodic ? nx - 1 : -1) : r0 - 1;
+    const int ie = (r1 == nx) ? (periodic ? 0 : -1) : r1;
+    const unsigned magic = (unsigned)(((1ull << 32) + (unsigned)ny - 1) / (unsigned)ny);
+
+    // ------------------------------------------------------------ prologue
+    double dt = 1.0;
+    if (L.rhs_mode == 1) dt = L.dt_ptr ? *L.dt_ptr : L.dt_const;
+    double csum[CFD2D_MAX_COMPONENTS + 1];
+#pragma unroll
+    for (int k = 0; k <= CFD2D_MAX_COMPONENTS; ++k) csum[k] = 0.0;
+    for (int c = tid; c < nloc; c += kSlabThreads) {
+        const int gidx = goff + c;
+        const uint8_t nb = op.nbr[gidx];
+        NB[c] = nb;
+        const double x0 = op.x0[gidx];
+        X[c] = x0;
+        DI[c] = op.dinv[gidx];
+        DG[c] = op.diag[gidx];
+        double braw = 0.0;
+        if (nb & 0x80) {
+            if (L.rhs_mode == 0) {
+                braw = L.rhs[gidx];
+            } else {
+                // div(F, G) / dt at interior cell (i+1, j+1) (cfd2d/solver.py:264-266)
+                const int li = (int)__umulhi((unsigned)c, magic);
+                const int j = c - li * ny;
+                const int pu = ny + 2, pv = ny + 1;
+                const int ig = r0 + li + 1, jg = j + 1;
+                const double div = (L.F[ig * pu + jg] - L.F[(ig - 1) * pu + jg]) / L.dx +
+                                   (L.G[ig * pv + jg] - L.G[ig * pv + jg - 1]) / L.dy;
+                braw = div / dt;
+            }
+            const int lab = op.ncomp > 0 ? op.label[gidx] : -1;
+#pragma unroll
+            for (int k = 0; k < CFD2D_MAX_COMPONENTS; ++k)
+                if (k == lab) csum[k] += braw;
+            if (x0 != 0.0) csum[CFD2D_MAX_COMPONENTS] += 1.0;
+        }
+        R[c] = braw;
+    }
+    // x0 of the halo rows: written by the caller before the launch, rewritten by this
+    // kernel only in its epilogue, which no CTA reaches before every CTA is past here
+    for (int t = tid; t < 2 * ny; t += kSlabThreads) {
+        const int row = t < ny ? iw : ie;
+        HP[t] = row >= 0 ? op.x0[(size_t)row * ny + (t < ny ? t : t - ny)] : 0.0;
+    }
+    // scipy computes A x0 only if x0 has a nonzero; Neumann-component sums of b
+    if (!grid_sum<CFD2D_MAX_COMPONENTS + 1>(csum, red_smem, parts, bar, status, ++seq)) return;
+    const bool x_any = csum[CFD2D_MAX_COMPONENTS] > 0.0;
+    const int ncomp = op.ncomp;
+    if (tid < ncomp) cmean[tid] = csum[tid] / op.comp_count[tid];
+    __syncthreads();
+
+    double part[3] = {0.0, 0.0, 0.0};
+    for (int c = tid; c < nloc; c += kSlabThreads) {
+        const uint8_t nb = NB[c];
+        if (!(nb & 0x80)) { P1[c] = 0.0; P0[c] = 0.0; R[c] = 0.0; Z[c] = 0.0; continue; }
+        double b = R[c];
+        if (ncomp > 0) {
+            const int lab = op.label[goff + c];
+            if (lab >= 0) b = b - cmean[lab];
+        }
+        b = -b;
+        P1[c] = b;  // kept for the ||b|| == 0 return
+        double r = b;
+        if (x_any) {
+            const int li = (int)__umulhi((unsigned)c, magic);
+            const int j = c - li * ny;
+            double tW = 0.0, tS = 0.0, tN = 0.0, tE = 0.0;
+            if (nb & 2) tS = mdy2 * X[c - 1];
+            if (nb & 4) tN = mdy2 * X[c + 1];
+            if (nb & 1) tW = mdx2 * ((li > 0) ? X[c - ny] : HP[j]);
+            if (nb & 8) tE = mdx2 * ((li < rows - 1) ? X[c + ny] : HP[ny + j]);
+            r = b - row_sum(periodic, r0 + li, nx, tW, tS, DG[c] * X[c], tN, tE);
+        }
+        R[c] = r;
+        P0[c] = 0.0;
+        const double z = DI[c] * r;
+        Z[c] = z;
+        part[0] += b * b;
+        part[1] += r * r;
+        part[2] += r * z;
+    }
+    __syncthreads();
+    __syncthreads();
+    // boundary rows of z for the neighbours, then the grid reduction of b.b, r.r, r.z
+    for (int t = tid; t < 2 * ny; t += kSlabThreads) {
+        const int lr = t < ny ? 0 : rows - 1;
+        const int j = t < ny ? t : t - ny;
+        GZ[(size_t)(r0 + lr) * ny + j] = Z[lr * ny + j];
+    }
+    if (!grid_sum<3>(part, red_smem, parts, bar, status, ++seq)) return;
+    const double bnrm2 = sqrt(part[0]);
+    double rr = part[1];
+    double rho = part[2];
+    const double atol = L.rtol * bnrm2;
+    int it = 0;
+    bool converged = false;
+    // w = A z of the thread's cell pairs, kept in registers until the next update
+    double w[2 * CPT];
+    // row-sum of A z at pair c (cells c, c + 1 of local row li) from shared memory
+    auto az_pair = [&](int c, int li, double& w0, double& w1) {
+        const unsigned nb2 = *reinterpret_cast<const uint16_t*>(NB + c);
+        const unsigned nb0 = nb2 & 0xFFu, nb1 = nb2 >> 8;
+        w0 = 0.0;
+        w1 = 0.0;
+        if (!((nb0 | nb1) & 0x80u)) return;
+        const int j = c - li * ny;
+        const double2 z2 = *reinterpret_cast<const double2*>(Z + c);
+        double tW0 = 0.0, tW1 = 0.0, tE0 = 0.0, tE1 = 0.0;
+        const double tS0 = (nb0 & 2) ? mdy2 * Z[c - 1] : 0.0;
+        const double tN0 = (nb0 & 4) ? mdy2 * z2.y : 0.0;
+        const double tS1 = (nb1 & 2) ? mdy2 * z2.x : 0.0;
+        const double tN1 = (nb1 & 4) ? mdy2 * Z[c + 2] : 0.0;
+        if ((nb0 | nb1) & 1) {
+            const double2 g = *reinterpret_cast<const double2*>(li > 0 ? (Z + c - ny) : (HZ + j));
+            if (nb0 & 1) tW0 = mdx2 * g.x;
+            if (nb1 & 1) tW1 = mdx2 * g.y;
+        }
+        if ((nb0 | nb1) & 8) {
+            const double2 g = *reinterpret_cast<const double2*>(li < rows - 1 ? (Z + c + ny) : (HZ + ny + j));
+            if (nb0 & 8) tE0 = mdx2 * g.x;
+            if (nb1 & 8) tE1 = mdx2 * g.y;
+        }
+        const double2 dg = *reinterpret_cast<const double2*>(DG + c);
+        const int i = r0 + li;
+        w0 = row_sum(periodic, i, nx, tW0, tS0, dg.x * z2.x, tN0, tE0);
+        w1 = row_sum(periodic, i, nx, tW1, tS1, dg.y * z2.y, tN1, tE1);
+    };
+    // neighbours' boundary rows of z for sequence number zs: wait (bounded) for their
+    // words, then load the rows into HZ. Returns false on a timeout (uniform).
+    auto halo_z = [&](unsigned int zs) -> bool {
+        __shared__ int hok;
+        if (tid < 2) {
+            const int row = tid == 0 ? iw : ie;
+            int okl = 1;
+            if (row >= 0) {
+                const int o = owner_of(row, nx, G);
+                long long spins = 0;
+                while ((int)(ld_acquire_gpu(zflag + o) - zs) < 0) {
+                    if (++spins > (1LL << 24)) {
+                        okl = 0;
+                        if (status) atomicOr(status, CFD2D_S_BARRIER_TIMEOUT);
+                        break;
+                    }
+                }
+                __threadfence();
+            }
+            if (tid == 0) hok = 1;
+            __syncwarp(0x3u);
+            if (!okl) hok = 0;
+        }
+        __syncthreads();
+        if (!hok) return false;
+        for (int t = tid; t < 2 * ny; t += kSlabThreads) {
+            const int row = t < ny ? iw : ie;
+            HZ[t] = row >= 0 ? __ldcg(GZ + (size_t)row * ny + (t < ny ? t : t - ny)) : 0.0;
+        }
+        __syncthreads();
+        return true;
+    };
+    // w and delta = z.w of the initial z (the grid reduction above made every CTA's
+    // boundary rows of z visible; sequence 0 needs no wait)
+    double delta;
+    {
+        for (int t = tid; t < 2 * ny; t += kSlabThreads) {
+            const int row = t < ny ? iw : ie;
+            HZ[t] = row >= 0 ? __ldcg(GZ + (size_t)row * ny + (t < ny ? t : t - ny)) : 0.0;
+        }
+        __syncthreads();
+        double d[1] = {0.0};
+#pragma unroll
+        for (int k = 0; k < CPT; ++k) {
+            const int c = 2 * (tid + k * kSlabThreads);
+            if (c >= nloc) { w[2 * k] = w[2 * k + 1] = 0.0; continue; }
+            const int li = (int)__umulhi((unsigned)c, magic);
+            az_pair(c, li, w[2 * k], w[2 * k + 1]);
+            const double2 z2 = *reinterpret_cast<const double2*>(Z + c);
+            d[0] += z2.x * w[2 * k];
+            d[0] += z2.y * w[2 * k + 1];
+        }
+        if (!grid_sum<1>(d, red_smem, parts, bar, status, ++seq)) return;
+        delta = d[0];
+    }
+    if (bnrm2 == 0.0) {
+        for (int c = tid; c < nloc; c += kSlabThreads) X[c] = P1[c];
+        converged = true;
+    } else {
+        double rho_prev = 1.0, alpha_prev = 1.0;
+        for (it = 0; it < L.maxiter; ++it) {
+            if (sqrt(rr) < atol) { converged = true; break; }
+            const bool first = (it == 0);
+            // single-reduction recurrence (Chronopoulos and Gear): p = z + beta p,
+            // q = w + beta q (= A p), p.q = delta - beta rho / alpha_prev
+            double beta = 0.0, pq = delta;
+            if (!first) {
+                beta = rho / rho_prev;
+                pq = delta - (beta * rho) / alpha_prev;
+            }
+            const double alpha = rho / pq;
+            double v3[3] = {0.0, 0.0, 0.0};  // r.z, z.w, r.r
+#pragma unroll
+            for (int k = 0; k < CPT; ++k) {
+                const int c = 2 * (tid + k * kSlabThreads);
+                if (c >= nloc) continue;
+                const unsigned nb2 = *reinterpret_cast<const uint16_t*>(NB + c);
+                const bool f0 = nb2 & 0x80u, f1 = (nb2 >> 8) & 0x80u;
+                if (!(f0 || f1)) continue;
+                double2 x2 = *reinterpret_cast<const double2*>(X + c);
+                double2 r2 = *reinterpret_cast<const double2*>(R + c);
+                double2 z2 = *reinterpret_cast<const double2*>(Z + c);
+                double2 p2 = *reinterpret_cast<const double2*>(P0 + c);
+                double2 q2 = *reinterpret_cast<const double2*>(P1 + c);
+                const double2 d2 = *reinterpret_cast<const double2*>(DI + c);
+                if (first) {
+                    p2 = z2;
+                    q2 = make_double2(w[2 * k], w[2 * k + 1]);
+                } else {
+                    p2 = make_double2(p2.x * beta + z2.x, p2.y * beta + z2.y);
+                    q2 = make_double2(q2.x * beta + w[2 * k], q2.y * beta + w[2 * k + 1]);
+                }
+                if (f0) {
+                    x2.x = x2.x + alpha * p2.x;
+                    r2.x = r2.x - alpha * q2.x;
+                    z2.x = d2.x * r2.x;
+                    v3[0] += r2.x * z2.x;
+                    v3[2] += r2.x * r2.x;
+                }
+                if (f1) {
+                    x2.y = x2.y + alpha * p2.y;
+                    r2.y = r2.y - alpha * q2.y;
+                    z2.y = d2.y * r2.y;
+                    v3[0] += r2.y * z2.y;
+                    v3[2] += r2.y * r2.y;
+                }
+                *reinterpret_cast<double2*>(X + c) = x2;
+                *reinterpret_cast<double2*>(R + c) = r2;
+                *reinterpret_cast<double2*>(Z + c) = z2;
+                *reinterpret_cast<double2*>(P0 + c) = p2;
+                *reinterpret_cast<double2*>(P1 + c) = q2;
+            }
+            __syncthreads();
+            // boundary rows of the new z, then this CTA's sequence word (release)
+            for (int t = tid; t < 2 * ny; t += kSlabThreads) {
+                const int lr = t < ny ? 0 : rows - 1;
+                const int j = t < ny ? t : t - ny;
+                GZ[(size_t)(r0 + lr) * ny + j] = Z[lr * ny + j];
+            }
+            __syncthreads();
+            const unsigned int zs = (unsigned int)it + 1u;
+            if (tid == 0) {
+                __threadfence();
+                asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(zflag + me), "r"(zs) : "memory");
+            }
+            // w = A z of the inner rows while the neighbours' rows travel
+#pragma unroll
+            for (int k = 0; k < CPT; ++k) {
+                const int c = 2 * (tid + k * kSlabThreads);
+                if (c >= nloc) { w[2 * k] = w[2 * k + 1] = 0.0; continue; }
+                const int li = (int)__umulhi((unsigned)c, magic);
+                if (li == 0 || li == rows - 1) continue;
+                az_pair(c, li, w[2 * k], w[2 * k + 1]);
+                const double2 z2 = *reinterpret_cast<const double2*>(Z + c);
+                v3[1] += z2.x * w[2 * k];
+                v3[1] += z2.y * w[2 * k + 1];
+            }
+            if (!halo_z(zs)) return;
+#pragma unroll
+            for (int k = 0; k < CPT; ++k) {
+                const int c = 2 * (tid + k * kSlabThreads);
+                if (c >= nloc) continue;
+                const int li = (int)__umulhi((unsigned)c, magic);
+                if (!(li == 0 || li == rows - 1)) continue;
+                az_pair(c, li, w[2 * k], w[2 * k + 1]);
+                const double2 z2 = *reinterpret_cast<const double2*>(Z + c);
+                v3[1] += z2.x * w[2 * k];
+                v3[1] += z2.y * w[2 * k + 1];
+            }
+            if (!grid_sum<3>(v3, red_smem, parts, bar, status, ++seq)) return;
+            rho_prev = rho;
+            alpha_prev = alpha;
+            rho = v3[0];
+            delta = v3[1];
+            rr = v3[2];
+        }
+    }
+    // ------------------------------------------------------------ epilogue
+    __syncthreads();
+    double xs[CFD2D_MAX_COMPONENTS];
+#pragma unroll
+    for (int k = 0; k < CFD2D_MAX_COMPONENTS; ++k) xs[k] = 0.0;
+    for (int c = tid; c < nloc; c += kSlabThreads) {
+        op.x0[goff + c] = X[c];
+        if (op.ncomp > 0 && (NB[c] & 0x80)) {
+            const int lab = op.label[goff + c];
+#pragma unroll
+            for (int k = 0; k < CFD2D_MAX_COMPONENTS; ++k)
+                if (k == lab) xs[k] += X[c];
+        }
+    }
+    if (ncomp > 0) {
+        if (!grid_sum<CFD2D_MAX_COMPONENTS>(xs, red_smem, parts, bar, status, ++seq)) return;
+        if (tid < ncomp) cmean[tid] = xs[tid] / op.comp_count[tid];
+    }
+    __syncthreads();
+    const int pp = ny + 2;
+    for (int c = tid; c < nloc; c += kSlabThreads) {
+        const int li = (int)__umulhi((unsigned)c, magic);
+        const int j = c - li * ny;
+        const int i = r0 + li;
+        double pv = 0.0;
+        if (NB[c] & 0x80) {
+            pv = X[c];
+            if (ncomp > 0) {
+                const int lab = op.label[goff + c];
+                if (lab >= 0) pv = pv - cmean[lab];
+            }
+        }
+        if (!L.p_padded) {
+            L.p_out[goff + c] = pv;
+        } else {
+            L.p_out[(i + 1) * pp + j + 1] = pv;
+            // periodic ghost rows: p[0,:] = p[nx,:], p[nx+1,:] = p[1,:]
+            if (periodic && i == nx - 1) L.p_out[j + 1] = pv;
+            if (periodic && i == 0) L.p_out[(nx + 1) * pp + j + 1] = pv;
+        }
+    }
+    if (L.p_padded) {
+        for (int i = r0 + tid; i < r1; i += kSlabThreads) {
+            L.p_out[(i + 1) * pp] = 0.0;
+            L.p_out[(i + 1) * pp + ny + 1] = 0.0;
+        }
+        if (me == 0) {
+            for (int j = tid; j < pp; j += kSlabThreads)
+                if (!periodic || j == 0 || j == ny + 1) L.p_out[j] = 0.0;
+        }
+        if (me == G - 1) {
+            for (int j = tid; j < pp; j += kSlabThreads)
+                if (!periodic || j == 0 || j == ny + 1) L.p_out[(nx + 1) * pp + j] = 0.0;
+        }
+    }
+    if (me == 0 && tid == 0) {
+        if (L.iters_out) *L.iters_out = it;
+        if (L.iters_out2) *L.iters_out2 = it;
+        if (L.status_out && !converged) atomicOr(L.status_out, CFD2D_S_CG_MAXITER);
+    }
+}
+
 namespace {
 
 constexpr int kMaxDevices = 64;
@@ -1685,27 +2081,30 @@ bool slab_plan(int nx, int ny, int* G_out, int* cap_out) {
     return true;
 }
 
-template <int CPT>
+template <int CPT, bool SINGLE>
 cudaError_t launch_slab(const PcgLaunch& L0, int G, int cap, cudaStream_t s) {
     static bool configured[kMaxDevices];
+    auto kern = SINGLE ? k_pcg_slab1<CPT> : k_pcg_slab<CPT>;
     const DevLimits d = dev_limits();
     if (d.sms <= 0 || d.dev >= kMaxDevices) return cudaErrorInvalidDevice;
     const size_t bytes = pcg_slab_smem_bytes(cap, L0.op.ny);
     if (!configured[d.dev]) {
         const int dyn = d.smem_optin - (int)((32 * kSlot + kSlot + CFD2D_MAX_COMPONENTS) * sizeof(double)) - 1024;
-        cudaError_t e = cudaFuncSetAttribute(k_pcg_slab<CPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
         if (e != cudaSuccess) return e;
         configured[d.dev] = true;
     }
     PcgLaunch L = L0;
     L.cap_cells = cap;
     const size_t n = (size_t)L.op.nx * L.op.ny;
-    // the barrier counter starts from zero on every launch, whatever an earlier launch
-    // that gave up on a wait left behind
-    cudaError_t e = cudaMemsetAsync(L.op.work + 3 * n + (size_t)2 * G * kSlot, 0, sizeof(double), s);
+    // the barrier counter (and the single-reduction form's per-CTA sequence words)
+    // start from zero on every launch, whatever an earlier launch that gave up on a
+    // wait left behind
+    cudaError_t e = cudaMemsetAsync(L.op.work + 3 * n + (size_t)2 * G * kSlot, 0,
+                                    sizeof(double) + (size_t)G * sizeof(unsigned int), s);
     if (e != cudaSuccess) return e;
     void* args[] = {&L};
-    return cudaLaunchCooperativeKernel((const void*)k_pcg_slab<CPT>, dim3(G), dim3(kSlabThreads), args, bytes, s);
+    return cudaLaunchCooperativeKernel((const void*)kern, dim3(G), dim3(kSlabThreads), args, bytes, s);
 }
 
 }  // namespace
@@ -1750,17 +2149,25 @@ template <bool VAR>
 cudaError_t pcg_grid_launch_t(const PcgLaunch& L, cudaStream_t s) {
     const int n = L.op.nx * L.op.ny;
     const bool cl = L.op.grid_ctas == 16;
-    if (L.op.grid_ctas != 0 && L.op.grid_ctas != -1 && !cl) return cudaErrorInvalidValue;
+    if (L.op.grid_ctas != 0 && L.op.grid_ctas != -1 && L.op.grid_ctas != -2 && !cl) return cudaErrorInvalidValue;
     if (L.op.work == nullptr || L.op.work_bytes < pcg_grid_workspace_doubles(L.op.nx, L.op.ny) * sizeof(double))
         return cudaErrorInvalidValue;
     if constexpr (!VAR) {
         int Gs = 0, cap = 0;
-        if (L.op.grid_ctas == 0 && !L.snap && slab_plan(L.op.nx, L.op.ny, &Gs, &cap)) {
+        if ((L.op.grid_ctas == 0 || L.op.grid_ctas == -2) && !L.snap && slab_plan(L.op.nx, L.op.ny, &Gs, &cap)) {
+            if (L.op.grid_ctas == 0) {
+                switch (slab_cpt_for(cap)) {
+                    case 1: return launch_slab<1, true>(L, Gs, cap, s);
+                    case 2: return launch_slab<2, true>(L, Gs, cap, s);
+                    case 4: return launch_slab<4, true>(L, Gs, cap, s);
+                    default: return launch_slab<8, true>(L, Gs, cap, s);
+                }
+            }
             switch (slab_cpt_for(cap)) {
-                case 1: return launch_slab<1>(L, Gs, cap, s);
-                case 2: return launch_slab<2>(L, Gs, cap, s);
-                case 4: return launch_slab<4>(L, Gs, cap, s);
-                default: return launch_slab<8>(L, Gs, cap, s);
+                case 1: return launch_slab<1, false>(L, Gs, cap, s);
+                case 2: return launch_slab<2, false>(L, Gs, cap, s);
+                case 4: return launch_slab<4, false>(L, Gs, cap, s);
+                default: return launch_slab<8, false>(L, Gs, cap, s);
             }
         }
     }

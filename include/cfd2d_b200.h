@@ -101,10 +101,13 @@ typedef struct cfd2d_poisson {
                                  0: the FP64 scipy-form iteration */
     int grid_ctas;            /* cluster == 0 only: 0 = cooperative launch over every SM,
                                  each CTA holding a slab of rows in shared memory when the
-                                 slabs fit (constant coefficients, even ny), else vectors in
-                                 the workspace; -1 = over every SM with the vectors in the
-                                 workspace; 16 = one 16-CTA cluster (vectors in the workspace,
-                                 cluster barriers), which leaves the other SMs to other solves */
+                                 slabs fit (constant coefficients, even ny <= 1024), with one
+                                 grid reduction per iteration (Chronopoulos-Gear), else
+                                 vectors in the workspace; -2 = the slabs with scipy's two
+                                 reductions per iteration; -1 = over every SM with the vectors
+                                 in the workspace; 16 = one 16-CTA cluster (vectors in the
+                                 workspace, cluster barriers), which leaves the other SMs to
+                                 other solves */
     const double* bx;         /* NULL: constant coefficients. Else div(b grad p) with face
                                  coefficients b = 1/rho (cfd2d/pressure.py:187-244):
                                  bx (nx+1)(ny+2) on the x faces, periodic face nx coupling

@@ -333,16 +333,17 @@ def test_misc_runs(pkg):
 
 
 # ---------------------------------------------------------------- grid-persistent solver
-GRID_CTAS = {"grid": 0, "grid-l2": -1, "cluster-l2": 16}
+GRID_CTAS = {"grid": 0, "grid-slab2": -2, "grid-l2": -1, "cluster-l2": 16}
 
 
-@pytest.mark.parametrize("variant", ["grid", "grid-l2", "cluster-l2"])
+@pytest.mark.parametrize("variant", ["grid", "grid-slab2", "grid-l2", "cluster-l2"])
 @pytest.mark.parametrize("name", ["cav", "cyl", "per", "two"])
 def test_pressure_solve_grid_variant(pkg, name, variant, monkeypatch):
     """The grid-persistent CG (used beyond on-chip capacity) on the same fixtures: over
-    every SM with shared-memory slabs ("grid"; the workspace form where ny is odd),
-    over every SM with the vectors in the workspace ("grid-l2"), on one 16-CTA cluster
-    ("cluster-l2")."""
+    every SM with shared-memory slabs and one reduction per iteration ("grid"; the
+    workspace form where ny is odd), the slabs with scipy's two reductions
+    ("grid-slab2"), over every SM with the vectors in the workspace ("grid-l2"), on one
+    16-CTA cluster ("cluster-l2")."""
     monkeypatch.setenv("CFD2D_PCG_VARIANT", variant)
     g = golden("golden_pressure")
     sim = _pressure_sim(pkg, name)
@@ -356,7 +357,7 @@ def test_pressure_solve_grid_variant(pkg, name, variant, monkeypatch):
         assert rel(p, g[name + "_p" + key]) < 1e-7
 
 
-@pytest.mark.parametrize("grid_ctas", [0, -1, 16])
+@pytest.mark.parametrize("grid_ctas", [0, -2, -1, 16])
 def test_large_grid_uses_grid_variant_and_matches_oracle(pkg, grid_ctas):
     """A grid beyond one cluster's shared memory: solve against the oracle's CG."""
     import oracle as O
@@ -379,7 +380,7 @@ def test_large_grid_uses_grid_variant_and_matches_oracle(pkg, grid_ctas):
     assert abs(ps.last_iterations - ref.pressure.last_iterations) <= max(3, ref.pressure.last_iterations // 20)
 
 
-@pytest.mark.parametrize("variant", ["grid", "grid-l2", "cluster-l2"])
+@pytest.mark.parametrize("variant", ["grid", "grid-slab2", "grid-l2", "cluster-l2"])
 def test_cavity_step_with_grid_variant(pkg, variant, monkeypatch):
     """Whole steps with the workspace solver agree with the golden run."""
     monkeypatch.setenv("CFD2D_PCG_VARIANT", variant)
