@@ -21,6 +21,8 @@ learned   = the same workload with the pressure solved by flexible CG with the
             shipped learned preconditioner (to the same 1e-8): per-step time and
             cell-updates/s inside sim.step(), and Poisson ms and iterations of
             both solvers on the same system from the same warm start.
+single_reduction = the headline workload with the slab solver's single-reduction
+            form (one grid reduction per CG iteration instead of scipy's two).
 grid_2048x1024 = the same generator and seed at 2048 x 1024: plain steps and the
             Poisson comparison (the CG cap is raised so that both reach 1e-8).
 cylinder_440x82 = the cylinder channel with a van Leer scalar (plain FP64 path).
@@ -558,6 +560,29 @@ def _graph_steps(sim, steps: int, warmup: int, flush, clock_name: str | None = N
     return step_ms, solve_ms, int(knodes.value), clk
 
 
+def single_reduction_section(steps: int, warmup: int, flush) -> dict:
+    """The headline workload with the slab solver's single-reduction form
+    (PressureSolver.grid_ctas = -2: Chronopoulos-Gear recurrence, one grid reduction
+    per CG iteration instead of scipy's two), graph-timed like the headline."""
+    import numpy as np
+
+    from cfd2d_b200 import cases
+
+    case = cases.obstacle_flow(SEED, NX, NY, pressure_solver="cg")
+    sim = case.sim
+    sim.pressure.tol = CG_RTOL
+    sim.pressure.grid_ctas = -2
+    step_ms, solve_ms, knodes, _ = _graph_steps(sim, steps, warmup, flush)
+    its = np.array(sim.history.extra["cg_iterationen"][-steps:], dtype=float)
+    dev_s = sum(step_ms) / 1e3
+    solve_s = sum(solve_ms) / 1e3
+    cells = NX * NY
+    return {"workload": WORKLOAD + "; single-reduction CG recurrence", "steps": steps,
+            "ms_per_step": 1e3 * dev_s / steps, "cell_updates_per_s": cells * steps / dev_s,
+            "poisson_ms": 1e3 * solve_s / steps, "poisson_iters_per_step": float(its.mean()),
+            "us_per_iteration": 1e6 * solve_s / its.sum()}
+
+
 def cylinder_section(steps: int, warmup: int, flush) -> dict:
     """The cylinder channel with a passive scalar (plain FP64 path), graph-timed."""
     import numpy as np
@@ -819,6 +844,7 @@ def run_b200(args, dist, rank, world):
 
     learned_rec = _optional(args.no_learned, learned_all)
     big = _optional(args.no_large, lambda: grid2048_section(3, flush))
+    single = _optional(args.no_single, lambda: single_reduction_section(args.steps, args.warmup, flush))
     cyl = _optional(args.no_cylinder, lambda: cylinder_section(100, 10, flush))
     stencils = _optional(args.no_stencils, lambda: stencil_roofline(peak))
     mixed = _optional(args.no_mixed, mixed_section)
@@ -852,6 +878,7 @@ def run_b200(args, dist, rank, world):
         "cpu_baseline": cpu,
         "clocks": clocks,
         "learned": learned_rec,
+        "single_reduction": single,
         "grid_2048x1024": big,
         "cylinder_440x82": cyl,
         "stencils": stencils,
@@ -943,6 +970,7 @@ def main():
     ap.add_argument("--no-configs", action="store_true", help="skip the cavity and SST channel section")
     ap.add_argument("--no-large", action="store_true", help="skip the 2048 x 1024 section")
     ap.add_argument("--no-cylinder", action="store_true", help="skip the cylinder 440 x 82 section")
+    ap.add_argument("--no-single", action="store_true", help="skip the single-reduction solver section")
     ap.add_argument("--workload", choices=["obstacles", "batch"], default="obstacles",
                     help="obstacles: the headline; batch: 256 uneven cavities stepped together")
     ap.add_argument("--batch-cases", type=int, default=256)

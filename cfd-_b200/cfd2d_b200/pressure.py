@@ -137,7 +137,7 @@ class PressureSolver:
         # > 0: CTAs of the on-chip cluster solver; 0: grid-persistent solver with a workspace.
         # CFD2D_PCG_VARIANT=grid (or grid-l2, cluster-l2) selects the workspace solver for any size.
         variant = os.environ.get("CFD2D_PCG_VARIANT")
-        self.cluster = 0 if variant in ("grid", "grid-slab2", "grid-l2", "cluster-l2") else cl.value
+        self.cluster = 0 if variant in ("grid", "grid-slab1", "grid-l2", "cluster-l2") else cl.value
         self._work = None
         if self.cluster == 0:
             nbytes = int(_lib.lib().cfd2d_pcg_workspace_bytes(nx, ny))
@@ -159,8 +159,8 @@ class PressureSolver:
         P.mixed = 0
         # CFD2D_PCG_VARIANT=cluster-l2: the workspace solver on one 16-CTA cluster;
         # grid-l2: over every SM with the vectors in the workspace (no shared-memory slabs);
-        # grid-slab2: the shared-memory slabs with scipy's two reductions per iteration
-        P.grid_ctas = {"cluster-l2": 16, "grid-l2": -1, "grid-slab2": -2}.get(variant, 0) if self.cluster == 0 else 0
+        # grid-slab1: the shared-memory slabs with one reduction per iteration
+        P.grid_ctas = {"cluster-l2": 16, "grid-l2": -1, "grid-slab1": -2}.get(variant, 0) if self.cluster == 0 else 0
         self.op = P
 
     def ensure_workspace(self) -> None:
@@ -179,10 +179,11 @@ class PressureSolver:
     def grid_ctas(self) -> int:
         """For grids beyond one on-chip cluster: 0 = the solver spreads over every SM
         (cooperative launch; each CTA keeps a slab of rows in shared memory when the
-        slabs fit, iterating with one grid reduction per iteration, else the vectors
-        live in the workspace); -2 = the slabs with scipy's two reductions per
-        iteration; -1 = over every SM with the vectors in the workspace; 16 = on one
-        16-CTA cluster, leaving the other SMs to other solves (cfd2d_b200.batch)."""
+        slabs fit, else the vectors live in the workspace); -2 = the slabs with one
+        grid reduction per iteration (Chronopoulos-Gear recurrence: the same iteration
+        counts, p rounded differently); -1 = over every SM with the vectors in the
+        workspace; 16 = on one 16-CTA cluster, leaving the other SMs to other solves
+        (cfd2d_b200.batch)."""
         return int(self.op.grid_ctas)
 
     @grid_ctas.setter

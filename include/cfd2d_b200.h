@@ -101,10 +101,10 @@ typedef struct cfd2d_poisson {
                                  0: the FP64 scipy-form iteration */
     int grid_ctas;            /* cluster == 0 only: 0 = cooperative launch over every SM,
                                  each CTA holding a slab of rows in shared memory when the
-                                 slabs fit (constant coefficients, even ny <= 1024), with one
-                                 grid reduction per iteration (Chronopoulos-Gear), else
-                                 vectors in the workspace; -2 = the slabs with scipy's two
-                                 reductions per iteration; -1 = over every SM with the vectors
+                                 slabs fit (constant coefficients, even ny <= 1024), else
+                                 vectors in the workspace; -2 = the slabs with one grid
+                                 reduction per iteration (Chronopoulos-Gear recurrence instead
+                                 of scipy's two); -1 = over every SM with the vectors
                                  in the workspace; 16 = one 16-CTA cluster (vectors in the
                                  workspace, cluster barriers), which leaves the other SMs to
                                  other solves */

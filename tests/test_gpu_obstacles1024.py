@@ -29,6 +29,7 @@ from conftest import golden
 
 TOL = 1e-10
 TOL_P = 2e-9
+TOL_P_SINGLE = 5e-9
 
 
 def _fixture():
@@ -47,13 +48,20 @@ def test_fixture_spec_is_the_generator_seed():
 
 
 @pytest.mark.gpu
-def test_obstacle_flow_1024x512_three_steps(cuda_lib):
+@pytest.mark.parametrize("grid_ctas, tol_p", [(0, TOL_P), (-2, TOL_P_SINGLE)])
+def test_obstacle_flow_1024x512_three_steps(cuda_lib, grid_ctas, tol_p):
+    """The default slab solver (scipy's two reductions per iteration) and its
+    single-reduction form (grid_ctas = -2, Chronopoulos-Gear recurrence), whose p.q
+    comes from a recurrence instead of a dot product and moves the unconverged part of
+    p further: measured 2.4e-9 after the first step, with the same iteration counts
+    and u, v within 1e-12."""
     from cfd2d_b200 import cases
 
     g = _fixture()
     case = cases.obstacle_flow(13, 1024, 512, pressure_solver="cg")
     sim = case.sim
     sim.pressure.tol = 1e-8
+    sim.pressure.grid_ctas = grid_ctas
     flags = np.packbits(sim.grid.fluid.astype(np.uint8), axis=None)
     assert np.array_equal(flags, g["obs1024_fluid_bits"])
     errs = {}
@@ -71,7 +79,7 @@ def test_obstacle_flow_1024x512_three_steps(cuda_lib):
     its = np.array(sim.history.extra["cg_iterationen"][-3:])
     print("iterations", its, "reference", g["obs1024_its"])
     print({k: f"{v:.2e}" for k, v in errs.items()})
-    bad = {k: v for k, v in errs.items() if not v < (TOL_P if k[1] == "p" else TOL)}
+    bad = {k: v for k, v in errs.items() if not v < (tol_p if k[1] == "p" else TOL)}
     assert not bad, bad
     assert np.abs(its - g["obs1024_its"]).max() <= 3, (its, g["obs1024_its"])
     np.testing.assert_allclose(sim.history.dt[-3:], g["obs1024_dt"], rtol=1e-12)

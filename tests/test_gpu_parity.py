@@ -333,17 +333,16 @@ def test_misc_runs(pkg):
 
 
 # ---------------------------------------------------------------- grid-persistent solver
-GRID_CTAS = {"grid": 0, "grid-slab2": -2, "grid-l2": -1, "cluster-l2": 16}
+GRID_CTAS = {"grid": 0, "grid-slab1": -2, "grid-l2": -1, "cluster-l2": 16}
 
 
-@pytest.mark.parametrize("variant", ["grid", "grid-slab2", "grid-l2", "cluster-l2"])
+@pytest.mark.parametrize("variant", ["grid", "grid-slab1", "grid-l2", "cluster-l2"])
 @pytest.mark.parametrize("name", ["cav", "cyl", "per", "two"])
 def test_pressure_solve_grid_variant(pkg, name, variant, monkeypatch):
     """The grid-persistent CG (used beyond on-chip capacity) on the same fixtures: over
-    every SM with shared-memory slabs and one reduction per iteration ("grid"; the
-    workspace form where ny is odd), the slabs with scipy's two reductions
-    ("grid-slab2"), over every SM with the vectors in the workspace ("grid-l2"), on one
-    16-CTA cluster ("cluster-l2")."""
+    every SM with shared-memory slabs ("grid"; the workspace form where ny is odd), the
+    slabs with one reduction per iteration ("grid-slab1"), over every SM with the
+    vectors in the workspace ("grid-l2"), on one 16-CTA cluster ("cluster-l2")."""
     monkeypatch.setenv("CFD2D_PCG_VARIANT", variant)
     g = golden("golden_pressure")
     sim = _pressure_sim(pkg, name)
@@ -380,7 +379,7 @@ def test_large_grid_uses_grid_variant_and_matches_oracle(pkg, grid_ctas):
     assert abs(ps.last_iterations - ref.pressure.last_iterations) <= max(3, ref.pressure.last_iterations // 20)
 
 
-@pytest.mark.parametrize("variant", ["grid", "grid-slab2", "grid-l2", "cluster-l2"])
+@pytest.mark.parametrize("variant", ["grid", "grid-slab1", "grid-l2", "cluster-l2"])
 def test_cavity_step_with_grid_variant(pkg, variant, monkeypatch):
     """Whole steps with the workspace solver agree with the golden run."""
     monkeypatch.setenv("CFD2D_PCG_VARIANT", variant)
