@@ -222,9 +222,9 @@ def lib():
         "cfd2d_lpc_conv": ([i, i, vp, i, vp, vp, vp, vp, i, i, i, i, i, vp], i),
         "cfd2d_lpc_pool2": ([vp, vp, i, i, vp], i),
         "cfd2d_lpc_pool_mask": ([vp, vp, i, i, vp], i),
-        "cfd2d_lpc_upadd": ([vp, vp, vp, i, i, vp], i),
+        "cfd2d_lpc_upadd": ([vp, vp, vp, i, i, C.c_float, vp], i),
         "cfd2d_lpc_relu_bwd": ([vp, vp, vp, vp, i, i, i, vp], i),
-        "cfd2d_lpc_upadd_bwd": ([vp, vp, i, i, vp], i),
+        "cfd2d_lpc_upadd_bwd": ([vp, vp, i, i, C.c_float, vp], i),
         "cfd2d_lpc_pool_bwd": ([vp, vp, i, i, vp], i),
         "cfd2d_lpc_conv_dw_partial_floats": ([i, i, i, i, i], sz),
         "cfd2d_lpc_conv_dw": ([i, i, vp, i, vp, i, i, i, vp, vp, vp], i),

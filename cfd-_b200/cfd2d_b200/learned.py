@@ -1,38 +1,44 @@
 """Learned Poisson preconditioner inside flexible CG (no counterpart in the reference).
 
-Network (4 levels, 32 channels, 3x3 convolutions, BF16 weights and activations,
-FP32 accumulation, 65,025 parameters):
+Network: a U-Net over as many levels as the grid needs for its coarsest level to
+be at most ``coarsest`` cells on a side (8 by default: 7 levels at 256 x 256, 8 at
+1024 x 512, 9 at 2048 x 1024), 32 channels, 3x3 convolutions, BF16 weights and
+activations, FP32 accumulation. Nine weight tensors (65,088 parameters), the
+deepest encoder and decoder shared by every level from ``shared`` (3) down, so one
+set of weights serves every grid size:
 
-    a0  = relu(conv 1->32 (r / ||r||))                      level 0 (CUDA cores)
-    a0b = relu(conv 32->32 (a0))                            level 0 (tensor cores)
-    a1  = relu(conv 32->32 (pool a0b))                      level 1
-    a2  = relu(conv 32->32 (pool a1))                       level 2
-    a3  = relu(conv 32->32 (pool a2))                       level 3
-    d2  = relu(conv 32->32 (up a3 + a2))                    level 2
-    d1  = relu(conv 32->32 (up d2 + a1))                    level 1
-    d0  = relu(conv 32->32 (up d1 + a0b))                   level 0
-    out = conv 32->1 (d0)                                   level 0 (CUDA cores)
+    a_0 = f(conv_a0 (r / ||r||))                              level 0 (1 -> 32)
+    a_l = f(conv_e(l) (pool a_{l-1}))   (nrep times at l >= 3) levels 1 .. L-1
+    d_{L-1} = a_{L-1}
+    d_l = f(conv_d(l) (scale * up d_{l+1} + a_l))  (nrep times at l >= 3)
+    out = conv_out (d_0)                                      level 0 (32 -> 1)
 
-Every layer output is multiplied by the fluid mask of its level. The 32->32
-layers run on tcgen05 (``cfd2d_lpc_conv32``); the 1-channel layers, pooling,
-upsampling and the whole backward pass are hand-written CUDA-core kernels of the
-same library (``net_forward`` / ``net_backward``); the optimiser (Adam) is
-PyTorch's, on FP32 master weights.
+with e(l) = e1, e2, e3, e3, ... and d(l) = d0, d1, d2, d3, d3, ...; every layer
+output is multiplied by the fluid mask of its level (a coarse cell is fluid if any
+child is). f is the identity by default (``act="linear"``: the network is then a
+fixed linear operator, odd and homogeneous by construction, as a preconditioner
+must be) or ReLU. ``scale`` = 4 makes a coarse level contribute in the units of the
+finer one: the network approximates Ah^-1 with Ah = h^2 A, and the same
+dimensionless operator on a grid of twice the spacing is 4 times weaker, so a
+correction computed on level l counts 4^l times on level 0.
 
-The network works on the dimensionless operator Ah = h^2 A (h^2 = 2 / (1/dx^2 +
-1/dy^2)), so one set of weights serves every grid spacing: for a residual r it
-approximates Ah^-1 (r / ||r||). Training minimises the energy-norm error of that
-approximation, (e - o)^T Ah (e - o) with e = Ah^-1 r_hat, i.e. o^T Ah o - 2 o.r_hat
-(the constant e^T Ah e dropped), over residuals harvested from the plain solver's
-own iterations. Inside flexible CG (Notay's form, one stored direction) the preconditioner is
-M(r) = h^2 ||r|| net(r / ||r||) + omega D^-1 r; the loop runs on the device inside
-one CUDA graph (a WHILE node) and falls back to the plain Jacobi-PCG from the
-current iterate when it stalls.
+The 32->32 layers run on tcgen05 (``cfd2d_lpc_conv32``); the 1-channel layers,
+pooling, upsampling and the whole backward pass are hand-written CUDA-core kernels
+of the same library (``net_forward`` / ``net_backward``, replaying one op list per
+grid size); the optimiser (Adam) is PyTorch's, on FP32 master weights.
+
+Training minimises the energy-norm error of net(r_hat) against Ah^-1 r_hat,
+o^T Ah o - 2 o.r_hat (the constant e^T Ah e dropped), over residuals harvested from
+the plain solver's own iterations. Inside flexible CG (Notay's form, one stored
+direction) the preconditioner is M(r) = h^2 ||r|| net(r / ||r||) + omega D^-1 r; the
+loop runs on the device inside one CUDA graph (a WHILE node) and falls back to the
+plain Jacobi-PCG from the current iterate when it stalls.
 """
 
 from __future__ import annotations
 
 import ctypes as C
+import json
 import math
 import time
 
@@ -41,45 +47,85 @@ import numpy as np
 from . import _lib
 
 CH = 32
-LAYERS = [  # name, cin, cout, level, relu
-    ("a0", 1, CH, 0, True), ("a0b", CH, CH, 0, True), ("a1", CH, CH, 1, True), ("a2", CH, CH, 2, True),
-    ("a3", CH, CH, 3, True), ("d2", CH, CH, 2, True), ("d1", CH, CH, 1, True), ("d0", CH, CH, 0, True),
-    ("out", CH, 1, 0, False),
-]
-NLEVELS = 4
+# weight tensors: name -> (cin, cout)
+WEIGHTS = {"a0": (1, CH), "e1": (CH, CH), "e2": (CH, CH), "e3": (CH, CH), "d0": (CH, CH), "d1": (CH, CH),
+           "d2": (CH, CH), "d3": (CH, CH), "out": (CH, 1)}
+DEFAULT_ARCH = {"act": "linear", "scale": 4.0, "nrep": 2, "coarsest": 8, "shared": 3}
 
 
 def _t():
     return _lib.torch()
 
 
-def level_shapes(H, W):
+def nlevels(H: int, W: int, coarsest: int) -> int:
+    """Levels of an H x W grid: halve (rounding up) until both sides are <= coarsest."""
+    L = 1
+    while max(H, W) > coarsest:
+        H, W = (H + 1) // 2, (W + 1) // 2
+        L += 1
+    return L
+
+
+def level_shapes(H, W, L):
     shapes = [(H, W)]
-    for _ in range(NLEVELS - 1):
+    for _ in range(L - 1):
         h, w = shapes[-1]
         shapes.append(((h + 1) // 2, (w + 1) // 2))
     return shapes
+
+
+def op_list(L: int, arch: dict):
+    """The network as a list of ops over named buffers, in execution order:
+    ("conv", weight, level, src, dst), ("pool", level, src, dst) (src on level - 1),
+    ("upadd", level, coarse, skip, dst)."""
+    S, nrep = arch["shared"], arch["nrep"]
+    ops = [("conv", "a0", 0, "in", "a0.0")]
+    cur = "a0.0"
+    for lvl in range(1, L):
+        ops.append(("pool", lvl, cur, f"p{lvl}"))
+        cur = f"p{lvl}"
+        w = f"e{min(lvl, S)}"
+        for k in range(nrep if lvl >= S else 1):
+            ops.append(("conv", w, lvl, cur, f"a{lvl}.{k}"))
+            cur = f"a{lvl}.{k}"
+    skips = {}
+    for op in ops:
+        if op[0] == "conv" and op[1] != "out":
+            skips[op[2]] = op[4]  # last conv output of each level
+    for lvl in range(L - 2, -1, -1):
+        ops.append(("upadd", lvl, cur, skips[lvl], f"u{lvl}"))
+        cur = f"u{lvl}"
+        w = f"d{min(lvl, S)}"
+        for k in range(nrep if lvl >= S else 1):
+            ops.append(("conv", w, lvl, cur, f"d{lvl}.{k}"))
+            cur = f"d{lvl}.{k}"
+    ops.append(("conv", "out", 0, cur, "out"))
+    return ops
 
 
 class LPCNet:
     """Weights (FP32 masters) and the packed BF16 tensor-core images of the 32->32 layers.
 
     With ``bias=False`` (the default) the biases stay zero and are not trained: the
-    network is then positively homogeneous, net(a r) = a net(r) for a > 0, and with
-    sign-flipped training samples close to odd, as a preconditioner inside CG must
-    be (a trained bias adds a fixed field to every preconditioned residual, and the
-    flexible CG stalls on it)."""
+    network is then positively homogeneous, net(a r) = a net(r) for a > 0 (and, with
+    the linear activation, linear), as a preconditioner inside CG must be (a trained
+    bias adds a fixed field to every preconditioned residual, and the flexible CG
+    stalls on it)."""
 
-    def __init__(self, seed: int = 0, bias: bool = False):
+    def __init__(self, seed: int = 0, bias: bool = False, arch: dict | None = None):
         t = _t()
         self.bias = bias
+        self.arch = dict(DEFAULT_ARCH, **(arch or {}))
         g = t.Generator().manual_seed(seed)
         self.w, self.b = {}, {}
-        for name, cin, cout, _lvl, relu in LAYERS:
-            # uniform in +-1/sqrt(fan_in), the output layer ten times smaller: the
-            # network starts close to zero and the Jacobi term leads the first steps
+        for name, (cin, cout) in WEIGHTS.items():
+            # uniform in +-1/sqrt(fan_in) (the linear form: scaled so that a layer
+            # roughly keeps the norm), the output layer ten times smaller: the network
+            # starts close to zero and the Jacobi term leads the first steps
             bound = 1.0 / math.sqrt(cin * 9)
-            if not relu:
+            if self.arch["act"] == "linear":
+                bound *= math.sqrt(3.0) / math.sqrt(3.0 if cin > 1 else 1.0)
+            if name == "out":
                 bound *= 0.1
             self.w[name] = ((t.rand((cout, cin, 3, 3), generator=g) * 2.0 - 1.0) * bound).to(_lib.device())
             self.b[name] = t.zeros(cout, device=_lib.device())
@@ -88,12 +134,16 @@ class LPCNet:
         self.repack()
 
     @property
+    def relu(self) -> int:
+        return 1 if self.arch["act"] == "relu" else 0
+
+    @property
     def n_params(self) -> int:
         return sum(v.numel() for v in self.w.values()) + sum(v.numel() for v in self.b.values())
 
     def parameters(self):
         out = []
-        for name, *_ in LAYERS:
+        for name in WEIGHTS:
             out += [self.w[name], self.b[name]] if self.bias else [self.w[name]]
         return out
 
@@ -104,32 +154,37 @@ class LPCNet:
         t = _t()
         L = _lib.lib()
         nbytes = int(L.cfd2d_lpc_w32_bytes())
-        for name, cin, cout, _lvl, _relu in LAYERS:
+        for name, (cin, cout) in WEIGHTS.items():
             if not (cin == CH and cout == CH):
                 q = self.wq(name)
                 if name in self._wq:
                     self._wq[name].copy_(q)
                 else:
                     self._wq[name] = q
-            if cin == CH and cout == CH:
-                img = self._images.get(name)
-                if img is None:
-                    img = t.zeros(nbytes // 2, dtype=t.bfloat16, device=_lib.device())
-                    self._images[name] = img
-                w = self.w[name].detach().float().contiguous()
-                _lib.check(L.cfd2d_lpc_pack_w32(_lib.ptr(w), _lib.ptr(img), _lib.stream_ptr()), "pack_w32")
+                continue
+            img = self._images.get(name)
+            if img is None:
+                img = t.zeros(nbytes // 2, dtype=t.bfloat16, device=_lib.device())
+                self._images[name] = img
+            w = self.w[name].detach().float().contiguous()
+            _lib.check(L.cfd2d_lpc_pack_w32(_lib.ptr(w), _lib.ptr(img), _lib.stream_ptr()), "pack_w32")
 
     def wq(self, name):
-        """The BF16-rounded weights the kernels use, as FP32 (for the CUDA-core layers)."""
+        """The BF16-rounded weights the kernels use, as FP32."""
         return self.w[name].detach().to(_t().bfloat16).float().contiguous()
 
     def state_dict(self):
-        return {f"{k}.w": v.detach().cpu() for k, v in self.w.items()} | \
-               {f"{k}.b": v.detach().cpu() for k, v in self.b.items()}
+        t = _t()
+        d = {f"{k}.w": v.detach().cpu() for k, v in self.w.items()} | \
+            {f"{k}.b": v.detach().cpu() for k, v in self.b.items()}
+        d["arch"] = t.tensor(list(json.dumps(self.arch).encode()), dtype=t.uint8)
+        return d
 
     def load_state_dict(self, d):
-        self.bias = any(float(d[f"{name}.b"].abs().max()) > 0.0 for name, *_ in LAYERS)
-        for name, *_ in LAYERS:
+        if "arch" in d:
+            self.arch = dict(DEFAULT_ARCH, **json.loads(bytes(d["arch"].tolist()).decode()))
+        self.bias = any(float(d[f"{name}.b"].abs().max()) > 0.0 for name in WEIGHTS)
+        for name in WEIGHTS:
             self.w[name].copy_(d[f"{name}.w"].to(self.w[name].device))
             self.b[name].copy_(d[f"{name}.b"].to(self.b[name].device))
         self.repack()
@@ -145,39 +200,40 @@ def _take_net_error(ws) -> bool:
 
 
 class Workspace:
-    """Activation buffers of one grid size (reused across applications)."""
+    """Masks and activation buffers of one grid size and architecture (reused across
+    applications): one BF16 buffer per op output, named as in ``op_list``."""
 
-    def __init__(self, H: int, W: int, mask):
+    def __init__(self, H: int, W: int, mask, arch: dict | None = None):
         t = _t()
         dev = _lib.device()
-        L = _lib.lib()
+        self.arch = dict(DEFAULT_ARCH, **(arch or {}))
         self.H, self.W = H, W
-        self.shapes = level_shapes(H, W)
+        self.L = nlevels(H, W, self.arch["coarsest"])
+        self.shapes = level_shapes(H, W, self.L)
+        self.ops = op_list(self.L, self.arch)
         self.masks = [t.zeros(s, dtype=t.uint8, device=dev) for s in self.shapes]
         self.mask_src = None
         self.set_mask(mask)
-        act = lambda lvl: t.zeros(self.shapes[lvl] + (CH,), dtype=t.bfloat16, device=dev)  # noqa: E731
-        self.a = {name: act(lvl) for name, cin, cout, lvl, _ in LAYERS if cout == CH}
-        self.pool = {lvl: act(lvl) for lvl in (1, 2, 3)}
-        self.up = {lvl: act(lvl) for lvl in (0, 1, 2)}
+        self.buf = {}
+        for op in self.ops:
+            lvl, dst = (op[2], op[4]) if op[0] == "conv" else (op[1], op[-1])
+            if dst == "out":
+                continue
+            self.buf[dst] = t.zeros(self.shapes[lvl] + (CH,), dtype=t.bfloat16, device=dev)
         self.out = t.zeros((H, W), dtype=t.float32, device=dev)
         self.err = t.zeros(1, dtype=t.int32, device=dev)
 
-
-def _ws_set_mask(self, mask):
-    """Fluid mask of level 0 (H, W) and its pooled masks (any child fluid)."""
-    t = _t()
-    L = _lib.lib()
-    m0 = mask if isinstance(mask, t.Tensor) else _lib.to_dev(np.asarray(mask, dtype=np.uint8))
-    self.masks[0].copy_(m0.reshape(self.H, self.W).to(t.uint8))
-    for lvl in range(1, NLEVELS):
-        h, w = self.shapes[lvl - 1]
-        _lib.check(L.cfd2d_lpc_pool_mask(_lib.ptr(self.masks[lvl - 1]), _lib.ptr(self.masks[lvl]), h, w,
-                                         _lib.stream_ptr()), "pool_mask")
-    self.mask_src = mask
-
-
-Workspace.set_mask = _ws_set_mask
+    def set_mask(self, mask):
+        """Fluid mask of level 0 (H, W) and its pooled masks (any child fluid)."""
+        t = _t()
+        L = _lib.lib()
+        m0 = mask if isinstance(mask, t.Tensor) else _lib.to_dev(np.asarray(mask, dtype=np.uint8))
+        self.masks[0].copy_(m0.reshape(self.H, self.W).to(t.uint8))
+        for lvl in range(1, self.L):
+            h, w = self.shapes[lvl - 1]
+            _lib.check(L.cfd2d_lpc_pool_mask(_lib.ptr(self.masks[lvl - 1]), _lib.ptr(self.masks[lvl]), h, w,
+                                             _lib.stream_ptr()), "pool_mask")
+        self.mask_src = mask
 
 
 def net_forward(net: LPCNet, ws: Workspace, x_in):
@@ -186,116 +242,116 @@ def net_forward(net: LPCNet, ws: Workspace, x_in):
     s = _lib.stream_ptr()
     P = _lib.ptr
     sh = ws.shapes
-
-    def conv32(name, src, lvl, skip=None):
-        h, w = sh[lvl]
-        rc = L.cfd2d_lpc_conv32(P(src), P(net._images[name]), P(net.b[name]), P(skip), P(ws.masks[lvl]),
-                                P(ws.a[name]), h, w, 1, P(ws.err), s)
-        _lib.check(rc, "lpc_conv32")
-
-    H, W = sh[0]
-    _lib.check(L.cfd2d_lpc_conv(1, CH, P(x_in), 0, P(net._wq["a0"]), P(net.b["a0"]), P(ws.masks[0]), P(ws.a["a0"]),
-                                1, H, W, 1, 0, s), "lpc_conv a0")
-    conv32("a0b", ws.a["a0"], 0)
-    prev = ws.a["a0b"]
-    for lvl, name in ((1, "a1"), (2, "a2"), (3, "a3")):
-        h, w = sh[lvl - 1]
-        _lib.check(L.cfd2d_lpc_pool2(P(prev), P(ws.pool[lvl]), h, w, s), "pool2")
-        conv32(name, ws.pool[lvl], lvl)
-        prev = ws.a[name]
-    for lvl, name, skip in ((2, "d2", "a2"), (1, "d1", "a1"), (0, "d0", "a0b")):
-        h, w = sh[lvl]
-        _lib.check(L.cfd2d_lpc_upadd(P(prev), P(ws.a[skip]), P(ws.up[lvl]), h, w, s), "upadd")
-        conv32(name, ws.up[lvl], lvl)
-        prev = ws.a[name]
-    _lib.check(L.cfd2d_lpc_conv(CH, 1, P(prev), 1, P(net._wq["out"]), P(net.b["out"]), P(ws.masks[0]), P(ws.out),
-                                0, H, W, 0, 0, s), "lpc_conv out")
+    relu = net.relu
+    scale = float(net.arch["scale"])
+    for op in ws.ops:
+        if op[0] == "conv":
+            _, name, lvl, src, dst = op
+            h, w = sh[lvl]
+            cin, cout = WEIGHTS[name]
+            if cin == CH and cout == CH:
+                rc = L.cfd2d_lpc_conv32(P(ws.buf[src]), P(net._images[name]), P(net.b[name]), None, P(ws.masks[lvl]),
+                                        P(ws.buf[dst]), h, w, relu, P(ws.err), s)
+                _lib.check(rc, "lpc_conv32")
+            elif cin == 1:
+                _lib.check(L.cfd2d_lpc_conv(1, CH, P(x_in), 0, P(net._wq[name]), P(net.b[name]), P(ws.masks[lvl]),
+                                            P(ws.buf[dst]), 1, h, w, relu, 0, s), "lpc_conv in")
+            else:
+                _lib.check(L.cfd2d_lpc_conv(CH, 1, P(ws.buf[src]), 1, P(net._wq[name]), P(net.b[name]),
+                                            P(ws.masks[lvl]), P(ws.out), 0, h, w, 0, 0, s), "lpc_conv out")
+        elif op[0] == "pool":
+            _, lvl, src, dst = op
+            h, w = sh[lvl - 1]
+            _lib.check(L.cfd2d_lpc_pool2(P(ws.buf[src]), P(ws.buf[dst]), h, w, s), "pool2")
+        else:
+            _, lvl, coarse, skip, dst = op
+            h, w = sh[lvl]
+            _lib.check(L.cfd2d_lpc_upadd(P(ws.buf[coarse]), P(ws.buf[skip]), P(ws.buf[dst]), h, w, scale, s),
+                       "upadd")
     return ws.out
 
 
 def net_backward(net: LPCNet, ws: Workspace, x_in, dout):
     """Gradients of sum(out * dout) w.r.t. every weight and bias (FP32), from the
-    activations left in ``ws`` by net_forward(x_in)."""
+    activations left in ``ws`` by net_forward(x_in): the op list replayed in reverse
+    with the hand-written backward kernels; shared weights sum their gradients over
+    the levels that use them."""
     t = _t()
     L = _lib.lib()
     s = _lib.stream_ptr()
     P = _lib.ptr
     sh = ws.shapes
     dev = _lib.device()
-    grads = {}
+    relu = net.relu
+    scale = float(net.arch["scale"])
+    grads = {name: (t.zeros((cout, cin, 3, 3), device=dev), t.zeros(cout, device=dev))
+             for name, (cin, cout) in WEIGHTS.items()}
+    g = {"out": dout.contiguous()}  # gradient of every buffer, FP32
 
-    def zeros(lvl, ch=CH):
-        return t.zeros(sh[lvl] + (ch,), dtype=t.float32, device=dev)
+    def add(name, val):
+        if name in g:
+            g[name].add_(val)
+        else:
+            g[name] = val
 
-    def dw(name, cin, cout, x, xbf, g, lvl):
-        h, w = sh[lvl]
-        ppb = 256
-        part = t.empty(int(L.cfd2d_lpc_conv_dw_partial_floats(cin, cout, h, w, ppb)), dtype=t.float32, device=dev)
-        out = t.empty(cout * cin * 9 + cout, dtype=t.float32, device=dev)
-        _lib.check(L.cfd2d_lpc_conv_dw(cin, cout, P(x), xbf, P(g), h, w, ppb, P(part), P(out), s), "conv_dw")
-        grads[name] = (out[:cout * cin * 9].view(cout, cin, 3, 3), out[cout * cin * 9:])
-
-    def relu_g(dy, y, lvl, relu=True, ch=CH):
-        h, w = sh[lvl]
-        g = t.empty_like(dy)
-        _lib.check(L.cfd2d_lpc_relu_bwd(P(dy), P(y), P(ws.masks[lvl]), P(g), h * w, ch, int(relu), s), "relu_bwd")
-        return g
-
-    def conv_t(name, cin_f, cout_f, g, lvl):
-        # data gradient of a forward layer (cin_f -> cout_f): adjoint conv of g (cout_f channels)
-        h, w = sh[lvl]
-        dx = zeros(lvl, cin_f)
-        _lib.check(L.cfd2d_lpc_conv(cout_f, cin_f, P(g), 0, P(net.wq(name)), None, None, P(dx), 0, h, w, 0, 1, s),
-                   "conv transposed")
-        return dx
-
-    H, W = sh[0]
-    g = relu_g(dout.contiguous(), None, 0, relu=False, ch=1)
-    dw("out", CH, 1, ws.a["d0"], 1, g, 0)
-    dd = conv_t("out", CH, 1, g, 0)
-    skip_grad = {}
-    for lvl, name, skip, inp in ((0, "d0", "a0b", ws.up[0]), (1, "d1", "a1", ws.up[1]), (2, "d2", "a2", ws.up[2])):
-        g = relu_g(dd, ws.a[name], lvl)
-        dw(name, CH, CH, inp, 1, g, lvl)
-        du = conv_t(name, CH, CH, g, lvl)
-        skip_grad[skip] = du
-        h, w = sh[lvl]
-        dc = zeros(lvl + 1)
-        _lib.check(L.cfd2d_lpc_upadd_bwd(P(du), P(dc), h, w, s), "upadd_bwd")
-        dd = dc
-    # encoder, deepest first: da3 = dd
-    da = dd
-    for lvl, name in ((3, "a3"), (2, "a2"), (1, "a1")):
-        g = relu_g(da, ws.a[name], lvl)
-        dw(name, CH, CH, ws.pool[lvl], 1, g, lvl)
-        dp = conv_t(name, CH, CH, g, lvl)
-        below = {3: "a2", 2: "a1", 1: "a0b"}[lvl]
-        nxt = skip_grad[below].clone()
-        h, w = sh[lvl - 1]
-        _lib.check(L.cfd2d_lpc_pool_bwd(P(dp), P(nxt), h, w, s), "pool_bwd")
-        da = nxt
-    g = relu_g(da, ws.a["a0b"], 0)
-    dw("a0b", CH, CH, ws.a["a0"], 1, g, 0)
-    da0 = conv_t("a0b", CH, CH, g, 0)
-    g = relu_g(da0, ws.a["a0"], 0)
-    dw("a0", 1, CH, x_in.contiguous(), 0, g, 0)
+    for op in reversed(ws.ops):
+        if op[0] == "conv":
+            _, name, lvl, src, dst = op
+            h, w = sh[lvl]
+            cin, cout = WEIGHTS[name]
+            gy = g.pop(dst)
+            # through the mask (and the ReLU) of the layer output
+            gp = t.empty_like(gy)
+            yb = ws.buf[dst] if dst != "out" else None
+            r = relu if dst != "out" else 0
+            _lib.check(L.cfd2d_lpc_relu_bwd(P(gy), P(yb), P(ws.masks[lvl]), P(gp), h * w, cout, r, s), "relu_bwd")
+            xsrc, xbf = (x_in.contiguous(), 0) if src == "in" else (ws.buf[src], 1)
+            ppb = 256
+            part = t.empty(int(L.cfd2d_lpc_conv_dw_partial_floats(cin, cout, h, w, ppb)), dtype=t.float32, device=dev)
+            dwb = t.empty(cout * cin * 9 + cout, dtype=t.float32, device=dev)
+            _lib.check(L.cfd2d_lpc_conv_dw(cin, cout, P(xsrc), xbf, P(gp), h, w, ppb, P(part), P(dwb), s), "conv_dw")
+            grads[name][0].add_(dwb[:cout * cin * 9].view(cout, cin, 3, 3))
+            grads[name][1].add_(dwb[cout * cin * 9:])
+            if src != "in":
+                dx = t.zeros(sh[lvl] + (cin,), dtype=t.float32, device=dev)
+                _lib.check(L.cfd2d_lpc_conv(cout, cin, P(gp), 0, P(net.wq(name)), None, None, P(dx), 0, h, w, 0, 1,
+                                            s), "conv transposed")
+                add(src, dx)
+        elif op[0] == "pool":
+            _, lvl, src, dst = op
+            h, w = sh[lvl - 1]
+            gy = g.pop(dst)
+            dfine = g[src] if src in g else t.zeros(sh[lvl - 1] + (CH,), dtype=t.float32, device=dev)
+            _lib.check(L.cfd2d_lpc_pool_bwd(P(gy), P(dfine), h, w, s), "pool_bwd")
+            g[src] = dfine
+        else:
+            _, lvl, coarse, skip, dst = op
+            h, w = sh[lvl]
+            gy = g.pop(dst)
+            dc = t.empty(sh[lvl + 1] + (CH,), dtype=t.float32, device=dev)
+            _lib.check(L.cfd2d_lpc_upadd_bwd(P(gy), P(dc), h, w, scale, s), "upadd_bwd")
+            add(coarse, dc)
+            add(skip, gy.clone())
     return grads
 
 
-def torch_reference_forward(net: LPCNet, x_in, masks):
+def torch_reference_forward(net, x_in, masks, arch: dict | None = None):
     """The same network in PyTorch (CPU, FP32 on BF16-rounded weights and activations):
     the reference computation for the CUDA kernels and their gradients."""
     t = _t()
     F = t.nn.functional
+    arch = dict(DEFAULT_ARCH, **(arch or getattr(net, "arch", {}) or {}))
+    relu = arch["act"] == "relu"
+    scale = float(arch["scale"])
 
     def bf(a):
         return a.to(t.bfloat16).float()
 
-    def conv(name, a, relu, lvl, round_out=True):
+    def conv(name, a, lvl, act, round_out=True):
         bias = net.b[name]
         bias = bias.detach().cpu() if bias.is_cuda else bias
         y = F.conv2d(a, net.wq(name).cpu(), bias, padding=1)
-        if relu:
+        if act:
             y = t.relu(y)
         y = y * masks[lvl]
         return bf(y) if round_out else y
@@ -310,18 +366,22 @@ def torch_reference_forward(net: LPCNet, x_in, masks):
     def up(a, skip):
         h, w = skip.shape[-2:]
         u = a.repeat_interleave(2, -2).repeat_interleave(2, -1)[..., :h, :w]
-        return bf(u + skip)
+        return bf(scale * u + skip)
 
-    x = x_in.cpu().float()[None, None]
-    a0 = conv("a0", x, True, 0)
-    a0b = conv("a0b", a0, True, 0)
-    a1 = conv("a1", pool(a0b), True, 1)
-    a2 = conv("a2", pool(a1), True, 2)
-    a3 = conv("a3", pool(a2), True, 3)
-    d2 = conv("d2", up(a3, a2), True, 2)
-    d1 = conv("d1", up(d2, a1), True, 1)
-    d0 = conv("d0", up(d1, a0b), True, 0)
-    return conv("out", d0, False, 0, round_out=False)[0, 0]
+    Lv = len(masks)
+    buf = {"in": x_in.cpu().float()[None, None]}
+    for op in op_list(Lv, arch):
+        if op[0] == "conv":
+            _, name, lvl, src, dst = op
+            last = dst == "out"
+            buf[dst] = conv(name, buf[src], lvl, relu and not last, round_out=not last)
+        elif op[0] == "pool":
+            _, lvl, src, dst = op
+            buf[dst] = pool(buf[src])
+        else:
+            _, lvl, coarse, skip, dst = op
+            buf[dst] = up(buf[coarse], buf[skip])
+    return buf["out"][0, 0]
 
 
 # ------------------------------------------------------------------ flexible CG
@@ -363,7 +423,7 @@ class LearnedPCG:
         self.scal = t.zeros(C.sizeof(_lib.FcgScalars) // 8, dtype=t.float64, device=dev)
         self.mask = pressure._d_nbr.view(self.nx, self.ny) >= 0x80
         self.mask_u8 = self.mask.to(t.uint8).contiguous()
-        self.ws = Workspace(self.nx, self.ny, self.mask_u8)
+        self.ws = Workspace(self.nx, self.ny, self.mask_u8, net.arch)
         self.hist = t.zeros(maxiter + 1, dtype=t.float64, device=dev)
         self.ctl = t.zeros(C.sizeof(_lib.FcgControl), dtype=t.uint8, device=dev)
         self._graphs = {}
@@ -535,20 +595,27 @@ def obstacle_case(rng, nx: int, ny: int, pressure_solver: str = "cg", lx: float 
 
 
 class TrainingSet:
-    """Normalised residuals r_k / ||r_k|| (FP32, (N, H, W), on the device), the case
-    each one belongs to, and per case the pressure operator (for Ah o in the loss),
-    its h^2 and its fluid mask."""
+    """Normalised residuals r_k / ||r_k|| (FP32 (H, W) tensors on the device, grids of
+    any size), the case each one belongs to, and per case the pressure operator (for
+    Ah o in the loss), its h^2 and its fluid mask."""
 
     def __init__(self, R, case_of, solvers, masks):
-        self.R, self.case_of, self.solvers, self.masks = R, case_of, solvers, masks
+        self.R, self.case_of, self.solvers, self.masks = list(R), list(case_of), list(solvers), list(masks)
         self.h2 = [h2_of(ps) for ps in solvers]
 
     def __len__(self):
-        return int(self.R.shape[0])
+        return len(self.R)
+
+    def merge(self, other: "TrainingSet") -> "TrainingSet":
+        """The samples of both sets (case indices of ``other`` shifted after this one's)."""
+        n = len(self.solvers)
+        return TrainingSet(self.R + other.R, self.case_of + [c + n for c in other.case_of],
+                           self.solvers + other.solvers, self.masks + other.masks)
 
 
 def harvest_residuals(n_cases: int = 24, nx: int = 256, ny: int = 128, seed: int = 0, steps: int = 3,
-                      every: int = 8, max_snaps: int = 100, rtol: float = 1e-11) -> TrainingSet:
+                      every: int = 8, max_snaps: int = 100, rtol: float = 1e-11, lx: float = 2.0,
+                      ly: float = 1.0) -> TrainingSet:
     """Residuals from the solver's own runs.
 
     For each seeded obstacle case: a few projection steps, then the pressure system
@@ -566,7 +633,7 @@ def harvest_residuals(n_cases: int = 24, nx: int = 256, ny: int = 128, seed: int
     rng = np.random.default_rng(seed)
     Rs, case_of, solvers, masks = [], [], [], []
     for ci in range(n_cases):
-        case = obstacle_case(rng, nx, ny)
+        case = obstacle_case(rng, nx, ny, lx=lx, ly=ly)
         sim = case.sim
         sim.pressure.tol = 1e-8
         sim.advance(steps)
@@ -606,7 +673,7 @@ def harvest_residuals(n_cases: int = 24, nx: int = 256, ny: int = 128, seed: int
             case_of.append(ci)
         solvers.append(ps)
         masks.append(mask)
-    return TrainingSet(t.stack(Rs), case_of, solvers, masks)
+    return TrainingSet(Rs, case_of, solvers, masks)
 
 
 def energy_loss_grad(ps, h2: float, out, r_hat):
@@ -635,9 +702,7 @@ def train(net: LPCNet, data: TrainingSet, steps: int = 1000, batch: int = 4, lr:
     for p_ in params:
         p_.requires_grad_(False)
     opt = t.optim.Adam(params, lr=lr)
-    H, W = data.R.shape[1:]
-    ws = Workspace(H, W, data.masks[0])
-    cur_mask = 0
+    wss = {}  # one workspace per grid size, with the mask of the case it last served
     gen = np.random.default_rng(seed)
     log = []
     t0 = time.time()
@@ -649,14 +714,18 @@ def train(net: LPCNet, data: TrainingSet, steps: int = 1000, batch: int = 4, lr:
         for grp in opt.param_groups:
             grp["lr"] = lr * 0.5 * (1.0 + math.cos(math.pi * min(1.0, frac)))
         idx = gen.integers(0, len(data), batch)
-        acc = {name: (t.zeros_like(net.w[name]), t.zeros_like(net.b[name])) for name, *_ in LAYERS}
+        acc = {name: (t.zeros_like(net.w[name]), t.zeros_like(net.b[name])) for name in WEIGHTS}
         loss = t.zeros((), dtype=t.float64, device=_lib.device())
         for k in idx:
             ci = data.case_of[k]
-            if ci != cur_mask:
-                ws.set_mask(data.masks[ci])
-                cur_mask = ci
             x = data.R[k].contiguous()
+            H, W = x.shape
+            if (H, W) not in wss:
+                wss[(H, W)] = [Workspace(H, W, data.masks[ci], net.arch), ci]
+            ws, cur = wss[(H, W)]
+            if cur != ci:
+                ws.set_mask(data.masks[ci])
+                wss[(H, W)][1] = ci
             if gen.random() < 0.5:
                 x = -x  # residuals of both signs: the target is odd in r
             out = net_forward(net, ws, x)
@@ -667,7 +736,7 @@ def train(net: LPCNet, data: TrainingSet, steps: int = 1000, batch: int = 4, lr:
                 acc[name][0].add_(grads[name][0])
                 acc[name][1].add_(grads[name][1])
         opt.zero_grad(set_to_none=False)
-        for name, *_ in LAYERS:
+        for name in WEIGHTS:
             net.w[name].grad = acc[name][0]
             if net.bias:
                 net.b[name].grad = acc[name][1]
@@ -676,7 +745,7 @@ def train(net: LPCNet, data: TrainingSet, steps: int = 1000, batch: int = 4, lr:
         opt.step()
         net.repack()
         log.append(float(loss))
-        if _take_net_error(ws):
+        if any(_take_net_error(w_[0]) for w_ in wss.values()):
             raise RuntimeError("a tensor-core convolution gave up waiting for its MMAs during training")
         if log_every and step % log_every == 0:
             print(f"train step {step}: loss {np.mean(log[-log_every:]):.4f}", flush=True)
@@ -698,37 +767,83 @@ def load_weights(path, net: LPCNet | None = None) -> LPCNet:
 
 
 def pretrained():
-    """The shipped network: trained on 1920 residuals of 24 seeded 256 x 128
-    obstacle flows (plain Jacobi-PCG iterates), 1500 Adam steps of batch 4 with a
-    cosine learning rate from 1e-3, by ``train`` (``python -m cfd2d_b200.learned``
-    with ``--steps 1500`` reproduces the recipe)."""
+    """The shipped network (``data/lpc_weights.npz``), trained by ``train`` on about
+    10k residuals of seeded obstacle flows from the obstacle-flow generator: 256 x 256
+    grids on a unit square and 256 x 128 grids on the benchmark's 2 x 1 channel
+    (plain Jacobi-PCG iterates); ``python -m cfd2d_b200.learned train OUT.npz``
+    reproduces the recipe (its defaults)."""
     from pathlib import Path
 
     return load_weights(Path(__file__).resolve().parent / "data" / "lpc_weights.npz")
 
 
+def harvest_recipe(cases: int = 50, snaps: int = 100, seed: int = 0, kind: str = "channel") -> TrainingSet:
+    """Training sets. "channel": ``cases`` seeded obstacle flows of the generator on the
+    2 x 1 channel at 256 x 128 and a third as many at 512 x 256 (square cells, as the
+    benchmark grids); "mixed": ``cases`` on 256 x 256 (unit square) and as many at
+    256 x 128. Up to ``snaps`` residuals of the plain solver's iterates per case."""
+    if kind == "mixed":
+        sq = harvest_residuals(n_cases=cases, nx=256, ny=256, seed=seed, every=12, max_snaps=snaps, lx=1.0, ly=1.0)
+        ch = harvest_residuals(n_cases=cases, nx=256, ny=128, seed=seed + 1000, every=8, max_snaps=snaps)
+        return sq.merge(ch)
+    small = harvest_residuals(n_cases=cases, nx=256, ny=128, seed=seed + 1000, every=8, max_snaps=snaps)
+    big = harvest_residuals(n_cases=max(1, cases // 3), nx=512, ny=256, seed=seed + 2000, every=16,
+                            max_snaps=snaps)
+    return small.merge(big)
+
+
 def main(argv=None):
-    """Harvest residuals, train, save the weights: python -m cfd2d_b200.learned OUT.npz"""
+    """python -m cfd2d_b200.learned train OUT.npz [options]: harvest residuals, train,
+    save the weights. python -m cfd2d_b200.learned apply NX NY [--reps N]: one
+    obstacle flow (generator seed 13) of NX x NY, N applications of the shipped
+    network's preconditioner, event-timed (the command the network's profiles use)."""
     import argparse
 
     ap = argparse.ArgumentParser(description=main.__doc__)
-    ap.add_argument("out")
-    ap.add_argument("--cases", type=int, default=24)
-    ap.add_argument("--nx", type=int, default=256)
-    ap.add_argument("--ny", type=int, default=128)
-    ap.add_argument("--seconds", type=float, default=0.0, help="time budget (0: none)")
-    ap.add_argument("--steps", type=int, default=1500)
-    ap.add_argument("--batch", type=int, default=4)
-    ap.add_argument("--lr", type=float, default=1e-3)
-    ap.add_argument("--seed", type=int, default=0)
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    tr = sub.add_parser("train")
+    tr.add_argument("out")
+    tr.add_argument("--cases", type=int, default=50)
+    tr.add_argument("--snaps", type=int, default=100)
+    tr.add_argument("--seconds", type=float, default=0.0, help="time budget (0: none)")
+    tr.add_argument("--steps", type=int, default=6000)
+    tr.add_argument("--batch", type=int, default=4)
+    tr.add_argument("--lr", type=float, default=1e-3)
+    tr.add_argument("--seed", type=int, default=0)
+    tr.add_argument("--recipe", choices=["channel", "mixed"], default="channel")
+    apl = sub.add_parser("apply")
+    apl.add_argument("nx", type=int)
+    apl.add_argument("ny", type=int)
+    apl.add_argument("--reps", type=int, default=5)
     a = ap.parse_args(argv)
-    data = harvest_residuals(n_cases=a.cases, nx=a.nx, ny=a.ny, seed=a.seed, every=8, max_snaps=80)
-    print(f"residuals {tuple(data.R.shape)}", flush=True)
-    net = LPCNet(seed=a.seed)
-    log = train(net, data, steps=a.steps, batch=a.batch, lr=a.lr, seed=a.seed, log_every=200,
-                time_budget_s=a.seconds or None)
-    print(f"steps {len(log)} loss first {np.mean(log[:50]):.4f} last {np.mean(log[-50:]):.4f}", flush=True)
-    save_weights(net, a.out)
+    if a.cmd == "train":
+        t0 = time.time()
+        data = harvest_recipe(cases=a.cases, snaps=a.snaps, seed=a.seed, kind=a.recipe)
+        print(f"residuals {len(data)} from {len(data.solvers)} cases in {time.time() - t0:.0f}s", flush=True)
+        net = LPCNet(seed=a.seed)
+        log = train(net, data, steps=a.steps, batch=a.batch, lr=a.lr, seed=a.seed, log_every=500,
+                    time_budget_s=a.seconds or None)
+        print(f"steps {len(log)} loss first {np.mean(log[:50]):.4f} last {np.mean(log[-50:]):.4f}", flush=True)
+        save_weights(net, a.out)
+        return
+    from . import cases
+
+    t = _t()
+    case = cases.obstacle_flow(13, a.nx, a.ny, pressure_solver="cg")
+    sim = case.sim
+    sim.advance(1)
+    fcg = LearnedPCG(sim.pressure, pretrained())
+    fcg.r.copy_(t.randn_like(fcg.r))
+    ev = [t.cuda.Event(enable_timing=True) for _ in range(2)]
+    fcg.precondition()
+    t.cuda.synchronize()
+    ev[0].record()
+    for _ in range(a.reps):
+        fcg.precondition()
+    ev[1].record()
+    t.cuda.synchronize()
+    print(json.dumps({"grid": [a.nx, a.ny], "levels": fcg.ws.L, "ms_per_application": ev[0].elapsed_time(ev[1]) / a.reps}))
+    fcg.close()
 
 
 if __name__ == "__main__":

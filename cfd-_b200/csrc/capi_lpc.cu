@@ -51,9 +51,9 @@ int cfd2d_lpc_pool_mask(const uint8_t* m, uint8_t* mc, int H, int W, void* strea
     return status_of(lpc::pool_mask(m, mc, H, W, as_stream(stream)));
 }
 
-int cfd2d_lpc_upadd(const void* coarse, const void* skip, void* y, int H, int W, void* stream) {
+int cfd2d_lpc_upadd(const void* coarse, const void* skip, void* y, int H, int W, float scale, void* stream) {
     if (!coarse || !skip || !y || !hw_ok(H, W)) return CFD2D_E_ARG;
-    return status_of(lpc::upadd(bf(coarse), bf(skip), bfw(y), H, W, as_stream(stream)));
+    return status_of(lpc::upadd(bf(coarse), bf(skip), bfw(y), H, W, scale, as_stream(stream)));
 }
 
 int cfd2d_lpc_relu_bwd(const float* dy, const void* y, const uint8_t* mask, float* g, int npix, int ch,
@@ -62,9 +62,9 @@ int cfd2d_lpc_relu_bwd(const float* dy, const void* y, const uint8_t* mask, floa
     return status_of(lpc::relu_bwd(dy, bf(y), mask, g, npix, ch, relu, as_stream(stream)));
 }
 
-int cfd2d_lpc_upadd_bwd(const float* dy, float* dcoarse, int H, int W, void* stream) {
+int cfd2d_lpc_upadd_bwd(const float* dy, float* dcoarse, int H, int W, float scale, void* stream) {
     if (!dy || !dcoarse || !hw_ok(H, W)) return CFD2D_E_ARG;
-    return status_of(lpc::upadd_bwd(dy, dcoarse, H, W, as_stream(stream)));
+    return status_of(lpc::upadd_bwd(dy, dcoarse, H, W, scale, as_stream(stream)));
 }
 
 int cfd2d_lpc_pool_bwd(const float* dcoarse, float* dfine, int H, int W, void* stream) {

@@ -494,7 +494,7 @@ __global__ void k_pool2(const __nv_bfloat16* __restrict__ x, __nv_bfloat16* __re
 
 // y[p] = coarse[parent(p)] + skip[p]; one thread per 8 channels of a pixel
 __global__ void k_upadd(const __nv_bfloat16* __restrict__ coarse, const __nv_bfloat16* __restrict__ skip,
-                        __nv_bfloat16* __restrict__ y, int H, int W) {
+                        __nv_bfloat16* __restrict__ y, int H, int W, float scale) {
     const int Wc = (W + 1) / 2;
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= H * W * (CH / 8)) return;
@@ -506,7 +506,7 @@ __global__ void k_upadd(const __nv_bfloat16* __restrict__ coarse, const __nv_bfl
     const __nv_bfloat16* sh = reinterpret_cast<const __nv_bfloat16*>(&sv);
     __align__(16) __nv_bfloat16 out[8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) out[k] = __float2bfloat16(bf2f(ch[k]) + bf2f(sh[k]));
+    for (int k = 0; k < 8; ++k) out[k] = __float2bfloat16(scale * bf2f(ch[k]) + bf2f(sh[k]));
     reinterpret_cast<uint4*>(y)[e] = *reinterpret_cast<const uint4*>(out);
 }
 
@@ -540,7 +540,7 @@ __global__ void k_relu_bwd(const float* __restrict__ dy, const __nv_bfloat16* __
 }
 
 // dcoarse[q] = sum over children of dfine[p]  (upsample backward), dfine given FP32
-__global__ void k_upadd_bwd(const float* __restrict__ dy, float* __restrict__ dcoarse, int H, int W) {
+__global__ void k_upadd_bwd(const float* __restrict__ dy, float* __restrict__ dcoarse, int H, int W, float scale) {
     const int Hc = (H + 1) / 2, Wc = (W + 1) / 2;
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= Hc * Wc * CH) return;
@@ -552,7 +552,7 @@ __global__ void k_upadd_bwd(const float* __restrict__ dy, float* __restrict__ dc
             const int i = 2 * ic + a, j = 2 * jc + b;
             if (i < H && j < W) s += dy[((size_t)i * W + j) * CH + c];
         }
-    dcoarse[e] = s;
+    dcoarse[e] = scale * s;
 }
 
 // dfine[p] += dcoarse[parent(p)] / n_children(parent)   (pool backward, accumulating)
@@ -685,9 +685,9 @@ cudaError_t pool_mask(const uint8_t* m, uint8_t* mc, int H, int W, cudaStream_t 
     return cudaGetLastError();
 }
 
-cudaError_t upadd(const __nv_bfloat16* coarse, const __nv_bfloat16* skip, __nv_bfloat16* y, int H, int W,
+cudaError_t upadd(const __nv_bfloat16* coarse, const __nv_bfloat16* skip, __nv_bfloat16* y, int H, int W, float scale,
                   cudaStream_t s) {
-    k_upadd<<<cdiv((long long)H * W * (CH / 8), 256), 256, 0, s>>>(coarse, skip, y, H, W);
+    k_upadd<<<cdiv((long long)H * W * (CH / 8), 256), 256, 0, s>>>(coarse, skip, y, H, W, scale);
     return cudaGetLastError();
 }
 
@@ -697,9 +697,9 @@ cudaError_t relu_bwd(const float* dy, const __nv_bfloat16* y, const uint8_t* mas
     return cudaGetLastError();
 }
 
-cudaError_t upadd_bwd(const float* dy, float* dcoarse, int H, int W, cudaStream_t s) {
+cudaError_t upadd_bwd(const float* dy, float* dcoarse, int H, int W, float scale, cudaStream_t s) {
     const int n = ((H + 1) / 2) * ((W + 1) / 2) * CH;
-    k_upadd_bwd<<<cdiv(n, 256), 256, 0, s>>>(dy, dcoarse, H, W);
+    k_upadd_bwd<<<cdiv(n, 256), 256, 0, s>>>(dy, dcoarse, H, W, scale);
     return cudaGetLastError();
 }
 

@@ -20,11 +20,11 @@ cudaError_t conv_generic(int cin, int cout, const void* x, int xbf, const float*
                          cudaStream_t s);
 cudaError_t pool2(const __nv_bfloat16* x, __nv_bfloat16* y, int H, int W, cudaStream_t s);
 cudaError_t pool_mask(const uint8_t* m, uint8_t* mc, int H, int W, cudaStream_t s);
-cudaError_t upadd(const __nv_bfloat16* coarse, const __nv_bfloat16* skip, __nv_bfloat16* y, int H, int W,
+cudaError_t upadd(const __nv_bfloat16* coarse, const __nv_bfloat16* skip, __nv_bfloat16* y, int H, int W, float scale,
                   cudaStream_t s);
 cudaError_t relu_bwd(const float* dy, const __nv_bfloat16* y, const uint8_t* mask, float* g, int npix, int ch,
                      int relu, cudaStream_t s);
-cudaError_t upadd_bwd(const float* dy, float* dcoarse, int H, int W, cudaStream_t s);
+cudaError_t upadd_bwd(const float* dy, float* dcoarse, int H, int W, float scale, cudaStream_t s);
 cudaError_t pool_bwd(const float* dcoarse, float* dfine, int H, int W, cudaStream_t s);
 size_t conv_dw_partial_floats(int cin, int cout, int H, int W, int pix_per_block);
 cudaError_t conv_dw(int cin, int cout, const void* x, int xbf, const float* g, int H, int W, int pix_per_block,

@@ -477,10 +477,12 @@ int cfd2d_lpc_conv(int cin, int cout, const void* x, int x_bf16, const float* w,
                    void* stream);
 int cfd2d_lpc_pool2(const void* x, void* y, int H, int W, void* stream);
 int cfd2d_lpc_pool_mask(const uint8_t* m, uint8_t* mc, int H, int W, void* stream);
-int cfd2d_lpc_upadd(const void* coarse, const void* skip, void* y, int H, int W, void* stream);
+/* y = scale * upsample(coarse) + skip (nearest, (H+1)/2 x (W+1)/2 -> H x W, 32 channels,
+ * BF16); the backward pass writes dcoarse = scale * (sum of the children of dy). */
+int cfd2d_lpc_upadd(const void* coarse, const void* skip, void* y, int H, int W, float scale, void* stream);
 int cfd2d_lpc_relu_bwd(const float* dy, const void* y, const uint8_t* mask, float* g, int npix, int ch,
                        int relu, void* stream);
-int cfd2d_lpc_upadd_bwd(const float* dy, float* dcoarse, int H, int W, void* stream);
+int cfd2d_lpc_upadd_bwd(const float* dy, float* dcoarse, int H, int W, float scale, void* stream);
 int cfd2d_lpc_pool_bwd(const float* dcoarse, float* dfine, int H, int W, void* stream);
 size_t cfd2d_lpc_conv_dw_partial_floats(int cin, int cout, int H, int W, int pix_per_block);
 /* weight and bias gradient: out = [dw (cout*cin*9), db (cout)] */
