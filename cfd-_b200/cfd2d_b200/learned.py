@@ -599,8 +599,9 @@ class TrainingSet:
     any size), the case each one belongs to, and per case the pressure operator (for
     Ah o in the loss), its h^2 and its fluid mask."""
 
-    def __init__(self, R, case_of, solvers, masks):
+    def __init__(self, R, case_of, solvers, masks, rhs=None):
         self.R, self.case_of, self.solvers, self.masks = list(R), list(case_of), list(solvers), list(masks)
+        self.rhs = list(rhs) if rhs is not None else [None] * len(self.solvers)
         self.h2 = [h2_of(ps) for ps in solvers]
 
     def __len__(self):
@@ -610,7 +611,11 @@ class TrainingSet:
         """The samples of both sets (case indices of ``other`` shifted after this one's)."""
         n = len(self.solvers)
         return TrainingSet(self.R + other.R, self.case_of + [c + n for c in other.case_of],
-                           self.solvers + other.solvers, self.masks + other.masks)
+                           self.solvers + other.solvers, self.masks + other.masks, self.rhs + other.rhs)
+
+    def with_samples(self, R, case_of) -> "TrainingSet":
+        """This set plus more residuals of its own cases."""
+        return TrainingSet(self.R + list(R), self.case_of + list(case_of), self.solvers, self.masks, self.rhs)
 
 
 def harvest_residuals(n_cases: int = 24, nx: int = 256, ny: int = 128, seed: int = 0, steps: int = 3,
@@ -631,7 +636,7 @@ def harvest_residuals(n_cases: int = 24, nx: int = 256, ny: int = 128, seed: int
     t = _t()
     L = _lib.lib()
     rng = np.random.default_rng(seed)
-    Rs, case_of, solvers, masks = [], [], [], []
+    Rs, case_of, solvers, masks, rhss = [], [], [], [], []
     for ci in range(n_cases):
         case = obstacle_case(rng, nx, ny, lx=lx, ly=ly)
         sim = case.sim
@@ -673,7 +678,42 @@ def harvest_residuals(n_cases: int = 24, nx: int = 256, ny: int = 128, seed: int
             case_of.append(ci)
         solvers.append(ps)
         masks.append(mask)
-    return TrainingSet(Rs, case_of, solvers, masks)
+        rhss.append(rd)
+    return TrainingSet(Rs, case_of, solvers, masks, rhss)
+
+
+def harvest_fcg_residuals(net: LPCNet, data: TrainingSet, iters: int = 300, every: int = 10,
+                          tol: float = 1e-10):
+    """Residuals the flexible CG with ``net`` meets on the cases of ``data`` (each
+    case's pressure system from zero, ``iters`` iterations at most, one residual every
+    ``every``): the residuals the preconditioner handles worst are the ones that
+    survive its own iterations, and the plain solver's iterates do not contain them.
+    Returns (residuals, case indices) to add to ``data``."""
+    t = _t()
+    Rs, case_of = [], []
+    for ci, ps in enumerate(data.solvers):
+        rhs = data.rhs[ci]
+        if rhs is None:
+            continue
+        fcg = LearnedPCG(ps, net, maxiter=iters + 1, stall_window=iters + 1)
+        nx, ny = fcg.nx, fcg.ny
+        fcg.rhs_buf.copy_(rhs.reshape(-1))
+        ps._d_x0.zero_()
+        fcg._set_control(tol)
+        fcg._init(rhs=fcg.rhs_buf)
+        _lib.check(_lib.lib().cfd2d_fcg_gate(_lib.ptr(fcg.scal), _lib.ptr(fcg.ctl), 0, _lib.stream_ptr()), "gate")
+        for it in range(iters):
+            fcg._body(0)
+            if (it + 1) % every == 0:
+                if fcg._control().reason != _lib.FCG_RUNNING:
+                    break
+                r = fcg.r.view(nx, ny) * fcg.mask
+                rn = float(t.linalg.vector_norm(r))
+                if rn > 0.0 and math.isfinite(rn):
+                    Rs.append((r / rn).float().contiguous())
+                    case_of.append(ci)
+        fcg.close()
+    return Rs, case_of
 
 
 def energy_loss_grad(ps, h2: float, out, r_hat):
@@ -767,11 +807,13 @@ def load_weights(path, net: LPCNet | None = None) -> LPCNet:
 
 
 def pretrained():
-    """The shipped network (``data/lpc_weights.npz``), trained by ``train`` on about
-    10k residuals of seeded obstacle flows from the obstacle-flow generator: 256 x 256
-    grids on a unit square and 256 x 128 grids on the benchmark's 2 x 1 channel
-    (plain Jacobi-PCG iterates); ``python -m cfd2d_b200.learned train OUT.npz``
-    reproduces the recipe (its defaults)."""
+    """The shipped network (``data/lpc_weights.npz``), trained by ``train`` on the
+    "channel" recipe: residuals of the plain Jacobi-PCG's iterates on 60 seeded
+    obstacle flows of the generator at 256 x 128 and 20 at 512 x 256 (the benchmark's
+    2 x 1 channel, square cells), 6000 Adam steps; then one on-policy round: the
+    residuals the flexible CG with the trained network meets on the same cases are
+    added (about 2.4k) and training goes on for 3000 steps at half the learning rate.
+    ``python -m cfd2d_b200.learned train OUT.npz`` reproduces it (its defaults)."""
     from pathlib import Path
 
     return load_weights(Path(__file__).resolve().parent / "data" / "lpc_weights.npz")
@@ -811,6 +853,8 @@ def main(argv=None):
     tr.add_argument("--lr", type=float, default=1e-3)
     tr.add_argument("--seed", type=int, default=0)
     tr.add_argument("--recipe", choices=["channel", "mixed"], default="channel")
+    tr.add_argument("--onpolicy", type=int, default=1,
+                    help="rounds of adding the flexible CG's own residuals and training on")
     apl = sub.add_parser("apply")
     apl.add_argument("nx", type=int)
     apl.add_argument("ny", type=int)
@@ -824,6 +868,13 @@ def main(argv=None):
         log = train(net, data, steps=a.steps, batch=a.batch, lr=a.lr, seed=a.seed, log_every=500,
                     time_budget_s=a.seconds or None)
         print(f"steps {len(log)} loss first {np.mean(log[:50]):.4f} last {np.mean(log[-50:]):.4f}", flush=True)
+        for rnd in range(a.onpolicy):
+            R, co = harvest_fcg_residuals(net, data)
+            data = data.with_samples(R, co)
+            print(f"round {rnd + 1}: {len(R)} residuals of the flexible CG added ({len(data)} in all)", flush=True)
+            log = train(net, data, steps=a.steps // 2, batch=a.batch, lr=a.lr / 2, seed=a.seed + rnd + 1,
+                        log_every=500)
+            print(f"steps {len(log)} loss last {np.mean(log[-50:]):.4f}", flush=True)
         save_weights(net, a.out)
         return
     from . import cases
