@@ -220,7 +220,6 @@ def lib():
         "cfd2d_lpc_pack_w32": ([vp, vp, vp], i),
         "cfd2d_lpc_conv32": ([vp, vp, vp, vp, vp, vp, i, i, i, vp, vp], i),
         "cfd2d_lpc_conv": ([i, i, vp, i, vp, vp, vp, vp, i, i, i, i, i, vp], i),
-        "cfd2d_lpc_conv32_fused": ([i, vp, i, i, vp, C.c_float, vp, vp, vp, vp, vp, i, i, i, vp, vp], i),
         "cfd2d_lpc_pool2": ([vp, vp, i, i, vp], i),
         "cfd2d_lpc_pool_mask": ([vp, vp, i, i, vp], i),
         "cfd2d_lpc_upadd": ([vp, vp, vp, i, i, C.c_float, vp], i),
@@ -269,7 +268,7 @@ def exported_symbols():
         "cfd2d_graph_capture_steps_ex", "cfd2d_events_create", "cfd2d_events_destroy",
         "cfd2d_event_elapsed_ms", "cfd2d_sim_step_begin", "cfd2d_sim_step_finish", "cfd2d_poisson_matvec",
         "cfd2d_pressure_solve_snapshots", "cfd2d_lpc_w32_bytes", "cfd2d_lpc_pack_w32", "cfd2d_lpc_conv32",
-        "cfd2d_lpc_conv", "cfd2d_lpc_conv32_fused", "cfd2d_lpc_pool2", "cfd2d_lpc_pool_mask", "cfd2d_lpc_upadd", "cfd2d_lpc_relu_bwd",
+        "cfd2d_lpc_conv", "cfd2d_lpc_pool2", "cfd2d_lpc_pool_mask", "cfd2d_lpc_upadd", "cfd2d_lpc_relu_bwd",
         "cfd2d_lpc_upadd_bwd", "cfd2d_lpc_pool_bwd", "cfd2d_lpc_conv_dw_partial_floats", "cfd2d_lpc_conv_dw",
         "cfd2d_fcg_partial_doubles", "cfd2d_fcg_init", "cfd2d_fcg_pq", "cfd2d_fcg_update", "cfd2d_fcg_zr",
         "cfd2d_fcg_dir", "cfd2d_fcg_net_in", "cfd2d_fcg_net_out", "cfd2d_fcg_scatter_p",

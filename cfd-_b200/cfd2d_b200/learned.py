@@ -236,41 +236,15 @@ class Workspace:
         self.mask_src = mask
 
 
-def net_forward(net: LPCNet, ws: Workspace, x_in, keep: bool = True):
-    """out = net(x_in) on the device (x_in: FP32 (H, W)); activations stay in ``ws``.
-    Every pooling and every upsample-add feeds a 32->32 layer, which forms that input
-    itself while staging its rows (``cfd2d_lpc_conv32_fused``: one launch instead of
-    two, the same bits); ``keep`` also writes the formed inputs to their buffers, which
-    the backward pass reads (inference passes False)."""
+def net_forward(net: LPCNet, ws: Workspace, x_in):
+    """out = net(x_in) on the device (x_in: FP32 (H, W)); activations stay in ``ws``."""
     L = _lib.lib()
     s = _lib.stream_ptr()
     P = _lib.ptr
     sh = ws.shapes
     relu = net.relu
     scale = float(net.arch["scale"])
-    ops = ws.ops
-    k = 0
-    while k < len(ops):
-        op = ops[k]
-        nxt = ops[k + 1] if k + 1 < len(ops) else None
-        if op[0] in ("pool", "upadd") and nxt is not None and nxt[0] == "conv" and nxt[3] == op[-1] \
-                and WEIGHTS[nxt[1]] == (CH, CH):
-            _, name, lvl, _src, dst = nxt
-            h, w = sh[lvl]
-            staged = P(ws.buf[op[-1]]) if keep else None
-            if op[0] == "pool":
-                hs, wsz = sh[lvl - 1]
-                rc = L.cfd2d_lpc_conv32_fused(1, P(ws.buf[op[2]]), hs, wsz, None, 1.0, staged, P(net._images[name]),
-                                              P(net.b[name]), P(ws.masks[lvl]), P(ws.buf[dst]), h, w, relu,
-                                              P(ws.err), s)
-            else:
-                hs, wsz = sh[lvl + 1]
-                rc = L.cfd2d_lpc_conv32_fused(2, P(ws.buf[op[2]]), hs, wsz, P(ws.buf[op[3]]), scale, staged,
-                                              P(net._images[name]), P(net.b[name]), P(ws.masks[lvl]),
-                                              P(ws.buf[dst]), h, w, relu, P(ws.err), s)
-            _lib.check(rc, "lpc_conv32_fused")
-            k += 2
-            continue
+    for op in ws.ops:
         if op[0] == "conv":
             _, name, lvl, src, dst = op
             h, w = sh[lvl]
@@ -294,7 +268,6 @@ def net_forward(net: LPCNet, ws: Workspace, x_in, keep: bool = True):
             h, w = sh[lvl]
             _lib.check(L.cfd2d_lpc_upadd(P(ws.buf[coarse]), P(ws.buf[skip]), P(ws.buf[dst]), h, w, scale, s),
                        "upadd")
-        k += 1
     return ws.out
 
 
@@ -473,7 +446,7 @@ class LearnedPCG:
         P = _lib.ptr
         n = self.nx * self.ny
         _lib.check(L.cfd2d_fcg_net_in(n, P(self.r), P(self.scal), P(self.mask_u8), P(self.net_in), s), "net_in")
-        out = net_forward(self.net, self.ws, self.net_in, keep=False)
+        out = net_forward(self.net, self.ws, self.net_in)
         _lib.check(L.cfd2d_fcg_net_out(n, P(out), P(self.r), P(self.ps._d_dinv), P(self.mask_u8), P(self.scal),
                                        self.h2, self.omega, P(self.z), s), "net_out")
 

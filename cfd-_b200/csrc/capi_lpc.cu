@@ -32,15 +32,6 @@ int cfd2d_lpc_conv32(const void* x, const void* image, const float* bias, const 
                                     reinterpret_cast<int*>(err), as_stream(stream)));
 }
 
-int cfd2d_lpc_conv32_fused(int in_mode, const void* x, int Hs, int Ws, const void* src2, float scale,
-                           void* staged_out, const void* image, const float* bias, const uint8_t* mask, void* y,
-                           int H, int W, int relu, int* err, void* stream) {
-    if (!x || !image || !bias || !y || !hw_ok(H, W) || !hw_ok(Hs, Ws) || (in_mode != 1 && in_mode != 2))
-        return CFD2D_E_ARG;
-    return status_of(lpc::conv32_tc_fused(in_mode, bf(x), Hs, Ws, bf(src2), scale, bfw(staged_out), bf(image), bias,
-                                          mask, bfw(y), H, W, relu, err, as_stream(stream)));
-}
-
 int cfd2d_lpc_conv(int cin, int cout, const void* x, int x_bf16, const float* w, const float* bias,
                    const uint8_t* mask, void* y, int y_bf16, int H, int W, int relu, int transposed,
                    void* stream) {

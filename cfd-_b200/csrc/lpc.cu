@@ -88,23 +88,14 @@ constexpr int NT = 256;
 constexpr int ST_BYTES = TM * 5 * 16;      // epilogue staging of one row: 128 pixels x 80 bytes
 __host__ __device__ constexpr int x_bytes(int rows) { return (rows + 2) * XROW; }
 
-// The staged input can be formed on the fly (IN): 0 = x itself (H x W); 1 = the 2x2
-// mean of x over the in-range children (x is the finer level, Hs x Ws: what k_pool2
-// writes); 2 = scale * x (the coarser level, Hs x Ws, nearest upsampling) + src2 (this
-// level): what k_upadd writes. Each staged chunk is rounded to BF16 exactly as those
-// kernels round their outputs, so the result is the same as pooling or upsampling
-// first. With staged_out non-null the CTA also writes the staged values of its own
-// rows and pixels there (the input the backward pass needs).
-template <int ROWS, int IN>
+template <int ROWS>
 __global__ void __launch_bounds__(NT) k_conv32_tc(const __nv_bfloat16* __restrict__ x,
                                                   const uint4* __restrict__ wpack,
                                                   const float* __restrict__ bias,
                                                   const __nv_bfloat16* __restrict__ skip,
                                                   const uint8_t* __restrict__ mask,
                                                   __nv_bfloat16* __restrict__ y, int H, int W,
-                                                  int relu, int* __restrict__ err,
-                                                  const __nv_bfloat16* __restrict__ src2, int Hs, int Ws,
-                                                  float scale, __nv_bfloat16* __restrict__ staged_out) {
+                                                  int relu, int* __restrict__ err) {
     constexpr int XQ = (ROWS + 2) * XP * 4;    // 16-byte chunks staged per CTA
     constexpr int XPER = (XQ + NT - 1) / NT;   // per thread
     constexpr int BQ = B_BYTES / 16, BPER = (BQ + NT - 1) / NT;
@@ -144,63 +135,26 @@ __global__ void __launch_bounds__(NT) k_conv32_tc(const __nv_bfloat16* __restric
     // staged input rows: consecutive threads take consecutive 16-byte chunks in global
     // order (chunk fastest, then pixel), so each warp reads 512 contiguous bytes; the
     // loads go out in batches of XB per thread before their shared-memory stores
-    // pooling reads four children per chunk: fewer chunks per batch keep it in registers
-    constexpr int XBI = IN == 1 ? 6 : XB;
 #pragma unroll
-    for (int k0 = 0; k0 < XPER; k0 += XBI) {
-        uint4 v[XBI];
+    for (int k0 = 0; k0 < XPER; k0 += XB) {
+        uint4 v[XB];
 #pragma unroll
-        for (int k = 0; k < XBI; ++k) {
+        for (int k = 0; k < XB; ++k) {
             const int q = tid + (k0 + k) * NT;
             const int c = q & 3, t = q >> 2;
             const int r = t / XP, px = t - r * XP;
             const int ii = i0 - 1 + r, jj = j0 - 1 + px;
             v[k] = make_uint4(0u, 0u, 0u, 0u);
-            if (k0 + k < XPER && q < XQ && ii >= 0 && ii < H && jj >= 0 && jj < W) {
-                if constexpr (IN == 0) {
-                    v[k] = reinterpret_cast<const uint4*>(x + ((size_t)ii * W + jj) * CH)[c];
-                } else if constexpr (IN == 1) {
-                    float acc8[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-                    int nch = 0;
-                    for (int a = 0; a < 2; ++a)
-                        for (int b2 = 0; b2 < 2; ++b2) {
-                            const int fi = 2 * ii + a, fj = 2 * jj + b2;
-                            if (fi < Hs && fj < Ws) {
-                                const uint4 cv = reinterpret_cast<const uint4*>(x + ((size_t)fi * Ws + fj) * CH)[c];
-                                const __nv_bfloat16* h = reinterpret_cast<const __nv_bfloat16*>(&cv);
-#pragma unroll
-                                for (int e = 0; e < 8; ++e) acc8[e] += bf2f(h[e]);
-                                ++nch;
-                            }
-                        }
-                    __align__(16) __nv_bfloat16 o8[8];
-#pragma unroll
-                    for (int e = 0; e < 8; ++e) o8[e] = __float2bfloat16(acc8[e] / (float)nch);
-                    v[k] = *reinterpret_cast<const uint4*>(o8);
-                } else {
-                    const uint4 cv = reinterpret_cast<const uint4*>(x + ((size_t)(ii / 2) * Ws + jj / 2) * CH)[c];
-                    const uint4 sv = reinterpret_cast<const uint4*>(src2 + ((size_t)ii * W + jj) * CH)[c];
-                    const __nv_bfloat16* ch = reinterpret_cast<const __nv_bfloat16*>(&cv);
-                    const __nv_bfloat16* sh = reinterpret_cast<const __nv_bfloat16*>(&sv);
-                    __align__(16) __nv_bfloat16 o8[8];
-#pragma unroll
-                    for (int e = 0; e < 8; ++e) o8[e] = __float2bfloat16(scale * bf2f(ch[e]) + bf2f(sh[e]));
-                    v[k] = *reinterpret_cast<const uint4*>(o8);
-                }
-            }
+            if (k0 + k < XPER && q < XQ && ii >= 0 && ii < H && jj >= 0 && jj < W)
+                v[k] = reinterpret_cast<const uint4*>(x + ((size_t)ii * W + jj) * CH)[c];
         }
 #pragma unroll
-        for (int k = 0; k < XBI; ++k) {
+        for (int k = 0; k < XB; ++k) {
             const int q = tid + (k0 + k) * NT;
             if (k0 + k < XPER && q < XQ) {
                 const int c = q & 3, t = q >> 2;
                 const int r = t / XP, px = t - r * XP;
                 *reinterpret_cast<uint4*>(Xs + r * XROW + c * XCHUNK + px * 16) = v[k];
-                if constexpr (IN != 0) {
-                    const int ii = i0 - 1 + r, jj = j0 - 1 + px;
-                    if (staged_out && r >= 1 && r <= ROWS && px >= 1 && px <= TM && ii < H && jj < W)
-                        reinterpret_cast<uint4*>(staged_out + ((size_t)ii * W + jj) * CH)[c] = v[k];
-                }
             }
         }
     }
@@ -659,66 +613,33 @@ inline int cdiv(long long a, int b) { return (int)((a + b - 1) / b); }
 
 size_t conv32_smem_bytes(int rows) { return (size_t)B_BYTES + x_bytes(rows); }
 
-constexpr int kMaxDev = 64;
-
-template <int ROWS, int IN>
+template <int ROWS>
 static cudaError_t conv32_launch(const __nv_bfloat16* x, const __nv_bfloat16* wpack, const float* bias,
                                  const __nv_bfloat16* skip, const uint8_t* mask, __nv_bfloat16* y, int H, int W,
-                                 int relu, int* err, const __nv_bfloat16* src2, int Hs, int Ws, float scale,
-                                 __nv_bfloat16* staged_out, cudaStream_t s) {
-    // the shared-memory opt-in is a per-device attribute of the kernel
-    static bool configured[kMaxDev];
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= kMaxDev) return cudaErrorInvalidDevice;
-    if (!configured[dev]) {
-        e = cudaFuncSetAttribute(k_conv32_tc<ROWS, IN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)conv32_smem_bytes(ROWS));
+                                 int relu, int* err, cudaStream_t s) {
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(k_conv32_tc<ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)conv32_smem_bytes(ROWS));
         if (e != cudaSuccess) return e;
-        configured[dev] = true;
+        configured = true;
     }
     dim3 grid(cdiv(W, TM), cdiv(H, ROWS));
-    k_conv32_tc<ROWS, IN><<<grid, NT, conv32_smem_bytes(ROWS), s>>>(
-        x, reinterpret_cast<const uint4*>(wpack), bias, skip, mask, y, H, W, relu, err, src2, Hs, Ws, scale,
-        staged_out);
+    k_conv32_tc<ROWS><<<grid, NT, conv32_smem_bytes(ROWS), s>>>(x, reinterpret_cast<const uint4*>(wpack), bias,
+                                                                 skip, mask, y, H, W, relu, err);
     return cudaGetLastError();
 }
 
-template <int IN>
-static cudaError_t conv32_rows(const __nv_bfloat16* x, const __nv_bfloat16* wpack, const float* bias,
-                               const __nv_bfloat16* skip, const uint8_t* mask, __nv_bfloat16* y, int H, int W,
-                               int relu, int* err, const __nv_bfloat16* src2, int Hs, int Ws, float scale,
-                               __nv_bfloat16* staged_out, cudaStream_t s) {
-    // Rows per CTA: two where that still leaves about six CTAs per SM (two waves at the
-    // four CTAs of 52 KB that fit), else one, so that the small levels of the network
-    // spread over the SMs. (Four rows per CTA halve the halo reads but fit only three
-    // CTAs per SM and measured slower: 36.4 against 32.5 us at 1024 x 512.)
-    const long long segs = cdiv(W, TM);
-    if (segs * cdiv(H, 2) >= 6 * 148)
-        return conv32_launch<2, IN>(x, wpack, bias, skip, mask, y, H, W, relu, err, src2, Hs, Ws, scale, staged_out,
-                                    s);
-    return conv32_launch<1, IN>(x, wpack, bias, skip, mask, y, H, W, relu, err, src2, Hs, Ws, scale, staged_out, s);
-}
-
+// Rows per CTA: two where that still leaves about six CTAs per SM (two waves at the
+// four CTAs of 52 KB that fit), else one, so that the small levels of the network
+// spread over the SMs. (Four rows per CTA halve the halo reads but fit only three CTAs
+// per SM and measured slower: 36.4 against 32.5 us at 1024 x 512.)
 cudaError_t conv32_tc(const __nv_bfloat16* x, const __nv_bfloat16* wpack, const float* bias,
                       const __nv_bfloat16* skip, const uint8_t* mask, __nv_bfloat16* y, int H, int W, int relu,
                       int* err, cudaStream_t s) {
-    return conv32_rows<0>(x, wpack, bias, skip, mask, y, H, W, relu, err, nullptr, H, W, 1.0f, nullptr, s);
-}
-
-cudaError_t conv32_tc_fused(int in_mode, const __nv_bfloat16* x, int Hs, int Ws, const __nv_bfloat16* src2,
-                            float scale, __nv_bfloat16* staged_out, const __nv_bfloat16* wpack, const float* bias,
-                            const uint8_t* mask, __nv_bfloat16* y, int H, int W, int relu, int* err, cudaStream_t s) {
-    if (in_mode == 1) {
-        if ((Hs + 1) / 2 != H || (Ws + 1) / 2 != W) return cudaErrorInvalidValue;
-        return conv32_rows<1>(x, wpack, bias, nullptr, mask, y, H, W, relu, err, nullptr, Hs, Ws, scale, staged_out, s);
-    }
-    if (in_mode == 2) {
-        if ((H + 1) / 2 != Hs || (W + 1) / 2 != Ws || !src2) return cudaErrorInvalidValue;
-        return conv32_rows<2>(x, wpack, bias, nullptr, mask, y, H, W, relu, err, src2, Hs, Ws, scale, staged_out, s);
-    }
-    return cudaErrorInvalidValue;
+    const long long segs = cdiv(W, TM);
+    if (segs * cdiv(H, 2) >= 6 * 148) return conv32_launch<2>(x, wpack, bias, skip, mask, y, H, W, relu, err, s);
+    return conv32_launch<1>(x, wpack, bias, skip, mask, y, H, W, relu, err, s);
 }
 
 cudaError_t pack_w32(const float* w, __nv_bfloat16* img, cudaStream_t s) {

@@ -14,12 +14,6 @@ size_t conv32_smem_bytes(int rows);
 cudaError_t conv32_tc(const __nv_bfloat16* x, const __nv_bfloat16* wpack, const float* bias,
                       const __nv_bfloat16* skip, const uint8_t* mask, __nv_bfloat16* y, int H, int W, int relu,
                       int* err, cudaStream_t s);
-// The same convolution with its input formed on the fly: in_mode 1 = 2x2 mean of x
-// (Hs x Ws, the finer level), in_mode 2 = scale * upsampled x (Hs x Ws, the coarser
-// level) + src2; staged_out (nullable) receives that input for the own rows.
-cudaError_t conv32_tc_fused(int in_mode, const __nv_bfloat16* x, int Hs, int Ws, const __nv_bfloat16* src2,
-                            float scale, __nv_bfloat16* staged_out, const __nv_bfloat16* wpack, const float* bias,
-                            const uint8_t* mask, __nv_bfloat16* y, int H, int W, int relu, int* err, cudaStream_t s);
 cudaError_t pack_w32(const float* w, __nv_bfloat16* img, cudaStream_t s);
 cudaError_t conv_generic(int cin, int cout, const void* x, int xbf, const float* w, const float* bias,
                          const uint8_t* mask, void* y, int ybf, int H, int W, int relu, int transposed,

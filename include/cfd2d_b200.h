@@ -472,16 +472,6 @@ int cfd2d_lpc_conv32(const void* x, const void* image, const float* bias, const 
                      const uint8_t* mask, void* y, int H, int W, int relu, int32_t* err, void* stream);
 /* CUDA-core 3x3 convolution for cin, cout in {1, 32}: x and y FP32 or BF16
  * (x_bf16, y_bf16 flags); transposed != 0 applies the adjoint (data gradient). */
-/* The 32->32 convolution with its input formed on the fly (no reference counterpart):
- * in_mode 1 = the 2x2 mean of x over its in-range children (x: Hs x Ws x 32, the finer
- * level, H = (Hs+1)/2, W = (Ws+1)/2), as cfd2d_lpc_pool2 forms it; in_mode 2 = scale *
- * nearest-upsampled x (Hs x Ws, the coarser level, Hs = (H+1)/2) + src2 (H x W), as
- * cfd2d_lpc_upadd forms it. Rounded to BF16 like those kernels, so the output equals
- * pooling or upsampling first and convolving after. staged_out (nullable) receives the
- * formed input (H x W x 32), which the backward pass reads. No skip term. */
-int cfd2d_lpc_conv32_fused(int in_mode, const void* x, int Hs, int Ws, const void* src2, float scale,
-                           void* staged_out, const void* image, const float* bias, const uint8_t* mask, void* y,
-                           int H, int W, int relu, int* err, void* stream);
 int cfd2d_lpc_conv(int cin, int cout, const void* x, int x_bf16, const float* w, const float* bias,
                    const uint8_t* mask, void* y, int y_bf16, int H, int W, int relu, int transposed,
                    void* stream);

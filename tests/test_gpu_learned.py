@@ -291,48 +291,3 @@ def test_learned_pressure_solve_inside_the_step(L):
     (up, vp, ip), (ul, vl, il) = out["plain"], out["learned"]
     assert relerr(ul, up) < 1e-6 and relerr(vl, vp) < 1e-6
     assert all(a > 0 for a in il) and sum(il) < sum(ip), (il, ip)
-
-
-@pytest.mark.parametrize("H,W", [(37, 200), (300, 129)])
-def test_fused_pool_and_upsample_conv_equal_the_separate_kernels(L, H, W):
-    """cfd2d_lpc_conv32_fused forms its input while staging (2x2 mean of the finer
-    level, or 4 x the upsampled coarser level plus the skip): the output and the formed
-    input it writes back are bit-identical to pooling or upsampling first."""
-    torch, _lib, learned = L
-    lib = _lib.lib()
-    P = _lib.ptr
-    dev = _lib.device()
-    g = torch.Generator().manual_seed(9)
-    img = torch.zeros(int(lib.cfd2d_lpc_w32_bytes()) // 2, dtype=torch.bfloat16, device=dev)
-    wd = (torch.randn((32, 32, 3, 3), generator=g) * 0.1).to(dev).contiguous()
-    _lib.check(lib.cfd2d_lpc_pack_w32(P(wd), P(img), _lib.stream_ptr()), "pack")
-    b = torch.zeros(32, device=dev)
-    mask = (torch.rand((H, W), generator=g) > 0.2).to(torch.uint8).to(dev)
-    err = torch.zeros(1, dtype=torch.int32, device=dev)
-    s = _lib.stream_ptr()
-    # mode 1: the finer level is 2H-1 x 2W (odd rows leave partial children)
-    Hf, Wf = 2 * H - 1, 2 * W
-    xf = torch.randn((Hf, Wf, 32), generator=g).to(torch.bfloat16).to(dev)
-    pooled = torch.zeros((H, W, 32), dtype=torch.bfloat16, device=dev)
-    _lib.check(lib.cfd2d_lpc_pool2(P(xf), P(pooled), Hf, Wf, s), "pool2")
-    y_sep = torch.zeros((H, W, 32), dtype=torch.bfloat16, device=dev)
-    _lib.check(lib.cfd2d_lpc_conv32(P(pooled), P(img), P(b), None, P(mask), P(y_sep), H, W, 0, P(err), s), "conv")
-    y_fus = torch.zeros_like(y_sep)
-    staged = torch.zeros_like(pooled)
-    _lib.check(lib.cfd2d_lpc_conv32_fused(1, P(xf), Hf, Wf, None, 1.0, P(staged), P(img), P(b), P(mask), P(y_fus),
-                                          H, W, 0, P(err), s), "fused pool")
-    torch.cuda.synchronize()
-    assert torch.equal(y_fus, y_sep) and torch.equal(staged, pooled)
-    # mode 2: coarse level (H+1)/2 x (W+1)/2, scale 4
-    Hc, Wc = (H + 1) // 2, (W + 1) // 2
-    xc = torch.randn((Hc, Wc, 32), generator=g).to(torch.bfloat16).to(dev)
-    skip = torch.randn((H, W, 32), generator=g).to(torch.bfloat16).to(dev)
-    up = torch.zeros((H, W, 32), dtype=torch.bfloat16, device=dev)
-    _lib.check(lib.cfd2d_lpc_upadd(P(xc), P(skip), P(up), H, W, 4.0, s), "upadd")
-    _lib.check(lib.cfd2d_lpc_conv32(P(up), P(img), P(b), None, P(mask), P(y_sep), H, W, 0, P(err), s), "conv")
-    staged.zero_()
-    _lib.check(lib.cfd2d_lpc_conv32_fused(2, P(xc), Hc, Wc, P(skip), 4.0, P(staged), P(img), P(b), P(mask),
-                                          P(y_fus), H, W, 0, P(err), s), "fused upadd")
-    torch.cuda.synchronize()
-    assert torch.equal(y_fus, y_sep) and torch.equal(staged, up)
-    assert int(err.item()) == 0
