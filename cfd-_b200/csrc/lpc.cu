@@ -617,12 +617,18 @@ template <int ROWS>
 static cudaError_t conv32_launch(const __nv_bfloat16* x, const __nv_bfloat16* wpack, const float* bias,
                                  const __nv_bfloat16* skip, const uint8_t* mask, __nv_bfloat16* y, int H, int W,
                                  int relu, int* err, cudaStream_t s) {
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(k_conv32_tc<ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)conv32_smem_bytes(ROWS));
+    // the shared-memory opt-in is a per-device attribute of the kernel
+    constexpr int kMaxDev = 64;
+    static bool configured[kMaxDev];
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDev) return cudaErrorInvalidDevice;
+    if (!configured[dev]) {
+        e = cudaFuncSetAttribute(k_conv32_tc<ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)conv32_smem_bytes(ROWS));
         if (e != cudaSuccess) return e;
-        configured = true;
+        configured[dev] = true;
     }
     dim3 grid(cdiv(W, TM), cdiv(H, ROWS));
     k_conv32_tc<ROWS><<<grid, NT, conv32_smem_bytes(ROWS), s>>>(x, reinterpret_cast<const uint4*>(wpack), bias,
