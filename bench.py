@@ -772,7 +772,12 @@ def run_b200(args, dist, rank, world):
     torch.cuda.set_device(local)
     from cfd2d_b200 import _lib, cases
 
-    case = cases.obstacle_flow(SEED, NX, NY, pressure_solver="cg")
+    # the headline workload: the obstacle flow (default) or, with --workload cylinder,
+    # the cylinder channel with a scalar (the form its committed profiles capture)
+    cyl_head = args.workload == "cylinder"
+    nxh, nyh = (CYL_NX, CYL_NY) if cyl_head else (NX, NY)
+    workload = CYL_WORKLOAD if cyl_head else WORKLOAD
+    case = cases.build_case(CYL_SPEC) if cyl_head else cases.obstacle_flow(SEED, NX, NY, pressure_solver="cg")
     sim = case.sim
     sim.pressure.tol = CG_RTOL
     stream = sim._stream
@@ -787,7 +792,7 @@ def run_b200(args, dist, rank, world):
     its = np.array(sim.history.extra["cg_iterationen"][-args.steps:], dtype=float)
     dev_s = sum(step_ms) / 1e3
     dev_s_max = _max_over_ranks(dist, dev_s)
-    cells = NX * NY
+    cells = nxh * nyh
     value = world * cells * args.steps / dev_s_max
     solve_s = sum(solve_ms) / 1e3
     iters = float(its.mean())
@@ -851,7 +856,7 @@ def run_b200(args, dist, rank, world):
     other = _optional(args.no_configs, configs_section)
     vof = _optional(args.no_vof, vof_section)
     cpu = None
-    if world == 1 and not args.no_cpu_baseline:
+    if world == 1 and not args.no_cpu_baseline and not cyl_head:
         d = cpu_oracle_sample(0, 1, 2, 1, iters_per_step=iters)
         cpu = {"value": d["rate"], "unit": "cell-updates/s", "cores": 1, "kind": "port",
                "sample": f"oracle step on 1 thread (NumPy stencils, scipy cg + Jacobi as cfd2d/pressure.py:171): "
@@ -862,18 +867,21 @@ def run_b200(args, dist, rank, world):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dev_s_max / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded obstacle flow from rest, as the reference's cases start)",
-        "config": {"workload": WORKLOAD, "grid": [NX, NY], "cells": cells, "fluid_cells": fluid_cells,
+        "config": {"workload": workload, "grid": [nxh, nyh], "cells": cells, "fluid_cells": fluid_cells,
                    "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"replicas x{world}",
-                   "solver": "plain FP64 Jacobi-PCG (k_pcg_slab)"},
+                   "solver": "plain FP64 Jacobi-PCG (%s)" % ("k_pcg_cluster" if cyl_head else "k_pcg_slab")},
         "poisson_ms": 1e3 * solve_s / args.steps,
         "poisson_iters_per_step": iters,
         "e2e": {"value": e2e, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "steps": e2e_steps},
         "gpu_launches": knodes * args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": _ncu_traffic("pcg_slab_obstacles1024x512.txt"),
-                     "kernel": "k_pcg_slab (FP64 Jacobi-PCG, one persistent launch per solve, vectors in "
-                               "shared memory)",
+                     "frac": achieved / peak,
+                     "traffic": _ncu_traffic("pcg_cluster_cylinder440x82.txt" if cyl_head
+                                             else "pcg_slab_obstacles1024x512.txt"),
+                     "kernel": ("k_pcg_cluster (FP64 Jacobi-PCG on one thread-block cluster)" if cyl_head else
+                                "k_pcg_slab (FP64 Jacobi-PCG, one persistent launch per solve, vectors in "
+                                "shared memory)"),
                      "peak_kind": peak_kind},
         "cpu_baseline": cpu,
         "clocks": clocks,
@@ -971,8 +979,9 @@ def main():
     ap.add_argument("--no-large", action="store_true", help="skip the 2048 x 1024 section")
     ap.add_argument("--no-cylinder", action="store_true", help="skip the cylinder 440 x 82 section")
     ap.add_argument("--no-single", action="store_true", help="skip the single-reduction solver section")
-    ap.add_argument("--workload", choices=["obstacles", "batch"], default="obstacles",
-                    help="obstacles: the headline; batch: 256 uneven cavities stepped together")
+    ap.add_argument("--workload", choices=["obstacles", "cylinder", "batch"], default="obstacles",
+                    help="obstacles: the headline; cylinder: the cylinder channel as the headline workload "
+                         "(the form the cylinder profiles capture); batch: 256 uneven cavities stepped together")
     ap.add_argument("--batch-cases", type=int, default=256)
     args = ap.parse_args()
     if args.warmup < 3:
