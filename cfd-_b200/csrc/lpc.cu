@@ -408,69 +408,60 @@ __global__ void __launch_bounds__(FP) k_conv_1to32(const float* __restrict__ x, 
     }
 }
 
-// 32 -> 1 layer on 2D tiles: a block of FP threads takes R32 rows x FP columns of the
-// output (thread t: column j0 + t, rows i0 .. i0 + R32 - 1), staging the R32 + 2 input
-// rows it reads once (each input row is staged by about (R32 + 2) / R32 blocks instead
-// of 3); the per-pixel sum runs over taps, then channels, in the same order as before.
-constexpr int R32 = 4;
 __global__ void __launch_bounds__(FP) k_conv_32to1(const __nv_bfloat16* __restrict__ x,
                                                    const float* __restrict__ w, const float* __restrict__ bias,
                                                    const uint8_t* __restrict__ mask, float* __restrict__ y, int H,
                                                    int W, int relu) {
-    constexpr int SP = FP + 2;                 // staged pixels per row
-    constexpr int SR = R32 + 2;                // staged rows
-    constexpr int SQ = SR * SP * 4;            // staged 16-byte chunks
+    constexpr int SP = FP + 2;             // staged pixels per tap row
+    constexpr int SQ = 3 * SP * 4;         // staged 16-byte chunks (1560)
     constexpr int SPER = (SQ + FP - 1) / FP;
-    constexpr int SB = 8;                      // loads in flight per thread and batch
     __shared__ __align__(16) float ws[9 * CH];
-    extern __shared__ uint4 xs[];              // SR * SP * PSTRIDE
+    __shared__ uint4 xs[3 * SP * PSTRIDE];
     for (int e = threadIdx.x; e < CH * 9; e += blockDim.x) ws[(e % 9) * CH + e / 9] = w[e];
-    const int j0 = blockIdx.x * FP, i0 = blockIdx.y * R32;
+    const long long n = (long long)H * W;
+    const long long p0 = (long long)blockIdx.x * FP;
+    // tap row d (di = d - 1) holds pixels p0 + di*W - 1 .. p0 + di*W + FP; taps that
+    // leave the grid are skipped below, so the clamp to [0, n) only avoids reading
+    // outside the array
     const uint4* x4 = reinterpret_cast<const uint4*>(x);
+    {
+        uint4 v[SPER];
 #pragma unroll
-    for (int k0 = 0; k0 < SPER; k0 += SB) {
-        uint4 v[SB];
-#pragma unroll
-        for (int k = 0; k < SB; ++k) {
-            const int q = threadIdx.x + (k0 + k) * FP;
-            const int r = q / (SP * 4), rem = q - r * (SP * 4);
-            const int ii = i0 - 1 + r, jj = j0 - 1 + (rem >> 2);
+        for (int k = 0; k < SPER; ++k) {
+            const int q = threadIdx.x + k * FP;
+            const int d = q / (SP * 4), rem = q - d * (SP * 4);
+            const long long g = p0 + (long long)(d - 1) * W - 1 + (rem >> 2);
             v[k] = make_uint4(0u, 0u, 0u, 0u);
-            if (k0 + k < SPER && q < SQ && ii >= 0 && ii < H && jj >= 0 && jj < W)
-                v[k] = x4[((size_t)ii * W + jj) * 4 + (rem & 3)];
+            if (q < SQ && g >= 0 && g < n) v[k] = x4[g * 4 + (rem & 3)];
         }
 #pragma unroll
-        for (int k = 0; k < SB; ++k) {
-            const int q = threadIdx.x + (k0 + k) * FP;
-            const int r = q / (SP * 4), rem = q - r * (SP * 4);
-            if (k0 + k < SPER && q < SQ) xs[(r * SP + (rem >> 2)) * PSTRIDE + (rem & 3)] = v[k];
+        for (int k = 0; k < SPER; ++k) {
+            const int q = threadIdx.x + k * FP;
+            const int d = q / (SP * 4), rem = q - d * (SP * 4);
+            if (q < SQ) xs[(d * SP + (rem >> 2)) * PSTRIDE + (rem & 3)] = v[k];
         }
     }
     __syncthreads();
-    const int j = j0 + threadIdx.x;
-    if (j >= W) return;
-    for (int r = 0; r < R32; ++r) {
-        const int i = i0 + r;
-        if (i >= H) break;
-        float acc = bias ? bias[0] : 0.0f;
+    const long long p = p0 + threadIdx.x;
+    if (p >= n) return;
+    const int i = (int)(p / W), j = (int)(p - (long long)i * W);
+    float acc = bias ? bias[0] : 0.0f;
 #pragma unroll
-        for (int tap = 0; tap < 9; ++tap) {
-            const int di = tap / 3 - 1, dj = tap % 3 - 1;
-            const int ii = i + di, jj = j + dj;
-            if (ii < 0 || ii >= H || jj < 0 || jj >= W) continue;
-            const uint4* src = xs + ((r + di + 1) * SP + threadIdx.x + dj + 1) * PSTRIDE;
-            uint4 v[4];
+    for (int tap = 0; tap < 9; ++tap) {
+        const int di = tap / 3 - 1, dj = tap % 3 - 1;
+        const int ii = i + di, jj = j + dj;
+        if (ii < 0 || ii >= H || jj < 0 || jj >= W) continue;
+        const uint4* src = xs + ((di + 1) * SP + threadIdx.x + dj + 1) * PSTRIDE;
+        uint4 v[4];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) v[q] = src[q];
-            const __nv_bfloat16* xv = reinterpret_cast<const __nv_bfloat16*>(v);
+        for (int q = 0; q < 4; ++q) v[q] = src[q];
+        const __nv_bfloat16* xv = reinterpret_cast<const __nv_bfloat16*>(v);
 #pragma unroll
-            for (int c = 0; c < CH; ++c) acc += ws[tap * CH + c] * bf2f(xv[c]);
-        }
-        if (relu) acc = fmaxf(acc, 0.0f);
-        const size_t p = (size_t)i * W + j;
-        const bool fl = mask ? (mask[p] != 0) : true;
-        y[p] = fl ? acc : 0.0f;
+        for (int c = 0; c < CH; ++c) acc += ws[tap * CH + c] * bf2f(xv[c]);
     }
+    if (relu) acc = fmaxf(acc, 0.0f);
+    const bool fl = mask ? (mask[p] != 0) : true;
+    y[p] = fl ? acc : 0.0f;
 }
 
 // ---------------------------------------------------------------- pooling, upsampling
@@ -673,21 +664,8 @@ cudaError_t conv_generic(int cin, int cout, const void* x, int xbf, const float*
         return cudaGetLastError();
     }
     if (!transposed && cin == 32 && cout == 1 && xbf && !ybf) {
-        const size_t smem = (size_t)(R32 + 2) * (FP + 2) * PSTRIDE * sizeof(uint4);
-        constexpr int kMaxDev = 64;
-        static bool configured[kMaxDev];
-        int dev = 0;
-        cudaError_t e = cudaGetDevice(&dev);
-        if (e != cudaSuccess) return e;
-        if (dev < 0 || dev >= kMaxDev) return cudaErrorInvalidDevice;
-        if (!configured[dev]) {
-            e = cudaFuncSetAttribute(k_conv_32to1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e != cudaSuccess) return e;
-            configured[dev] = true;
-        }
-        k_conv_32to1<<<dim3(cdiv(W, FP), cdiv(H, R32)), FP, smem, s>>>(static_cast<const __nv_bfloat16*>(x), w,
-                                                                        bias, mask, static_cast<float*>(y), H, W,
-                                                                        relu);
+        k_conv_32to1<<<cdiv(n, FP), FP, 0, s>>>(static_cast<const __nv_bfloat16*>(x), w, bias, mask,
+                                                   static_cast<float*>(y), H, W, relu);
         return cudaGetLastError();
     }
     if (cin == 1 && cout == 32)
