@@ -23,6 +23,9 @@ learned   = the same workload with the pressure solved by flexible CG with the
             both solvers on the same system from the same warm start.
 single_reduction = the headline workload with the slab solver's single-reduction
             form (one grid reduction per CG iteration instead of scipy's two).
+batch_64_cavities = 64 seeded uneven cavities stepped together against the per-case loop.
+sst_channel_mixed_precision = the k-omega SST channel 128 x 192 over 2000 steps with the FP64 and the
+            mixed-precision solver: time and the mixed run's error in the u profile, nu_t, tau_w, c_f.
 grid_2048x1024 = the same generator and seed at 2048 x 1024: plain steps and the
             Poisson comparison (the CG cap is raised so that both reach 1e-8).
 cylinder_440x82 = the cylinder channel with a van Leer scalar (plain FP64 path).
@@ -707,10 +710,6 @@ def configs_section(cavity_steps: int = 2000, sst_steps: int = 500) -> dict:
     import torch
 
     from cfd2d_b200 import cases
-    from cfd2d_b200.boundary import BoundaryCondition as BC
-    from cfd2d_b200.grid import Grid
-    from cfd2d_b200.solver import Simulation
-    from cfd2d_b200.turbulence import KOmegaSST
 
     def timed(sim, n):
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
@@ -731,6 +730,22 @@ def configs_section(cavity_steps: int = 2000, sst_steps: int = 500) -> dict:
     case = cases.lid_driven_cavity(re=100, n=64, scheme="ab2", gamma=0.1, tau=0.5, pressure_solver="cg")
     case.sim.pressure.tol = CG_RTOL
     cav = timed(case.sim, cavity_steps)
+    sim = sst_channel_sim()
+    return {"cavity_64x64": {"steps": cavity_steps, **cav},
+            "sst_channel_128x192": {"steps": sst_steps, **timed(sim, sst_steps)}}
+
+
+def sst_channel_sim(precision: str = "fp64"):
+    """The periodic k-omega SST channel 128 x 192 (domain 2 pi x 2, bulk velocity 1,
+    Re_b 1e4 held by volume-flow forcing, laminar profile with 5 % seeded noise,
+    k = 1e-3 and omega = 10, CG rtol 1e-8), re-projected, ready to step."""
+    import numpy as np
+
+    from cfd2d_b200.boundary import BoundaryCondition as BC
+    from cfd2d_b200.grid import Grid
+    from cfd2d_b200.solver import Simulation
+    from cfd2d_b200.turbulence import KOmegaSST
+
     nx, ny = 128, 192
     grid = Grid(nx, ny, 2 * np.pi, 2.0)
     bcs = dict(left=BC("periodic"), right=BC("periodic"), bottom=BC("noslip"), top=BC("noslip"))
@@ -738,6 +753,7 @@ def configs_section(cavity_steps: int = 2000, sst_steps: int = 500) -> dict:
     sst = KOmegaSST(intensity=np.sqrt(1e-3 / 1.5), viscosity_ratio=1e-3 / (nu * 10.0), U_ref=1.0)
     sim = Simulation(grid, bcs, nu=nu, flow_rate=1.0, models=[sst], pressure_solver="cg")
     sim.pressure.tol = CG_RTOL
+    sim.pressure.precision = precision
     rng = np.random.default_rng(0)
     y = (np.arange(ny) + 0.5) * grid.dy
     u = sim.u
@@ -748,8 +764,47 @@ def configs_section(cavity_steps: int = 2000, sst_steps: int = 500) -> dict:
     v[~sim.v_fluid] = 0.0
     sim._apply_bc()
     sim._project_initial()
-    return {"cavity_64x64": {"steps": cavity_steps, **cav},
-            "sst_channel_128x192": {"steps": sst_steps, **timed(sim, sst_steps)}}
+    return sim
+
+
+def sst_mixed_section(steps: int = 2000) -> dict:
+    """The SST channel over ``steps`` steps with the FP64 pressure solver and with the
+    mixed one (FP32 CG iterations, FP64 refinement and reductions): ms per step, and
+    the mixed run's error against the FP64 run (which follows the reference's CPU run
+    to 6e-13 over 500 steps, tests/test_gpu_parity.py) in the x-mean u profile, nu_t and
+    the wall shear stress and skin friction of cfd2d/report.py:455-462
+    (tau_w = nu (u_1 + u_ny) / 2 / (dy / 2) on column i = 2, c_f = 2 tau_w / U^2)."""
+    import numpy as np
+    import torch
+
+    out, res = {}, {}
+    for prec in ("fp64", "mixed"):
+        sim = sst_channel_sim(prec)
+        sim.advance(2)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        torch.cuda.synchronize()
+        with torch.cuda.stream(sim.stream):
+            ev[0].record()
+            sim.launch_steps(steps - 2)
+            ev[1].record()
+        sim.finish_steps()
+        torch.cuda.synchronize()
+        g = sim.grid
+        u = sim.u
+        ucol = u[2, 1:-1]
+        tau_w = sim.nu * 0.5 * (ucol[0] + ucol[-1]) / (0.5 * g.dy)
+        res[prec] = {"profile": u[1:g.nx + 1, 1:-1].mean(axis=0), "nut": sim.nu_t.copy(), "tau_w": float(tau_w),
+                     "cf": float(2.0 * tau_w / 1.0 ** 2)}
+        its = np.array(sim.history.extra["cg_iterationen"][-(steps - 2):], dtype=float)
+        out[prec] = {"ms_per_step": ev[0].elapsed_time(ev[1]) / (steps - 2), "poisson_iters_per_step": float(its.mean())}
+    a, b = res["mixed"], res["fp64"]
+    out["mixed_vs_fp64"] = {
+        "u_profile_rel": float(np.abs(a["profile"] - b["profile"]).max() / np.abs(b["profile"]).max()),
+        "nu_t_rel": float(np.abs(a["nut"] - b["nut"]).max() / np.abs(b["nut"]).max()),
+        "tau_w_rel": abs(a["tau_w"] / b["tau_w"] - 1.0), "c_f_rel": abs(a["cf"] / b["cf"] - 1.0)}
+    out["fp64"]["c_f"] = b["cf"]
+    out["workload"] = f"k-omega SST channel 128x192, {steps} steps from the perturbed laminar profile"
+    return out
 
 
 # ------------------------------------------------------------------ GPU arm
@@ -855,6 +910,8 @@ def run_b200(args, dist, rank, world):
     mixed = _optional(args.no_mixed, mixed_section)
     other = _optional(args.no_configs, configs_section)
     vof = _optional(args.no_vof, vof_section)
+    bat = _optional(args.no_batch, lambda: batch_section(64, 3, 2))
+    sstm = _optional(args.no_mixed, sst_mixed_section)
     cpu = None
     if world == 1 and not args.no_cpu_baseline and not cyl_head:
         d = cpu_oracle_sample(0, 1, 2, 1, iters_per_step=iters)
@@ -892,36 +949,40 @@ def run_b200(args, dist, rank, world):
         "stencils": stencils,
         "mixed_precision": mixed,
         "vof_dam_break": vof,
+        "batch_64_cavities": bat,
+        "sst_channel_mixed_precision": sstm,
         "other_workloads": other,
     }
     print(json.dumps(line), flush=True)
 
 
 # ------------------------------------------------------------------ batched uneven cases
-def run_batch(args, dist, rank, world):
-    """256 seeded uneven cavities (half lid-driven, half heated), every step of all of
-    them queued on their own streams before any is waited for (grids beyond one
-    on-chip cluster solve on one 16-CTA cluster each, so their solves overlap), against
-    the per-case loop (the same cases one after another, each with the solver it would
-    use alone). Replicas over ranks as the main arm."""
+def batch_section(n_cases: int, steps: int, warmup: int, dist=None, clk_name: str | None = None) -> dict:
+    """Seeded uneven cavities (half lid-driven, half heated; side uniform in 32..512),
+    every step of all of them queued on their own streams before any is waited for
+    (grids beyond one on-chip cluster solve on one 16-CTA cluster each, so their solves
+    overlap), against the per-case loop (the same cases one after another, each with
+    the solver it would use alone), both timed on the device."""
     import numpy as np
     import torch
 
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
     from cfd2d_b200 import batch
 
     t0 = time.perf_counter()
-    cs = batch.uneven_cavities(n_cases=args.batch_cases, seed=0)
+    cs = batch.uneven_cavities(n_cases=n_cases, seed=0)
     for c in cs:
         c.sim.pressure.tol = CG_RTOL
     b = batch.Batch([c.sim for c in cs])
     setup_s = time.perf_counter() - t0
-    b.advance(args.warmup)
+    b.advance(warmup)
     _barrier(dist)
     torch.cuda.synchronize()
-    with _Clocks(_clocks_path(f"clocks_batch_rank{rank}.csv")) as clk:
-        ms = b.timed_advance(args.steps, concurrent=True)
+    clk = _Clocks(_clocks_path(clk_name)).__enter__() if clk_name else None
+    try:
+        ms = b.timed_advance(steps, concurrent=True)
+    finally:
+        if clk is not None:
+            clk.__exit__(None, None, None)
     ms_max = _max_over_ranks(dist, ms)
     # per-case loop: each case alone, one after another, timed per case on the device,
     # with the solver each case would use alone (the large grids over every SM)
@@ -934,32 +995,47 @@ def run_batch(args, dist, rank, world):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(main)
         sim.stream.wait_event(e0)
-        sim.launch_steps(args.steps)
+        sim.launch_steps(steps)
         e1.record(sim.stream)
         sim.finish_steps()
         e1.synchronize()
-        per_case.append(e0.elapsed_time(e1) / args.steps)
-    loop_ms = sum(per_case) * args.steps
+        per_case.append(e0.elapsed_time(e1) / steps)
+    loop_ms = sum(per_case) * steps
     cells = b.cells
+    sizes = [sm.grid.nx for sm in b.sims]
+    return {"workload": f"{len(b.sims)} cavities, side uniform in 32..512 step 32, half lid-driven "
+                        f"(Re log-uniform 100-5000), half heated (Ra log-uniform 1e3-1e6, Pr 0.71), "
+                        f"FP64 Jacobi-PCG rtol 1e-8",
+            "steps": steps, "cells_per_step": cells, "ms_per_step": ms_max / steps,
+            "cell_updates_per_s": cells * steps / (ms_max / 1e3),
+            "cluster_solver_cases": sum(1 for sm in b.sims if sm.pressure.cluster > 0),
+            "side_min_max": [min(sizes), max(sizes)], "setup_s": setup_s,
+            "per_case_loop": {"cell_updates_per_s": cells * steps / (loop_ms / 1e3), "ms_per_step": loop_ms / steps,
+                              "case_step_ms_p50": float(np.percentile(per_case, 50)),
+                              "case_step_ms_p99": float(np.percentile(per_case, 99))},
+            "speedup_vs_per_case_loop": loop_ms / ms_max,
+            "clocks": clk.summary(int(os.environ.get("LOCAL_RANK", "0"))) if clk is not None else None}
+
+
+def run_batch(args, dist, rank, world):
+    """The batch as the headline workload (--workload batch): replicas over ranks as the
+    main arm."""
+    import torch
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    rec = batch_section(args.batch_cases, args.steps, args.warmup, dist, f"clocks_batch_rank{rank}.csv")
     if rank != 0:
         return
-    sizes = [s.grid.nx for s in b.sims]
     line = {
-        "metric": "aggregate cell-updates/s, 256 uneven cavities stepped together", "value":
-            world * cells * args.steps / (ms_max / 1e3), "unit": "cell-updates/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+        "metric": f"aggregate cell-updates/s, {args.batch_cases} uneven cavities stepped together",
+        "value": world * rec["cell_updates_per_s"], "unit": "cell-updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": rec["ms_per_step"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded cases from rest)",
-        "config": {"workload": f"{len(b.sims)} cavities, side uniform in 32..512 step 32, half lid-driven "
-                               f"(Re log-uniform 100-5000), half heated (Ra log-uniform 1e3-1e6, Pr 0.71), "
-                               f"FP64 Jacobi-PCG rtol 1e-8", "cells_per_step": cells,
-                   "cluster_solver_cases": sum(1 for s in b.sims if s.pressure.cluster > 0),
-                   "batched_large_grids": "workspace solver on one 16-CTA cluster each",
-                   "side_min_max": [min(sizes), max(sizes)], "setup_s": setup_s},
-        "per_case_loop": {"value": cells * args.steps / (loop_ms / 1e3), "ms_per_step": loop_ms / args.steps,
-                          "case_step_ms_p50": float(np.percentile(per_case, 50)),
-                          "case_step_ms_p99": float(np.percentile(per_case, 99))},
-        "clocks": clk.summary(local),
+        "config": {k: rec[k] for k in ("workload", "cells_per_step", "cluster_solver_cases", "side_min_max",
+                                         "setup_s")},
+        "per_case_loop": rec["per_case_loop"], "clocks": rec["clocks"],
     }
     print(json.dumps(line), flush=True)
 
@@ -979,6 +1055,7 @@ def main():
     ap.add_argument("--no-large", action="store_true", help="skip the 2048 x 1024 section")
     ap.add_argument("--no-cylinder", action="store_true", help="skip the cylinder 440 x 82 section")
     ap.add_argument("--no-single", action="store_true", help="skip the single-reduction solver section")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 64-cavity batch section")
     ap.add_argument("--workload", choices=["obstacles", "cylinder", "batch"], default="obstacles",
                     help="obstacles: the headline; cylinder: the cylinder channel as the headline workload "
                          "(the form the cylinder profiles capture); batch: 256 uneven cavities stepped together")
