@@ -60,6 +60,29 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint
 
 __device__ __forceinline__ float bf2f(__nv_bfloat16 x) { return __bfloat162float(x); }
 
+// Programmatic dependent launch: the network's kernels are launched so that each may
+// start while its predecessor finishes. Before pdl_wait() a kernel touches only what
+// no predecessor writes (its weights, shared memory, TMEM); pdl_wait() returns once the
+// predecessor grid has completed and its memory is visible. pdl_trigger() lets the
+// successor start as soon as every CTA of this grid has issued it.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------- 32 -> 32 conv (tensor cores)
@@ -132,6 +155,9 @@ __global__ void __launch_bounds__(NT) k_conv32_tc(const __nv_bfloat16* __restric
         for (int k = 0; k < BPER; ++k)
             if (tid + k * NT < BQ) reinterpret_cast<uint4*>(Bs)[tid + k * NT] = v[k];
     }
+    // everything below reads what the predecessor kernel wrote
+    pdl_trigger();
+    pdl_wait();
     // staged input rows: consecutive threads take consecutive 16-byte chunks in global
     // order (chunk fastest, then pixel), so each warp reads 512 contiguous bytes; the
     // loads go out in batches of XB per thread before their shared-memory stores
@@ -370,6 +396,8 @@ __global__ void __launch_bounds__(FP) k_conv_1to32(const float* __restrict__ x, 
     __shared__ __align__(16) float ws[9 * CH];
     __shared__ uint4 os[FP * PSTRIDE];
     for (int e = threadIdx.x; e < CH * 9; e += blockDim.x) ws[(e % 9) * CH + e / 9] = w[e];
+    pdl_trigger();
+    pdl_wait();
     __syncthreads();
     const long long n = (long long)H * W;
     const long long p0 = (long long)blockIdx.x * FP;
@@ -418,6 +446,8 @@ __global__ void __launch_bounds__(FP) k_conv_32to1(const __nv_bfloat16* __restri
     __shared__ __align__(16) float ws[9 * CH];
     __shared__ uint4 xs[3 * SP * PSTRIDE];
     for (int e = threadIdx.x; e < CH * 9; e += blockDim.x) ws[(e % 9) * CH + e / 9] = w[e];
+    pdl_trigger();
+    pdl_wait();
     const long long n = (long long)H * W;
     const long long p0 = (long long)blockIdx.x * FP;
     // tap row d (di = d - 1) holds pixels p0 + di*W - 1 .. p0 + di*W + FP; taps that
@@ -468,6 +498,8 @@ __global__ void __launch_bounds__(FP) k_conv_32to1(const __nv_bfloat16* __restri
 // coarse (Hc, Wc) = (ceil(H/2), ceil(W/2)): mean of the in-range children; one thread
 // per 8 channels of a coarse pixel (one 16-byte vector)
 __global__ void k_pool2(const __nv_bfloat16* __restrict__ x, __nv_bfloat16* __restrict__ y, int H, int W) {
+    pdl_trigger();
+    pdl_wait();
     const int Hc = (H + 1) / 2, Wc = (W + 1) / 2;
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= Hc * Wc * (CH / 8)) return;
@@ -495,6 +527,8 @@ __global__ void k_pool2(const __nv_bfloat16* __restrict__ x, __nv_bfloat16* __re
 // y[p] = coarse[parent(p)] + skip[p]; one thread per 8 channels of a pixel
 __global__ void k_upadd(const __nv_bfloat16* __restrict__ coarse, const __nv_bfloat16* __restrict__ skip,
                         __nv_bfloat16* __restrict__ y, int H, int W, float scale) {
+    pdl_trigger();
+    pdl_wait();
     const int Wc = (W + 1) / 2;
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= H * W * (CH / 8)) return;
@@ -631,9 +665,8 @@ static cudaError_t conv32_launch(const __nv_bfloat16* x, const __nv_bfloat16* wp
         configured[dev] = true;
     }
     dim3 grid(cdiv(W, TM), cdiv(H, ROWS));
-    k_conv32_tc<ROWS><<<grid, NT, conv32_smem_bytes(ROWS), s>>>(x, reinterpret_cast<const uint4*>(wpack), bias,
-                                                                 skip, mask, y, H, W, relu, err);
-    return cudaGetLastError();
+    return launch_pdl(k_conv32_tc<ROWS>, grid, dim3(NT), conv32_smem_bytes(ROWS), s, x,
+                      reinterpret_cast<const uint4*>(wpack), bias, skip, mask, y, H, W, relu, err);
 }
 
 // Rows per CTA: two where that still leaves about six CTAs per SM (two waves at the
@@ -659,14 +692,12 @@ cudaError_t conv_generic(int cin, int cout, const void* x, int xbf, const float*
     const int n = H * W;
     const int blk = 128;
     if (!transposed && cin == 1 && cout == 32 && !xbf && ybf) {
-        k_conv_1to32<<<cdiv(n, FP), FP, 0, s>>>(static_cast<const float*>(x), w, bias, mask,
-                                                   static_cast<__nv_bfloat16*>(y), H, W, relu);
-        return cudaGetLastError();
+        return launch_pdl(k_conv_1to32, dim3(cdiv(n, FP)), dim3(FP), 0, s, static_cast<const float*>(x), w, bias,
+                          mask, static_cast<__nv_bfloat16*>(y), H, W, relu);
     }
     if (!transposed && cin == 32 && cout == 1 && xbf && !ybf) {
-        k_conv_32to1<<<cdiv(n, FP), FP, 0, s>>>(static_cast<const __nv_bfloat16*>(x), w, bias, mask,
-                                                   static_cast<float*>(y), H, W, relu);
-        return cudaGetLastError();
+        return launch_pdl(k_conv_32to1, dim3(cdiv(n, FP)), dim3(FP), 0, s, static_cast<const __nv_bfloat16*>(x), w,
+                          bias, mask, static_cast<float*>(y), H, W, relu);
     }
     if (cin == 1 && cout == 32)
         k_conv_generic<1, 32><<<cdiv(n, blk), blk, 0, s>>>(x, xbf, w, bias, mask, y, ybf, H, W, relu, transposed);
@@ -681,7 +712,8 @@ cudaError_t conv_generic(int cin, int cout, const void* x, int xbf, const float*
 
 cudaError_t pool2(const __nv_bfloat16* x, __nv_bfloat16* y, int H, int W, cudaStream_t s) {
     const int n = ((H + 1) / 2) * ((W + 1) / 2) * (CH / 8);
-    k_pool2<<<cdiv(n, 256), 256, 0, s>>>(x, y, H, W);
+    cudaError_t e = launch_pdl(k_pool2, dim3(cdiv(n, 256)), dim3(256), 0, s, x, y, H, W);
+    if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
 
@@ -693,7 +725,9 @@ cudaError_t pool_mask(const uint8_t* m, uint8_t* mc, int H, int W, cudaStream_t 
 
 cudaError_t upadd(const __nv_bfloat16* coarse, const __nv_bfloat16* skip, __nv_bfloat16* y, int H, int W, float scale,
                   cudaStream_t s) {
-    k_upadd<<<cdiv((long long)H * W * (CH / 8), 256), 256, 0, s>>>(coarse, skip, y, H, W, scale);
+    cudaError_t e = launch_pdl(k_upadd, dim3(cdiv((long long)H * W * (CH / 8), 256)), dim3(256), 0, s, coarse, skip,
+                               y, H, W, scale);
+    if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
 
