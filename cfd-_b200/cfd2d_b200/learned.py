@@ -853,6 +853,7 @@ def main(argv=None):
     tr.add_argument("--lr", type=float, default=1e-3)
     tr.add_argument("--seed", type=int, default=0)
     tr.add_argument("--recipe", choices=["channel", "mixed"], default="channel")
+    tr.add_argument("--arch", default="{}", help="JSON overrides of the architecture (e.g. '{\"nrep\": 1}')")
     tr.add_argument("--onpolicy", type=int, default=1,
                     help="rounds of adding the flexible CG's own residuals and training on")
     apl = sub.add_parser("apply")
@@ -864,7 +865,7 @@ def main(argv=None):
         t0 = time.time()
         data = harvest_recipe(cases=a.cases, snaps=a.snaps, seed=a.seed, kind=a.recipe)
         print(f"residuals {len(data)} from {len(data.solvers)} cases in {time.time() - t0:.0f}s", flush=True)
-        net = LPCNet(seed=a.seed)
+        net = LPCNet(seed=a.seed, arch=json.loads(a.arch))
         log = train(net, data, steps=a.steps, batch=a.batch, lr=a.lr, seed=a.seed, log_every=500,
                     time_budget_s=a.seconds or None)
         print(f"steps {len(log)} loss first {np.mean(log[:50]):.4f} last {np.mean(log[-50:]):.4f}", flush=True)
