@@ -261,6 +261,38 @@ print(json.dumps({{"est_s": est, "raw_s": raw, "sampled_iters": its, "full_iters
     return d
 
 
+def cpu_direct_lu_rate(steps: int = 3) -> dict:
+    """The reference's other pressure solver on the same workload, timed in a child
+    process on one host thread: the oracle's step with the pressure system factorised
+    once by SuperLU (COLAMD ordering, as cfd2d/pressure.py:137) and solved by the
+    factors every step."""
+    env = dict(os.environ)
+    for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        env[k] = "1"
+    obst, re = _obstacle_spec()
+    code = f"""
+import sys, time, json, warnings
+sys.path.insert(0, {str(ROOT)!r})
+warnings.simplefilter("ignore")
+import oracle as O
+t0 = time.perf_counter()
+sim = O.custom_obstacles({obst!r}, lx=2.0, ly=1.0, nx={NX}, ny={NY}, re={re!r}, tol={CG_RTOL},
+                         pressure_solver="direct")
+setup = time.perf_counter() - t0
+sim.step()
+t0 = time.perf_counter()
+for _ in range({steps}):
+    sim.step()
+print(json.dumps({{"setup_s": setup, "seconds": time.perf_counter() - t0}}))
+"""
+    out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, check=True)
+    d = json.loads(out.stdout.strip().splitlines()[-1])
+    return {"value": NX * NY * steps / d["seconds"], "unit": "cell-updates/s", "ms_per_step": 1e3 * d["seconds"] / steps,
+            "setup_s_incl_factorisation": d["setup_s"], "cores": 1, "steps": steps,
+            "what": "oracle step with the pressure solved by SuperLU factors (the reference's 'direct' solver), "
+                    "factorised once at set-up"}
+
+
 def run_reference(args, dist, rank, world):
     """The CPU arm: the oracle (the reference's algorithm restated; its CG is scipy's
     cg as the reference calls it) on the headline workload with every host thread
@@ -287,6 +319,7 @@ def run_reference(args, dist, rank, world):
         "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "poisson_iters_per_step": float(d["full_iters"]),
         "raw_sample_ms_per_step": 1e3 * sum(d["raw_s"]) / len(d["raw_s"]),
+        "direct_lu": cpu_direct_lu_rate(),
     }
     print(json.dumps(line), flush=True)
 

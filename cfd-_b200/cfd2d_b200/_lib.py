@@ -218,6 +218,7 @@ def lib():
         "cfd2d_pressure_solve_snapshots": ([vp, vp, vp, d, i, vp, i, i, vp, vp, vp], i),
         "cfd2d_lpc_w32_bytes": ([], sz),
         "cfd2d_lpc_pack_w32": ([vp, vp, vp], i),
+        "cfd2d_lpc_pack_w32_adjoint": ([vp, vp, vp], i),
         "cfd2d_lpc_conv32": ([vp, vp, vp, vp, vp, vp, i, i, i, vp, vp], i),
         "cfd2d_lpc_conv": ([i, i, vp, i, vp, vp, vp, vp, i, i, i, i, i, vp], i),
         "cfd2d_lpc_pool2": ([vp, vp, i, i, vp], i),
@@ -267,7 +268,7 @@ def exported_symbols():
         "cfd2d_streamfunction", "cfd2d_vtk_pack", "cfd2d_graph_capture_steps", "cfd2d_graph_launch", "cfd2d_graph_destroy",
         "cfd2d_graph_capture_steps_ex", "cfd2d_events_create", "cfd2d_events_destroy",
         "cfd2d_event_elapsed_ms", "cfd2d_sim_step_begin", "cfd2d_sim_step_finish", "cfd2d_poisson_matvec",
-        "cfd2d_pressure_solve_snapshots", "cfd2d_lpc_w32_bytes", "cfd2d_lpc_pack_w32", "cfd2d_lpc_conv32",
+        "cfd2d_pressure_solve_snapshots", "cfd2d_lpc_w32_bytes", "cfd2d_lpc_pack_w32", "cfd2d_lpc_pack_w32_adjoint", "cfd2d_lpc_conv32",
         "cfd2d_lpc_conv", "cfd2d_lpc_pool2", "cfd2d_lpc_pool_mask", "cfd2d_lpc_upadd", "cfd2d_lpc_relu_bwd",
         "cfd2d_lpc_upadd_bwd", "cfd2d_lpc_pool_bwd", "cfd2d_lpc_conv_dw_partial_floats", "cfd2d_lpc_conv_dw",
         "cfd2d_fcg_partial_doubles", "cfd2d_fcg_init", "cfd2d_fcg_pq", "cfd2d_fcg_update", "cfd2d_fcg_zr",

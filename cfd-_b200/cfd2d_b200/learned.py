@@ -130,6 +130,7 @@ class LPCNet:
             self.w[name] = ((t.rand((cout, cin, 3, 3), generator=g) * 2.0 - 1.0) * bound).to(_lib.device())
             self.b[name] = t.zeros(cout, device=_lib.device())
         self._images = {}
+        self._adj_images = {}
         self._wq = {}
         self.repack()
 
@@ -166,8 +167,12 @@ class LPCNet:
             if img is None:
                 img = t.zeros(nbytes // 2, dtype=t.bfloat16, device=_lib.device())
                 self._images[name] = img
+                self._adj_images[name] = t.zeros(nbytes // 2, dtype=t.bfloat16, device=_lib.device())
             w = self.w[name].detach().float().contiguous()
             _lib.check(L.cfd2d_lpc_pack_w32(_lib.ptr(w), _lib.ptr(img), _lib.stream_ptr()), "pack_w32")
+            # the data-gradient convolution of the same layer, for the backward pass
+            _lib.check(L.cfd2d_lpc_pack_w32_adjoint(_lib.ptr(w), _lib.ptr(self._adj_images[name]),
+                                                    _lib.stream_ptr()), "pack_w32_adjoint")
 
     def wq(self, name):
         """The BF16-rounded weights the kernels use, as FP32."""
@@ -271,11 +276,15 @@ def net_forward(net: LPCNet, ws: Workspace, x_in):
     return ws.out
 
 
-def net_backward(net: LPCNet, ws: Workspace, x_in, dout):
+def net_backward(net: LPCNet, ws: Workspace, x_in, dout, tc_dgrad: bool = True):
     """Gradients of sum(out * dout) w.r.t. every weight and bias (FP32), from the
     activations left in ``ws`` by net_forward(x_in): the op list replayed in reverse
     with the hand-written backward kernels; shared weights sum their gradients over
-    the levels that use them."""
+    the levels that use them. With ``tc_dgrad`` the data gradient of every 32->32 layer
+    runs on the tensor cores (the forward tcgen05 convolution with the adjoint weight
+    image: channels swapped, taps mirrored; the gradient rounded to BF16 on the way
+    in and out, FP32 accumulation); else on the CUDA-core transposed convolution in
+    FP32. Weight gradients are CUDA-core reductions over the pixels."""
     t = _t()
     L = _lib.lib()
     s = _lib.stream_ptr()
@@ -287,6 +296,7 @@ def net_backward(net: LPCNet, ws: Workspace, x_in, dout):
     grads = {name: (t.zeros((cout, cin, 3, 3), device=dev), t.zeros(cout, device=dev))
              for name, (cin, cout) in WEIGHTS.items()}
     g = {"out": dout.contiguous()}  # gradient of every buffer, FP32
+    zero_bias = t.zeros(CH, dtype=t.float32, device=dev)
 
     def add(name, val):
         if name in g:
@@ -313,9 +323,16 @@ def net_backward(net: LPCNet, ws: Workspace, x_in, dout):
             grads[name][0].add_(dwb[:cout * cin * 9].view(cout, cin, 3, 3))
             grads[name][1].add_(dwb[cout * cin * 9:])
             if src != "in":
-                dx = t.zeros(sh[lvl] + (cin,), dtype=t.float32, device=dev)
-                _lib.check(L.cfd2d_lpc_conv(cout, cin, P(gp), 0, P(net.wq(name)), None, None, P(dx), 0, h, w, 0, 1,
-                                            s), "conv transposed")
+                if tc_dgrad and cin == CH and cout == CH:
+                    gb = gp.to(t.bfloat16)
+                    dxb = t.empty(sh[lvl] + (cin,), dtype=t.bfloat16, device=dev)
+                    _lib.check(L.cfd2d_lpc_conv32(P(gb), P(net._adj_images[name]), P(zero_bias), None, None, P(dxb),
+                                                  h, w, 0, P(ws.err), s), "conv32 data gradient")
+                    dx = dxb.float()
+                else:
+                    dx = t.zeros(sh[lvl] + (cin,), dtype=t.float32, device=dev)
+                    _lib.check(L.cfd2d_lpc_conv(cout, cin, P(gp), 0, P(net.wq(name)), None, None, P(dx), 0, h, w, 0,
+                                                1, s), "conv transposed")
                 add(src, dx)
         elif op[0] == "pool":
             _, lvl, src, dst = op

@@ -22,7 +22,12 @@ size_t cfd2d_lpc_w32_bytes(void) { return (size_t)32 * 288 * 2; }
 
 int cfd2d_lpc_pack_w32(const float* w, void* image, void* stream) {
     if (!w || !image) return CFD2D_E_ARG;
-    return status_of(lpc::pack_w32(w, bfw(image), as_stream(stream)));
+    return status_of(lpc::pack_w32(w, bfw(image), 0, as_stream(stream)));
+}
+
+int cfd2d_lpc_pack_w32_adjoint(const float* w, void* image, void* stream) {
+    if (!w || !image) return CFD2D_E_ARG;
+    return status_of(lpc::pack_w32(w, bfw(image), 1, as_stream(stream)));
 }
 
 int cfd2d_lpc_conv32(const void* x, const void* image, const float* bias, const void* skip,

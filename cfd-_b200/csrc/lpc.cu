@@ -324,12 +324,15 @@ __global__ void __launch_bounds__(NT) k_conv32_tc(const __nv_bfloat16* __restric
 }
 
 // Pack w[n][c][3][3] (float, PyTorch OIHW) into the B operand image.
-__global__ void k_pack_w32(const float* __restrict__ w, __nv_bfloat16* __restrict__ img) {
+// adjoint = 1: the image of the data-gradient convolution of the same layer,
+// dx[p][c] = sum_{tap, o} w[o][c][tap] dy[p - tap][o], i.e. a forward convolution
+// with input and output channels swapped and the taps mirrored (tap -> 8 - tap).
+__global__ void k_pack_w32(const float* __restrict__ w, __nv_bfloat16* __restrict__ img, int adjoint) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;  // over n * 288
     if (e >= CH * KDIM) return;
     const int n = e / KDIM, k = e % KDIM;
     const int tap = k / CH, c = k % CH;
-    const float v = w[(n * CH + c) * 9 + tap];
+    const float v = adjoint ? w[(c * CH + n) * 9 + (8 - tap)] : w[(n * CH + c) * 9 + tap];
     const int off = (n >> 3) * SBO + (k >> 3) * CORE_BYTES + (n & 7) * 16 + (k & 7) * 2;
     img[off / 2] = __float2bfloat16(v);
 }
@@ -681,8 +684,8 @@ cudaError_t conv32_tc(const __nv_bfloat16* x, const __nv_bfloat16* wpack, const 
     return conv32_launch<1>(x, wpack, bias, skip, mask, y, H, W, relu, err, s);
 }
 
-cudaError_t pack_w32(const float* w, __nv_bfloat16* img, cudaStream_t s) {
-    k_pack_w32<<<cdiv(CH * KDIM, 256), 256, 0, s>>>(w, img);
+cudaError_t pack_w32(const float* w, __nv_bfloat16* img, int adjoint, cudaStream_t s) {
+    k_pack_w32<<<cdiv(CH * KDIM, 256), 256, 0, s>>>(w, img, adjoint);
     return cudaGetLastError();
 }
 

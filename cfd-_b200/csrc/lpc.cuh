@@ -14,7 +14,7 @@ size_t conv32_smem_bytes(int rows);
 cudaError_t conv32_tc(const __nv_bfloat16* x, const __nv_bfloat16* wpack, const float* bias,
                       const __nv_bfloat16* skip, const uint8_t* mask, __nv_bfloat16* y, int H, int W, int relu,
                       int* err, cudaStream_t s);
-cudaError_t pack_w32(const float* w, __nv_bfloat16* img, cudaStream_t s);
+cudaError_t pack_w32(const float* w, __nv_bfloat16* img, int adjoint, cudaStream_t s);
 cudaError_t conv_generic(int cin, int cout, const void* x, int xbf, const float* w, const float* bias,
                          const uint8_t* mask, void* y, int ybf, int H, int W, int relu, int transposed,
                          cudaStream_t s);

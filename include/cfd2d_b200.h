@@ -466,6 +466,9 @@ int cfd2d_pressure_solve_static(const cfd2d_poisson* op, const double* rhs, doub
 size_t cfd2d_lpc_w32_bytes(void);
 /* Pack w[32][32][3][3] (float32, out x in x kh x kw) into the tensor-core image. */
 int cfd2d_lpc_pack_w32(const float* w, void* image, void* stream);
+/* Pack the data-gradient convolution of the same layer (channels swapped, taps
+ * mirrored): cfd2d_lpc_conv32 with this image maps dy to dx on the tensor cores. */
+int cfd2d_lpc_pack_w32_adjoint(const float* w, void* image, void* stream);
 /* y = act(conv3x3(x, w) + bias (+ skip)) masked; tcgen05 implicit GEMM. err: device
  * int set to 1 if the bounded wait for the accumulator gave up (may be NULL). */
 int cfd2d_lpc_conv32(const void* x, const void* image, const float* bias, const void* skip,

@@ -153,10 +153,13 @@ def test_network_forward_matches_torch(L):
     assert relerr(out, ref) < 3e-2
 
 
-def test_backward_kernels_match_autograd(L):
+@pytest.mark.parametrize("tc_dgrad", [True, False])
+def test_backward_kernels_match_autograd(L, tc_dgrad):
     """Every weight gradient of the hand-written backward kernels against PyTorch
-    autograd; 72 x 65 has five levels, so the shared deepest encoder and decoder
-    (applied twice on level 3 and below) are used and checked as well."""
+    autograd, with the data gradients of the 32->32 layers on the tensor cores (BF16
+    in and out) and on the CUDA cores (FP32); 72 x 65 has five levels, so the shared
+    deepest encoder and decoder (applied twice on level 3 and below) are used and
+    checked as well."""
     torch, _lib, learned = L
     H, W = 72, 65
     net = learned.LPCNet(seed=5)
@@ -166,7 +169,8 @@ def test_backward_kernels_match_autograd(L):
     x = (torch.randn((H, W), generator=g) * torch.from_numpy(mask)).float()
     dout = torch.randn((H, W), generator=g) * torch.from_numpy(mask)
     learned.net_forward(net, ws, x.to(_lib.device()).contiguous())
-    grads = learned.net_backward(net, ws, x.to(_lib.device()).contiguous(), dout.to(_lib.device()).contiguous())
+    grads = learned.net_backward(net, ws, x.to(_lib.device()).contiguous(), dout.to(_lib.device()).contiguous(),
+                                 tc_dgrad=tc_dgrad)
     # autograd on the CPU reference with leaf copies of the BF16-rounded weights
     masks = [m.cpu().float()[None, None] for m in ws.masks]
     saved = {k: (v.clone(), net.b[k].clone()) for k, v in net.w.items()}
