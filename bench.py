@@ -358,7 +358,8 @@ def stencil_roofline(peak: float, reps: int = 10) -> dict:
     diff = torch.full((nx + 2, ny + 2), 1e-3, dtype=torch.float64, device=dev)
     out = torch.zeros_like(phi)
     hu, hv = torch.zeros_like(u), torch.zeros_like(v)
-    nu = torch.full((1,), 1e-3, dtype=torch.float64, device=dev)
+    # a cell field, as the reference's; the constant-viscosity form reads nu[1, 1]
+    nu = torch.full((nx + 2, ny + 2), 1e-3, dtype=torch.float64, device=dev)
     bt = {k: torch.zeros(n, dtype=torch.int64, device=dev) for k, n in (("l", ny), ("r", ny), ("b", nx), ("t", nx))}
     bv = {k: torch.zeros(n, dtype=torch.float64, device=dev) for k, n in (("l", ny), ("r", ny), ("b", nx), ("t", nx))}
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)

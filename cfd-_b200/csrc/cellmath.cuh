@@ -3,9 +3,13 @@
 // Every function evaluates one face or one cell in exactly the operation order of
 // the reference (Python/Numba, IEEE float64, no fused multiply-add), so results
 // are bit-identical to cfd2d when compiled with -fmad=false (nvcc) or
-// -ffp-contract=off (host compilers). The functions are __host__ __device__: the
-// CUDA kernels call them per thread, and the test-only host build
-// (tests/hostemu) calls them in loops to check the arithmetic on a CPU.
+// -ffp-contract=off (host compilers). The functions are __host__ __device__ so that
+// host code can evaluate the same expressions.
+//
+// The stencil functions read their inputs through an accessor (by global face and
+// cell index): the *Arrays views read the reference's arrays in HBM, the transport
+// kernels' tile view reads a block's copy in shared memory. The arithmetic is
+// written once.
 //
 // Layout (reference cfd2d/grid.py:1-18): p-like and u arrays have row pitch
 // ny+2, v arrays ny+1; fluid flags (nx+2)(ny+2) bytes.
@@ -62,74 +66,92 @@ CFD_HD MomCoef mom_coef_inv(const InvSpacing& s, double gamma, double nu0) {
     return m;
 }
 
+// The arrays of the momentum stencil in the reference's layout. ue(i, j) is u on the
+// face east of face i, face 1 for i = nx (periodic; cfd2d/kernels.py:90).
+struct MomArrays {
+    const double *u, *v, *nu, *rho;
+    const uint8_t* fl;
+    Grid2 g;
+    CFD_HD bool f(int i, int j) const { return fl[g.c(i, j)] != 0; }
+    CFD_HD double U(int i, int j) const { return u[g.u(i, j)]; }
+    CFD_HD double ue(int i, int j) const { return u[g.u((i < g.nx) ? i + 1 : 1, j)]; }
+    CFD_HD double V(int i, int j) const { return v[g.v(i, j)]; }
+    CFD_HD double Nu(int i, int j) const { return nu[g.c(i, j)]; }
+    CFD_HD double Rho(int i, int j) const { return rho[g.c(i, j)]; }
+};
+
 // u-momentum tendency on face (i, j), i in 1..imax, j in 1..ny
 // (cfd2d/kernels.py:85-119). Returns 0 for faces not between two fluid cells.
-CFD_HD double mom_u(const double* u, const double* v, const uint8_t* fl, const double* nu,
-                    const double* rho, Grid2 g, const MomCoef& m, bool variable, bool var_density,
-                    int i, int j) {
-    if (!(fl[g.c(i, j)] && fl[g.c(i + 1, j)])) return 0.0;
-    const int ip = (i < g.nx) ? i + 1 : 1;
-    const double uc = u[g.u(i, j)], ue = u[g.u(ip, j)], uw = u[g.u(i - 1, j)];
-    const double un = u[g.u(i, j + 1)], us = u[g.u(i, j - 1)];
+template <class A>
+CFD_HD double mom_u_at(const A& a, const MomCoef& m, bool variable, bool var_density, int i, int j) {
+    if (!(a.f(i, j) && a.f(i + 1, j))) return 0.0;
+    const double uc = a.U(i, j), ue = a.ue(i, j), uw = a.U(i - 1, j);
+    const double un = a.U(i, j + 1), us = a.U(i, j - 1);
     double diff;
     if (variable) {
-        const double nu_e = nu[g.c(i + 1, j)];
-        const double nu_w = nu[g.c(i, j)];
-        const double nu_n = 0.25 * (((nu[g.c(i, j)] + nu[g.c(i + 1, j)]) + nu[g.c(i, j + 1)]) +
-                                    nu[g.c(i + 1, j + 1)]);
-        const double nu_s = 0.25 * (((nu[g.c(i, j)] + nu[g.c(i + 1, j)]) + nu[g.c(i, j - 1)]) +
-                                    nu[g.c(i + 1, j - 1)]);
-        const double vn = (v[g.v(i + 1, j)] - v[g.v(i, j)]) * m.idx;
-        const double vs = (v[g.v(i + 1, j - 1)] - v[g.v(i, j - 1)]) * m.idx;
+        const double nu_e = a.Nu(i + 1, j);
+        const double nu_w = a.Nu(i, j);
+        const double nu_n = 0.25 * (((a.Nu(i, j) + a.Nu(i + 1, j)) + a.Nu(i, j + 1)) + a.Nu(i + 1, j + 1));
+        const double nu_s = 0.25 * (((a.Nu(i, j) + a.Nu(i + 1, j)) + a.Nu(i, j - 1)) + a.Nu(i + 1, j - 1));
+        const double vn = (a.V(i + 1, j) - a.V(i, j)) * m.idx;
+        const double vs = (a.V(i + 1, j - 1) - a.V(i, j - 1)) * m.idx;
         diff = ((2.0 * nu_e) * (ue - uc) - (2.0 * nu_w) * (uc - uw)) * m.idx2 +
                m.idy * (nu_n * ((un - uc) * m.idy + vn) - nu_s * ((uc - us) * m.idy + vs));
     } else {
         diff = m.nu0 * (((ue - 2.0 * uc) + uw) * m.idx2 + ((un - 2.0 * uc) + us) * m.idy2);
     }
-    if (var_density) diff = diff / (0.5 * (rho[g.c(i, j)] + rho[g.c(i + 1, j)]));
+    if (var_density) diff = diff / (0.5 * (a.Rho(i, j) + a.Rho(i + 1, j)));
     const double a_e = 0.5 * (uc + ue);
     const double a_w = 0.5 * (uw + uc);
     const double du2dx = m.idx * (a_e * a_e - a_w * a_w) +
                          m.gx * ((fabs(a_e) * 0.5) * (uc - ue) - (fabs(a_w) * 0.5) * (uw - uc));
-    const double v_n = 0.5 * (v[g.v(i, j)] + v[g.v(i + 1, j)]);
-    const double v_s = 0.5 * (v[g.v(i, j - 1)] + v[g.v(i + 1, j - 1)]);
+    const double v_n = 0.5 * (a.V(i, j) + a.V(i + 1, j));
+    const double v_s = 0.5 * (a.V(i, j - 1) + a.V(i + 1, j - 1));
     const double duvdy = m.idy * ((v_n * 0.5) * (uc + un) - (v_s * 0.5) * (us + uc)) +
                          m.gy * ((fabs(v_n) * 0.5) * (uc - un) - (fabs(v_s) * 0.5) * (us - uc));
     return (diff - du2dx) - duvdy;
 }
 
 // v-momentum tendency on face (i, j), i in 1..nx, j in 1..ny-1 (cfd2d/kernels.py:122-155).
-CFD_HD double mom_v(const double* u, const double* v, const uint8_t* fl, const double* nu,
-                    const double* rho, Grid2 g, const MomCoef& m, bool variable, bool var_density,
-                    int i, int j) {
-    if (!(fl[g.c(i, j)] && fl[g.c(i, j + 1)])) return 0.0;
-    const double vc = v[g.v(i, j)], ve = v[g.v(i + 1, j)], vw = v[g.v(i - 1, j)];
-    const double vn = v[g.v(i, j + 1)], vs = v[g.v(i, j - 1)];
+template <class A>
+CFD_HD double mom_v_at(const A& a, const MomCoef& m, bool variable, bool var_density, int i, int j) {
+    if (!(a.f(i, j) && a.f(i, j + 1))) return 0.0;
+    const double vc = a.V(i, j), ve = a.V(i + 1, j), vw = a.V(i - 1, j);
+    const double vn = a.V(i, j + 1), vs = a.V(i, j - 1);
     double diff;
     if (variable) {
-        const double nu_n = nu[g.c(i, j + 1)];
-        const double nu_s = nu[g.c(i, j)];
-        const double nu_e = 0.25 * (((nu[g.c(i, j)] + nu[g.c(i + 1, j)]) + nu[g.c(i, j + 1)]) +
-                                    nu[g.c(i + 1, j + 1)]);
-        const double nu_w = 0.25 * (((nu[g.c(i, j)] + nu[g.c(i - 1, j)]) + nu[g.c(i, j + 1)]) +
-                                    nu[g.c(i - 1, j + 1)]);
-        const double ue_ = (u[g.u(i, j + 1)] - u[g.u(i, j)]) * m.idy;
-        const double uw_ = (u[g.u(i - 1, j + 1)] - u[g.u(i - 1, j)]) * m.idy;
+        const double nu_n = a.Nu(i, j + 1);
+        const double nu_s = a.Nu(i, j);
+        const double nu_e = 0.25 * (((a.Nu(i, j) + a.Nu(i + 1, j)) + a.Nu(i, j + 1)) + a.Nu(i + 1, j + 1));
+        const double nu_w = 0.25 * (((a.Nu(i, j) + a.Nu(i - 1, j)) + a.Nu(i, j + 1)) + a.Nu(i - 1, j + 1));
+        const double ue_ = (a.U(i, j + 1) - a.U(i, j)) * m.idy;
+        const double uw_ = (a.U(i - 1, j + 1) - a.U(i - 1, j)) * m.idy;
         diff = ((2.0 * nu_n) * (vn - vc) - (2.0 * nu_s) * (vc - vs)) * m.idy2 +
                m.idx * (nu_e * ((ve - vc) * m.idx + ue_) - nu_w * ((vc - vw) * m.idx + uw_));
     } else {
         diff = m.nu0 * (((ve - 2.0 * vc) + vw) * m.idx2 + ((vn - 2.0 * vc) + vs) * m.idy2);
     }
-    if (var_density) diff = diff / (0.5 * (rho[g.c(i, j)] + rho[g.c(i, j + 1)]));
+    if (var_density) diff = diff / (0.5 * (a.Rho(i, j) + a.Rho(i, j + 1)));
     const double b_n = 0.5 * (vc + vn);
     const double b_s = 0.5 * (vs + vc);
     const double dv2dy = m.idy * (b_n * b_n - b_s * b_s) +
                          m.gy * ((fabs(b_n) * 0.5) * (vc - vn) - (fabs(b_s) * 0.5) * (vs - vc));
-    const double u_e = 0.5 * (u[g.u(i, j)] + u[g.u(i, j + 1)]);
-    const double u_w = 0.5 * (u[g.u(i - 1, j)] + u[g.u(i - 1, j + 1)]);
+    const double u_e = 0.5 * (a.U(i, j) + a.U(i, j + 1));
+    const double u_w = 0.5 * (a.U(i - 1, j) + a.U(i - 1, j + 1));
     const double duvdx = m.idx * ((u_e * 0.5) * (vc + ve) - (u_w * 0.5) * (vw + vc)) +
                          m.gx * ((fabs(u_e) * 0.5) * (vc - ve) - (fabs(u_w) * 0.5) * (vw - vc));
     return (diff - duvdx) - dv2dy;
+}
+
+CFD_HD double mom_u(const double* u, const double* v, const uint8_t* fl, const double* nu,
+                    const double* rho, Grid2 g, const MomCoef& m, bool variable, bool var_density,
+                    int i, int j) {
+    return mom_u_at(MomArrays{u, v, nu, rho, fl, g}, m, variable, var_density, i, j);
+}
+CFD_HD double mom_v(const double* u, const double* v, const uint8_t* fl, const double* nu,
+                    const double* rho, Grid2 g, const MomCoef& m, bool variable, bool var_density,
+                    int i, int j) {
+    return mom_v_at(MomArrays{u, v, nu, rho, fl, g}, m, variable, var_density, i, j);
 }
 
 // New value of u face (i, j) after the obstacle condition (cfd2d/kernels.py:170-187);
@@ -189,40 +211,61 @@ struct ScalarBCView {
     const double* bv[4];
 };
 
-// Flux F through interior x face with index fi joining cells L (west) and R (east)
-// (cfd2d/kernels.py:304-330). Both cells are fluid.
-CFD_HD double xflux(const double* phi, const double* u, const uint8_t* fl, const double* diff,
-                    Grid2 g, double dx, int limiter_kind, bool periodic, int fi, int L, int R,
-                    int j) {
-    const double uf = u[g.u(fi, j)];
+// The cell arrays the interior transport fluxes read, in the reference's layout.
+struct TransportArrays {
+    const double* phi;
+    const uint8_t* fl;
+    const double* diff;
+    Grid2 g;
+    CFD_HD double ph(int i, int j) const { return phi[g.c(i, j)]; }
+    CFD_HD bool f(int i, int j) const { return fl[g.c(i, j)] != 0; }
+    CFD_HD double d(int i, int j) const { return diff[g.c(i, j)]; }
+};
+
+// Flux F through an interior x face with velocity uf joining cells L (west) and R
+// (east) (cfd2d/kernels.py:304-330). Both cells are fluid.
+template <class A>
+CFD_HD double xflux_at(const A& a, double uf, int nx, double dx, int limiter_kind, bool periodic, int L, int R,
+                       int j) {
     int C, D, Ui;
     if (uf >= 0.0) {
         C = L; D = R; Ui = L - 1;
-        if (Ui < 1) Ui = periodic ? g.nx : -1;
+        if (Ui < 1) Ui = periodic ? nx : -1;
     } else {
         C = R; D = L; Ui = R + 1;
-        if (Ui > g.nx) Ui = periodic ? 1 : -1;
+        if (Ui > nx) Ui = periodic ? 1 : -1;
     }
-    const bool has_u = Ui >= 1 && fl[g.c(Ui, j)];
-    const double phu = has_u ? phi[g.c(Ui, j)] : 0.0;
-    const double phf = face_value(phu, phi[g.c(C, j)], phi[g.c(D, j)], has_u, limiter_kind);
-    const double df = harmonic(diff[g.c(L, j)], diff[g.c(R, j)]);
-    return uf * phf - (df * (phi[g.c(R, j)] - phi[g.c(L, j)])) / dx;
+    const bool has_u = Ui >= 1 && a.f(Ui, j);
+    const double phu = has_u ? a.ph(Ui, j) : 0.0;
+    const double phf = face_value(phu, a.ph(C, j), a.ph(D, j), has_u, limiter_kind);
+    const double df = harmonic(a.d(L, j), a.d(R, j));
+    return uf * phf - (df * (a.ph(R, j) - a.ph(L, j))) / dx;
 }
 
-// Flux through interior y face j joining cells B = j (south) and T = j + 1.
-CFD_HD double yflux(const double* phi, const double* v, const uint8_t* fl, const double* diff,
-                    Grid2 g, double dy, int limiter_kind, int i, int B) {
+// Flux through the interior y face with velocity vf joining cells B (south) and
+// T = B + 1 of row i (cfd2d/kernels.py:361-383).
+template <class A>
+CFD_HD double yflux_at(const A& a, double vf, int ny, double dy, int limiter_kind, int i, int B) {
     const int T = B + 1;
-    const double vf = v[g.v(i, B)];
     int C, D, Uj;
     if (vf >= 0.0) { C = B; D = T; Uj = B - 1; }
     else { C = T; D = B; Uj = T + 1; }
-    const bool has_u = Uj >= 1 && Uj <= g.ny && fl[g.c(i, Uj)];
-    const double phu = has_u ? phi[g.c(i, Uj)] : 0.0;
-    const double phf = face_value(phu, phi[g.c(i, C)], phi[g.c(i, D)], has_u, limiter_kind);
-    const double df = harmonic(diff[g.c(i, B)], diff[g.c(i, T)]);
-    return vf * phf - (df * (phi[g.c(i, T)] - phi[g.c(i, B)])) / dy;
+    const bool has_u = Uj >= 1 && Uj <= ny && a.f(i, Uj);
+    const double phu = has_u ? a.ph(i, Uj) : 0.0;
+    const double phf = face_value(phu, a.ph(i, C), a.ph(i, D), has_u, limiter_kind);
+    const double df = harmonic(a.d(i, B), a.d(i, T));
+    return vf * phf - (df * (a.ph(i, T) - a.ph(i, B))) / dy;
+}
+
+// The same fluxes on the arrays in HBM, the x face with index fi
+CFD_HD double xflux(const double* phi, const double* u, const uint8_t* fl, const double* diff,
+                    Grid2 g, double dx, int limiter_kind, bool periodic, int fi, int L, int R,
+                    int j) {
+    return xflux_at(TransportArrays{phi, fl, diff, g}, u[g.u(fi, j)], g.nx, dx, limiter_kind, periodic, L, R, j);
+}
+CFD_HD double yflux(const double* phi, const double* v, const uint8_t* fl, const double* diff,
+                    Grid2 g, double dy, int limiter_kind, int i, int B) {
+    return yflux_at(TransportArrays{phi, fl, diff, g}, v[g.v(i, B)], g.ny, dy, limiter_kind, i, B);
 }
 
 // Boundary inflow term for a domain face (cfd2d/kernels.py:278-302, 338-359):

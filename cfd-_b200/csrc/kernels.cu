@@ -30,18 +30,49 @@ __device__ __forceinline__ bool v_fluid(const cfd2d_sim& S, Grid2 g, int i, int 
 // that the stencil rows a block reads are shared through L1 by its warps
 constexpr int kTileX = 32, kTileY = 8;
 
+// A block's copy of phi, diff and the fluid flags for the transport stencil: rows
+// ib - 2 .. ib + TY + 1 and columns j0 - 2 .. j0 + kTileX + 1, every cell an interior
+// face flux of the tile or its upwind neighbour reads. Periodic in x, the rows beyond
+// 1..nx hold the rows they wrap to, so a wrapped index (L = nx for the face of cell 1,
+// the upwind cell nx or 1) may be looked up at any of its copies; otherwise cells
+// outside the grid hold 0 and are never read.
+template <int TY>
+struct TransportStage {
+    static constexpr int kR = TY + 4, kC = kTileX + 4;
+    double phi[kR][kC];
+    double diff[kR][kC];
+    uint8_t fl[kR][kC];
+};
+
+// TransportArrays' interface (cellmath.cuh) on a TransportStage
+template <int TY>
+struct TransportTileView {
+    const TransportStage<TY>* s;
+    int ib, j0, nx;
+    __device__ __forceinline__ int r(int i) const {
+        int d = i - ib + 2;
+        if (d < 0) d += nx;
+        else if (d >= TransportStage<TY>::kR) d -= nx;
+        return d;
+    }
+    __device__ __forceinline__ int c(int j) const { return j - j0 + 2; }
+    __device__ __forceinline__ double ph(int i, int j) const { return s->phi[r(i)][c(j)]; }
+    __device__ __forceinline__ bool f(int i, int j) const { return s->fl[r(i)][c(j)] != 0; }
+    __device__ __forceinline__ double d(int i, int j) const { return s->diff[r(i)][c(j)]; }
+};
+
 // TVD transport (cfd2d/kernels.py:271-391) of the (kTileY * ROWS) x kTileX cells of
 // one block, every interior face flux computed once and shared by its two cells.
-// Thread (tx, ty) takes cells (i0 + ty + kTileY r, j0 + tx), r < ROWS, so each warp
-// stays on one row and its loads stay coalesced; all ROWS face fluxes of a thread are
-// computed before the block synchronises, which puts ROWS independent chains of
-// (data-dependent) loads in flight per thread. FX[q][c] holds xflux/dx of the west
-// face of cell (i0 + q, j0 + c) (row kTileY ROWS: the east face of the tile's last
-// row, which is also the periodic face nx -> 1); FY[q][c] holds yflux/dy of the south
-// face of cell (i0 + q, j0 + c). Each cell then assembles ((west + east) + south) +
-// north exactly as transport_cell does, with -FX / -FY for its east and north faces,
-// so the result is bit-identical. Every thread of the block must call it (it
-// synchronises the block); out[r] receives the value of its row r.
+// Thread (tx, ty) takes cells (ib + ty + kTileY r, j0 + tx), r < ROWS. The block first
+// loads its tile of phi, diff and the flags with halo into shared memory (independent,
+// coalesced loads; the upwind reads, whose addresses depend on the face velocity,
+// then hit shared memory), each thread its face velocities into registers. FX[q][c]
+// holds xflux/dx of the west face of cell (ib + q, j0 + c) (row kTileY ROWS: the east
+// face of the tile's last row, which is also the periodic face nx -> 1); FY[q][c]
+// holds yflux/dy of the south face of cell (ib + q, j0 + c). Each cell then assembles
+// ((west + east) + south) + north exactly as transport_cell does, with -FX / -FY for
+// its east and north faces, so the result is bit-identical. Every thread of the block
+// must call it (it synchronises the block); res[r] receives the value of its row r.
 template <int ROWS>
 __device__ __forceinline__ void transport_tile(const double* __restrict__ phi, const double* __restrict__ u,
                                                const double* __restrict__ v, const uint8_t* __restrict__ fl,
@@ -49,40 +80,91 @@ __device__ __forceinline__ void transport_tile(const double* __restrict__ phi, c
                                                int lim, bool periodic, const ScalarBCView& bc, int obs_t,
                                                double obs_v, double (&res)[ROWS]) {
     constexpr int TY = kTileY * ROWS;
+    using Stage = TransportStage<TY>;
+    __shared__ Stage st;
     __shared__ double FX[TY + 1][kTileX];
     __shared__ double FY[TY][kTileX + 1];
     const int nx = g.nx, ny = g.ny;
     const int tx = threadIdx.x, ty = threadIdx.y;
-    const int j = blockIdx.x * kTileX + tx;
+    const int j0 = blockIdx.x * kTileX;
+    const int j = j0 + tx;
     const int ib = blockIdx.y * TY;
     const bool jin = (j >= 1 && j <= ny);
-    // west face of cell ii (1 <= ii <= nx + 1); the domain faces are not shared
-    auto west = [&](int ii) -> double {
-        int L, R, fi;
-        if (ii == 1 || ii == nx + 1) {
-            if (!periodic) return 0.0;
-            L = nx; R = 1; fi = nx;
-        } else {
-            L = ii - 1; R = ii; fi = ii - 1;
+    // x face index of the west face of cell ii (1 <= ii <= nx + 1; periodic: the
+    // domain faces are face nx), -1 for a domain face without flux
+    auto west_face = [&](int ii) -> int {
+        if (ii == 1 || ii == nx + 1) return periodic ? nx : -1;
+        return ii - 1;
+    };
+    // this thread's face velocities
+    double uW[ROWS], vS[ROWS], vN[ROWS], uE = 0.0;
+#pragma unroll
+    for (int r = 0; r < ROWS; ++r) {
+        const int q = ty + kTileY * r;
+        const int i = ib + q;
+        uW[r] = 0.0;
+        vS[r] = 0.0;
+        vN[r] = 0.0;
+        if (jin && i >= 1 && i <= nx + 1) {
+            const int fi = west_face(i);
+            if (fi >= 0) uW[r] = u[g.u(fi, j)];
+            if (q == TY - 1 && i + 1 <= nx + 1) {
+                const int fe = west_face(i + 1);
+                if (fe >= 0) uE = u[g.u(fe, j)];
+            }
         }
-        if (!(fl[g.c(L, j)] && fl[g.c(R, j)])) return 0.0;
-        return xflux(phi, u, fl, diff, g, dx, lim, periodic, fi, L, R, j) / dx;
+        if (i >= 1 && i <= nx && j >= 2 && j <= ny) vS[r] = v[g.v(i, j - 1)];
+        if (tx == kTileX - 1 && i >= 1 && i <= nx && j + 1 >= 2 && j + 1 <= ny) vN[r] = v[g.v(i, j)];
+    }
+    // the tile with its halo
+    {
+        constexpr int kN = Stage::kR * Stage::kC;
+        const int tid = ty * kTileX + tx;
+#pragma unroll 4
+        for (int k = tid; k < kN; k += kTileX * kTileY) {
+            const int lr = k / Stage::kC, lc = k - lr * Stage::kC;
+            int gi = ib - 2 + lr;
+            const int gj = j0 - 2 + lc;
+            if (periodic && (gi < 1 || gi > nx)) gi = ((gi - 1) % nx + nx) % nx + 1;
+            double a = 0.0, b = 0.0;
+            uint8_t f = 0;
+            if (gi >= 0 && gi <= nx + 1 && gj >= 0 && gj <= ny + 1) {
+                a = phi[g.c(gi, gj)];
+                b = diff[g.c(gi, gj)];
+                f = fl[g.c(gi, gj)];
+            }
+            st.phi[lr][lc] = a;
+            st.diff[lr][lc] = b;
+            st.fl[lr][lc] = f;
+        }
+    }
+    __syncthreads();
+    const TransportTileView<TY> a{&st, ib, j0, nx};
+    auto west = [&](int ii, double uf) -> double {
+        int L, R;
+        if (ii == 1 || ii == nx + 1) {
+            L = nx; R = 1;
+        } else {
+            L = ii - 1; R = ii;
+        }
+        if (!(a.f(L, j) && a.f(R, j))) return 0.0;
+        return xflux_at(a, uf, nx, dx, lim, periodic, L, R, j) / dx;
     };
     // south face of cell (ii, jj) (2 <= jj <= ny)
-    auto south = [&](int ii, int jj) -> double {
-        if (!(fl[g.c(ii, jj - 1)] && fl[g.c(ii, jj)])) return 0.0;
-        return yflux(phi, v, fl, diff, g, dy, lim, ii, jj - 1) / dy;
+    auto south = [&](int ii, int jj, double vf) -> double {
+        if (!(a.f(ii, jj - 1) && a.f(ii, jj))) return 0.0;
+        return yflux_at(a, vf, ny, dy, lim, ii, jj - 1) / dy;
     };
 #pragma unroll
     for (int r = 0; r < ROWS; ++r) {
         const int q = ty + kTileY * r;
         const int i = ib + q;
         if (jin && i >= 1 && i <= nx + 1) {
-            FX[q][tx] = west(i);
-            if (q == TY - 1 && i + 1 <= nx + 1) FX[TY][tx] = west(i + 1);
+            FX[q][tx] = (west_face(i) >= 0) ? west(i, uW[r]) : 0.0;
+            if (q == TY - 1 && i + 1 <= nx + 1) FX[TY][tx] = (west_face(i + 1) >= 0) ? west(i + 1, uE) : 0.0;
         }
-        if (i >= 1 && i <= nx && j >= 2 && j <= ny) FY[q][tx] = south(i, j);
-        if (tx == kTileX - 1 && i >= 1 && i <= nx && j + 1 >= 2 && j + 1 <= ny) FY[q][kTileX] = south(i, j + 1);
+        if (i >= 1 && i <= nx && j >= 2 && j <= ny) FY[q][tx] = south(i, j, vS[r]);
+        if (tx == kTileX - 1 && i >= 1 && i <= nx && j + 1 >= 2 && j + 1 <= ny) FY[q][kTileX] = south(i, j + 1, vN[r]);
     }
     __syncthreads();
 #pragma unroll
@@ -90,34 +172,34 @@ __device__ __forceinline__ void transport_tile(const double* __restrict__ phi, c
         const int q = ty + kTileY * r;
         const int i = ib + q;
         res[r] = 0.0;
-        if (!(jin && i >= 1 && i <= nx) || !fl[g.c(i, j)]) continue;
-        const double phP = phi[g.c(i, j)];
-        const double DP = diff[g.c(i, j)];
+        if (!(jin && i >= 1 && i <= nx) || !a.f(i, j)) continue;
+        const double phP = a.ph(i, j);
+        const double DP = a.d(i, j);
         double xw = 0.0, xe = 0.0, ys = 0.0, yn = 0.0;
         if (i == 1 && !periodic) {
             xw = boundary_term(u[g.u(0, j)], phP, DP, bc.bt[0][j - 1], bc.bv[0][j - 1], dx);
         } else {
             const int L = (i == 1) ? nx : i - 1;
-            if (fl[g.c(L, j)]) xw = FX[q][tx];
+            if (a.f(L, j)) xw = FX[q][tx];
             else if (obs_t == 1) xw = ((DP * (obs_v - phP)) / (0.5 * dx)) / dx;
         }
         if (i == nx && !periodic) {
             xe = boundary_term(-u[g.u(nx, j)], phP, DP, bc.bt[1][j - 1], bc.bv[1][j - 1], dx);
         } else {
             const int R = (i == nx) ? 1 : i + 1;
-            if (fl[g.c(R, j)]) xe = -FX[q + 1][tx];
+            if (a.f(R, j)) xe = -FX[q + 1][tx];
             else if (obs_t == 1) xe = ((DP * (obs_v - phP)) / (0.5 * dx)) / dx;
         }
         if (j == 1) {
             ys = boundary_term(v[g.v(i, 0)], phP, DP, bc.bt[2][i - 1], bc.bv[2][i - 1], dy);
         } else {
-            if (fl[g.c(i, j - 1)]) ys = FY[q][tx];
+            if (a.f(i, j - 1)) ys = FY[q][tx];
             else if (obs_t == 1) ys = ((DP * (obs_v - phP)) / (0.5 * dy)) / dy;
         }
         if (j == ny) {
             yn = boundary_term(-v[g.v(i, ny)], phP, DP, bc.bt[3][i - 1], bc.bv[3][i - 1], dy);
         } else {
-            if (fl[g.c(i, j + 1)]) yn = -FY[q][tx + 1];
+            if (a.f(i, j + 1)) yn = -FY[q][tx + 1];
             else if (obs_t == 1) yn = ((DP * (obs_v - phP)) / (0.5 * dy)) / dy;
         }
         res[r] = ((xw + xe) + ys) + yn;
@@ -125,7 +207,7 @@ __device__ __forceinline__ void transport_tile(const double* __restrict__ phi, c
 }
 
 // rows per thread of the transport tile
-constexpr int kTransportRows = 4;
+constexpr int kTransportRows = 2;
 
 // Inputs and outputs never alias (the C ABI requires it): __restrict__ lets the
 // compiler issue every stencil load of a thread before its stores.

@@ -257,7 +257,8 @@ typedef struct cfd2d_sim {
 /* ---- kernel-level entry points (drop-in for cfd2d/kernels.py) ------------ */
 
 /* hu, hv = diffusion - convection on fluid faces; zero elsewhere. hu and hv must
- * not overlap any input array.
+ * not overlap any input array. nu is a cell field of (nx+2)*(ny+2) doubles, as the
+ * reference's; with variable = 0 only nu[1][1] is read.
  * Replaces cfd2d/kernels.py:44-46 momentum_tendencies(u, v, fluid, nx, ny, dx,
  * dy, nu, variable, gamma, periodic, hu, hv, rho, var_density). */
 int cfd2d_momentum_tendencies(const double* u, const double* v, const uint8_t* fluid, int nx,

@@ -275,6 +275,45 @@ def test_trained_network_reduces_iterations(L):
         fcg.close()
 
 
+def test_learned_solve_is_faster_on_the_1024x512_obstacle_flow(L):
+    """The time the shipped network gains: one pressure system of the seeded 1024x512
+    obstacle flow (its fourth step, from the previous step's pressure) solved to 1e-8 by
+    the plain Jacobi-PCG and by flexible CG with the learned preconditioner, each timed
+    with CUDA events after one untimed solve of the same system. The learned solve must
+    converge without falling back and take at most 85 % of the plain solve's time."""
+    torch, _lib, learned = L
+    from cfd2d_b200 import cases
+
+    sim = cases.obstacle_flow(13, 1024, 512, pressure_solver="cg").sim
+    ps = sim.pressure
+    ps.tol = 1e-8
+    sim.advance(3)
+    xprev = ps._d_x0.clone()
+    sim.advance(1)
+    g = sim.grid
+    F, G = sim.F, sim.G
+    rhs = torch.from_numpy(((F[1:, 1:-1] - F[:-1, 1:-1]) / g.dx + (G[1:-1, 1:] - G[1:-1, :-1]) / g.dy)
+                           / sim.dt).cuda()
+    fcg = learned.LearnedPCG(ps, learned.pretrained())
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ms, sol = {}, {}
+    for name, solve in (("plain", lambda: ps.solve(rhs)), ("learned", lambda: fcg.solve(rhs))):
+        for _timed in (False, True):
+            ps._d_x0.copy_(xprev)
+            torch.cuda.synchronize()
+            ev[0].record()
+            out = solve()
+            ev[1].record()
+            torch.cuda.synchronize()
+        ms[name] = ev[0].elapsed_time(ev[1])
+        sol[name] = np.asarray(out.cpu() if hasattr(out, "cpu") else out)
+    assert fcg.last_reason == _lib.FCG_CONVERGED, (fcg.last_reason, fcg.last_iterations)
+    assert fcg.last_total_iterations < 0.1 * ps.last_iterations, (fcg.last_total_iterations, ps.last_iterations)
+    assert ms["learned"] <= 0.85 * ms["plain"], ms
+    assert relerr(sol["learned"], sol["plain"]) < 1e-4
+    fcg.close()
+
+
 def test_learned_pressure_solve_inside_the_step(L):
     """Simulation.set_pressure_preconditioner: the same steps from the same state
     with the plain and the learned pressure solve agree to the solver tolerance."""
