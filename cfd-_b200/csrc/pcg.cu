@@ -829,6 +829,7 @@ namespace {
 // per SM (84 -> 54 us per iteration at 2048 x 1024 against 256 x 2 at 108 registers).
 constexpr int kGridThreads = 512;
 constexpr int kGridMinBlocks = 2;
+constexpr int kGridUnroll = 2;  // cells a thread of the workspace solver has in flight
 constexpr int kClusterL2Threads = 512;  // one 16-CTA cluster, vectors in global memory
 
 struct GridWork {
@@ -1162,26 +1163,38 @@ __global__ void __launch_bounds__(CL ? kClusterL2Threads : kGridThreads, CL ? 1 
             const double* Po = cur ? W.P0 : W.P1;
             const bool first = (it == 0);
             double pq = 0.0;
-            for (int c = c0 + tid; c < c1; c += TPB) {
-                const uint8_t nb = op.nbr[c];
-                if (!(nb & 0x80)) continue;
-                const RowPos rp = row_pos(c, n, ny, nx);
-#define PNEWG(idx) (first ? (op.dinv[idx] * R[idx]) : (Po[idx] * beta + op.dinv[idx] * R[idx]))
-                const double pC = PNEWG(c);
-                double tW = 0.0, tS = 0.0, tN = 0.0, tE = 0.0;
-                double kS = mdy2, kN = mdy2, kW = mdx2, kE = mdx2;
-                if constexpr (VAR) {
-                    const Coef<true> k(op, c / ny, c % ny);
-                    kS = k.s; kN = k.n; kW = k.w; kE = k.e;
-                }
-                if (nb & 2) tS = kS * PNEWG(c - 1);
-                if (nb & 4) tN = kN * PNEWG(c + 1);
-                if (nb & 1) tW = kW * PNEWG(rp.w);
-                if (nb & 8) tE = kE * PNEWG(rp.e);
+            {
+                // the vectors never alias: the loads of the next cells may pass this
+                // cell's store (several cells' loads in flight per thread)
+                const double* __restrict__ po = Po;
+                double* __restrict__ pn = Pn;
+                const double* __restrict__ rv = R;
+                const double* __restrict__ dv = op.dinv;
+                const double* __restrict__ dg = op.diag;
+                const uint8_t* __restrict__ nbr = op.nbr;
+#pragma unroll(kGridUnroll)
+                for (int c = c0 + tid; c < c1; c += TPB) {
+                    const uint8_t nb = nbr[c];
+                    if (nb & 0x80) {
+                        const RowPos rp = row_pos(c, n, ny, nx);
+#define PNEWG(idx) (first ? (dv[idx] * rv[idx]) : (po[idx] * beta + dv[idx] * rv[idx]))
+                        const double pC = PNEWG(c);
+                        double tW = 0.0, tS = 0.0, tN = 0.0, tE = 0.0;
+                        double kS = mdy2, kN = mdy2, kW = mdx2, kE = mdx2;
+                        if constexpr (VAR) {
+                            const Coef<true> k(op, c / ny, c % ny);
+                            kS = k.s; kN = k.n; kW = k.w; kE = k.e;
+                        }
+                        if (nb & 2) tS = kS * PNEWG(c - 1);
+                        if (nb & 4) tN = kN * PNEWG(c + 1);
+                        if (nb & 1) tW = kW * PNEWG(rp.w);
+                        if (nb & 8) tE = kE * PNEWG(rp.e);
 #undef PNEWG
-                const double qq = row_sum(op.periodic != 0, rp.row, nx, tW, tS, op.diag[c] * pC, tN, tE);
-                Pn[c] = pC;
-                pq += pC * qq;
+                        const double qq = row_sum(op.periodic != 0, rp.row, nx, tW, tS, dg[c] * pC, tN, tE);
+                        pn[c] = pC;
+                        pq += pC * qq;
+                    }
+                }
             }
             {
                 double v[1] = {pq};
@@ -1190,15 +1203,25 @@ __global__ void __launch_bounds__(CL ? kClusterL2Threads : kGridThreads, CL ? 1 
             }
             const double alpha = rho / pq;
             double v2[2] = {0.0, 0.0};
-            for (int c = c0 + tid; c < c1; c += TPB) {
-                const uint8_t nb = op.nbr[c];
-                if (!(nb & 0x80)) continue;
-                const double qq = apply_A_at<VAR>(op, Pn, c, row_pos(c, n, ny, nx), nb, op.diag[c]);
-                X[c] = X[c] + alpha * Pn[c];
-                const double r = R[c] - alpha * qq;
-                R[c] = r;
-                v2[0] += r * r;
-                v2[1] += r * (op.dinv[c] * r);
+            {
+                const double* __restrict__ pn = Pn;
+                double* __restrict__ xv = X;
+                double* __restrict__ rv = R;
+                const double* __restrict__ dv = op.dinv;
+                const double* __restrict__ dg = op.diag;
+                const uint8_t* __restrict__ nbr = op.nbr;
+#pragma unroll(kGridUnroll)
+                for (int c = c0 + tid; c < c1; c += TPB) {
+                    const uint8_t nb = nbr[c];
+                    if (nb & 0x80) {
+                        const double qq = apply_A_at<VAR>(op, pn, c, row_pos(c, n, ny, nx), nb, dg[c]);
+                        xv[c] = xv[c] + alpha * pn[c];
+                        const double r = rv[c] - alpha * qq;
+                        rv[c] = r;
+                        v2[0] += r * r;
+                        v2[1] += r * (dv[c] * r);
+                    }
+                }
             }
             if (L.snap) {
                 const int k = (it + 1) / L.snap_every;
