@@ -824,13 +824,20 @@ def load_weights(path, net: LPCNet | None = None) -> LPCNet:
 
 
 def pretrained():
-    """The shipped network (``data/lpc_weights.npz``), trained by ``train`` on the
+    """The shipped network (``data/lpc_weights.npz``). First trained by ``train`` on the
     "channel" recipe: residuals of the plain Jacobi-PCG's iterates on 60 seeded
     obstacle flows of the generator at 256 x 128 and 20 at 512 x 256 (the benchmark's
-    2 x 1 channel, square cells), 6000 Adam steps; then one on-policy round: the
-    residuals the flexible CG with the trained network meets on the same cases are
-    added (about 2.4k) and training goes on for 3000 steps at half the learning rate.
-    ``python -m cfd2d_b200.learned train OUT.npz`` reproduces it (its defaults)."""
+    2 x 1 channel, square cells), 6000 Adam steps, then one on-policy round (the
+    residuals the flexible CG with the trained network meets on the same cases, about
+    2.4k, added; 3000 more steps at half the learning rate):
+    ``python -m cfd2d_b200.learned train OUT.npz --cases 60``. Then fine-tuned by
+    ``finetune`` on larger grids, where the deeper levels of the U-Net first meet real
+    data: 20 channel-recipe cases replayed plus 3 seeded obstacle flows each at
+    1024 x 512 and 2048 x 1024 (their plain iterates' residuals), one round of the
+    flexible CG's own residuals, 2000 steps at 2e-4 (``finetune A.npz``); then from
+    that, 4 flows per size, two such rounds (``finetune B.npz --init A.npz --cases 4
+    --rounds 2 --seed 200``). The benchmark's flow (generator seed 13) is held out of
+    every set."""
     from pathlib import Path
 
     return load_weights(Path(__file__).resolve().parent / "data" / "lpc_weights.npz")
@@ -853,7 +860,9 @@ def harvest_recipe(cases: int = 50, snaps: int = 100, seed: int = 0, kind: str =
 
 def main(argv=None):
     """python -m cfd2d_b200.learned train OUT.npz [options]: harvest residuals, train,
-    save the weights. python -m cfd2d_b200.learned apply NX NY [--reps N]: one
+    save the weights. python -m cfd2d_b200.learned finetune OUT.npz [options]: go on
+    training a network (the shipped one by default) with residuals of larger obstacle
+    flows added, the flexible CG's own among them. python -m cfd2d_b200.learned apply NX NY [--reps N]: one
     obstacle flow (generator seed 13) of NX x NY, N applications of the shipped
     network's preconditioner, event-timed (the command the network's profiles use)."""
     import argparse
@@ -872,6 +881,18 @@ def main(argv=None):
     tr.add_argument("--recipe", choices=["channel", "mixed"], default="channel")
     tr.add_argument("--arch", default="{}", help="JSON overrides of the architecture (e.g. '{\"nrep\": 1}')")
     tr.add_argument("--onpolicy", type=int, default=1,
+                    help="rounds of adding the flexible CG's own residuals and training on")
+    ft = sub.add_parser("finetune")
+    ft.add_argument("out")
+    ft.add_argument("--init", default="", help="weights to start from (default: the shipped network)")
+    ft.add_argument("--sizes", default="1024x512,2048x1024", help="grids of the added obstacle flows")
+    ft.add_argument("--cases", type=int, default=3, help="seeded obstacle flows per size")
+    ft.add_argument("--replay", type=int, default=20, help="cases of the channel recipe kept in the set")
+    ft.add_argument("--steps", type=int, default=2000)
+    ft.add_argument("--batch", type=int, default=4)
+    ft.add_argument("--lr", type=float, default=2e-4)
+    ft.add_argument("--seed", type=int, default=100)
+    ft.add_argument("--rounds", type=int, default=1,
                     help="rounds of adding the flexible CG's own residuals and training on")
     apl = sub.add_parser("apply")
     apl.add_argument("nx", type=int)
@@ -892,6 +913,25 @@ def main(argv=None):
             print(f"round {rnd + 1}: {len(R)} residuals of the flexible CG added ({len(data)} in all)", flush=True)
             log = train(net, data, steps=a.steps // 2, batch=a.batch, lr=a.lr / 2, seed=a.seed + rnd + 1,
                         log_every=500)
+            print(f"steps {len(log)} loss last {np.mean(log[-50:]):.4f}", flush=True)
+        save_weights(net, a.out)
+        return
+    if a.cmd == "finetune":
+        t0 = time.time()
+        net = load_weights(a.init) if a.init else pretrained()
+        data = harvest_recipe(cases=a.replay, snaps=50, seed=a.seed, kind="channel")
+        for k, size in enumerate(a.sizes.split(",")):
+            nx, ny = (int(v) for v in size.lower().split("x"))
+            # seeds apart from the benchmark's generator seed (13), which stays held out
+            big = harvest_residuals(n_cases=a.cases, nx=nx, ny=ny, seed=a.seed + 3000 + k, every=max(8, nx // 10),
+                                    max_snaps=40)
+            data = data.merge(big)
+        print(f"residuals {len(data)} from {len(data.solvers)} cases in {time.time() - t0:.0f}s", flush=True)
+        for rnd in range(a.rounds):
+            R, co = harvest_fcg_residuals(net, data)
+            data = data.with_samples(R, co)
+            print(f"round {rnd + 1}: {len(R)} residuals of the flexible CG added ({len(data)} in all)", flush=True)
+            log = train(net, data, steps=a.steps, batch=a.batch, lr=a.lr, seed=a.seed + rnd, log_every=500)
             print(f"steps {len(log)} loss last {np.mean(log[-50:]):.4f}", flush=True)
         save_weights(net, a.out)
         return
