@@ -24,7 +24,7 @@ learned   = the same workload with the pressure solved by flexible CG with the
 single_reduction = the headline workload with the slab solver's single-reduction
             form (one grid reduction per CG iteration instead of scipy's two).
 batch_64_cavities = 64 seeded uneven cavities stepped together against the per-case loop.
-sst_channel_mixed_precision = the k-omega SST channel 128 x 192 over 2000 steps with the FP64 and the
+sst_channel_mixed_precision = the k-omega SST channel 128 x 192 over 5000 steps with the FP64 and the
             mixed-precision solver: time and the mixed run's error in the u profile, nu_t, tau_w, c_f.
 grid_2048x1024 = the same generator and seed at 2048 x 1024: plain steps and the
             Poisson comparison (the CG cap is raised so that both reach 1e-8).
@@ -801,7 +801,7 @@ def sst_channel_sim(precision: str = "fp64"):
     return sim
 
 
-def sst_mixed_section(steps: int = 2000) -> dict:
+def sst_mixed_section(steps: int = 5000) -> dict:
     """The SST channel over ``steps`` steps with the FP64 pressure solver and with the
     mixed one (FP32 CG iterations, FP64 refinement and reductions): ms per step, and
     the mixed run's error against the FP64 run (which follows the reference's CPU run
