@@ -44,15 +44,18 @@ struct TransportStage {
     uint8_t fl[kR][kC];
 };
 
-// TransportArrays' interface (cellmath.cuh) on a TransportStage
-template <int TY>
+// TransportArrays' interface (cellmath.cuh) on a TransportStage; only a periodic grid
+// has wrapped row indices to map back into the tile
+template <int TY, bool PERIODIC>
 struct TransportTileView {
     const TransportStage<TY>* s;
     int ib, j0, nx;
     __device__ __forceinline__ int r(int i) const {
         int d = i - ib + 2;
-        if (d < 0) d += nx;
-        else if (d >= TransportStage<TY>::kR) d -= nx;
+        if constexpr (PERIODIC) {
+            if (d < 0) d += nx;
+            else if (d >= TransportStage<TY>::kR) d -= nx;
+        }
         return d;
     }
     __device__ __forceinline__ int c(int j) const { return j - j0 + 2; }
@@ -73,13 +76,14 @@ struct TransportTileView {
 // ((west + east) + south) + north exactly as transport_cell does, with -FX / -FY for
 // its east and north faces, so the result is bit-identical. Every thread of the block
 // must call it (it synchronises the block); res[r] receives the value of its row r.
-template <int ROWS>
+template <int ROWS, bool PERIODIC>
 __device__ __forceinline__ void transport_tile(const double* __restrict__ phi, const double* __restrict__ u,
                                                const double* __restrict__ v, const uint8_t* __restrict__ fl,
                                                const double* __restrict__ diff, Grid2 g, double dx, double dy,
-                                               int lim, bool periodic, const ScalarBCView& bc, int obs_t,
-                                               double obs_v, double (&res)[ROWS]) {
+                                               int lim, const ScalarBCView& bc, int obs_t, double obs_v,
+                                               double (&res)[ROWS]) {
     constexpr int TY = kTileY * ROWS;
+    constexpr bool periodic = PERIODIC;
     using Stage = TransportStage<TY>;
     __shared__ Stage st;
     __shared__ double FX[TY + 1][kTileX];
@@ -139,7 +143,7 @@ __device__ __forceinline__ void transport_tile(const double* __restrict__ phi, c
         }
     }
     __syncthreads();
-    const TransportTileView<TY> a{&st, ib, j0, nx};
+    const TransportTileView<TY, PERIODIC> a{&st, ib, j0, nx};
     auto west = [&](int ii, double uf) -> double {
         int L, R;
         if (ii == 1 || ii == nx + 1) {
@@ -267,19 +271,20 @@ __global__ void k_obstacle_bc(double* u, double* v, const uint8_t* fl, int nx, i
     if (i >= 1 && i <= nx && j >= 1 && j <= ny - 1) v[g.v(i, j)] = obc_v(v, fl, g, i, j);
 }
 
+template <bool PERIODIC>
 __global__ void __launch_bounds__(256) k_scalar_transport(const double* __restrict__ phi,
                                                           const double* __restrict__ u,
                                                           const double* __restrict__ v,
                                                           const uint8_t* __restrict__ fl, int nx, int ny,
                                                           double dx, double dy, const double* __restrict__ diff,
-                                                          int limiter, int periodic, ScalarBCView bc, int obs_t,
+                                                          int limiter, ScalarBCView bc, int obs_t,
                                                           double obs_v, double* __restrict__ out,
                                                           const cfd2d_state* st) {
     if (!is_active(st)) return;  // uniform over the grid
     const Grid2 g{nx, ny};
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     double r[kTransportRows];
-    transport_tile<kTransportRows>(phi, u, v, fl, diff, g, dx, dy, limiter, periodic != 0, bc, obs_t, obs_v, r);
+    transport_tile<kTransportRows, PERIODIC>(phi, u, v, fl, diff, g, dx, dy, limiter, bc, obs_t, obs_v, r);
 #pragma unroll
     for (int k = 0; k < kTransportRows; ++k) {
         const int i = blockIdx.y * kTileY * kTransportRows + threadIdx.y + kTileY * k;
@@ -888,6 +893,7 @@ __global__ void k_scalar_turb_diff(cfd2d_sim S, int s) {
         sc.diff[c] = sc.D0 + S.nu_t[c] / sc.turb_div;
 }
 
+template <bool PERIODIC>
 __global__ void k_scalar_rhs(cfd2d_sim S, int s) {
     if (!is_active(S.state)) return;
     const int nx = S.nx, ny = S.ny;
@@ -898,8 +904,8 @@ __global__ void k_scalar_rhs(cfd2d_sim S, int s) {
     for (int k = 0; k < 4; ++k) { bc.bt[k] = sc.bt[k]; bc.bv[k] = sc.bv[k]; }
     // rhs does not overlap phi, u, v, diff or the flags
     double r[kTransportRows];
-    transport_tile<kTransportRows>(sc.phi, S.u, S.v, S.fluid, sc.diff, g, S.dx, S.dy, sc.limiter,
-                                   S.periodic != 0, bc, sc.obs_t, sc.obs_v, r);
+    transport_tile<kTransportRows, PERIODIC>(sc.phi, S.u, S.v, S.fluid, sc.diff, g, S.dx, S.dy, sc.limiter, bc,
+                                             sc.obs_t, sc.obs_v, r);
 #pragma unroll
     for (int k = 0; k < kTransportRows; ++k) {
         const int i = blockIdx.y * kTileY * kTransportRows + threadIdx.y + kTileY * k;
@@ -1226,9 +1232,13 @@ cudaError_t launch_scalar_transport(const double* phi, const double* u, const do
                                     const double* diff, int limiter, int periodic,
                                     const ScalarBCView& bc, int obs_t, double obs_v, double* out,
                                     cudaStream_t s) {
-    k_scalar_transport<<<grid_rows(ny + 2, (nx + 2 + kTransportRows - 1) / kTransportRows), kTile, 0, s>>>(phi, u, v, fl, nx, ny, dx, dy, diff,
-                                                                   limiter, periodic, bc, obs_t, obs_v,
-                                                                   out, nullptr);
+    const dim3 grd = grid_rows(ny + 2, (nx + 2 + kTransportRows - 1) / kTransportRows);
+    if (periodic)
+        k_scalar_transport<true><<<grd, kTile, 0, s>>>(phi, u, v, fl, nx, ny, dx, dy, diff, limiter, bc, obs_t,
+                                                        obs_v, out, nullptr);
+    else
+        k_scalar_transport<false><<<grd, kTile, 0, s>>>(phi, u, v, fl, nx, ny, dx, dy, diff, limiter, bc, obs_t,
+                                                         obs_v, out, nullptr);
     return last();
 }
 
@@ -1301,7 +1311,11 @@ cudaError_t stage_scalar(const cfd2d_sim& S, int slot, cudaStream_t s) {
     const cfd2d_scalar& sc = S.scalars[slot];
     if (sc.turb_div > 0.0 && S.variable_viscosity)
         k_scalar_turb_diff<<<reduction_blocks((S.nx + 2) * (S.ny + 2)), kBlock, 0, s>>>(S, slot);
-    k_scalar_rhs<<<grid_rows(S.ny + 2, (S.nx + 2 + kTransportRows - 1) / kTransportRows), kTile, 0, s>>>(S, slot);
+    const dim3 grd = grid_rows(S.ny + 2, (S.nx + 2 + kTransportRows - 1) / kTransportRows);
+    if (S.periodic)
+        k_scalar_rhs<true><<<grd, kTile, 0, s>>>(S, slot);
+    else
+        k_scalar_rhs<false><<<grd, kTile, 0, s>>>(S, slot);
     k_scalar_update<<<grid_tile(kStep, S.ny, S.nx), tile(kStep), 0, s>>>(S, slot);
     cudaError_t e = stage_scalar_ghosts(S, slot, s);
     if (e != cudaSuccess || sc.source != 2) return e;
