@@ -28,7 +28,8 @@ sst_channel_mixed_precision = the k-omega SST channel 128 x 192 over 5000 steps 
             mixed-precision solver: time and the mixed run's error in the u profile, nu_t, tau_w, c_f.
 grid_2048x1024 = the same generator and seed at 2048 x 1024: plain steps and the
             Poisson comparison (the CG cap is raised so that both reach 1e-8).
-cylinder_440x82 = the cylinder channel with a van Leer scalar (plain FP64 path).
+cylinder_440x82 = the cylinder channel with a van Leer scalar (plain FP64 path), and the same run with the
+            on-chip solver's single-reduction form.
 stencils  = the kernel-level stencil drop-ins on a 4096 x 2048 grid against the
             measured HBM peak (compulsory bytes per cell over event time).
 --impl reference times the CPU restatement of the reference (the oracle: NumPy
@@ -636,10 +637,24 @@ def cylinder_section(steps: int, warmup: int, flush) -> dict:
     cells = CYL_NX * CYL_NY
     achieved = (BYTES_PER_CELL_ITER * cells * its.sum() + BYTES_PER_CELL_SOLVE * cells * len(its)) / solve_s / 1e9
     peak, _ = _peaks()
-    return {"workload": CYL_WORKLOAD, "steps": steps, "ms_per_step": 1e3 * dev_s / steps,
-            "cell_updates_per_s": cells * steps / dev_s, "poisson_ms": 1e3 * solve_s / steps,
-            "poisson_iters_per_step": float(its.mean()), "kernels_per_step": knodes,
-            "solver": "k_pcg_cluster (on-chip)", "solver_equiv_gbs": achieved, "solver_equiv_frac": achieved / peak}
+    out = {"workload": CYL_WORKLOAD, "steps": steps, "ms_per_step": 1e3 * dev_s / steps,
+           "cell_updates_per_s": cells * steps / dev_s, "poisson_ms": 1e3 * solve_s / steps,
+           "poisson_iters_per_step": float(its.mean()), "kernels_per_step": knodes,
+           "solver": "k_pcg_cluster (on-chip)", "solver_equiv_gbs": achieved, "solver_equiv_frac": achieved / peak,
+           "us_per_iteration": 1e6 * solve_s / its.sum()}
+    # the same run with the on-chip solver's single-reduction form (grid_ctas = -2)
+    case = cases.build_case(CYL_SPEC)
+    sim = case.sim
+    sim.pressure.tol = CG_RTOL
+    sim.pressure.grid_ctas = -2
+    step_ms, solve_ms, _, _ = _graph_steps(sim, steps, warmup, flush)
+    its1 = np.array(sim.history.extra["cg_iterationen"][-steps:], dtype=float)
+    solve1 = sum(solve_ms) / 1e3
+    out["single_reduction"] = {"solver": "k_pcg_cluster1 (on-chip, one cluster reduction per iteration)",
+                               "ms_per_step": sum(step_ms) / steps, "poisson_ms": 1e3 * solve1 / steps,
+                               "poisson_iters_per_step": float(its1.mean()),
+                               "us_per_iteration": 1e6 * solve1 / its1.sum()}
+    return out
 
 
 # ------------------------------------------------------------------ mixed precision

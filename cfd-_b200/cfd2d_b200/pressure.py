@@ -159,8 +159,11 @@ class PressureSolver:
         P.mixed = 0
         # CFD2D_PCG_VARIANT=cluster-l2: the workspace solver on one 16-CTA cluster;
         # grid-l2: over every SM with the vectors in the workspace (no shared-memory slabs);
-        # grid-slab1: the shared-memory slabs with one reduction per iteration
+        # grid-slab1: the shared-memory slabs with one reduction per iteration;
+        # single: the single-reduction form of whichever solver the grid takes
         P.grid_ctas = {"cluster-l2": 16, "grid-l2": -1, "grid-slab1": -2}.get(variant, 0) if self.cluster == 0 else 0
+        if variant == "single":
+            P.grid_ctas = -2
         self.op = P
 
     def ensure_workspace(self) -> None:
@@ -177,21 +180,23 @@ class PressureSolver:
 
     @property
     def grid_ctas(self) -> int:
-        """For grids beyond one on-chip cluster: 0 = the solver spreads over every SM
-        (cooperative launch; each CTA keeps a slab of rows in shared memory when the
-        slabs fit, else the vectors live in the workspace); -2 = the slabs with one
-        grid reduction per iteration (Chronopoulos-Gear recurrence: the same iteration
-        counts, p rounded differently); -1 = over every SM with the vectors in the
-        workspace; 16 = on one 16-CTA cluster, leaving the other SMs to other solves
-        (cfd2d_b200.batch)."""
+        """The solver form. -2 = the single-reduction form (Chronopoulos-Gear recurrence:
+        one reduction per iteration, the same iteration counts, p rounded differently)
+        of whichever solver the grid takes: the on-chip cluster solver (even ny) or the
+        shared-memory slabs. For grids beyond one on-chip cluster: 0 = the solver spreads
+        over every SM (cooperative launch; each CTA keeps a slab of rows in shared memory
+        when the slabs fit, else the vectors live in the workspace); -1 = over every SM
+        with the vectors in the workspace; 16 = on one 16-CTA cluster, leaving the other
+        SMs to other solves (cfd2d_b200.batch). On a cluster grid 0, -1 and 16 all mean
+        the on-chip solver."""
         return int(self.op.grid_ctas)
 
     @grid_ctas.setter
     def grid_ctas(self, value: int) -> None:
         if int(value) not in (0, 16, -1, -2):
             raise ValueError("grid_ctas must be 0, -1, -2 or 16")
-        if self.cluster != 0:
-            return  # the on-chip solver is used; nothing to choose
+        if self.cluster != 0 and int(value) != -2:
+            value = 0  # the on-chip solver is used; only its form can be chosen
         self.op.grid_ctas = int(value)
         if self.on_change is not None:
             self.on_change()

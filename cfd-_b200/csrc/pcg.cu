@@ -516,6 +516,416 @@ __global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cluster(PcgLaunch L) {
 #undef SLOTS
 }
 
+// ---------------------------------------------------------------- single-reduction cluster form
+// The on-chip cluster solver with the Jacobi-PCG recurrence of Chronopoulos and Gear
+// (the slab solver's k_pcg_slab1 recurrence): one cluster barrier per iteration, the
+// reduction of r.z, z.w and r.r together. Even ny and constant coefficients (cell
+// pairs, as k_pcg_cluster<CPT, true, false>). Each iteration updates p = z + beta p,
+// q = w + beta q (= A p), x, r and z = D^-1 r of the CTA's own cells, then needs the
+// new z of the two halo rows for w = A z. Instead of a second barrier, every CTA has
+// exported the (r, q, w) of its first and last row before the previous reduction's
+// barrier, into one of two buffers by iteration parity, and each neighbour recomputes
+// the halo row's new z from them with the owner's own operations (the same bits). A
+// buffer is rewritten two iterations later, after a barrier that every reader passes
+// once done with it. Shared memory per CTA: the cluster layout plus 2 x 3 x 2 export
+// rows and the two halo rows of z (14 ny doubles). Selected by grid_ctas = -2 on the
+// grids the cluster solver takes.
+constexpr int kExportRows = 12;  // 2 parities x (r, q, w) x (first row, last row)
+constexpr int kHaloPer = 2;      // halo cells per thread: 2 ny <= 2 x 512
+
+inline size_t smem_bytes1(int cap, int ny) {
+    return (size_t)cap * (kArrays * sizeof(double) + 1) + (size_t)(kExportRows + 2) * ny * sizeof(double) + 16;
+}
+
+template <int CPT>
+__global__ void __launch_bounds__(kPcgThreads, 1) k_pcg_cluster1(PcgLaunch L) {
+    cg::cluster_group cluster = cg::this_cluster();
+    const int C = (int)cluster.num_blocks();
+    const int me = (int)cluster.block_rank();
+    if (L.active && *L.active == 0) return;  // uniform over the cluster
+
+    const cfd2d_poisson& op = L.op;
+    const int nx = op.nx, ny = op.ny;
+    const bool periodic = op.periodic != 0;
+    const int r0 = row0_of(me, nx, C), r1 = row0_of(me + 1, nx, C);
+    const int rows = r1 - r0;
+    const int nloc = rows * ny;
+    const int cap = L.cap_cells;
+    const int tid = threadIdx.x;
+    const double mdx2 = -op.dx2, mdy2 = -op.dy2;
+    const int goff = r0 * ny;
+
+    extern __shared__ __align__(16) double sm[];
+    double* X = sm;
+    double* R = X + cap;
+    double* P = R + cap;  // p
+    double* Q = P + cap;  // q = A p
+    double* DI = Q + cap;
+    double* DG = DI + cap;
+    double* Z = DG + cap;
+    double* EX = Z + cap;                       // [parity][r, q, w][first, last row][ny]
+    double* HZ = EX + (size_t)kExportRows * ny;  // new z of the west halo row at [0, ny), east at [ny, 2 ny)
+    uint8_t* NB = reinterpret_cast<uint8_t*>(HZ + 2 * ny);
+    __shared__ double red_smem[32 * kMaxK];
+    __shared__ double slotsA[16 * kMaxK];
+    __shared__ double slotsB[16 * kMaxK];
+    __shared__ double cmean[CFD2D_MAX_COMPONENTS];
+    int nred = 0;
+#define SLOTS() ((nred++ & 1) ? slotsB : slotsA)
+    const unsigned magic = (unsigned)(((1ull << 32) + (unsigned)ny - 1) / (unsigned)ny);
+
+    // halo rows: the west one is its owner's last row (export side 1), the east one its
+    // owner's first row (side 0). hb: the owner's shared memory (its X); ho: the halo
+    // row's first cell in the owner's numbering. The layout is the same in every CTA.
+    const int iw = (r0 == 0) ? (periodic ? nx - 1 : -1) : r0 - 1;
+    const int ie = (r1 == nx) ? (periodic ? 0 : -1) : r1;
+    const double* hbW = nullptr;
+    const double* hbE = nullptr;
+    int hoW = 0, hoE = 0;
+    if (iw >= 0) {
+        const int o = owner_of(iw, nx, C);
+        hbW = cluster.map_shared_rank(X, o);
+        hoW = (iw - row0_of(o, nx, C)) * ny;
+    }
+    if (ie >= 0) {
+        const int o = owner_of(ie, nx, C);
+        hbE = cluster.map_shared_rank(X, o);
+        hoE = (ie - row0_of(o, nx, C)) * ny;
+    }
+    const size_t exOff = (size_t)kArrays * cap;                               // EX from X
+    const size_t nbOff = ((size_t)kArrays * cap + (size_t)(kExportRows + 2) * ny) * sizeof(double);  // NB, bytes
+
+    // ------------------------------------------------------------ prologue
+    double dt = 1.0;
+    if (L.rhs_mode == 1) dt = L.dt_ptr ? *L.dt_ptr : L.dt_const;
+    double nzx = 0.0;
+    for (int c = tid; c < nloc; c += kPcgThreads) {
+        const int gidx = goff + c;
+        const uint8_t nb = op.nbr[gidx];
+        NB[c] = nb;
+        const double x0 = op.x0[gidx];
+        X[c] = x0;
+        DI[c] = op.dinv[gidx];
+        DG[c] = op.diag[gidx];
+        double braw = 0.0;
+        if (nb & 0x80) {
+            if (L.rhs_mode == 0) {
+                braw = L.rhs[gidx];
+            } else {
+                // div(F, G) / dt at interior cell (i+1, j+1) (cfd2d/solver.py:264-266)
+                const int li = (int)__umulhi((unsigned)c, magic);
+                const int j = c - li * ny;
+                const int pu = ny + 2, pv = ny + 1;
+                const int ig = r0 + li + 1, jg = j + 1;
+                const double div = (L.F[ig * pu + jg] - L.F[(ig - 1) * pu + jg]) / L.dx +
+                                   (L.G[ig * pv + jg] - L.G[ig * pv + jg - 1]) / L.dy;
+                braw = div / dt;
+            }
+            if (x0 != 0.0) nzx += 1.0;
+        }
+        R[c] = braw;
+    }
+    {
+        double v[1] = {nzx};
+        cluster_sum<1>(cluster, v, red_smem, SLOTS(), C, me);
+        nzx = v[0];
+    }
+    const bool x_any = nzx > 0.0;
+    const int ncomp = op.ncomp;
+    for (int k = 0; k < ncomp; ++k) {
+        double v[1] = {0.0};
+        for (int c = tid; c < nloc; c += kPcgThreads)
+            if ((NB[c] & 0x80) && op.label[goff + c] == k) v[0] += R[c];
+        cluster_sum<1>(cluster, v, red_smem, SLOTS(), C, me);
+        if (tid == 0) cmean[k] = v[0] / op.comp_count[k];
+    }
+    __syncthreads();
+    double part[3] = {0.0, 0.0, 0.0};
+    for (int c = tid; c < nloc; c += kPcgThreads) {
+        const uint8_t nb = NB[c];
+        if (!(nb & 0x80)) { P[c] = 0.0; Q[c] = 0.0; R[c] = 0.0; Z[c] = 0.0; continue; }
+        double b = R[c];
+        if (ncomp > 0) {
+            const int lab = op.label[goff + c];
+            if (lab >= 0) b = b - cmean[lab];
+        }
+        b = -b;
+        P[c] = b;  // kept for the ||b|| == 0 return
+        double r = b;
+        if (x_any) {
+            const int li = (int)__umulhi((unsigned)c, magic);
+            const int j = c - li * ny;
+            double tW = 0.0, tS = 0.0, tN = 0.0, tE = 0.0;
+            if (nb & 2) tS = mdy2 * X[c - 1];
+            if (nb & 4) tN = mdy2 * X[c + 1];
+            if (nb & 1) tW = mdx2 * ((li > 0) ? X[c - ny] : hbW[hoW + j]);
+            if (nb & 8) tE = mdx2 * ((li < rows - 1) ? X[c + ny] : hbE[hoE + j]);
+            r = b - row_sum(periodic, r0 + li, nx, tW, tS, DG[c] * X[c], tN, tE);
+        }
+        // R and Z are read by other CTAs only after the barrier of the reduction below;
+        // X (read here across CTAs) is unchanged until then
+        R[c] = r;
+        Q[c] = 0.0;
+        const double z = DI[c] * r;
+        Z[c] = z;
+        part[0] += b * b;
+        part[1] += r * r;
+        part[2] += r * z;
+    }
+    cluster_sum<3>(cluster, part, red_smem, SLOTS(), C, me);
+    const double bnrm2 = sqrt(part[0]);
+    double rr = part[1];
+    double rho = part[2];
+    const double atol = L.rtol * bnrm2;
+    int it = 0;
+    bool converged = false;
+
+    // w = A z of a cell pair (c, c + 1); the halo rows' z from HZ
+    auto az_pair = [&](int c, int li, double& w0, double& w1) {
+        const unsigned nb2 = *reinterpret_cast<const uint16_t*>(NB + c);
+        const unsigned nb0 = nb2 & 0xFFu, nb1 = nb2 >> 8;
+        w0 = 0.0;
+        w1 = 0.0;
+        if (!((nb0 | nb1) & 0x80u)) return;
+        const int j = c - li * ny;
+        const double2 z2 = *reinterpret_cast<const double2*>(Z + c);
+        double tW0 = 0.0, tW1 = 0.0, tE0 = 0.0, tE1 = 0.0;
+        const double tS0 = (nb0 & 2) ? mdy2 * Z[c - 1] : 0.0;
+        const double tN0 = (nb0 & 4) ? mdy2 * z2.y : 0.0;
+        const double tS1 = (nb1 & 2) ? mdy2 * z2.x : 0.0;
+        const double tN1 = (nb1 & 4) ? mdy2 * Z[c + 2] : 0.0;
+        if ((nb0 | nb1) & 1) {
+            const double2 g = *reinterpret_cast<const double2*>(li > 0 ? (Z + c - ny) : (HZ + j));
+            if (nb0 & 1) tW0 = mdx2 * g.x;
+            if (nb1 & 1) tW1 = mdx2 * g.y;
+        }
+        if ((nb0 | nb1) & 8) {
+            const double2 g = *reinterpret_cast<const double2*>(li < rows - 1 ? (Z + c + ny) : (HZ + ny + j));
+            if (nb0 & 8) tE0 = mdx2 * g.x;
+            if (nb1 & 8) tE1 = mdx2 * g.y;
+        }
+        const double2 dg = *reinterpret_cast<const double2*>(DG + c);
+        const int i = r0 + li;
+        w0 = row_sum(periodic, i, nx, tW0, tS0, dg.x * z2.x, tN0, tE0);
+        w1 = row_sum(periodic, i, nx, tW1, tS1, dg.y * z2.y, tN1, tE1);
+    };
+    double w[2 * CPT];
+    // w of every own pair and its z.w partial
+    auto apply_w = [&]() -> double {
+        double d = 0.0;
+#pragma unroll
+        for (int k = 0; k < CPT; ++k) {
+            const int c = 2 * (tid + k * kPcgThreads);
+            if (c >= nloc) { w[2 * k] = w[2 * k + 1] = 0.0; continue; }
+            const int li = (int)__umulhi((unsigned)c, magic);
+            az_pair(c, li, w[2 * k], w[2 * k + 1]);
+            const double2 z2 = *reinterpret_cast<const double2*>(Z + c);
+            d += z2.x * w[2 * k];
+            d += z2.y * w[2 * k + 1];
+        }
+        return d;
+    };
+    // this CTA's first and last row of (r, q, w) into export buffer par
+    auto export_rows = [&](int par) {
+        double* ex = EX + (size_t)par * 6 * ny;
+#pragma unroll
+        for (int k = 0; k < CPT; ++k) {
+            const int c = 2 * (tid + k * kPcgThreads);
+            if (c >= nloc) continue;
+            const int li = (int)__umulhi((unsigned)c, magic);
+            const int j = c - li * ny;
+#pragma unroll
+            for (int side = 0; side < 2; ++side) {
+                if (li != (side == 0 ? 0 : rows - 1)) continue;
+                *reinterpret_cast<double2*>(ex + (0 * 2 + side) * ny + j) = *reinterpret_cast<const double2*>(R + c);
+                *reinterpret_cast<double2*>(ex + (1 * 2 + side) * ny + j) = *reinterpret_cast<const double2*>(Q + c);
+                *reinterpret_cast<double2*>(ex + (2 * 2 + side) * ny + j) = make_double2(w[2 * k], w[2 * k + 1]);
+            }
+        }
+    };
+    // the halo rows' new z from their owners' export buffer par, with the owner's own
+    // operations: q = w (first iteration) or q beta + w, r - alpha q, D^-1 r on fluid
+    // cells. The loads (coupling bits, r, q, w, 1/diag; all in bounds, taken whether or
+    // not the cell is fluid) are issued at the start of the iteration into registers,
+    // so their latency passes under the update of the CTA's own cells; halo_store
+    // forms z and writes HZ afterwards. Thread t takes halo cells t, t + 512, ... (2 ny
+    // <= kHaloPer x 512).
+    double hr[kHaloPer], hq[kHaloPer], hw[kHaloPer], hd[kHaloPer];
+    uint8_t hn[kHaloPer];
+    auto halo_load = [&](int par) {
+#pragma unroll
+        for (int u = 0; u < kHaloPer; ++u) {
+            const int t = tid + u * kPcgThreads;
+            hn[u] = 0;
+            if (t >= 2 * ny) continue;
+            const bool west = t < ny;
+            const int j = west ? t : t - ny;
+            const double* hb = west ? hbW : hbE;
+            if (!hb) continue;
+            const int cell = (west ? hoW : hoE) + j;
+            const double* ex = hb + exOff + (size_t)par * 6 * ny + (west ? ny : 0) + j;
+            hn[u] = reinterpret_cast<const uint8_t*>(hb)[nbOff + cell];
+            hr[u] = ex[0];
+            hq[u] = ex[2 * ny];
+            hw[u] = ex[4 * ny];
+            hd[u] = hb[4 * (size_t)cap + cell];
+        }
+    };
+    auto halo_store = [&](bool first, double alpha, double beta) {
+#pragma unroll
+        for (int u = 0; u < kHaloPer; ++u) {
+            const int t = tid + u * kPcgThreads;
+            if (t >= 2 * ny) continue;
+            double z = 0.0;
+            if (hn[u] & 0x80) {
+                const double qn = first ? hw[u] : hq[u] * beta + hw[u];
+                const double rn = hr[u] - alpha * qn;
+                z = hd[u] * rn;
+            }
+            HZ[t] = z;
+        }
+    };
+
+    // w = A z and delta = z.w of the initial z: the reduction above made every CTA's z
+    // final, so the halo rows are read from their owners directly
+    double delta;
+    for (int t = tid; t < 2 * ny; t += kPcgThreads) {
+        const bool west = t < ny;
+        const double* hb = west ? hbW : hbE;
+        HZ[t] = hb ? hb[6 * (size_t)cap + (west ? hoW : hoE) + (west ? t : t - ny)] : 0.0;
+    }
+    __syncthreads();
+    {
+        double d[1] = {apply_w()};
+        export_rows(0);
+        cluster_sum<1>(cluster, d, red_smem, SLOTS(), C, me);
+        delta = d[0];
+    }
+    if (bnrm2 == 0.0) {
+        // scipy returns b itself
+        for (int c = tid; c < nloc; c += kPcgThreads) X[c] = P[c];
+        converged = true;
+    } else {
+        double rho_prev = 1.0, alpha_prev = 1.0;
+        for (it = 0; it < L.maxiter; ++it) {
+            if (sqrt(rr) < atol) { converged = true; break; }
+            const bool first = (it == 0);
+            double beta = 0.0, pq = delta;
+            if (!first) {
+                beta = rho / rho_prev;
+                pq = delta - (beta * rho) / alpha_prev;
+            }
+            const double alpha = rho / pq;
+            halo_load(it & 1);
+            double v3[3] = {0.0, 0.0, 0.0};  // r.z, z.w, r.r
+#pragma unroll
+            for (int k = 0; k < CPT; ++k) {
+                const int c = 2 * (tid + k * kPcgThreads);
+                if (c >= nloc) continue;
+                const unsigned nb2 = *reinterpret_cast<const uint16_t*>(NB + c);
+                const bool f0 = nb2 & 0x80u, f1 = (nb2 >> 8) & 0x80u;
+                if (!(f0 || f1)) continue;
+                double2 x2 = *reinterpret_cast<const double2*>(X + c);
+                double2 r2 = *reinterpret_cast<const double2*>(R + c);
+                double2 z2 = *reinterpret_cast<const double2*>(Z + c);
+                double2 p2 = *reinterpret_cast<const double2*>(P + c);
+                double2 q2 = *reinterpret_cast<const double2*>(Q + c);
+                const double2 d2 = *reinterpret_cast<const double2*>(DI + c);
+                if (first) {
+                    p2 = z2;
+                    q2 = make_double2(w[2 * k], w[2 * k + 1]);
+                } else {
+                    p2 = make_double2(p2.x * beta + z2.x, p2.y * beta + z2.y);
+                    q2 = make_double2(q2.x * beta + w[2 * k], q2.y * beta + w[2 * k + 1]);
+                }
+                if (f0) {
+                    x2.x = x2.x + alpha * p2.x;
+                    r2.x = r2.x - alpha * q2.x;
+                    z2.x = d2.x * r2.x;
+                    v3[0] += r2.x * z2.x;
+                    v3[2] += r2.x * r2.x;
+                }
+                if (f1) {
+                    x2.y = x2.y + alpha * p2.y;
+                    r2.y = r2.y - alpha * q2.y;
+                    z2.y = d2.y * r2.y;
+                    v3[0] += r2.y * z2.y;
+                    v3[2] += r2.y * r2.y;
+                }
+                *reinterpret_cast<double2*>(X + c) = x2;
+                *reinterpret_cast<double2*>(R + c) = r2;
+                *reinterpret_cast<double2*>(Z + c) = z2;
+                *reinterpret_cast<double2*>(P + c) = p2;
+                *reinterpret_cast<double2*>(Q + c) = q2;
+            }
+            halo_store(first, alpha, beta);
+            __syncthreads();
+            v3[1] = apply_w();
+            export_rows((it + 1) & 1);
+            cluster_sum<3>(cluster, v3, red_smem, SLOTS(), C, me);
+            rho_prev = rho;
+            alpha_prev = alpha;
+            rho = v3[0];
+            delta = v3[1];
+            rr = v3[2];
+        }
+    }
+    // ------------------------------------------------------------ epilogue
+    __syncthreads();
+    for (int c = tid; c < nloc; c += kPcgThreads) op.x0[goff + c] = X[c];
+    for (int k = 0; k < ncomp; ++k) {
+        double v[1] = {0.0};
+        for (int c = tid; c < nloc; c += kPcgThreads)
+            if ((NB[c] & 0x80) && op.label[goff + c] == k) v[0] += X[c];
+        cluster_sum<1>(cluster, v, red_smem, SLOTS(), C, me);
+        if (tid == 0) cmean[k] = v[0] / op.comp_count[k];
+    }
+    __syncthreads();
+    const int pp = ny + 2;
+    for (int c = tid; c < nloc; c += kPcgThreads) {
+        const int li = (int)__umulhi((unsigned)c, magic);
+        const int j = c - li * ny;
+        const int i = r0 + li;
+        double pv = 0.0;
+        if (NB[c] & 0x80) {
+            pv = X[c];
+            if (ncomp > 0) {
+                const int lab = op.label[goff + c];
+                if (lab >= 0) pv = pv - cmean[lab];
+            }
+        }
+        if (!L.p_padded) {
+            L.p_out[goff + c] = pv;
+        } else {
+            L.p_out[(i + 1) * pp + j + 1] = pv;
+            if (periodic && i == nx - 1) L.p_out[j + 1] = pv;
+            if (periodic && i == 0) L.p_out[(nx + 1) * pp + j + 1] = pv;
+        }
+    }
+    if (L.p_padded) {
+        for (int i = r0 + tid; i < r1; i += kPcgThreads) {
+            L.p_out[(i + 1) * pp] = 0.0;
+            L.p_out[(i + 1) * pp + ny + 1] = 0.0;
+        }
+        if (me == 0) {
+            for (int j = tid; j < pp; j += kPcgThreads)
+                if (!periodic || j == 0 || j == ny + 1) L.p_out[j] = 0.0;
+        }
+        if (me == C - 1) {
+            for (int j = tid; j < pp; j += kPcgThreads)
+                if (!periodic || j == 0 || j == ny + 1) L.p_out[(nx + 1) * pp + j] = 0.0;
+        }
+    }
+    if (me == 0 && tid == 0) {
+        if (L.iters_out) *L.iters_out = it;
+        if (L.iters_out2) *L.iters_out2 = it;
+        if (L.status_out && !converged) atomicOr(L.status_out, CFD2D_S_CG_MAXITER);
+    }
+    // keep every CTA's shared memory alive until all remote readers are done
+    cluster.sync();
+#undef SLOTS
+}
+
 // ---------------------------------------------------------------- mixed precision
 // Ordered row sum in FP32 (the inner iterations of the mixed solver).
 __device__ __forceinline__ float row_sum_f(bool periodic, int i, int nx, float tW, float tS, float tC, float tN,
@@ -2327,6 +2737,49 @@ cudaError_t launch_cpt(const PcgLaunch& L, int C, cudaStream_t s) {
     return cudaLaunchKernelEx(&cfg, kern, L);
 }
 
+// the single-reduction cluster form (k_pcg_cluster1): same attributes as configure_cpt
+template <int CPT>
+cudaError_t configure_cpt1() {
+    static bool done = false;
+    if (done) return cudaSuccess;
+    const DevLimits d = dev_limits();
+    if (d.sms <= 0) return cudaErrorInvalidDevice;
+    const int dyn = d.smem_optin - (int)((32 * kMaxK + 2 * 16 * kMaxK + CFD2D_MAX_COMPONENTS) * sizeof(double)) - 1024;
+    cudaError_t e = cudaFuncSetAttribute(k_pcg_cluster1<CPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_pcg_cluster1<CPT>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (e != cudaSuccess) return e;
+    done = true;
+    return cudaSuccess;
+}
+
+// whether the single-reduction form's extra rows fit beside the cluster layout
+bool cluster1_fits(int cap, int ny) {
+    const DevLimits d = dev_limits();
+    if (d.sms <= 0) return false;
+    const size_t dyn = (size_t)d.smem_optin - (32 * kMaxK + 2 * 16 * kMaxK + CFD2D_MAX_COMPONENTS) * sizeof(double) - 1024;
+    return 2 * ny <= kHaloPer * kPcgThreads && smem_bytes1(cap, ny) <= dyn;
+}
+
+template <int CPT>
+cudaError_t launch_cpt1(const PcgLaunch& L, int C, cudaStream_t s) {
+    cudaError_t e = configure_cpt1<CPT>();
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(C, 1, 1);
+    cfg.blockDim = dim3(kPcgThreads, 1, 1);
+    cfg.dynamicSmemBytes = smem_bytes1(L.cap_cells, L.op.ny);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_pcg_cluster1<CPT>, L);
+}
+
 // the mixed-precision solver: x and b in FP64, seven FP32 arrays, the coupling bits
 size_t smem_bytes_mixed(int cap) { return (size_t)cap * (2 * sizeof(double) + 7 * sizeof(float) + 1) + 16; }
 
@@ -2433,13 +2886,14 @@ int pcg_cluster_plan(int nx, int ny) {
             case 4: e = configure_cpt<4, false>(); f = (const void*)k_pcg_cluster<4, false, false>; break;
             default: e = configure_cpt<8, false>(); f = (const void*)k_pcg_cluster<8, false, false>; break;
         }
-        // the paired variant (even ny) has the same block size and shared memory
+        // the paired variant (even ny) has the same block size and shared memory; its
+        // single-reduction form is configured here too (attributes before any capture)
         if (e == cudaSuccess) {
             switch (cpt_for((int)((cells + 1) / 2))) {
-                case 1: e = configure_cpt<1, true>(); break;
-                case 2: e = configure_cpt<2, true>(); break;
-                case 4: e = configure_cpt<4, true>(); break;
-                default: e = configure_cpt<8, true>(); break;
+                case 1: e = configure_cpt<1, true>(); if (e == cudaSuccess) e = configure_cpt1<1>(); break;
+                case 2: e = configure_cpt<2, true>(); if (e == cudaSuccess) e = configure_cpt1<2>(); break;
+                case 4: e = configure_cpt<4, true>(); if (e == cudaSuccess) e = configure_cpt1<4>(); break;
+                default: e = configure_cpt<8, true>(); if (e == cudaSuccess) e = configure_cpt1<8>(); break;
             }
         }
         if (e != cudaSuccess) { cudaGetLastError(); continue; }
@@ -2475,6 +2929,16 @@ cudaError_t pcg_launch(const PcgLaunch& L0, cudaStream_t s) {
             case 2: return launch_mixed<2>(L, C, s);
             case 4: return launch_mixed<4>(L, C, s);
             case 8: return launch_mixed<8>(L, C, s);
+            default: return cudaErrorInvalidValue;
+        }
+    }
+    if (L.op.ny % 2 == 0 && L.op.grid_ctas == -2 && cluster1_fits(L.cap_cells, L.op.ny)) {
+        // the single-reduction form (opt-in; the default keeps scipy's two reductions)
+        switch (cpt_for((L.cap_cells + 1) / 2)) {
+            case 1: return launch_cpt1<1>(L, C, s);
+            case 2: return launch_cpt1<2>(L, C, s);
+            case 4: return launch_cpt1<4>(L, C, s);
+            case 8: return launch_cpt1<8>(L, C, s);
             default: return cudaErrorInvalidValue;
         }
     }

@@ -99,7 +99,7 @@ typedef struct cfd2d_poisson {
     int mixed;                /* 1: FP32 iterations with FP64 residual refinement and FP64
                                  reductions (on-chip solver only; no reference counterpart);
                                  0: the FP64 scipy-form iteration */
-    int grid_ctas;            /* cluster == 0 only: 0 = cooperative launch over every SM,
+    int grid_ctas;            /* cluster == 0: 0 = cooperative launch over every SM,
                                  each CTA holding a slab of rows in shared memory when the
                                  slabs fit (constant coefficients, even ny <= 1024), else
                                  vectors in the workspace; -2 = the slabs with one grid
@@ -107,7 +107,10 @@ typedef struct cfd2d_poisson {
                                  of scipy's two); -1 = over every SM with the vectors
                                  in the workspace; 16 = one 16-CTA cluster (vectors in the
                                  workspace, cluster barriers), which leaves the other SMs to
-                                 other solves */
+                                 other solves. cluster > 0: -2 = the on-chip solver with one
+                                 cluster reduction per iteration (same recurrence; FP64,
+                                 constant coefficients, even ny, when its 14 ny extra
+                                 doubles per CTA fit), any other value its default form */
     const double* bx;         /* NULL: constant coefficients. Else div(b grad p) with face
                                  coefficients b = 1/rho (cfd2d/pressure.py:187-244):
                                  bx (nx+1)(ny+2) on the x faces, periodic face nx coupling

@@ -399,6 +399,50 @@ def test_pressure_solve_grid_variant(pkg, name, variant, monkeypatch):
         assert rel(p, g[name + "_p" + key]) < 1e-7
 
 
+@pytest.mark.parametrize("name", ["cav", "cyl", "per", "two"])
+def test_pressure_solve_single_reduction_cluster(pkg, name):
+    """The on-chip cluster solver's single-reduction form (grid_ctas = -2; the form is
+    taken where ny is even) on the same fixtures."""
+    g = golden("golden_pressure")
+    sim = _pressure_sim(pkg, name)
+    ps = sim.pressure
+    assert ps.cluster > 0
+    ps.grid_ctas = -2
+    assert ps.grid_ctas == -2
+    ps.tol = 1e-10
+    for key in ("", "2"):
+        p = ps.solve(g[name + "_rhs" + key])
+        its = int(g[name + "_its" + key])
+        assert abs(ps.last_iterations - its) <= max(2, its // 20), (ps.last_iterations, its)
+        assert rel(p, g[name + "_p" + key]) < 1e-7
+
+
+def test_cylinder_single_reduction_cluster_10_steps(pkg):
+    """Cylinder 440 x 82 with a scalar (even ny: the cluster solver's single-reduction
+    form) against the reference's run: u, v and the scalar to 1e-10, p to 5e-9 (the
+    recurrence rounds differently from scipy's), the same CG iteration counts as the
+    default form within 2 per step."""
+    _, cases, _, _ = pkg
+    g = golden("golden_cylinder440")
+    its = {}
+    for form in (0, -2):
+        case = cases.build_case({"fall": "cylinder", "parameter": {"re": 100, "nx": 440, "ny": 82},
+                                 "numerik": {"pressure_solver": "cg"},
+                                 "skalar": {"name": "c", "diffusivity": 1e-3, "inflow_band": [0.15, 0.25],
+                                            "limiter": "vanleer"}})
+        sim = case.sim
+        assert sim.pressure.cluster > 0
+        sim.pressure.grid_ctas = form
+        sim.pressure.tol = 1e-8
+        sim.advance(10)
+        its[form] = np.array(sim.history.extra["cg_iterationen"])
+    for f in "uv":
+        assert rel(getattr(sim, f), g[f"cyl_{f}_10"]) < TOL, f
+    assert rel(sim.p, g["cyl_p_10"]) < 5e-9
+    assert rel(sim.scalars["c"].phi, g["cyl_c_10"]) < TOL
+    assert np.abs(its[-2] - its[0]).max() <= 2, (its[-2], its[0])
+
+
 @pytest.mark.parametrize("grid_ctas", [0, -2, -1, 16])
 def test_large_grid_uses_grid_variant_and_matches_oracle(pkg, grid_ctas):
     """A grid beyond one cluster's shared memory: solve against the oracle's CG."""
