@@ -18,8 +18,9 @@ namespace {
 // Workspace of the grid-persistent solver (pcg_grid_workspace_doubles) for the
 // largest grid this entry point accepts: R, P0, P1 (one double per cell each),
 // three partial-sum arrays of (4 + CFD2D_MAX_COMPONENTS) doubles for up to
-// 148 * 32 CTAs, and two barrier words. 8.2 MiB of device memory per device,
-// reserved when the library's module is loaded.
+// 148 * 32 CTAs (a B200's SMs times the CTAs an SM holds; on a device with more SMs
+// the capacity check below refuses the call), and two barrier words. 8.2 MiB of
+// device memory per device, reserved when the library's module is loaded.
 constexpr size_t kScratchDoubles =
     (size_t)3 * CFD2D_STATIC_MAX_CELLS + (size_t)3 * 148 * 32 * (4 + CFD2D_MAX_COMPONENTS) + 8;
 

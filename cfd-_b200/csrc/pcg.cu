@@ -31,9 +31,7 @@ namespace {
 
 constexpr int kPcgThreads = 512;
 constexpr int kSlot = 4 + CFD2D_MAX_COMPONENTS;  // doubles per CTA partial (grid kernel)
-// Upper bound on the CTAs of the workspace solver (its partial arrays are sized for
-// it; the launch checks the device's actual count against it): 148 SMs x 32.
-constexpr int kMaxGridCtas = 148 * 32;
+constexpr int kMaxCtasPerSm = 32;  // resident CTAs an SM can hold (compute capability 10.0)
 constexpr int kArrays = 7;                       // X, R, P0, P1, DI, DG, Z per cell
 constexpr int kMaxK = 4;                         // values per cluster reduction
 
@@ -2609,11 +2607,17 @@ cudaError_t pcg_matvec(const cfd2d_poisson& op, const double* x, double* y, cuda
     return cudaGetLastError();
 }
 
+// Upper bound on the CTAs of the workspace solver on the current device (its partial
+// arrays are sized for it): every SM times the most CTAs an SM can hold.
+int max_grid_ctas() {
+    const DevLimits d = dev_limits();
+    return d.sms > 0 ? d.sms * kMaxCtasPerSm : 0;
+}
+
 size_t pcg_grid_workspace_doubles(int nx, int ny) {
     // R, P0, P1 (the slab form: boundary rows of z and p) + three partial arrays for
-    // up to kMaxGridCtas CTAs (two used, as the parity sets of grid_sum) + barrier words
-
-    return (size_t)3 * nx * ny + (size_t)3 * kMaxGridCtas * kSlot + 8;
+    // up to max_grid_ctas() CTAs (two used, as the parity sets of grid_sum) + barrier words
+    return (size_t)3 * nx * ny + (size_t)3 * max_grid_ctas() * kSlot + 8;
 }
 
 template <bool VAR>
@@ -2643,7 +2647,7 @@ cudaError_t pcg_grid_launch_t(const PcgLaunch& L, cudaStream_t s) {
         }
     }
     const int G = cl ? 16 : grid_blocks_for<VAR>(n);
-    if (G < 1 || G > kMaxGridCtas) return cudaErrorInvalidConfiguration;
+    if (G < 1 || G > max_grid_ctas()) return cudaErrorInvalidConfiguration;
     PcgLaunch Lc = L;
     // the barrier words start from zero on every launch, whatever an earlier
     // launch that gave up on a wait left behind

@@ -319,7 +319,8 @@ int cfd2d_mask_image(int nx, int ny, double dx, double dy, const uint8_t* solid,
 
 /* ---- pressure Poisson (drop-in for cfd2d/pressure.py) -------------------- */
 
-/* Bytes of scratch the solver needs for an nx x ny grid (cfd2d_poisson.work). */
+/* Bytes of scratch the solver needs for an nx x ny grid (cfd2d_poisson.work) on the
+ * current device (its partial-sum arrays are sized by the device's SM count). */
 size_t cfd2d_pcg_workspace_bytes(int nx, int ny);
 
 /* Choose the solver variant for this grid on the current device: the number of
