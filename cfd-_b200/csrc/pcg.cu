@@ -2699,25 +2699,27 @@ size_t smem_bytes(int cap, bool var = false) {
     return (size_t)cap * ((kArrays + (var ? 4 : 0)) * sizeof(double) + 1) + 16;
 }
 
-// Kernel attributes are set once per instantiation, outside any stream capture
-// (cfd2d_pcg_plan runs before the first launch): the maximum dynamic shared
+// Kernel attributes are set once per instantiation and device, outside any stream
+// capture (cfd2d_pcg_plan runs before the first launch): the maximum dynamic shared
 // memory the hardware allows and permission for 16-CTA clusters.
+template <class K>
+cudaError_t configure_cluster_kernel(K kern, bool (&done)[kMaxDevices]) {
+    const DevLimits d = dev_limits();
+    if (d.sms <= 0 || d.dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    if (done[d.dev]) return cudaSuccess;
+    const int dyn = d.smem_optin - (int)((32 * kMaxK + 2 * 16 * kMaxK + CFD2D_MAX_COMPONENTS) * sizeof(double)) - 1024;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (e != cudaSuccess) return e;
+    done[d.dev] = true;
+    return cudaSuccess;
+}
+
 template <int CPT, bool PAIR, bool VAR = false>
 cudaError_t configure_cpt() {
-    static bool done = false;
-    if (done) return cudaSuccess;
-    int dev = 0, optin = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return e;
-    e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    if (e != cudaSuccess) return e;
-    const int dyn = optin - (int)((32 * kMaxK + 2 * 16 * kMaxK + CFD2D_MAX_COMPONENTS) * sizeof(double)) - 1024;
-    e = cudaFuncSetAttribute(k_pcg_cluster<CPT, PAIR, VAR>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_pcg_cluster<CPT, PAIR, VAR>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-    if (e != cudaSuccess) return e;
-    done = true;
-    return cudaSuccess;
+    static bool done[kMaxDevices];
+    return configure_cluster_kernel(k_pcg_cluster<CPT, PAIR, VAR>, done);
 }
 
 template <int CPT, bool PAIR, bool VAR = false>
@@ -2744,17 +2746,8 @@ cudaError_t launch_cpt(const PcgLaunch& L, int C, cudaStream_t s) {
 // the single-reduction cluster form (k_pcg_cluster1): same attributes as configure_cpt
 template <int CPT>
 cudaError_t configure_cpt1() {
-    static bool done = false;
-    if (done) return cudaSuccess;
-    const DevLimits d = dev_limits();
-    if (d.sms <= 0) return cudaErrorInvalidDevice;
-    const int dyn = d.smem_optin - (int)((32 * kMaxK + 2 * 16 * kMaxK + CFD2D_MAX_COMPONENTS) * sizeof(double)) - 1024;
-    cudaError_t e = cudaFuncSetAttribute(k_pcg_cluster1<CPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_pcg_cluster1<CPT>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-    if (e != cudaSuccess) return e;
-    done = true;
-    return cudaSuccess;
+    static bool done[kMaxDevices];
+    return configure_cluster_kernel(k_pcg_cluster1<CPT>, done);
 }
 
 // whether the single-reduction form's extra rows fit beside the cluster layout
@@ -2789,19 +2782,10 @@ size_t smem_bytes_mixed(int cap) { return (size_t)cap * (2 * sizeof(double) + 7 
 
 template <int CPT>
 cudaError_t launch_mixed(const PcgLaunch& L, int C, cudaStream_t s) {
-    static bool done = false;
-    if (!done) {
-        int dev = 0, optin = 0;
-        cudaError_t e = cudaGetDevice(&dev);
+    static bool done[kMaxDevices];
+    {
+        const cudaError_t e = configure_cluster_kernel(k_pcg_cluster_mixed<CPT>, done);
         if (e != cudaSuccess) return e;
-        e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-        if (e != cudaSuccess) return e;
-        const int dyn = optin - (int)((32 * kMaxK + 2 * 16 * kMaxK + CFD2D_MAX_COMPONENTS) * sizeof(double)) - 1024;
-        e = cudaFuncSetAttribute(k_pcg_cluster_mixed<CPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
-        if (e != cudaSuccess) return e;
-        e = cudaFuncSetAttribute(k_pcg_cluster_mixed<CPT>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-        if (e != cudaSuccess) return e;
-        done = true;
     }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(C, 1, 1);
