@@ -837,8 +837,10 @@ def pretrained():
     flexible CG's own residuals, 2000 steps at 2e-4 (``finetune A.npz``); then from
     that, 4 flows per size, two such rounds (``finetune B.npz --init A.npz --cases 4
     --rounds 2 --seed 200``); then 6 flows per size, two rounds of 3000 steps
-    (``finetune C.npz --init B.npz --cases 6 --rounds 2 --steps 3000 --seed 300``).
-    The benchmark's flow (generator seed 13) is held out of every set."""
+    (``finetune C.npz --init B.npz --cases 6 --rounds 2 --steps 3000 --seed 300``);
+    then the same with other flows at a lower rate (``finetune D.npz --init C.npz
+    --cases 6 --rounds 2 --steps 3000 --lr 1.5e-4 --seed 500``). The benchmark's flow
+    (generator seed 13) is held out of every set."""
     from pathlib import Path
 
     return load_weights(Path(__file__).resolve().parent / "data" / "lpc_weights.npz")
